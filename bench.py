@@ -1,0 +1,413 @@
+"""Benchmark of the cube Coulomb operator at 481^3 (the headline workload).
+
+Workload: 481^3 grid (80 cells x 6 + 1 per axis, step 0.1 bohr, box
+[-24, 24]^3), density = 32 seeded Gaussians (alpha log-uniform in [0.1, 20],
+q ~ U[0.5, 2], centres ~ U[-10, 10]^3), 64 t-points (32 Gauss-Legendre on
+[0, 2] + 32 log-mapped on [2, 1e3]).  One step = one application of the
+operator V = sum_p w_p (Tx (x) Ty (x) Tz)_p rho + coda rho to the resident
+density, energy integral included.  Metric: grid points per second (Mpts/s).
+
+Default run: the split-precision tensor-core operator (bf16x6) with the
+FP64 GPU operator timed beside it and the error of the former against the
+latter reported; `--precision fp64` benchmarks the drop-in alone.
+`--impl reference` times the CPU restatement of the reference algorithm
+(oracle/, DGEMM per mode product) on the host cores instead.
+
+Multi-GPU: the operator does not shard in this build; N ranks run N
+independent replicas ("scaling": "weak"), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELL = 80
+STEP = 0.1
+NLIN = NLOG = 32
+TLIN, TLOG = 2.0, 1.0e3
+SEED = 3
+N_GAUSS = 32
+METRIC = "Coulomb-op Mpts/s @481^3: mixed vs FP64 on B200 at <=1e-6 rel err; CPU ref shown"
+
+
+def gaussians(seed=SEED, ng=N_GAUSS):
+    rng = np.random.default_rng(seed)
+    q = rng.uniform(0.5, 2.0, ng)
+    a = np.exp(rng.uniform(np.log(0.1), np.log(20.0), ng))
+    c = rng.uniform(-10.0, 10.0, (ng, 3))
+    return q, a, c
+
+
+def axis_points(n_cell=N_CELL, step=STEP):
+    qmin = -0.5 * n_cell * 6 * step
+    return qmin + step * np.arange(n_cell * 6 + 1)
+
+
+def density_torch(pts, q, a, c, device):
+    """rho(x,y,z) on the device as a flat float64 tensor, x fastest."""
+    import torch
+
+    x = torch.tensor(pts, dtype=torch.float64, device=device)
+    n = len(pts)
+    rho = torch.zeros((n, n, n), dtype=torch.float64, device=device)  # [z, y, x]
+    for qi, ai, ci in zip(q, a, c):
+        norm = qi * (ai / np.pi) ** 1.5
+        ex = torch.exp(-ai * (x - ci[0]) ** 2)
+        ey = torch.exp(-ai * (x - ci[1]) ** 2)
+        ez = torch.exp(-ai * (x - ci[2]) ** 2)
+        rho += norm * ez[:, None, None] * ey[None, :, None] * ex[None, None, :]
+    return rho.reshape(-1)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s in sm if s > 0.5 * max(sm)]
+        return {"sm_mhz": float(np.median(load or sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        kv = dict(x.split("=", 1) for x in ln.split() if "=" in x)
+        if kv.get("kernel") == kernel and kv.get("workload") == workload:
+            try:
+                return float(kv["traffic_bytes_per_launch"])
+            except (KeyError, ValueError):
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU arms
+# ---------------------------------------------------------------------------
+_CPU_SETUP = {}
+
+
+def _cpu_setup(n_cell, step, n_t):
+    key = (n_cell, step, n_t)
+    if key not in _CPU_SETUP:
+        from oracle import oracle as O
+
+        qmin = -0.5 * n_cell * 6 * step
+        g = O.Grid3D.cube(qmin, n_cell, step)
+        q, a, c = gaussians()
+        rho = O.gauss_cube(g, q, a, c)
+        tp, tw = O.gauss_quad(NLIN, NLOG, 0.0, TLIN, TLOG)
+        idx = np.linspace(0, len(tp) - 1, n_t).round().astype(int)
+        T = O.coulomb_matrix(g.axes[0], g.axes[0].points, tp[idx])
+        w = O.coulomb_weights(tw)[idx]
+        _CPU_SETUP.clear()
+        _CPU_SETUP[key] = (g, rho, tp, T, w)
+    return _CPU_SETUP[key]
+
+
+def cpu_sample(n_cell=N_CELL, step=STEP, n_t=1, threads=None):
+    """Times the CPU restatement (oracle, numpy/OpenBLAS DGEMM per mode
+    product) on a bounded sample: n_t of the 64 t-points of the 481^3
+    operator.  Returns (Mpts/s scaled to all 64 t-points, seconds, sample
+    description, threads)."""
+    from oracle import oracle as O
+
+    g, rho, tp, T, w = _cpu_setup(n_cell, step, n_t)
+    t0 = time.perf_counter()
+    O.transform_cube_blas(T, T, T, w, rho, 0.0)
+    dt = time.perf_counter() - t0
+    npts = float(g.shape[0]) ** 3
+    per_apply = dt * len(tp) / n_t
+    ncores = threads or os.cpu_count()
+    return npts / per_apply / 1e6, dt, f"{n_t} of {len(tp)} t-points of the {g.shape[0]}^3 apply, scaled x{len(tp) / n_t:.0f}", ncores
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps = []
+    for i in range(args.warmup + args.steps):
+        v, dt, sample, cores = cpu_sample(n_t=1)
+        if i >= args.warmup:
+            steps.append(v)
+    value = float(np.median(steps))
+    n = N_CELL * 6 + 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpts/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(n ** 3 / value / 1e6 * 1e3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "coulomb_cube_481", "points_per_axis": n, "t_points": NLIN + NLOG,
+                   "gaussians": N_GAUSS, "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args, world, rank, local):
+    import torch
+
+    import dage_b200 as dage
+    from dage_b200 import build as b
+
+    b.build()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = N_CELL * 6 + 1
+    npts = float(n) ** 3
+    g = dage.Grid3D.cube(-0.5 * N_CELL * 6 * STEP, N_CELL, STEP)
+    quad = dage.GaussQuad(NLIN, NLOG, 0.0, TLIN, TLOG)
+    q, a, c = gaussians()
+    rho = density_torch(axis_points(), q, a, c, dev)
+    prec = args.precision
+    op = dage.Coulomb3D(g, quad=quad, precision=prec)
+    V = torch.empty_like(rho)
+
+    # -- device-resident timed region ---------------------------------------
+    for _ in range(args.warmup):
+        op.apply(rho, out=V, energy=True)
+    op.set_timing(True)
+    clk = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    energy = None
+    for _ in range(args.steps):
+        _, energy = op.apply(rho, out=V, energy=True)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = barrier_max(ms, world)
+    value = world * npts / (ms / 1e3) / 1e6
+    launches = sum(op.timing(k)[0] for k in range(3))
+    k_launches, k_ms = op.timing(0)
+    op.set_timing(False)
+
+    # -- dominant kernel roofline -------------------------------------------
+    pk, src = peaks()
+    nprod = {"fp64": 1, "bf16x3": 3, "bf16x6": 6}[prec]
+    stage_flops = 2.0 * n ** 4 * nprod  # per stage launch (M=n^2, N=K=n)
+    avg_launch_s = k_ms / max(k_launches, 1) / 1e3
+    achieved = stage_flops / avg_launch_s / 1e12
+    if prec == "fp64":
+        peak, peak_src = 40.0, "nominal B200 FP64 (no measured FP64 peak)"
+        kname = "stage_fp64_kernel"
+    else:
+        peak, peak_src = pk["bf16_tflops_sustained"], f"{src} bf16_tflops_sustained"
+        kname = "stage_bf16_kernel"
+    traffic = profiled_traffic(kname, f"coulomb_cube_{n}")
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": traffic, "kernel": kname,
+            "peak_source": peak_src,
+            "flops_per_launch": stage_flops, "avg_launch_ms": avg_launch_s * 1e3,
+            "launches_timed": k_launches}
+
+    # -- accuracy against the FP64 GPU operator and the analytic potential --
+    accuracy = None
+    fp64_mpts = None
+    if prec != "fp64" and not args.skip_fp64:
+        op64 = dage.Coulomb3D(g, quad=quad, precision="fp64")
+        V64 = torch.empty_like(rho)
+        _, E64 = op64.apply(rho, out=V64, energy=True)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        nrep = max(1, args.fp64_steps)
+        f0.record()
+        for _ in range(nrep):
+            op64.apply(rho, out=V64, energy=True)
+        f1.record()
+        torch.cuda.synchronize()
+        fp64_ms = f0.elapsed_time(f1) / nrep
+        fp64_mpts = npts / (fp64_ms / 1e3) / 1e6
+        d = (V - V64).abs()
+        accuracy = {
+            "vs": "fp64 GPU operator",
+            "max_rel": float(d.max() / V64.abs().max()),
+            "rms_rel": float(torch.sqrt((d * d).mean() / (V64 * V64).mean())),
+            "energy_rel": abs(energy - E64) / abs(E64),
+            "fp64_ms_per_step": fp64_ms,
+            "fp64_mpts": fp64_mpts,
+            "speedup_vs_fp64": fp64_ms / ms,
+        }
+        del V64, op64
+
+    # -- end to end through the public API with host buffers -----------------
+    rho_h = torch.empty(rho.numel(), dtype=torch.float64, pin_memory=True)
+    rho_h.copy_(rho.cpu())
+    V_h = torch.empty(rho.numel(), dtype=torch.float64, pin_memory=True)
+    rho_np = rho_h.numpy().reshape(n, n, n).T  # Fortran-ordered (x, y, z) view
+    V_np = V_h.numpy().reshape(n, n, n).T
+    op.apply(rho_np, out=V_np, energy=True)
+    barrier(world)
+    e2e_steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _, e_h = op.apply(rho_np, out=V_np, energy=True)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = barrier_max(e2e_s, world)
+    e2e = {"value": world * npts / e2e_s / 1e6, "unit": "Mpts/s",
+           "h2d_bytes_per_step": int(8 * npts), "d2h_bytes_per_step": int(8 * npts + 8),
+           "ms_per_step": e2e_s * 1e3, "steps": e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        v, dt, sample, cores = cpu_sample(n_t=1)
+        cpu = {"value": v, "unit": "Mpts/s", "cores": cores, "kind": "port", "sample": sample,
+               "seconds": dt}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16" if prec != "fp64" else "f64", "precision": prec,
+            "data": "synthetic",
+            "config": {"workload": f"coulomb_cube_{n}", "points_per_axis": n, "step_bohr": STEP,
+                       "t_points": NLIN + NLOG, "gaussians": N_GAUSS, "seed": SEED,
+                       "l2": "inputs larger than L2 (rho 0.89 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": int(launches), "accuracy": accuracy, "energy": energy,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dage", choices=["dage", "reference"])
+    ap.add_argument("--precision", default=os.environ.get("DAGE_BENCH_PRECISION", "bf16x6"),
+                    choices=["fp64", "bf16x3", "bf16x6"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_gpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,20 @@
+"""dage_b200: B200-native grid-based Coulomb/Helmholtz operator path of DAGE.
+
+All arithmetic happens in ``libdagegpu.so`` (hand-written sm_100a CUDA
+behind the C ABI declared in ``include/dage_gpu.h``); this package is the
+host-side mirror of the reference's Operator3D/Function3D interface.
+"""
+from ._capi import DageError, load  # noqa: F401
+from .operators import (  # noqa: F401
+    Coulomb3D,
+    GaussQuad,
+    Grid1D,
+    Grid3D,
+    Helmholtz3D,
+    Operator3D,
+    dot,
+    integrate,
+)
+
+__all__ = ["Coulomb3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
+           "DageError", "dot", "integrate", "load"]

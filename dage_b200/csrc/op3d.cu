@@ -1,0 +1,717 @@
+// op3d.cu -- the tensor-product cube operator (Coulomb3D / Helmholtz3D cube
+// part) on one B200: quadrature and operator matrices built on the GPU in
+// FP64, the FP64 contraction, the coda term and the fused LIP-weighted
+// energy, and the C ABI around them.
+//
+// Contraction layout.  V = sum_p w_p (T^x_p (x) T^y_p (x) T^z_p) rho is
+// computed as three "contract the fastest index and rotate" stages per
+// t-point:
+//     U(b,c,i) = sum_a rho(a,b,c) Tx(i,a)     rho: a fastest -> U: b fastest
+//     W(c,i,j) = sum_b U(b,c,i)  Ty(j,b)      -> W: c fastest
+//     V(i,j,k) = sum_c W(c,i,j)  Tz(k,c)      -> V: i fastest (input layout)
+// Every stage is the same GEMM D(R, n) = sum_K X(K, R) T(n, K) with both
+// operands contiguous in K and the result written R-fastest, so one kernel
+// (and one tensor-core kernel in op3d_mixed.cu) serves all three.  This is
+// the same arithmetic as the reference's per-slice DGEMMs
+// (src/bubbles/function3d.F90:4296-4332), reordered for coalescing.
+#include <cmath>
+#include <cstring>
+
+#include "expo.cuh"
+#include "op3d.cuh"
+
+namespace dage {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Gauss-Legendre t-points and weights (src/bubbles/gauss.F90:307-383):
+// Newton iteration on P_n from z = cos(pi (i - 1/4) / (n + 1/2)), then the
+// linear map to [tstart, tlin] and the logarithmic map to [tlin, tlog].
+// ---------------------------------------------------------------------------
+__global__ void quad_kernel(int nlin, int nlog, double tstart, double tlin, double tlog,
+                            double *tp, double *tw) {
+  const int seg = blockIdx.x;  // 0: linear part, 1: logarithmic tail
+  const int n = seg == 0 ? nlin : nlog;
+  const int i = threadIdx.x + 1;
+  const int m = (n + 1) / 2;
+  if (n <= 0 || i > m) return;
+  double *x = tp + (seg == 0 ? 0 : nlin);
+  double *w = tw + (seg == 0 ? 0 : nlin);
+  const double pi = acos(-1.0);
+  double z = cos(pi * (i - 0.25) / (n + 0.5));
+  double p1, p2, p3, pp, z1;
+  for (int it = 0; it < 100; ++it) {  // converges in a handful of steps
+    p1 = 1.0;
+    p2 = 0.0;
+    for (int j = 1; j <= n; ++j) {
+      p3 = p2;
+      p2 = p1;
+      p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+    }
+    pp = n * (z * p1 - p2) / (z * z - 1.0);
+    z1 = z;
+    z = z1 - p1 / pp;
+    if (!(fabs(z - z1) > 3.0e-15)) break;
+  }
+  const double wt = 2.0 / ((1.0 - z * z) * pp * pp);
+  const int idx[2] = {i - 1, n - i};
+  const double xs[2] = {-z, z};
+  for (int s = 0; s < 2; ++s) {
+    double t = xs[s], ww = wt;
+    if (seg == 0) {
+      t = 0.5 * ((tlin + tstart) + (tlin - tstart) * t);
+      ww = 0.5 * (tlin - tstart) * ww;
+    } else {
+      t = tlin * pow(tlog / tlin, 0.5 * (t + 1.0));
+      ww = 0.5 * log(tlog / tlin) * ww * t;
+    }
+    x[idx[s]] = t;
+    w[idx[s]] = ww;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Operator matrices (src/bubbles/exponentials.F90:178-346, no PBC images):
+//   T_p(i, j) = sum over the input cells c that contain point j of
+//     h_c * sum_k coeff[k][j - j0(c)] * I_{nlip-1-k}(first, last, t_p h_c, q_i)
+// with q_i = (x_i - celld_c)/h_c + first the output point in the cell's
+// coordinates.  One thread per (t-point, cell, output point); cells of one
+// parity per launch, so the two cells sharing a boundary point never write
+// it concurrently (the shared point receives c's term, then c+1's term).
+// ---------------------------------------------------------------------------
+struct TmatArgs {
+  const double *tp;
+  const double *celld;
+  const double *h;
+  const double *xout;
+  const double *coeff;  // nlip*nlip, coeff[k*nlip + j]
+  double first, last;
+  int P, ncell, n_in, n_out;
+  double *T;  // T[p][i_out][j_in]
+};
+
+template <int NLIP>
+__global__ void tmatrix_kernel(TmatArgs a, int parity) {
+  const int ncells_par = (a.ncell - parity + 1) / 2;
+  const long long total = (long long)a.P * ncells_par * a.n_out;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int io = (int)(id % a.n_out);
+    const long long rest = id / a.n_out;
+    const int c = parity + 2 * (int)(rest % ncells_par);
+    const int ip = (int)(rest / ncells_par);
+    const double h = a.h[c];
+    const double pst0 = (a.xout[io] - a.celld[c]) / h + a.first;
+    double vals[NLIP];
+    expo::integrals(a.first, a.last, a.tp[ip] * h, pst0, NLIP, vals);
+    double *row = a.T + ((size_t)ip * a.n_out + io) * a.n_in + (size_t)c * (NLIP - 1);
+#pragma unroll
+    for (int j = 0; j < NLIP; ++j) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NLIP; ++k) s += a.coeff[k * NLIP + j] * vals[k];
+      row[j] += s * h;
+    }
+  }
+}
+
+int launch_tmatrix(const TmatArgs &a, int nlip, cudaStream_t s) {
+  for (int parity = 0; parity < 2; ++parity) {
+    const long long total = (long long)a.P * ((a.ncell - parity + 1) / 2) * a.n_out;
+    if (total == 0) continue;
+    const int threads = 128;
+    const int blocks = (int)std::min<long long>((total + threads - 1) / threads, 148LL * 64);
+    switch (nlip) {
+      case 2: tmatrix_kernel<2><<<blocks, threads, 0, s>>>(a, parity); break;
+      case 3: tmatrix_kernel<3><<<blocks, threads, 0, s>>>(a, parity); break;
+      case 4: tmatrix_kernel<4><<<blocks, threads, 0, s>>>(a, parity); break;
+      case 5: tmatrix_kernel<5><<<blocks, threads, 0, s>>>(a, parity); break;
+      case 6: tmatrix_kernel<6><<<blocks, threads, 0, s>>>(a, parity); break;
+      case 7: tmatrix_kernel<7><<<blocks, threads, 0, s>>>(a, parity); break;
+      default: return fail(DAGE_E_UNSUPPORTED, "nlip=%d", nlip);
+    }
+    DAGE_CUDA_TRY(cudaGetLastError());
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 stage GEMM: 128x128 output tile per 256-thread block, 8x8 register
+// micro-tile per thread, K in steps of 8 with register-staged double
+// buffering through shared memory.
+// ---------------------------------------------------------------------------
+constexpr int BM = 128, BN = 128, BK = 8, PAD = 2;
+
+template <bool ACCUM>
+__global__ void __launch_bounds__(256) stage_fp64_kernel(const double *__restrict__ X,
+                                                         long long ldx, int M, int N, int K,
+                                                         const double *__restrict__ T,
+                                                         long long ldt, double *__restrict__ out,
+                                                         double alpha) {
+  __shared__ __align__(16) double As[2][BK][BM + PAD];
+  __shared__ __align__(16) double Bs[2][BK][BN + PAD];
+  const int tid = threadIdx.x;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tx = tid & 15, ty = tid >> 4;  // tx -> rows (R), ty -> columns (n)
+
+  double ra[4], rb[4];
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
+      const int m = m0 + r, n = n0 + r, k = k0 + kk;
+      ra[i] = (m < M && k < K) ? __ldg(X + (size_t)m * ldx + k) : 0.0;
+      rb[i] = (n < N && k < K) ? __ldg(T + (size_t)n * ldt + k) : 0.0;
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
+      As[buf][kk][r] = ra[i];
+      Bs[buf][kk][r] = rb[i];
+    }
+  };
+
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+
+  const int nk = (K + BK - 1) / BK;
+  gload(0);
+  sstore(0);
+  __syncthreads();
+  for (int kt = 0; kt < nk; ++kt) {
+    const int cur = kt & 1;
+    if (kt + 1 < nk) gload((kt + 1) * BK);
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      double a[8], b[8];
+      const double2 *ap = reinterpret_cast<const double2 *>(&As[cur][k][0]);
+      const double2 *bp = reinterpret_cast<const double2 *>(&Bs[cur][k][0]);
+      double2 t0 = ap[tx * 2], t1 = ap[tx * 2 + 1], t2 = ap[32 + tx * 2], t3 = ap[32 + tx * 2 + 1];
+      a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
+      a[4] = t2.x; a[5] = t2.y; a[6] = t3.x; a[7] = t3.y;
+      double2 u0 = bp[ty * 2], u1 = bp[ty * 2 + 1], u2 = bp[32 + ty * 2], u3 = bp[32 + ty * 2 + 1];
+      b[0] = u0.x; b[1] = u0.y; b[2] = u1.x; b[3] = u1.y;
+      b[4] = u2.x; b[5] = u2.y; b[6] = u3.x; b[7] = u3.y;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (kt + 1 < nk) {
+      sstore(cur ^ 1);
+      __syncthreads();
+    }
+  }
+
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int n = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+    if (n >= N) continue;
+    double *col = out + (size_t)n * M;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int m = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+      if (m >= M) continue;
+      if (ACCUM)
+        col[m] = col[m] + alpha * acc[i][j];
+      else
+        col[m] = alpha * acc[i][j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coda + LIP-weighted integral, deterministic two-pass FP64 reduction.
+// ---------------------------------------------------------------------------
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 148 * 4;
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  v = 0.0;
+  if (wid == 0) {
+    v = lane < (blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+    finalize_kernel(const double *__restrict__ f1, double *f2, const double *__restrict__ rho,
+                    double coda, const double *__restrict__ wx, const double *__restrict__ wy,
+                    const double *__restrict__ wz, int nx, int ny, int nz, double *partials,
+                    int want_integral) {
+  __shared__ double sh[32];
+  const long long n = (long long)nx * ny * nz;
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double v2 = 1.0;
+    if (f2) {
+      v2 = f2[i];
+      if (rho) {
+        v2 = v2 + coda * rho[i];
+        f2[i] = v2;
+      }
+    }
+    if (want_integral) {
+      const int x = (int)(i % nx);
+      const long long r = i / nx;
+      const int y = (int)(r % ny), z = (int)(r / ny);
+      s += f1[i] * v2 * (wx[x] * wy[y] * wz[z]);
+    }
+  }
+  if (!want_integral) return;
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void sum_partials_kernel(const double *partials, int n, double *result) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) *result = s;
+}
+
+}  // namespace
+
+int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,
+                      long long ldt, double *out, double alpha, bool accumulate,
+                      cudaStream_t s) {
+  dim3 grid(ceil_div(M, BM), ceil_div(N, BN));
+  if (grid.y > 65535) return fail(DAGE_E_UNSUPPORTED, "N=%d too large", N);
+  if (accumulate)
+    stage_fp64_kernel<true><<<grid, 256, 0, s>>>(X, ldx, M, N, K, T, ldt, out, alpha);
+  else
+    stage_fp64_kernel<false><<<grid, 256, 0, s>>>(X, ldx, M, N, K, T, ldt, out, alpha);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int finalize_partials_count() { return kRedBlocks + 1; }
+
+int launch_finalize(const double *f1, double *f2_or_V, const double *rho_for_coda, double coda,
+                    const double *wx, const double *wy, const double *wz, int nx, int ny,
+                    int nz, double *partials, int npartials, double *d_result,
+                    cudaStream_t s) {
+  const int want = d_result != nullptr;
+  if (!want && !rho_for_coda) return 0;
+  const int blocks = std::min(kRedBlocks, npartials - 1);
+  finalize_kernel<<<blocks, kRedThreads, 0, s>>>(f1, f2_or_V, rho_for_coda, coda, wx, wy, wz,
+                                                  nx, ny, nz, partials, want);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  if (want) {
+    sum_partials_kernel<<<1, 1024, 0, s>>>(partials, blocks, d_result);
+    DAGE_CUDA_TRY(cudaGetLastError());
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Operator construction
+// ---------------------------------------------------------------------------
+static int build_matrices(dage_op3d *op) {
+  cudaStream_t s = op->stream;
+  DevBuf d_tp, d_tw;
+  DAGE_TRY(d_tp.alloc(sizeof(double) * op->P));
+  DAGE_TRY(d_tw.alloc(sizeof(double) * op->P));
+  quad_kernel<<<2, 128, 0, s>>>(op->quad.nlin, op->quad.nlog, op->quad.tstart, op->quad.tlin,
+                                op->quad.tlog, d_tp.as<double>(), d_tw.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  op->tp.resize(op->P);
+  op->tw.resize(op->P);
+  DAGE_CUDA_TRY(cudaMemcpyAsync(op->tp.data(), d_tp.ptr, sizeof(double) * op->P,
+                                cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(op->tw.data(), d_tw.ptr, sizeof(double) * op->P,
+                                cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
+  op->w.resize(op->P);
+  for (int p = 0; p < op->P; ++p) op->w[p] = two_over_sqrtpi * op->tw[p];
+  op->coda = std::acos(-1.0) / (op->quad.tlog * op->quad.tlog);
+
+  for (int d = 0; d < 3; ++d) {
+    op->Towner[d] = d;
+    for (int e = 0; e < d; ++e)
+      if (same_axis(op->in[d], op->in[e]) && same_axis(op->out[d], op->out[e])) {
+        op->Towner[d] = op->Towner[e];
+        break;
+      }
+    if (op->Towner[d] != d) continue;
+    const Axis &ai = op->in[d];
+    const Axis &ao = op->out[d];
+    LipBasis L;
+    DAGE_TRY(make_lip_basis(ai.nlip, ai.grid_type, L));
+    const size_t nT = (size_t)op->P * ao.n() * ai.n();
+    DAGE_TRY(op->Tbuf[d].alloc(sizeof(double) * nT));
+    DAGE_CUDA_TRY(cudaMemsetAsync(op->Tbuf[d].ptr, 0, sizeof(double) * nT, s));
+    DevBuf d_celld, d_h, d_x, d_c;
+    DAGE_TRY(d_celld.alloc(sizeof(double) * ai.ncell));
+    DAGE_TRY(d_h.alloc(sizeof(double) * ai.ncell));
+    DAGE_TRY(d_x.alloc(sizeof(double) * ao.n()));
+    DAGE_TRY(d_c.alloc(sizeof(double) * L.coeff.size()));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(d_celld.ptr, ai.celld.data(), sizeof(double) * ai.ncell,
+                                  cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(d_h.ptr, ai.h.data(), sizeof(double) * ai.ncell,
+                                  cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(d_x.ptr, ao.points.data(), sizeof(double) * ao.n(),
+                                  cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(d_c.ptr, L.coeff.data(), sizeof(double) * L.coeff.size(),
+                                  cudaMemcpyHostToDevice, s));
+    TmatArgs a;
+    a.tp = d_tp.as<double>();
+    a.celld = d_celld.as<double>();
+    a.h = d_h.as<double>();
+    a.xout = d_x.as<double>();
+    a.coeff = d_c.as<double>();
+    a.first = L.first;
+    a.last = L.last;
+    a.P = op->P;
+    a.ncell = ai.ncell;
+    a.n_in = ai.n();
+    a.n_out = ao.n();
+    a.T = op->Tbuf[d].as<double>();
+    DAGE_TRY(launch_tmatrix(a, ai.nlip, s));
+    DAGE_CUDA_TRY(cudaStreamSynchronize(s));  // before the small buffers go
+    d_celld.release();
+    d_h.release();
+    d_x.release();
+    d_c.release();
+  }
+  d_tp.release();
+  d_tw.release();
+  return 0;
+}
+
+static int upload_weights(dage_op3d *op) {
+  DAGE_TRY(op->d_w.alloc(sizeof(double) * op->P));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(op->d_w.ptr, op->w.data(), sizeof(double) * op->P,
+                                cudaMemcpyHostToDevice, op->stream));
+  if (op->precision != DAGE_FP64) DAGE_TRY(mixed_set_weights(op));
+  return 0;
+}
+
+static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
+                       const dage_quad *quad, int precision, dage_op3d *op) {
+  if (!grid_in || !grid_out || !quad) return fail(DAGE_E_INVALID, "null argument");
+  if (quad->nlin < 0 || quad->nlog < 0 || quad->nlin + quad->nlog < 1 ||
+      quad->nlin > 256 || quad->nlog > 256)
+    return fail(DAGE_E_INVALID, "quadrature needs 1..512 t-points");
+  if (quad->nlog > 0 && !(quad->tlog > quad->tlin && quad->tlin > 0.0))
+    return fail(DAGE_E_INVALID, "logarithmic tail needs 0 < tlin < tlog");
+  if (precision != DAGE_FP64 && precision != DAGE_MIXED_BF16X3 &&
+      precision != DAGE_MIXED_BF16X6)
+    return fail(DAGE_E_INVALID, "unknown precision %d", precision);
+  op->precision = precision;
+  op->quad = *quad;
+  op->P = quad->nlin + quad->nlog;
+  DAGE_CUDA_TRY(cudaGetDevice(&op->device));
+  for (int d = 0; d < 3; ++d) {
+    DAGE_TRY(make_axis(grid_in[d], op->in[d]));
+    DAGE_TRY(make_axis(grid_out[d], op->out[d]));
+    op->nin[d] = op->in[d].n();
+    op->nout[d] = op->out[d].n();
+    if (op->in[d].nlip != op->in[0].nlip || op->in[d].grid_type != op->in[0].grid_type)
+      return fail(DAGE_E_UNSUPPORTED, "all axes must share nlip and grid_type");
+  }
+  op->same_grid = same_axis(op->in[0], op->out[0]) && same_axis(op->in[1], op->out[1]) &&
+                  same_axis(op->in[2], op->out[2]);
+  DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->own_stream, cudaStreamNonBlocking));
+  op->stream = op->own_stream;
+  DAGE_CUDA_TRY(cudaEventCreate(&op->ev0));
+  DAGE_CUDA_TRY(cudaEventCreate(&op->ev1));
+  DAGE_TRY(build_matrices(op));
+  for (int d = 0; d < 3; ++d) {
+    DAGE_TRY(op->wts[d].alloc(sizeof(double) * op->nout[d]));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(op->wts[d].ptr, op->out[d].weights.data(),
+                                  sizeof(double) * op->nout[d], cudaMemcpyHostToDevice,
+                                  op->stream));
+  }
+  DAGE_TRY(op->partials.alloc(sizeof(double) * (finalize_partials_count() + 1)));
+  if (precision != DAGE_FP64) DAGE_TRY(mixed_setup(op));
+  DAGE_TRY(upload_weights(op));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
+  return 0;
+}
+
+static void destroy_impl(dage_op3d *op) {
+  if (!op) return;
+  if (op->stream) cudaStreamSynchronize(op->stream);
+  mixed_destroy(op);
+  for (int d = 0; d < 3; ++d) {
+    op->Tbuf[d].release();
+    op->wts[d].release();
+  }
+  op->d_w.release();
+  op->d_rho.release();
+  op->d_V.release();
+  op->tmp1.release();
+  op->tmp2.release();
+  op->partials.release();
+  for (cudaEvent_t e : op->tev) cudaEventDestroy(e);
+  if (op->ev0) cudaEventDestroy(op->ev0);
+  if (op->ev1) cudaEventDestroy(op->ev1);
+  if (op->own_stream) cudaStreamDestroy(op->own_stream);
+  delete op;
+}
+
+static int apply_fp64(dage_op3d *op, const double *rho, double *V, bool accumulate) {
+  cudaStream_t s = op->stream;
+  const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
+  const int nox = op->nout[0], noy = op->nout[1], noz = op->nout[2];
+  DAGE_TRY(op->tmp1.alloc(sizeof(double) * (size_t)niy * niz * nox));
+  DAGE_TRY(op->tmp2.alloc(sizeof(double) * (size_t)niz * nox * noy));
+  double *U = op->tmp1.as<double>(), *W = op->tmp2.as<double>();
+  const size_t sx = (size_t)nox * nix, sy = (size_t)noy * niy, sz = (size_t)noz * niz;
+  for (int p = 0; p < op->P; ++p) {
+    int t = op->tmark_begin(0);
+    DAGE_TRY(launch_stage_fp64(rho, nix, niy * niz, nox, nix, op->T(0) + sx * p, nix, U, 1.0,
+                               false, s));
+    op->tmark_end(t);
+    t = op->tmark_begin(0);
+    DAGE_TRY(launch_stage_fp64(U, niy, niz * nox, noy, niy, op->T(1) + sy * p, niy, W, 1.0,
+                               false, s));
+    op->tmark_end(t);
+    t = op->tmark_begin(0);
+    DAGE_TRY(launch_stage_fp64(W, niz, nox * noy, noz, niz, op->T(2) + sz * p, niz, V,
+                               op->w[p], accumulate || p > 0, s));
+    op->tmark_end(t);
+  }
+  return 0;
+}
+
+}  // namespace dage
+
+using namespace dage;
+
+int dage_op3d::tmark_begin(int kind) {
+  if (!timing) return -1;
+  const size_t slot = tq.size();
+  while (tev.size() < 2 * (slot + 1)) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    tev.push_back(e);
+  }
+  cudaEventRecord(tev[2 * slot], stream);
+  tq.push_back({kind, (int)(2 * slot)});
+  return (int)slot;
+}
+
+void dage_op3d::tmark_end(int slot) {
+  if (slot < 0) return;
+  cudaEventRecord(tev[tq[slot].second + 1], stream);
+}
+
+int dage_op3d::tcollect() {
+  for (auto &q : tq) {
+    float ms = 0.0f;
+    DAGE_CUDA_TRY(cudaEventElapsedTime(&ms, tev[q.second], tev[q.second + 1]));
+    t_ms[q.first] += ms;
+    t_launches[q.first] += 1;
+  }
+  tq.clear();
+  return 0;
+}
+
+extern "C" {
+
+int dage_op3d_create(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
+                     const dage_quad *quad, int precision, dage_op3d **out) {
+  clear_error();
+  if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
+  *out = nullptr;
+  dage_op3d *op = new dage_op3d();
+  int rc = create_impl(grid_in, grid_out, quad, precision, op);
+  if (rc) {
+    destroy_impl(op);
+    return rc;
+  }
+  *out = op;
+  return 0;
+}
+
+int dage_op3d_destroy(dage_op3d *op) {
+  clear_error();
+  destroy_impl(op);
+  return 0;
+}
+
+int dage_op3d_set_stream(dage_op3d *op, void *stream) {
+  if (!op) return fail(DAGE_E_INVALID, "null handle");
+  op->stream = stream ? (cudaStream_t)stream : op->own_stream;
+  return 0;
+}
+
+int dage_op3d_set_weights(dage_op3d *op, int P, const double *w) {
+  clear_error();
+  if (!op || !w) return fail(DAGE_E_INVALID, "null argument");
+  if (P != op->P) return fail(DAGE_E_INVALID, "expected %d weights, got %d", op->P, P);
+  op->w.assign(w, w + P);
+  DAGE_TRY(upload_weights(op));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
+  return 0;
+}
+
+int dage_op3d_set_energy(dage_op3d *op, double energy) {
+  if (!op) return fail(DAGE_E_INVALID, "null handle");
+  const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
+  std::vector<double> w(op->P);
+  for (int p = 0; p < op->P; ++p) {
+    double tw = op->tw[p];
+    if (energy < -0.005) tw = tw * std::exp(2.0 * energy / (4.0 * (op->tp[p] * op->tp[p])));
+    w[p] = two_over_sqrtpi * tw;
+  }
+  return dage_op3d_set_weights(op, op->P, w.data());
+}
+
+int dage_op3d_set_coda(dage_op3d *op, double coda) {
+  if (!op) return fail(DAGE_E_INVALID, "null handle");
+  op->coda = coda;
+  return 0;
+}
+
+int dage_op3d_get_quadrature(const dage_op3d *op, int *P, double *tp, double *w) {
+  if (!op) return fail(DAGE_E_INVALID, "null handle");
+  if (P) *P = op->P;
+  if (tp) std::memcpy(tp, op->tp.data(), sizeof(double) * op->P);
+  if (w) std::memcpy(w, op->w.data(), sizeof(double) * op->P);
+  return 0;
+}
+
+int dage_op3d_get_matrix(const dage_op3d *op, int axis, double *T_host) {
+  clear_error();
+  if (!op || !T_host || axis < 0 || axis > 2) return fail(DAGE_E_INVALID, "bad argument");
+  const int ni = op->nin[axis], no = op->nout[axis];
+  std::vector<double> tmp((size_t)op->P * ni * no);
+  DAGE_CUDA_TRY(cudaMemcpy(tmp.data(), op->T(axis), sizeof(double) * tmp.size(),
+                           cudaMemcpyDeviceToHost));
+  // device layout T[p][i_out][j_in] -> host T(i_out, j_in, p) column-major
+  for (int p = 0; p < op->P; ++p)
+    for (int i = 0; i < no; ++i)
+      for (int j = 0; j < ni; ++j)
+        T_host[(size_t)p * no * ni + (size_t)j * no + i] = tmp[((size_t)p * no + i) * ni + j];
+  return 0;
+}
+
+int dage_op3d_last_time_ms(const dage_op3d *op, float *ms) {
+  if (!op || !ms) return fail(DAGE_E_INVALID, "null argument");
+  *ms = op->last_ms;
+  return 0;
+}
+
+int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
+                    double *energy) {
+  clear_error();
+  if (!op || !rho || !V) return fail(DAGE_E_INVALID, "null argument");
+  if ((flags & DAGE_ENERGY) && !energy) return fail(DAGE_E_INVALID, "energy pointer is null");
+  DAGE_CUDA_TRY(cudaSetDevice(op->device));
+  cudaStream_t s = op->stream;
+  const size_t nin = (size_t)op->nin[0] * op->nin[1] * op->nin[2];
+  const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
+  const bool dev = (flags & DAGE_DEVICE_PTRS) != 0;
+  const bool acc = (flags & DAGE_ACCUMULATE) != 0;
+  const double *d_rho = rho;
+  double *d_V = V;
+  DAGE_CUDA_TRY(cudaEventRecord(op->ev0, s));
+  if (!dev) {
+    DAGE_TRY(op->d_rho.alloc(sizeof(double) * nin));
+    DAGE_TRY(op->d_V.alloc(sizeof(double) * nout));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(op->d_rho.ptr, rho, sizeof(double) * nin,
+                                  cudaMemcpyHostToDevice, s));
+    if (acc)
+      DAGE_CUDA_TRY(cudaMemcpyAsync(op->d_V.ptr, V, sizeof(double) * nout,
+                                    cudaMemcpyHostToDevice, s));
+    d_rho = op->d_rho.as<double>();
+    d_V = op->d_V.as<double>();
+  }
+  if (op->precision == DAGE_FP64) {
+    DAGE_TRY(apply_fp64(op, d_rho, d_V, acc));
+  } else {
+    if (acc) return fail(DAGE_E_UNSUPPORTED, "DAGE_ACCUMULATE with a mixed operator");
+    DAGE_TRY(mixed_apply(op, d_rho, d_V, s));
+  }
+  const bool coda = op->same_grid && op->coda != 0.0 && !(flags & DAGE_NO_CODA);
+  double *d_res = (flags & DAGE_ENERGY) ? op->partials.as<double>() + finalize_partials_count()
+                                        : nullptr;
+  const int tf = op->tmark_begin(2);
+  DAGE_TRY(launch_finalize(d_rho, d_V, coda ? d_rho : nullptr, op->coda, op->wts[0].as<double>(),
+                           op->wts[1].as<double>(), op->wts[2].as<double>(), op->nout[0],
+                           op->nout[1], op->nout[2], op->partials.as<double>(),
+                           finalize_partials_count(), d_res, s));
+  op->tmark_end(tf);
+  if (!dev)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+  if (d_res) DAGE_CUDA_TRY(cudaMemcpyAsync(energy, d_res, sizeof(double), cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaEventRecord(op->ev1, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  DAGE_CUDA_TRY(cudaEventElapsedTime(&op->last_ms, op->ev0, op->ev1));
+  DAGE_TRY(op->tcollect());
+  return 0;
+}
+
+int dage_op3d_set_timing(dage_op3d *op, int enable) {
+  if (!op) return fail(DAGE_E_INVALID, "null handle");
+  op->timing = enable != 0;
+  for (int k = 0; k < dage_op3d::kKinds; ++k) {
+    op->t_launches[k] = 0;
+    op->t_ms[k] = 0.0;
+  }
+  op->tq.clear();
+  return 0;
+}
+
+int dage_op3d_get_timing(const dage_op3d *op, int kind, long long *launches, double *ms) {
+  if (!op || kind < 0 || kind >= dage_op3d::kKinds) return fail(DAGE_E_INVALID, "bad argument");
+  if (launches) *launches = op->t_launches[kind];
+  if (ms) *ms = op->t_ms[kind];
+  return 0;
+}
+
+int dage_integrate(const dage_grid1d grid[3], const double *f1, const double *f2,
+                   unsigned flags, double *out) {
+  clear_error();
+  if (!grid || !f1 || !out) return fail(DAGE_E_INVALID, "null argument");
+  Axis ax[3];
+  for (int d = 0; d < 3; ++d) DAGE_TRY(make_axis(grid[d], ax[d]));
+  const size_t n = (size_t)ax[0].n() * ax[1].n() * ax[2].n();
+  const bool dev = (flags & DAGE_DEVICE_PTRS) != 0;
+  DevBuf w[3], b1, b2, part;
+  for (int d = 0; d < 3; ++d) {
+    DAGE_TRY(w[d].alloc(sizeof(double) * ax[d].n()));
+    DAGE_CUDA_TRY(cudaMemcpy(w[d].ptr, ax[d].weights.data(), sizeof(double) * ax[d].n(),
+                             cudaMemcpyHostToDevice));
+  }
+  const double *d1 = f1;
+  double *d2 = const_cast<double *>(f2);
+  if (!dev) {
+    DAGE_TRY(b1.alloc(sizeof(double) * n));
+    DAGE_CUDA_TRY(cudaMemcpy(b1.ptr, f1, sizeof(double) * n, cudaMemcpyHostToDevice));
+    d1 = b1.as<double>();
+    if (f2) {
+      DAGE_TRY(b2.alloc(sizeof(double) * n));
+      DAGE_CUDA_TRY(cudaMemcpy(b2.ptr, f2, sizeof(double) * n, cudaMemcpyHostToDevice));
+      d2 = b2.as<double>();
+    }
+  }
+  DAGE_TRY(part.alloc(sizeof(double) * (finalize_partials_count() + 1)));
+  double *res = part.as<double>() + finalize_partials_count();
+  DAGE_TRY(launch_finalize(d1, d2, nullptr, 0.0, w[0].as<double>(), w[1].as<double>(),
+                           w[2].as<double>(), ax[0].n(), ax[1].n(), ax[2].n(),
+                           part.as<double>(), finalize_partials_count(), res, 0));
+  DAGE_CUDA_TRY(cudaMemcpy(out, res, sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // extern "C"

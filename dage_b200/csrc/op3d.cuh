@@ -1,0 +1,80 @@
+// op3d.cuh -- internal state of a tensor-product cube operator handle and
+// the kernel launchers shared by its FP64 and mixed-precision paths.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "grid_host.h"
+
+struct dage_op3d {
+  int precision = DAGE_FP64;
+  int device = 0;
+  dage::Axis in[3], out[3];
+  int nin[3] = {0, 0, 0}, nout[3] = {0, 0, 0};
+  bool same_grid = false;
+
+  // quadrature
+  dage_quad quad{};
+  int P = 0;
+  std::vector<double> tp, tw, w;  // host copies; w = weights in use
+  double coda = 0.0;
+
+  // FP64 matrices, per axis: T[p][i_out][j_in] (row-major in j_in).  Axes
+  // with identical input/output grids share one buffer (owner index).
+  dage::DevBuf Tbuf[3];
+  int Towner[3] = {0, 1, 2};
+  const double *T(int axis) const { return Tbuf[Towner[axis]].as<double>(); }
+
+  // per-point LIP integration weights of the output grid (energy)
+  dage::DevBuf wts[3];
+  dage::DevBuf d_w;          // weights w_p on the device
+  dage::DevBuf d_rho, d_V;   // staging for host pointers
+  dage::DevBuf tmp1, tmp2;   // intermediates of the FP64 path
+  dage::DevBuf partials;     // energy reduction partial sums
+
+  // mixed-precision state (op3d_mixed.cu)
+  void *mixed = nullptr;
+
+  // per-kernel timing (dage_op3d_set_timing)
+  static constexpr int kKinds = 3;
+  bool timing = false;
+  std::vector<cudaEvent_t> tev;          // event pool
+  std::vector<std::pair<int, int>> tq;   // (kind, first event index) queued
+  long long t_launches[kKinds] = {0, 0, 0};
+  double t_ms[kKinds] = {0, 0, 0};
+  int tmark_begin(int kind);             // returns slot or -1
+  void tmark_end(int slot);
+  int tcollect();                        // after stream sync
+
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.0f;
+};
+
+namespace dage {
+
+// FP64 "contract the fastest index and rotate" stage:
+//   out[R + n*M] (= or +=) alpha * sum_K X[R*ldx + K] * T[n*ldt + K]
+int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,
+                      long long ldt, double *out, double alpha, bool accumulate,
+                      cudaStream_t s);
+
+// V += coda * rho (when coda != 0) and the LIP-weighted integral of
+// f1 * f2 (f2 may be null: integral of f1).  The result lands in *d_result
+// (device) after a deterministic two-pass reduction.
+int launch_finalize(const double *f1, double *f2_or_V, const double *rho_for_coda,
+                    double coda, const double *wx, const double *wy, const double *wz,
+                    int nx, int ny, int nz, double *partials, int npartials,
+                    double *d_result, cudaStream_t s);
+
+int finalize_partials_count();
+
+// mixed-precision path (op3d_mixed.cu)
+int mixed_setup(dage_op3d *op);
+int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s);
+int mixed_set_weights(dage_op3d *op);
+void mixed_destroy(dage_op3d *op);
+
+}  // namespace dage

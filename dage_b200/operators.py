@@ -1,0 +1,293 @@
+"""Host-side mirror of the reference's operator interface for this path.
+
+The names follow DAGE's Fortran types (``GaussQuad``, ``Grid1D``,
+``Grid3D``, ``Coulomb3D``, ``Helmholtz3D``, ``Function3D``-style
+``dot``/``integrate``) so that code written against the reference's
+``Operator3D``/``Function3D`` API reads the same:
+
+    V = Coulomb3D(grid) .apply(rho)           # Operator3D .apply.
+    E = integrate(grid, rho, V)               # rho .dot. V
+
+Cubes are numpy arrays in Fortran order ``(nx, ny, nz)`` (host memory) or
+torch CUDA tensors whose storage is the same column-major cube (device
+memory, e.g. ``t = torch.empty(nz, ny, nx)``; x fastest).  All arithmetic
+runs in libdagegpu.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+from ._capi import DageGrid1D, DageQuad, check, load
+
+PRECISIONS = {
+    "fp64": _capi.DAGE_FP64,
+    "bf16x3": _capi.DAGE_MIXED_BF16X3,
+    "bf16x6": _capi.DAGE_MIXED_BF16X6,
+}
+
+
+@dataclass
+class GaussQuad:
+    """GaussQuad (src/bubbles/gauss.F90:55-122); same defaults."""
+
+    nlin: int = 10
+    nlog: int = 8
+    tstart: float = 0.0
+    tlin: float = 2.0
+    tlog: float = 1.0e3
+
+    def c(self) -> DageQuad:
+        return DageQuad(self.nlin, self.nlog, self.tstart, self.tlin, self.tlog)
+
+    @property
+    def npoints(self) -> int:
+        return self.nlin + self.nlog
+
+
+@dataclass
+class Grid1D:
+    """One axis of LIP cells (src/bubbles/grid.F90:446-534)."""
+
+    qmin: float
+    ncell: int
+    nlip: int = 7
+    grid_type: int = 1
+    cell_scales: np.ndarray = field(default=None)
+
+    def __post_init__(self):
+        if self.cell_scales is None:
+            raise ValueError("cell_scales required")
+        self.cell_scales = np.ascontiguousarray(
+            np.broadcast_to(np.asarray(self.cell_scales, dtype=np.float64), (self.ncell,)))
+
+    @classmethod
+    def equidistant(cls, qmin: float, ncell: int, step: float, nlip: int = 7, grid_type: int = 1):
+        return cls(float(qmin), int(ncell), nlip, grid_type, np.full(ncell, float(step)))
+
+    @property
+    def n(self) -> int:
+        return self.ncell * (self.nlip - 1) + 1
+
+    def c(self) -> DageGrid1D:
+        return DageGrid1D(self.ncell, self.nlip, self.grid_type, self.qmin,
+                          self.cell_scales.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def coordinates(self) -> np.ndarray:
+        """Grid point coordinates (equidistant cells only)."""
+        if self.grid_type != 1:
+            raise NotImplementedError("coordinates() for equidistant cells")
+        pts = [self.qmin]
+        x = self.qmin
+        for h in self.cell_scales:
+            start = x
+            for k in range(1, self.nlip):
+                pts.append(start + k * h)
+            x = pts[-1]
+        return np.asarray(pts)
+
+
+@dataclass
+class Grid3D:
+    axes: tuple
+
+    @classmethod
+    def cube(cls, qmin: float, ncell: int, step: float, nlip: int = 7, grid_type: int = 1):
+        ax = Grid1D.equidistant(qmin, ncell, step, nlip, grid_type)
+        return cls((ax, ax, ax))
+
+    @property
+    def shape(self):
+        return tuple(a.n for a in self.axes)
+
+    def c(self):
+        arr = (DageGrid1D * 3)(*[a.c() for a in self.axes])
+        return arr
+
+
+def _ptr(a, nelem: int):
+    """(pointer, is_device) of a float64 cube with nelem elements."""
+    try:
+        import torch  # noqa: F401
+
+        if hasattr(a, "is_cuda"):
+            if a.dtype != torch.float64 or not a.is_contiguous():
+                raise TypeError("torch cube must be contiguous float64")
+            if a.numel() != nelem:
+                raise ValueError(f"cube has {a.numel()} elements, expected {nelem}")
+            return ctypes.c_void_p(a.data_ptr()), a.is_cuda
+    except ImportError:
+        pass
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64:
+        raise TypeError("cube must be a float64 numpy array or torch tensor")
+    if not a.flags.f_contiguous:
+        raise TypeError("numpy cube must be Fortran-ordered (x fastest)")
+    if a.size != nelem:
+        raise ValueError(f"cube has {a.size} elements, expected {nelem}")
+    return ctypes.c_void_p(a.ctypes.data), False
+
+
+class Operator3D:
+    """Tensor-product cube operator, V = sum_p w_p (T^x_p (x) T^y_p (x) T^z_p) rho
+    (+ coda rho).  ``Coulomb3D`` and ``Helmholtz3D`` are its two kernels."""
+
+    def __init__(self, gridin: Grid3D, gridout: Grid3D | None = None,
+                 quad: GaussQuad | None = None, precision: str = "fp64"):
+        lib = load()
+        self.gridin = gridin
+        self.gridout = gridout if gridout is not None else gridin
+        self.quad = quad if quad is not None else GaussQuad()
+        self.precision = precision
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {list(PRECISIONS)}")
+        self._keep = (self.gridin.c(), self.gridout.c(), self.quad.c())
+        h = ctypes.c_void_p()
+        check(lib.dage_op3d_create(self._keep[0], self._keep[1], ctypes.byref(self._keep[2]),
+                                   PRECISIONS[precision], ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                load().dage_op3d_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # -- quadrature -------------------------------------------------------
+    def quadrature(self):
+        P = self.quad.npoints
+        tp = np.zeros(P)
+        w = np.zeros(P)
+        n = ctypes.c_int()
+        dp = ctypes.POINTER(ctypes.c_double)
+        check(load().dage_op3d_get_quadrature(self._h, ctypes.byref(n), tp.ctypes.data_as(dp),
+                                              w.ctypes.data_as(dp)))
+        return tp, w
+
+    @property
+    def tpoints(self):
+        return self.quadrature()[0]
+
+    @property
+    def weights(self):
+        return self.quadrature()[1]
+
+    def set_transformation_weights(self, w) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        check(load().dage_op3d_set_weights(self._h, len(w),
+                                           w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def set_coda(self, coda: float) -> None:
+        check(load().dage_op3d_set_coda(self._h, float(coda)))
+
+    def set_stream(self, stream) -> None:
+        """Run on a caller's CUDA stream (a torch.cuda.Stream or raw handle)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        check(load().dage_op3d_set_stream(self._h, ctypes.c_void_p(handle or 0)))
+
+    def matrix(self, axis: int) -> np.ndarray:
+        """FP64 matrix of one axis, T(i_out, j_in, p)."""
+        no = self.gridout.axes[axis].n
+        ni = self.gridin.axes[axis].n
+        T = np.zeros((no, ni, self.quad.npoints), order="F")
+        check(load().dage_op3d_get_matrix(self._h, axis,
+                                          T.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return T
+
+    def set_timing(self, enable: bool = True) -> None:
+        """Per-kernel CUDA-event timing of later applies (resets totals)."""
+        check(load().dage_op3d_set_timing(self._h, int(bool(enable))))
+
+    def timing(self, kind: int = 0):
+        """(launches, total ms) of one kernel kind since set_timing():
+        0 = contraction stages, 1 = precision split, 2 = finalize."""
+        n = ctypes.c_longlong()
+        ms = ctypes.c_double()
+        check(load().dage_op3d_get_timing(self._h, kind, ctypes.byref(n), ctypes.byref(ms)))
+        return n.value, ms.value
+
+    @property
+    def last_time_ms(self) -> float:
+        v = ctypes.c_float()
+        check(load().dage_op3d_last_time_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+    # -- application ------------------------------------------------------
+    def apply(self, rho, out=None, energy: bool = False, coda: bool = True,
+              accumulate: bool = False):
+        """V = self .apply. rho.  Returns V, or (V, integral of rho*V) when
+        ``energy`` is set.  ``rho``/``out`` may be host (numpy, Fortran
+        order) or device (torch CUDA) cubes; the output follows the input."""
+        nin = int(np.prod(self.gridin.shape))
+        nout = int(np.prod(self.gridout.shape))
+        rp, rdev = _ptr(rho, nin)
+        if out is None:
+            if rdev:
+                import torch
+
+                out = torch.zeros(self.gridout.shape[::-1], dtype=torch.float64,
+                                  device=rho.device)
+            else:
+                out = np.zeros(self.gridout.shape, order="F")
+        vp, vdev = _ptr(out, nout)
+        if rdev != vdev:
+            raise ValueError("rho and out must both be host or both be device cubes")
+        flags = (_capi.DAGE_DEVICE_PTRS if rdev else 0) | (_capi.DAGE_ENERGY if energy else 0)
+        flags |= 0 if coda else _capi.DAGE_NO_CODA
+        flags |= _capi.DAGE_ACCUMULATE if accumulate else 0
+        e = ctypes.c_double(0.0)
+        check(load().dage_op3d_apply(self._h, rp, vp, flags, ctypes.byref(e)))
+        return (out, e.value) if energy else out
+
+    __call__ = apply
+
+
+class Coulomb3D(Operator3D):
+    """Coulomb3D (src/bubbles/coulomb.F90:109-195), cube part:
+    w_p = 2/sqrt(pi) tw_p, coda = pi/tlog^2."""
+
+
+class Helmholtz3D:
+    """Helmholtz3D (src/bubbles/helmholtz3d.F90:367-481): a Coulomb operator
+    whose weights are rescaled to 2/sqrt(pi) tw_p exp(2E/(4 t_p^2)) for the
+    duration of one application, then reset to E = 0."""
+
+    def __init__(self, coulomb_operator: Operator3D, energy: float):
+        self.coulomb_operator = coulomb_operator
+        self.energy = energy
+
+    def set_energy(self, energy: float) -> None:
+        self.energy = energy
+        check(load().dage_op3d_set_energy(self.coulomb_operator._h, float(energy)))
+
+    def apply(self, rho, out=None, energy: bool = False, coda: bool = True):
+        self.set_energy(self.energy)
+        try:
+            return self.coulomb_operator.apply(rho, out, energy=energy, coda=coda)
+        finally:
+            check(load().dage_op3d_set_energy(self.coulomb_operator._h, 0.0))
+
+    __call__ = apply
+
+
+def integrate(grid: Grid3D, f1, f2=None) -> float:
+    """Cube part of Function3D_integrate / Function3D_dot_product: the
+    LIP-weighted integral of f1 (times f2 when given)."""
+    n = int(np.prod(grid.shape))
+    p1, d1 = _ptr(f1, n)
+    p2, d2 = (ctypes.c_void_p(0), d1) if f2 is None else _ptr(f2, n)
+    if d1 != d2:
+        raise ValueError("f1 and f2 must both be host or both be device cubes")
+    out = ctypes.c_double()
+    g = grid.c()
+    check(load().dage_integrate(g, p1, p2, _capi.DAGE_DEVICE_PTRS if d1 else 0,
+                                ctypes.byref(out)))
+    return out.value
+
+
+dot = integrate

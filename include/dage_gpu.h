@@ -1,0 +1,154 @@
+/*
+ * dage_gpu.h -- C ABI of the B200-native grid-based Coulomb/Helmholtz
+ * operator path (libdagegpu.so).
+ *
+ * Conventions shared by every entry point
+ *  - Cubes are Fortran column-major cube(x, y, z), x fastest, FP64, exactly
+ *    as the reference's Function3D cubes (src/bubbles/function3d.F90:86-190).
+ *  - Pointers are host pointers unless the call takes a flags word with
+ *    DAGE_DEVICE_PTRS set, in which case they are device pointers on the
+ *    device that was current when the handle was created.
+ *  - Every function returns 0 on success and a negative DAGE_E_* code on
+ *    failure; dage_last_error() then returns a message for the calling
+ *    thread.  No function prints or exits (the reference prints and calls
+ *    exit(-1), src/bubbles/cuda_blas.cu:36-47).
+ *  - A handle owns its CUDA stream and device buffers.  Calls on distinct
+ *    handles may run concurrently from different host threads; calls on one
+ *    handle must be serialised by the caller.
+ *  - Indices are 0-based.
+ */
+#ifndef DAGE_GPU_H
+#define DAGE_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DAGE_ABI_VERSION 1
+
+/* status codes */
+#define DAGE_OK 0
+#define DAGE_E_INVALID (-1)   /* bad argument (null pointer, bad shape) */
+#define DAGE_E_CUDA (-2)      /* a CUDA runtime/driver call failed */
+#define DAGE_E_NOMEM (-3)     /* device allocation failed */
+#define DAGE_E_UNSUPPORTED (-4)
+#define DAGE_E_TIMEOUT (-5)   /* a bounded device-side wait ran out */
+
+/* flags for apply-style calls */
+#define DAGE_DEVICE_PTRS 1u   /* input/output pointers are device pointers */
+#define DAGE_ENERGY 2u        /* also return the integral of rho * V */
+#define DAGE_NO_CODA 4u       /* skip the coda term for this call */
+#define DAGE_ACCUMULATE 8u    /* V += result instead of V = result */
+
+/* operator precisions */
+#define DAGE_FP64 0            /* FP64 everywhere: the drop-in */
+#define DAGE_MIXED_BF16X3 1    /* 2-way BF16 splits, 3 products, FP32 accum */
+#define DAGE_MIXED_BF16X6 2    /* 3-way BF16 splits, 6 products, FP32 accum */
+
+/* One axis of a Grid3D: ncell LIP cells of nlip points each; the axis holds
+ * ncell*(nlip-1)+1 points (src/bubbles/grid.F90:446-534, Grid1D_init_step).
+ * grid_type 1 = equidistant points in a cell, 2 = Gauss-Lobatto points. */
+typedef struct dage_grid1d {
+  int ncell;
+  int nlip;
+  int grid_type;
+  double qmin;
+  const double *cell_scales; /* ncell host values (step length per cell) */
+} dage_grid1d;
+
+/* GaussQuad parameters (src/bubbles/gauss.F90:55-122): nlin Gauss-Legendre
+ * t-points on [tstart, tlin] and nlog log-mapped points on [tlin, tlog]. */
+typedef struct dage_quad {
+  int nlin;
+  int nlog;
+  double tstart;
+  double tlin;
+  double tlog;
+} dage_quad;
+
+typedef struct dage_op3d dage_op3d;
+
+/* ---------------------------------------------------------------------------
+ * Tensor-product cube operator (Coulomb3D / Helmholtz3D cube part)
+ * ------------------------------------------------------------------------ */
+
+/* Builds the operator on the current CUDA device: quadrature, weights
+ * w_p = 2/sqrt(pi) tw_p, coda = pi/tlog^2, and the per-axis matrices
+ * T_p(i_out, j_in), all in FP64 on the GPU.
+ * Replaces Coulomb3D_init_explicit_sub + make_Coulomb3D_matrices
+ * (src/bubbles/coulomb.F90:109-176, src/bubbles/exponentials.F90:602-639)
+ * and Operator3D_cuda_init (src/bubbles/function3d.F90:4172-4209). */
+int dage_op3d_create(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
+                     const dage_quad *quad, int precision, dage_op3d **op);
+
+/* Applies the operator to one cube: V = sum_p w_p (T^x_p (x) T^y_p (x) T^z_p)
+ * rho [+ coda * rho when the input and output grids coincide].  With
+ * DAGE_ENERGY, *energy receives the LIP-weighted integral of rho*V over the
+ * output grid (FP64).  rho and V may be host or device pointers (flags).
+ * Replaces Operator3D_operator_cube's CUDA branch and
+ * Operator3D_transform_cuda_cube (src/bubbles/function3d.F90:3795-3882,
+ * 4354-4480); the coda follows the CPU branch (function3d.F90:4327-4332). */
+int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
+                    double *energy);
+
+/* Replaces the quadrature weights (length P = nlin+nlog).
+ * Operator3D%set_transformation_weights, used by Helmholtz3D_set_energy
+ * (src/bubbles/helmholtz3d.F90:411-444). */
+int dage_op3d_set_weights(dage_op3d *op, int P, const double *w);
+
+/* Helmholtz weights w_p = 2/sqrt(pi) tw_p exp(2E/(4 t_p^2)) for E < -0.005,
+ * else the Coulomb weights (src/bubbles/helmholtz3d.F90:411-444). */
+int dage_op3d_set_energy(dage_op3d *op, double energy);
+
+/* Sets the coda coefficient (coulomb.F90:151 sets pi/tlog^2; 0 disables). */
+int dage_op3d_set_coda(dage_op3d *op, double coda);
+
+/* Uses the caller's cudaStream_t for all later work of this handle
+ * (NULL restores the handle's own stream). */
+int dage_op3d_set_stream(dage_op3d *op, void *stream);
+
+/* Number of t-points and the t-points/weights in use (host copies). */
+int dage_op3d_get_quadrature(const dage_op3d *op, int *P, double *tp, double *w);
+
+/* Copies the FP64 matrix of one axis (0=x,1=y,2=z), layout T(i_out, j_in, p)
+ * column-major, n_out*n_in*P values, to host memory. */
+int dage_op3d_get_matrix(const dage_op3d *op, int axis, double *T_host);
+
+/* Milliseconds of device time of the last apply (CUDA events). */
+int dage_op3d_last_time_ms(const dage_op3d *op, float *ms);
+
+/* Per-kernel device timing of later applies: with timing enabled, every
+ * kernel launch of an apply is bracketed by CUDA events on the handle's
+ * stream and its duration is added to a per-kind total.
+ * kind: 0 = contraction stage kernel, 1 = precision split of the input,
+ * 2 = finalize (coda + energy).  get_timing returns totals since enabling. */
+int dage_op3d_set_timing(dage_op3d *op, int enable);
+int dage_op3d_get_timing(const dage_op3d *op, int kind, long long *launches, double *ms);
+
+int dage_op3d_destroy(dage_op3d *op);
+
+/* ---------------------------------------------------------------------------
+ * Integration (Function3D_integrate / Function3D_dot_product cube part)
+ * ------------------------------------------------------------------------ */
+
+/* out = integral of f (or of f1*f2 when f2 != NULL) over the grid with LIP
+ * weights.  Replaces integrator3d_integrate / SerialInfo_integrate_cube
+ * (src/bubbles/parallel_info.F90:512-528, src/bubbles/integrator.cu:321-372)
+ * and the cube part of Function3D_dot_product (function3d.F90:1499-1523). */
+int dage_integrate(const dage_grid1d grid[3], const double *f1, const double *f2,
+                   unsigned flags, double *out);
+
+/* ---------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------ */
+const char *dage_last_error(void);
+int dage_abi_version(void);
+/* Device-side timeout (in device clock cycles) for bounded waits. */
+int dage_set_wait_limit(long long cycles);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DAGE_GPU_H */

@@ -1,0 +1,111 @@
+/*
+ * dage_oracle.h -- CPU FP64 oracle for the DAGE grid-based Coulomb/Helmholtz
+ * operator path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA
+ * product is compared against.  Only tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py may load it.  The product library
+ * (dage_b200/libdagegpu.so) never links, loads or calls it.
+ *
+ * Every routine restates, in plain C++, the algorithm of the reference
+ * Fortran file named in its comment (paths relative to the DAGE source tree).
+ * Layout conventions follow the reference: cubes are Fortran column-major
+ * cube(x, y, z) with x fastest; matrices are column-major.
+ */
+#ifndef DAGE_ORACLE_H
+#define DAGE_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Gaussian quadrature in t (src/bubbles/gauss.F90:81-122, 307-383) --- */
+/* nlin Gauss-Legendre points on [tstart, tlin] followed by nlog log-mapped
+ * points on [tlin, tlog].  tp, tw: nlin+nlog values. */
+void orc_gauss_quad(int nlin, int nlog, double tstart, double tlin, double tlog,
+                    double *tp, double *tw);
+/* plain Gauss-Legendre rule on [-1, 1] (gauss.F90:344-383) */
+void orc_gauleg(int n, double *x, double *w);
+
+/* ---- LIP basis (src/bubbles/lip.F90) ------------------------------------ */
+/* coeffs: nlip*nlip, column-major p(j,k) = coefficient of x^(nlip-k) of basis
+ * polynomial j (lip.F90:285-362).  first/last: cell extent in cell units. */
+int orc_lip_coeffs(int nlip, int grid_type, double *coeffs, double *first,
+                   double *last);
+/* integrals of each basis polynomial over [first, last] (lip.F90:392-411) */
+int orc_lip_integrals(int nlip, int grid_type, double *ints);
+
+/* ---- 1-D grids (src/bubbles/grid.F90) ----------------------------------- */
+/* Grid1D_init_step (grid.F90:446-534): points (ncell*(nlip-1)+1 values) and
+ * cell starts celld (ncell values). */
+int orc_grid1d_points(double qmin, int ncell, int nlip, int grid_type,
+                      const double *cell_scales, double *points, double *celld);
+/* Grid1D_init_spheres + Grid1D_init_equidistant (grid.F90:539-640): the
+ * default grid of a Gaussian generator along one axis.  Returns ncell. */
+int orc_grid1d_spheres(int n, const double *centers, const double *radii,
+                       double step, int nlip, double *qmin, double *cell_scale);
+/* LIP-weighted integration weights per grid point (sum over the cells that
+ * share a point; the weights the reference Integrator applies,
+ * src/bubbles/evaluators.F90:1023-1098). */
+int orc_grid1d_weights(int ncell, int nlip, int grid_type,
+                       const double *cell_scales, double *weights);
+
+/* ---- Coulomb operator matrices (src/bubbles/exponentials.F90) ----------- */
+/* integrals(a,b,t,p,n) (exponentials.F90:647-666): values[n-1-i] =
+ * int_a^b x^i exp(-t^2 (x-p)^2) dx, i = 0..n-1. */
+void orc_expo_integrals(double a, double b, double t, double p, int n,
+                        double *values);
+/* exponentials() (exponentials.F90:178-346) for one axis, no PBC images.
+ * Input grid: (qmin_in, ncell_in, nlip, grid_type, cell_scales_in).  Output
+ * points: n_out coordinates.  T: n_out x n_in x P, column-major,
+ * T(i_out, j_in, p).  The reference stores the y and z matrices transposed
+ * (trsp='t'); callers transpose as needed. */
+int orc_coulomb_matrix(double qmin_in, int ncell_in, int nlip, int grid_type,
+                       const double *cell_scales_in, int n_out,
+                       const double *out_points, int P, const double *tp,
+                       double *T);
+/* Same, but only the border rows/columns that border_exponentials()
+ * (exponentials.F90:348-600) evaluates; other entries are zero. */
+int orc_coulomb_border_matrix(double qmin_in, int ncell_in, int nlip,
+                              int grid_type, const double *cell_scales_in,
+                              int n_out, const double *out_points, int P,
+                              const double *tp, double *T);
+
+/* ---- Operator application (src/bubbles/function3d.F90:4230-4349) ------- */
+/* V = sum_p w[p] (Tx_p (x) Ty_p (x) Tz_p) rho + coda * rho.
+ * Tx: nox x nix x P  (T(i_out, j_in, p) for x)
+ * Ty: noy x niy x P, Tz: noz x niz x P  (same orientation; NOT transposed).
+ * rho: nix*niy*niz (x fastest); V: nox*noy*noz (overwritten).
+ * coda is added only when the input and output grids coincide
+ * (cube_project of identical grids is a copy); pass 0 to skip it. */
+int orc_transform_cube(int nix, int niy, int niz, int nox, int noy, int noz,
+                       int P, const double *Tx, const double *Ty,
+                       const double *Tz, const double *w, double coda,
+                       const double *rho, double *V);
+
+/* Integrator_eval (src/bubbles/evaluators.F90:1064-1098): integral of a cube
+ * with LIP weights, contracted x, then y, then z. */
+double orc_integrate_cube(int nlip, int grid_type, int ncx, const double *hx,
+                          int ncy, const double *hy, int ncz, const double *hz,
+                          const double *f);
+
+/* ---- Test densities (src/bubbles/gauss_generator.F90, analytical.F90) --- */
+/* GaussGenerator_gen_cubef (gauss_generator.F90:291-318) */
+void orc_gauss_cube(int ng, const double *q, const double *alpha,
+                    const double *centers, int nx, const double *x, int ny,
+                    const double *y, int nz, const double *z, double *cube);
+/* GaussPotGenerator_gen_cubef (gauss_generator.F90:384-429) */
+void orc_gauss_pot_cube(int ng, const double *q, const double *alpha,
+                        const double *centers, int nx, const double *x, int ny,
+                        const double *y, int nz, const double *z, double *cube);
+/* gauss_analytical_energy without PBC (analytical.F90:308-420) */
+double orc_gauss_analytical_energy(int ng, const double *q, const double *alpha,
+                                   const double *centers);
+/* extent of each Gaussian shell (gauss_generator.F90:262-281) */
+void orc_gauss_extent(int ng, const double *q, const double *alpha,
+                      double thres, double *extent);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,194 @@
+"""GPU parity tests of the FP64 cube operator (the drop-in) against the CPU
+oracle, through the C ABI.  Bar: <= 1e-10 relative (max-norm) for the
+potential, matching the reference's own known answers for the energy."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL_FP64 = 1e-10
+
+
+def _grids(dage, oracle, qmin, ncell, step, nlip=7, gt=1):
+    return (dage.Grid3D.cube(qmin, ncell, step, nlip, gt), oracle.Grid3D.cube(qmin, ncell, step, nlip, gt))
+
+
+def _relmax(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def test_quadrature_matches_oracle(dage, oracle):
+    g, _ = _grids(dage, oracle, -2.4, 4, 0.2)
+    for q in [(10, 8, 0.0, 2.0, 1e3), (32, 32, 0.0, 2.0, 1e3), (20, 16, 0.0, 2.0, 500.0), (7, 0, 0.0, 3.0, 10.0)]:
+        op = dage.Coulomb3D(g, quad=dage.GaussQuad(*q))
+        tp, w = op.quadrature()
+        tpo, two = oracle.gauss_quad(*q)
+        np.testing.assert_allclose(tp, tpo, rtol=1e-14)
+        np.testing.assert_allclose(w, oracle.coulomb_weights(two), rtol=1e-13)
+
+
+@pytest.mark.parametrize("ncell,step,nlip,gt", [(4, 0.2, 7, 1), (20, 0.2, 7, 1), (6, 0.1, 5, 1),
+                                                (5, 0.3, 7, 2), (3, 0.15, 6, 2)])
+def test_matrices_match_oracle(dage, oracle, ncell, step, nlip, gt):
+    qmin = -0.5 * ncell * (nlip - 1) * step
+    g, go = _grids(dage, oracle, qmin, ncell, step, nlip, gt)
+    quad = (16, 16, 0.0, 2.0, 1e3)
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(*quad))
+    tp, _ = oracle.gauss_quad(*quad)
+    T = op.matrix(0)
+    To = oracle.coulomb_matrix(go.axes[0], go.axes[0].points, tp)
+    for p in range(T.shape[2]):
+        assert np.abs(T[:, :, p] - To[:, :, p]).max() <= 1e-12 * np.abs(To[:, :, p]).max()
+
+
+def test_matrices_distinct_grids(dage, oracle):
+    """Input and output grids differ (the GBFMM near-field situation)."""
+    gi = dage.Grid3D.cube(-1.2, 2, 0.2)
+    go_ = dage.Grid3D((dage.Grid1D.equidistant(-2.4, 4, 0.2), dage.Grid1D.equidistant(-1.2, 2, 0.2),
+                       dage.Grid1D.equidistant(0.0, 3, 0.1)))
+    quad = (8, 8, 0.0, 2.0, 1e3)
+    op = dage.Coulomb3D(gi, go_, quad=dage.GaussQuad(*quad))
+    oi = oracle.Grid3D.cube(-1.2, 2, 0.2)
+    tp, tw = oracle.gauss_quad(*quad)
+    pts = [np.asarray(oracle.Grid1D.equidistant(-2.4, 4, 0.2).points),
+           np.asarray(oracle.Grid1D.equidistant(-1.2, 2, 0.2).points),
+           np.asarray(oracle.Grid1D.equidistant(0.0, 3, 0.1).points)]
+    Ts = [oracle.coulomb_matrix(oi.axes[d], pts[d], tp) for d in range(3)]
+    for d in range(3):
+        T = op.matrix(d)
+        assert T.shape == Ts[d].shape
+        assert np.abs(T - Ts[d]).max() <= 1e-12 * np.abs(Ts[d]).max()
+    rho = oracle.gauss_cube(oi, [1.0], [2.0], [[0.1, -0.1, 0.05]])
+    V = op.apply(np.asfortranarray(rho))
+    Vo = oracle.transform_cube(*Ts, oracle.coulomb_weights(tw), rho, 0.0)
+    assert _relmax(V, Vo) <= TOL_FP64
+
+
+@pytest.mark.parametrize("ncell,step,quad", [(4, 0.2, (6, 6, 0.0, 2.0, 1e3)),
+                                             (9, 0.2, (10, 8, 0.0, 2.0, 500.0)),
+                                             (7, 0.1, (12, 10, 0.0, 2.0, 1e3))])
+def test_apply_fp64_matches_oracle(dage, oracle, ncell, step, quad):
+    qmin = -3.0 * ncell * step
+    g, go = _grids(dage, oracle, qmin, ncell, step)
+    rng = np.random.default_rng(ncell)
+    q = rng.uniform(0.5, 2, 3)
+    a = rng.uniform(0.5, 4, 3)
+    c = rng.uniform(-1, 1, (3, 3))
+    rho = oracle.gauss_cube(go, q, a, c)
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(*quad))
+    V, E = op.apply(rho, energy=True)
+    Vo = oracle.coulomb_apply(go, rho, quad=quad)
+    assert _relmax(V, Vo) <= TOL_FP64
+    Eo = oracle.integrate_cube(go, rho * Vo)
+    assert abs(E - Eo) <= 1e-12 * abs(Eo)
+
+
+def test_committed_fixture(dage):
+    with open(os.path.join(GOLD, "oracle_small.json")) as f:
+        fx = json.load(f)
+    gd, qd = fx["grid"], fx["quadrature"]
+    g = dage.Grid3D.cube(gd["qmin"], gd["ncell"], gd["step"], gd["nlip"])
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(qd["nlin"], qd["nlog"], qd["tstart"], qd["tlin"], qd["tlog"]))
+    T = op.matrix(0)
+    np.testing.assert_allclose(T[0, :, 0], fx["T_row0_p0"], rtol=1e-12, atol=1e-13 * np.abs(T[0, :, 0]).max())
+    pts = g.axes[0].coordinates()
+    gs = fx["gauss"]
+    X, Y, Z = np.meshgrid(pts, pts, pts, indexing="ij")
+    rho = np.zeros(X.shape)
+    for q, a, c in zip(gs["q"], gs["alpha"], gs["centers"]):
+        rho += q * (a / np.pi) ** 1.5 * np.exp(-a * ((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2))
+    V, E = op.apply(np.asfortranarray(rho), energy=True)
+    for idx, val in fx["V_samples"]:
+        assert abs(V[tuple(idx)] - val) <= 1e-10 * abs(val)
+    assert abs(E - fx["energy"]) <= 1e-10 * abs(fx["energy"])
+
+
+def _kat():
+    with open(os.path.join(GOLD, "gauss_test_kat.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case", _kat()["cases"], ids=lambda c: c["name"])
+def test_gauss_test_kat_on_gpu(dage, oracle, case):
+    """The reference's own known answers, through the GPU operator."""
+    kat = _kat()
+    qd = kat["quadrature"]
+    og = oracle.Grid3D.gauss_default(case["q"], case["alpha"], case["centers"], step=case["step"],
+                                     nlip=case["nlip"], thres=case["thres"])
+    g = dage.Grid3D(tuple(dage.Grid1D(a.qmin, a.ncell, a.nlip, 1, a.cell_scales) for a in og.axes))
+    rho = oracle.gauss_cube(og, case["q"], case["alpha"], case["centers"])
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(qd["nlin"], qd["nlog"], qd["tstart"], qd["tlin"], qd["tlog"]))
+    V, E = op.apply(rho, energy=True)
+    assert abs(E - case["selfint"]) < 1e-13
+    assert abs(dage.integrate(g, rho, V) - E) < 1e-14
+
+
+def test_device_and_host_pointers_agree(dage, oracle):
+    import torch
+
+    g, go = _grids(dage, oracle, -3.6, 6, 0.2)
+    rho = oracle.gauss_cube(go, [1.0, -0.3], [1.0, 3.0], [[0, 0, 0], [0.4, 0.2, -0.3]])
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(8, 8))
+    Vh, Eh = op.apply(rho, energy=True)
+    rd = torch.from_numpy(rho.reshape(-1, order="F").copy()).cuda()
+    Vd, Ed = op.apply(rd, energy=True)
+    np.testing.assert_array_equal(Vd.cpu().numpy(), Vh.reshape(-1, order="F"))
+    assert Ed == Eh
+    # accumulate: V += op(rho)
+    V2 = op.apply(rd, out=Vd.clone(), accumulate=True)
+    ref = 2 * Vd.cpu().numpy()
+    got = V2.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+def test_helmholtz_matches_oracle(dage, oracle):
+    g, go = _grids(dage, oracle, -3.0, 5, 0.2)
+    quad = (12, 12, 0.0, 2.0, 1e3)
+    rho = oracle.gauss_cube(go, [1.0], [2.0], [[0.1, 0.2, -0.1]])
+    cop = dage.Coulomb3D(g, quad=dage.GaussQuad(*quad))
+    kappa = 1.3
+    E = -0.5 * kappa ** 2
+    hop = dage.Helmholtz3D(cop, E)
+    V = hop.apply(rho)
+    tp, tw = oracle.gauss_quad(*quad)
+    T = oracle.coulomb_matrix(go.axes[0], go.axes[0].points, tp)
+    Vo = oracle.transform_cube(T, T, T, oracle.helmholtz_weights(tp, tw, E), rho, oracle.coda_of(1e3))
+    assert _relmax(V, Vo) <= TOL_FP64
+    # the energy is reset to 0 afterwards (helmholtz3d.F90:479)
+    np.testing.assert_allclose(cop.weights, oracle.coulomb_weights(tw), rtol=1e-15)
+
+
+def test_config1_121_cube(dage, oracle):
+    """121^3, 2 seeded Gaussians, 40 t-points on [0, 1e3]: FP64 GPU vs oracle
+    (<= 1e-10) and vs the analytic potential."""
+    g, go = _grids(dage, oracle, -12.0, 20, 0.2)
+    rng = np.random.default_rng(1)
+    q = rng.uniform(0.5, 2, 2)
+    a = rng.uniform(0.5, 4, 2)
+    c = rng.uniform(-3, 3, (2, 3))
+    rho = oracle.gauss_cube(go, q, a, c)
+    quad = (20, 20, 0.0, 2.0, 1e3)
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(*quad))
+    V, E = op.apply(rho, energy=True)
+    Vo = oracle.coulomb_apply(go, rho, quad=quad)
+    assert _relmax(V, Vo) <= TOL_FP64
+    Va = oracle.gauss_pot_cube(go, q, a, c)
+    assert _relmax(V, Va) < 1e-3  # discretisation + quadrature error, reported not pinned
+
+
+def test_invalid_arguments_raise(dage):
+    g = dage.Grid3D.cube(-1.2, 2, 0.2)
+    with pytest.raises(ValueError):
+        dage.Coulomb3D(g, precision="fp8")
+    with pytest.raises(dage.DageError):
+        dage.Coulomb3D(g, quad=dage.GaussQuad(0, 0))
+    with pytest.raises(dage.DageError):
+        dage.Coulomb3D(dage.Grid3D.cube(-1.2, 2, 0.2, nlip=9))
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(4, 4))
+    with pytest.raises(dage.DageError):
+        op.set_transformation_weights(np.ones(3))
+    with pytest.raises(ValueError):
+        op.apply(np.zeros((3, 3, 3), order="F"))
