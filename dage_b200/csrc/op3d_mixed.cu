@@ -1,12 +1,712 @@
-// op3d_mixed.cu -- split-precision tensor-core path (placeholder until the
-// tcgen05 kernel lands): every entry point reports the path as unsupported.
+// op3d_mixed.cu -- split-precision tensor-core path of the cube operator.
+//
+// Each "contract the fastest index and rotate" stage (see op3d.cu)
+//     D(R, n) = sum_K X(K, R) T(n, K)
+// runs on the 5th-generation tensor cores (tcgen05.mma kind::f16, BF16 in,
+// FP32 accumulate in TMEM).  FP64 operands are represented as sums of BF16
+// parts: X = X0 + X1 [+ X2], T_p(n, :) / s_n = T0 + T1 [+ T2] with s_n the
+// row maximum of |T_p(n, :)| (the matrix entries span many decades as t
+// grows).  "bf16x3" uses two parts and the three products (0,0) (0,1) (1,0);
+// "bf16x6" uses three parts and the six products with part-index sum <= 2.
+// The epilogue rescales by s_n and writes the next stage's input already
+// split into BF16 parts; the last stage multiplies by w_p s_n and
+// accumulates V in FP64.  The sum over t-points is FP64.
+//
+// Kernel structure (one persistent CTA per SM, 6 warps):
+//   warp 0      TMA producer: X and T tiles -> shared-memory ring (SW128)
+//   warp 1      TMEM allocator + single-thread MMA issuer
+//   warps 2-5   epilogue: tcgen05.ld -> scale -> split -> global stores
+// Two TMEM accumulators let the epilogue of tile i overlap the MMAs of tile
+// i+1.  Every mbarrier wait is bounded (clock64 budget); on timeout the CTA
+// records DAGE_E_TIMEOUT in a device flag, drains its in-flight copies and
+// MMAs, frees TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+
 #include "op3d.cuh"
 
 namespace dage {
-int mixed_setup(dage_op3d *) { return fail(DAGE_E_UNSUPPORTED, "mixed precision not built"); }
-int mixed_apply(dage_op3d *, const double *, double *, cudaStream_t) {
-  return fail(DAGE_E_UNSUPPORTED, "mixed precision not built");
+
+extern long long g_wait_limit;
+
+namespace {
+
+constexpr int BM = 128;           // tile rows (TMEM lanes)
+constexpr int kThreads = 192;     // 6 warps
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of parity `parity` to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > limit) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// 32 lanes x 16 consecutive 32-bit columns; the wait takes the registers as
+// operands so no use of them can be scheduled before the load completes.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile written by TMA with a
+// 128-byte (BK = 64) or 64-byte (BK = 32) swizzle: rows of BK bf16, 8-row
+// swizzle atoms stacked at SBO = 8 * row bytes.
+template <int BK>
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  constexpr uint32_t row_bytes = BK * 2;
+  constexpr uint64_t layout = (BK == 64) ? 2 : 4;  // SWIZZLE_128B : SWIZZLE_64B
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;                         // LBO (unused for swizzled K-major)
+  d |= (uint64_t)((8 * row_bytes) >> 4) << 32;    // SBO
+  d |= (uint64_t)1 << 46;                         // descriptor version
+  d |= layout << 61;
+  return d;
+}
+
+// kind::f16 instruction descriptor: BF16 A and B, FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// ---------------------------------------------------------------------------
+// Split helpers
+// ---------------------------------------------------------------------------
+template <int NS>
+__device__ __forceinline__ void split_f32(float v, __nv_bfloat16 (&o)[NS]) {
+  float r = v;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    o[s] = __float2bfloat16_rn(r);
+    r = r - __bfloat162float(o[s]);
+  }
+}
+template <int NS>
+__device__ __forceinline__ void split_f64(double v, __nv_bfloat16 (&o)[NS]) {
+  double r = v;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    o[s] = __double2bfloat16(r);
+    r = r - (double)__bfloat162float(o[s]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage kernel
+// ---------------------------------------------------------------------------
+struct StageArgs {
+  int M, N, K;           // D is M x N, contraction length K
+  int n_ntiles, ntiles;  // tiles: m-tile major, n-tile minor
+  int nkb, last_k16;     // K blocks; MMAs of K=16 in the last block
+  int brow0;             // first row of this t-point in the T-part maps
+  const float *scale;    // s_n of this t-point (intermediate stages)
+  const double *scale64; // s_n of this t-point (final stage)
+  double wcoef;          // w_p (final stage)
+  // intermediate output: part s of element (R, n) at
+  //   out[s][(R / d0 + d1 * n) * ldn + R % d0]
+  __nv_bfloat16 *out0, *out1, *out2;
+  int d0, d1;
+  long long ldn;
+  // final output V[R + M * n] (FP64)
+  double *V;
+  int accumulate;
+  int *err;
+  long long wait_limit;
+};
+
+template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
+struct StageCfg {
+  static constexpr int kAParts = NSX;
+  static constexpr int kBParts = NSX;  // the same number of parts for T
+  static constexpr int kRowBytes = BK * 2;
+  static constexpr int kABytes = BM * kRowBytes;       // one part of the A tile
+  static constexpr int kBBytes = BN * kRowBytes;       // one part of the B tile
+  static constexpr int kStageBytes = NSX * kABytes + NSX * kBBytes;
+  static constexpr int kTmemCols = 2 * BN;             // two accumulators
+  static constexpr int kSmem = NS * kStageBytes + 1024 + 256;
+};
+
+// products (a-part, b-part), smallest terms first
+__device__ __forceinline__ void product(int nprod, int i, int &a, int &b) {
+  if (nprod == 3) {
+    const int pa[3] = {1, 0, 0}, pb[3] = {0, 1, 0};
+    a = pa[i];
+    b = pb[i];
+  } else {
+    const int pa[6] = {2, 1, 0, 1, 0, 0}, pb[6] = {0, 1, 2, 0, 1, 0};
+    a = pa[i];
+    b = pb[i];
+  }
+}
+
+template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
+__global__ void __launch_bounds__(kThreads, 1)
+    stage_bf16_kernel(const __grid_constant__ CUtensorMap mapA0,
+                      const __grid_constant__ CUtensorMap mapA1,
+                      const __grid_constant__ CUtensorMap mapA2,
+                      const __grid_constant__ CUtensorMap mapB0,
+                      const __grid_constant__ CUtensorMap mapB1,
+                      const __grid_constant__ CUtensorMap mapB2, const StageArgs a) {
+  using C = StageCfg<NSX, NPROD, BN, BK, NS, FINAL>;
+  // an earlier launch of this apply timed out: do nothing
+  if (*reinterpret_cast<volatile int *>(a.err)) return;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t *tiles = smem;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + NS * C::kStageBytes);
+  // bars: full[NS], empty[NS], tfull[2], tempty[2], drain[1]
+  uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * NS + 5);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto full = [&](int s) { return smem_u32(bars + s); };
+  auto empty = [&](int s) { return smem_u32(bars + NS + s); };
+  auto tfull = [&](int i) { return smem_u32(bars + 2 * NS + i); };
+  auto tempty = [&](int i) { return smem_u32(bars + 2 * NS + 2 + i); };
+  const uint32_t drain = smem_u32(bars + 2 * NS + 4);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(empty(s), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(tfull(i), 1);
+      mbar_init(tempty(i), 128);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(tmem_holder), C::kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  auto on_timeout = [&]() {
+    *abort_flag = 1;
+    atomicCAS(a.err, 0, 1);
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      const CUtensorMap *mA[3] = {&mapA0, &mapA1, &mapA2};
+      const CUtensorMap *mB[3] = {&mapB0, &mapB1, &mapB2};
+      int s = 0;
+      uint32_t ph = 0;
+      int issued[NS];
+      uint32_t issued_ph[NS];
+      for (int i = 0; i < NS; ++i) issued[i] = 0, issued_ph[i] = 0;
+      for (int tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x) {
+        const int m0 = (tile / a.n_ntiles) * BM, n0 = (tile % a.n_ntiles) * BN;
+        for (int kb = 0; kb < a.nkb; ++kb) {
+          if (!mbar_wait(empty(s), ph ^ 1, a.wait_limit)) {
+            on_timeout();
+            break;
+          }
+          uint8_t *st = tiles + s * C::kStageBytes;
+          mbar_expect_tx(full(s), C::kStageBytes);
+#pragma unroll
+          for (int i = 0; i < NSX; ++i)
+            tma_load_2d(smem_u32(st + i * C::kABytes), mA[i], full(s), kb * BK, m0);
+#pragma unroll
+          for (int j = 0; j < NSX; ++j)
+            tma_load_2d(smem_u32(st + NSX * C::kABytes + j * C::kBBytes), mB[j], full(s),
+                        kb * BK, a.brow0 + n0);
+          issued[s] = 1;
+          issued_ph[s] = ph;
+          if (++s == NS) s = 0, ph ^= 1;
+        }
+      }
+      if (*abort_flag) {
+        // let every copy that was issued land before the CTA goes away
+        for (int i = 0; i < NS; ++i)
+          if (issued[i]) mbar_wait(full(i), issued_ph[i], a.wait_limit);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int t = 0;
+      for (int tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x, ++t) {
+        const int n0 = (tile % a.n_ntiles) * BN;
+        int nt = a.N - n0;
+        if (nt > BN) nt = BN;
+        nt = (nt + 15) & ~15;
+        const uint32_t idesc = idesc_bf16(BM, nt);
+        const int acc = t & 1;
+        if (!mbar_wait(tempty(acc), ((t >> 1) & 1) ^ 1, a.wait_limit)) {
+          on_timeout();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + acc * BN;
+        bool ok = true;
+        for (int kb = 0; kb < a.nkb; ++kb) {
+          if (!mbar_wait(full(s), ph, a.wait_limit)) {
+            on_timeout();
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = smem_u32(tiles + s * C::kStageBytes);
+          const int nk16 = (kb == a.nkb - 1) ? a.last_k16 : BK / 16;
+          for (int k = 0; k < nk16; ++k) {
+#pragma unroll
+            for (int pr = 0; pr < NPROD; ++pr) {
+              int ia, ib;
+              product(NPROD, pr, ia, ib);
+              const uint64_t ad = sdesc<BK>(st + ia * C::kABytes + k * 32);
+              const uint64_t bd = sdesc<BK>(st + NSX * C::kABytes + ib * C::kBBytes + k * 32);
+              umma_bf16(d, ad, bd, idesc, (kb | k | pr) != 0);
+            }
+          }
+          umma_commit(empty(s));
+          if (++s == NS) s = 0, ph ^= 1;
+        }
+        if (!ok) break;
+        umma_commit(tfull(acc));
+      }
+      // every MMA this thread issued has completed once `drain` fires
+      umma_commit(drain);
+      mbar_wait(drain, 0, a.wait_limit);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    int t = 0;
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++t) {
+      const int acc = t & 1;
+      const bool got = mbar_wait(tfull(acc), (t >> 1) & 1, a.wait_limit);
+      __syncwarp();
+      if (!got) {
+        on_timeout();
+        break;
+      }
+      tc_fence_after();
+      const int m0 = (tile / a.n_ntiles) * BM, n0 = (tile % a.n_ntiles) * BN;
+      const int R = m0 + 32 * q + lane;
+      const bool row_ok = R < a.M;
+      int nvalid = a.N - n0;
+      if (nvalid > BN) nvalid = BN;
+      const int nchunks = (nvalid + 15) >> 4;
+      long long r0 = 0, r1 = 0;
+      if (!FINAL) {
+        r0 = R % a.d0;
+        r1 = R / a.d0;
+      }
+      for (int c = 0; c < nchunks; ++c) {
+        uint32_t r[16];
+        __syncwarp();  // tcgen05.ld is warp-collective
+        tmem_ld16(tmem_base + ((uint32_t)(32 * q) << 16) + acc * BN + c * 16, r);
+        if (row_ok) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = n0 + c * 16 + j;
+          if (n >= a.N) break;
+          const float v = __uint_as_float(r[j]);
+          if (FINAL) {
+            double *dst = a.V + (size_t)R + (size_t)a.M * n;
+            const double add = a.wcoef * a.scale64[n] * (double)v;
+            *dst = a.accumulate ? *dst + add : add;
+          } else {
+            __nv_bfloat16 parts[NSX];
+            split_f32<NSX>(v * a.scale[n], parts);
+            const size_t off = (size_t)(r1 + (long long)a.d1 * n) * a.ldn + r0;
+            a.out0[off] = parts[0];
+            a.out1[off] = parts[1];
+            if (NSX > 2) a.out2[off] = parts[NSX > 2 ? 2 : 0];
+          }
+        }
+        }
+      }
+      __syncwarp();
+      tc_fence_before();
+      mbar_arrive(tempty(acc));
+    }
+  }
+
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, C::kTmemCols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Input and matrix preparation
+// ---------------------------------------------------------------------------
+// rho (FP64, x fastest) -> NSX BF16 parts, rows of ld elements.
+template <int NSX>
+__global__ void split_input_kernel(const double *__restrict__ rho, int K, long long rows,
+                                   long long ld, __nv_bfloat16 *o0, __nv_bfloat16 *o1,
+                                   __nv_bfloat16 *o2) {
+  const long long n = (long long)K * rows;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long r = i / K, k = i % K;
+    __nv_bfloat16 p[NSX];
+    split_f64<NSX>(rho[i], p);
+    const size_t off = (size_t)r * ld + k;
+    o0[off] = p[0];
+    o1[off] = p[1];
+    if (NSX > 2) o2[off] = p[NSX > 2 ? 2 : 0];
+  }
+}
+
+// One block per matrix row (p, n): s = max_K |T|, parts of T/s.
+template <int NSX>
+__global__ void split_matrix_kernel(const double *__restrict__ T, int K, long long ld,
+                                    float *scale, double *scale64, __nv_bfloat16 *o0,
+                                    __nv_bfloat16 *o1, __nv_bfloat16 *o2) {
+  const long long row = blockIdx.x;
+  const double *src = T + row * K;
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) m = fmax(m, fabs(src[k]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) red[0] = m;
+  }
+  __syncthreads();
+  // power-of-two scale: the division is exact
+  double s = red[0] > 0.0 ? exp2(ceil(log2(red[0]))) : 1.0;
+  if (threadIdx.x == 0) {
+    scale[row] = (float)s;
+    scale64[row] = s;
+  }
+  for (int k = threadIdx.x; k < (int)ld; k += blockDim.x) {
+    __nv_bfloat16 p[NSX];
+    split_f64<NSX>(k < K ? src[k] / s : 0.0, p);
+    const size_t off = (size_t)row * ld + k;
+    o0[off] = p[0];
+    o1[off] = p[1];
+    if (NSX > 2) o2[off] = p[NSX > 2 ? 2 : 0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 2-D BF16 map: inner extent `inner` (contiguous), `rows` rows of `ld`
+// elements; box = box_inner x box_rows with the swizzle matching BK.
+int make_map(CUtensorMap *m, const void *base, long long inner, long long rows, long long ld,
+             int box_inner, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return fail(DAGE_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if (reinterpret_cast<uintptr_t>(base) % 16 || (ld * 2) % 16)
+    return fail(DAGE_E_INVALID, "tensor map base/stride not 16-byte aligned");
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+  cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapSwizzle sw =
+      box_inner == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(DAGE_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return 0;
+}
+
+struct MixedState {
+  int nparts = 2;   // BF16 parts per operand
+  int nprod = 3;
+  int bn = 256, bk = 64;
+  long long ld[3];  // padded K extent of each stage's input rows
+  long long rows[3];
+  DevBuf X[3];      // stage inputs: nparts planes of rows x ld BF16
+  DevBuf Tp[3];     // per-axis matrix parts: nparts planes of P*n_out x ld
+  DevBuf sc[3], sc64[3];
+  int towner[3];
+  CUtensorMap mapA[3][3], mapB[3][3];
+  DevBuf err;
+};
+
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+__nv_bfloat16 *plane(DevBuf &b, int part, long long plane_elems) {
+  return b.as<__nv_bfloat16>() + (size_t)part * plane_elems;
+}
+
+template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
+int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, const StageArgs &base,
+                 cudaStream_t s) {
+  using C = StageCfg<NSX, NPROD, BN, BK, NS, FINAL>;
+  auto kern = stage_bf16_kernel<NSX, NPROD, BN, BK, NS, FINAL>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    DAGE_CUDA_TRY(
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
+    attr_set = true;
+  }
+  StageArgs a = base;
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  a.n_ntiles = ceil_div(N, BN);
+  a.ntiles = ceil_div(M, BM) * a.n_ntiles;
+  a.nkb = ceil_div(K, BK);
+  a.last_k16 = ceil_div(K - (a.nkb - 1) * BK, 16);
+  a.brow0 = p * N;
+  const int ax = stage;
+  const int grid = std::min(a.ntiles, sm_count());
+  const CUtensorMap *mA = st.mapA[stage];
+  const CUtensorMap *mB = st.mapB[st.towner[ax]];
+  kern<<<grid, kThreads, C::kSmem, s>>>(mA[0], mA[1], mA[NSX > 2 ? 2 : 1], mB[0], mB[1],
+                                        mB[NSX > 2 ? 2 : 1], a);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+template <int NSX, int NPROD, int BN, int BK, int NS>
+int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, cudaStream_t s) {
+  const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
+  const int nox = op->nout[0], noy = op->nout[1], noz = op->nout[2];
+  const long long pe[3] = {st.rows[0] * st.ld[0], st.rows[1] * st.ld[1], st.rows[2] * st.ld[2]};
+  // input split
+  {
+    const int t = op->tmark_begin(1);
+    const long long n = (long long)nix * st.rows[0];
+    const int blocks = (int)std::min<long long>((n + 255) / 256, sm_count() * 8LL);
+    split_input_kernel<NSX><<<blocks, 256, 0, s>>>(
+        d_rho, nix, st.rows[0], st.ld[0], plane(st.X[0], 0, pe[0]), plane(st.X[0], 1, pe[0]),
+        plane(st.X[0], NSX > 2 ? 2 : 1, pe[0]));
+    DAGE_CUDA_TRY(cudaGetLastError());
+    op->tmark_end(t);
+  }
+  StageArgs base{};
+  base.err = st.err.as<int>();
+  base.wait_limit = g_wait_limit;
+  const int ni[3] = {nix, niy, niz}, no[3] = {nox, noy, noz};
+  const long long M[3] = {(long long)niy * niz, (long long)niz * nox, (long long)nox * noy};
+  const int d0[3] = {niy, niz, 0}, d1[3] = {niz, nox, 0};
+  for (int p = 0; p < op->P; ++p) {
+    for (int stage = 0; stage < 3; ++stage) {
+      StageArgs a = base;
+      const int ow = st.towner[stage];
+      a.scale = st.sc[ow].as<float>() + (size_t)p * no[stage];
+      a.scale64 = st.sc64[ow].as<double>() + (size_t)p * no[stage];
+      const int t = op->tmark_begin(0);
+      if (stage < 2) {
+        a.out0 = plane(st.X[stage + 1], 0, pe[stage + 1]);
+        a.out1 = plane(st.X[stage + 1], 1, pe[stage + 1]);
+        a.out2 = plane(st.X[stage + 1], NSX > 2 ? 2 : 1, pe[stage + 1]);
+        a.d0 = d0[stage];
+        a.d1 = d1[stage];
+        a.ldn = st.ld[stage + 1];
+        DAGE_TRY((launch_stage<NSX, NPROD, BN, BK, NS, false>(st, stage, (int)M[stage],
+                                                               no[stage], ni[stage], p, a, s)));
+      } else {
+        a.V = d_V;
+        a.wcoef = op->w[p];
+        a.accumulate = p > 0;
+        DAGE_TRY((launch_stage<NSX, NPROD, BN, BK, NS, true>(st, stage, (int)M[stage], no[stage],
+                                                              ni[stage], p, a, s)));
+      }
+      op->tmark_end(t);
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+int mixed_setup(dage_op3d *op) {
+  auto *st = new MixedState();
+  op->mixed = st;
+  if (op->precision == DAGE_MIXED_BF16X3) {
+    st->nparts = 2;
+    st->nprod = 3;
+    st->bn = 256;
+  } else {
+    st->nparts = 3;
+    st->nprod = 6;
+    st->bn = 128;
+  }
+  st->bk = 64;
+  const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
+  const int nox = op->nout[0], noy = op->nout[1];
+  const int ni[3] = {nix, niy, niz};
+  st->rows[0] = (long long)niy * niz;
+  st->rows[1] = (long long)niz * nox;
+  st->rows[2] = (long long)nox * noy;
+  for (int s = 0; s < 3; ++s) {
+    st->ld[s] = round_up(ni[s], 8);
+    const long long pe = st->rows[s] * st->ld[s];
+    DAGE_TRY(st->X[s].alloc(sizeof(__nv_bfloat16) * pe * st->nparts));
+    DAGE_CUDA_TRY(cudaMemsetAsync(st->X[s].ptr, 0, st->X[s].bytes, op->stream));
+    for (int i = 0; i < st->nparts; ++i)
+      DAGE_TRY(make_map(&st->mapA[s][i], plane(st->X[s], i, pe), ni[s], st->rows[s], st->ld[s],
+                        st->bk, BM));
+  }
+  DAGE_TRY(st->err.alloc(sizeof(int)));
+  DAGE_CUDA_TRY(cudaMemsetAsync(st->err.ptr, 0, sizeof(int), op->stream));
+  for (int ax = 0; ax < 3; ++ax) {
+    st->towner[ax] = op->Towner[ax];
+    if (op->Towner[ax] != ax) continue;
+    const int K = op->nin[ax], N = op->nout[ax];
+    const long long ld = round_up(K, 8);
+    const long long nrows = (long long)op->P * N;
+    const long long pe = nrows * ld;
+    DAGE_TRY(st->Tp[ax].alloc(sizeof(__nv_bfloat16) * pe * st->nparts));
+    DAGE_TRY(st->sc[ax].alloc(sizeof(float) * nrows));
+    DAGE_TRY(st->sc64[ax].alloc(sizeof(double) * nrows));
+    __nv_bfloat16 *o0 = plane(st->Tp[ax], 0, pe), *o1 = plane(st->Tp[ax], 1, pe),
+                  *o2 = plane(st->Tp[ax], st->nparts > 2 ? 2 : 1, pe);
+    if (st->nparts == 2)
+      split_matrix_kernel<2><<<(unsigned)nrows, 256, 0, op->stream>>>(
+          op->T(ax), K, ld, st->sc[ax].as<float>(), st->sc64[ax].as<double>(), o0, o1, o2);
+    else
+      split_matrix_kernel<3><<<(unsigned)nrows, 256, 0, op->stream>>>(
+          op->T(ax), K, ld, st->sc[ax].as<float>(), st->sc64[ax].as<double>(), o0, o1, o2);
+    DAGE_CUDA_TRY(cudaGetLastError());
+    for (int i = 0; i < st->nparts; ++i)
+      DAGE_TRY(make_map(&st->mapB[ax][i], plane(st->Tp[ax], i, pe), K, nrows, ld, st->bk,
+                        st->bn));
+  }
+  // the A maps of stage s must describe the stage's input extent; ld must
+  // match the padded extent the previous stage writes
+  return 0;
+}
+
 int mixed_set_weights(dage_op3d *) { return 0; }
-void mixed_destroy(dage_op3d *) {}
+
+int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
+  auto *st = static_cast<MixedState *>(op->mixed);
+  if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
+  int rc;
+  if (st->nparts == 2)
+    rc = run_stages<2, 3, 256, 64, 2>(op, *st, d_rho, d_V, s);
+  else
+    rc = run_stages<3, 6, 128, 64, 2>(op, *st, d_rho, d_V, s);
+  if (rc) return rc;
+  int herr = 0;
+  DAGE_CUDA_TRY(cudaMemcpyAsync(&herr, st->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  if (herr) {
+    cudaMemsetAsync(st->err.ptr, 0, sizeof(int), s);
+    return fail(DAGE_E_TIMEOUT, "tensor-core stage kernel timed out waiting on an mbarrier");
+  }
+  return 0;
+}
+
+void mixed_destroy(dage_op3d *op) {
+  auto *st = static_cast<MixedState *>(op->mixed);
+  if (!st) return;
+  for (int i = 0; i < 3; ++i) {
+    st->X[i].release();
+    st->Tp[i].release();
+    st->sc[i].release();
+    st->sc64[i].release();
+  }
+  st->err.release();
+  delete st;
+  op->mixed = nullptr;
+}
+
 }  // namespace dage

@@ -105,6 +105,27 @@ double orc_gauss_analytical_energy(int ng, const double *q, const double *alpha,
 void orc_gauss_extent(int ng, const double *q, const double *alpha,
                       double thres, double *extent);
 
+/* ---- GBFMM pieces (src/bubbles/multipole.F90, harmonics.F90,
+ *      src/gbfmm/gbfmm_parallel_info.F90) ---------------------------------- */
+/* Racah-normalised real regular solid harmonics S_lm, lm = l(l+1)+m. */
+void orc_solid_harmonics(int lmax, double x, double y, double z, double *S);
+/* M2L interaction matrix T(d), N x N column-major, N = (lmax+1)^2. */
+int orc_interaction_matrix(int lmax, const double *d, double *T);
+/* M2M/L2L translation matrix, packed lower triangle (N(N+1)/2). */
+int orc_translation_matrix(int lmax, const double *d, double *W);
+void orc_dtpmv_lower_unit(int n, const double *A, double *x);
+/* octree boxes (1-based indices; 2^level boxes per axis) */
+void orc_box_vector(int ibox, int level, int *v);
+int orc_box_index(const int *v, int level);
+int orc_nearest_neighbors(int ibox, int level, int *out);
+int orc_local_farfield(int ibox, int level, int *out);
+/* multipole moments of one box and local-expansion evaluation */
+int orc_box_multipoles(int lmax, int nx, const double *px, const double *wx, int ny,
+                       const double *py, const double *wy, int nz, const double *pz,
+                       const double *wz, const double *cube, const double *center, double *q);
+int orc_l2p(int lmax, const double *L, const double *center, int nx, const double *px, int ny,
+            const double *py, int nz, const double *pz, double *out);
+
 #ifdef __cplusplus
 }
 #endif

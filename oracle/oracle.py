@@ -20,7 +20,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libdage_oracle.so")
-_lib = None
+_LIB_1ULP_PATH = os.path.join(_HERE, "_build", "libdage_oracle_1ulp.so")
+_libs = {}
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.c_int
@@ -29,16 +30,18 @@ _F = ctypes.c_double
 
 def build(force: bool = False) -> str:
     """Compile the oracle with ``make -C oracle``; returns the library path."""
-    if force or not os.path.exists(_LIB_PATH):
+    if force or not (os.path.exists(_LIB_PATH) and os.path.exists(_LIB_1ULP_PATH)):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
+def lib(libm_1ulp: bool = False):
+    """The oracle library; ``libm_1ulp`` selects the build whose erf/exp
+    results are moved by +-1 ulp (see operator_ref.cpp)."""
+    path = _LIB_1ULP_PATH if libm_1ulp else _LIB_PATH
+    if path not in _libs:
         build()
-        L = ctypes.CDLL(_LIB_PATH)
+        L = ctypes.CDLL(path)
         sig = {
             "orc_gauss_quad": (None, [_I, _I, _F, _F, _F, _D, _D]),
             "orc_gauleg": (None, [_I, _D, _D]),
@@ -56,13 +59,23 @@ def lib():
             "orc_gauss_pot_cube": (None, [_I, _D, _D, _D, _I, _D, _I, _D, _I, _D, _D]),
             "orc_gauss_analytical_energy": (_F, [_I, _D, _D, _D]),
             "orc_gauss_extent": (None, [_I, _D, _D, _F, _D]),
+            "orc_solid_harmonics": (None, [_I, _F, _F, _F, _D]),
+            "orc_interaction_matrix": (_I, [_I, _D, _D]),
+            "orc_translation_matrix": (_I, [_I, _D, _D]),
+            "orc_dtpmv_lower_unit": (None, [_I, _D, _D]),
+            "orc_box_vector": (None, [_I, _I, ctypes.POINTER(_I)]),
+            "orc_box_index": (_I, [ctypes.POINTER(_I), _I]),
+            "orc_nearest_neighbors": (_I, [_I, _I, ctypes.POINTER(_I)]),
+            "orc_local_farfield": (_I, [_I, _I, ctypes.POINTER(_I)]),
+            "orc_box_multipoles": (_I, [_I, _I, _D, _D, _I, _D, _D, _I, _D, _D, _D, _D, _D]),
+            "orc_l2p": (_I, [_I, _D, _D, _I, _D, _I, _D, _I, _D, _D]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _p(a: np.ndarray):
@@ -179,12 +192,14 @@ def expo_integrals(a, b, t, p, n=7):
     return v
 
 
-def coulomb_matrix(grid_in: Grid1D, out_points, tp, border_only=False) -> np.ndarray:
+def coulomb_matrix(grid_in: Grid1D, out_points, tp, border_only=False,
+                   libm_1ulp=False) -> np.ndarray:
     """T(i_out, j_in, p) for one axis (exponentials.F90:178-346)."""
     out = _f64(out_points)
     tp = _f64(tp)
     T = np.zeros((len(out), grid_in.n, len(tp)), order="F")
-    fn = lib().orc_coulomb_border_matrix if border_only else lib().orc_coulomb_matrix
+    L = lib(libm_1ulp)
+    fn = L.orc_coulomb_border_matrix if border_only else L.orc_coulomb_matrix
     rc = fn(grid_in.qmin, grid_in.ncell, grid_in.nlip, grid_in.grid_type,
             _p(grid_in.cell_scales), len(out), _p(out), len(tp), _p(tp), _p(T))
     if rc:
@@ -305,17 +320,19 @@ def gauss_analytical_energy(q, alpha, centers) -> float:
 # ---------------------------------------------------------------------------
 # Whole-operator helpers
 # ---------------------------------------------------------------------------
-def coulomb_operator_matrices(grid_in: Grid3D, grid_out: Grid3D, tp):
+def coulomb_operator_matrices(grid_in: Grid3D, grid_out: Grid3D, tp, libm_1ulp=False):
     """make_Coulomb3D_matrices (exponentials.F90:602-639), all three axes in
     the T(i_out, j_in, p) orientation."""
-    return tuple(coulomb_matrix(grid_in.axes[d], grid_out.axes[d].points, tp) for d in range(3))
+    return tuple(coulomb_matrix(grid_in.axes[d], grid_out.axes[d].points, tp,
+                                libm_1ulp=libm_1ulp) for d in range(3))
 
 
-def coulomb_apply(grid: Grid3D, rho, quad=(10, 8, 0.0, 2.0, 1.0e3), coda=True, weights=None):
+def coulomb_apply(grid: Grid3D, rho, quad=(10, 8, 0.0, 2.0, 1.0e3), coda=True, weights=None,
+                  libm_1ulp=False):
     """V = Coulomb3D(grid) .apply. rho (cube part), CPU semantics."""
     nlin, nlog, tstart, tlin, tlog = quad
     tp, tw = gauss_quad(nlin, nlog, tstart, tlin, tlog)
-    Tx, Ty, Tz = coulomb_operator_matrices(grid, grid, tp)
+    Tx, Ty, Tz = coulomb_operator_matrices(grid, grid, tp, libm_1ulp)
     w = coulomb_weights(tw) if weights is None else weights
     return transform_cube(Tx, Ty, Tz, w, rho, coda_of(tlog) if coda else 0.0)
 
@@ -324,3 +341,201 @@ def selfint(grid: Grid3D, rho, quad=(10, 8, 0.0, 2.0, 1.0e3), coda=True) -> floa
     """rho .dot. (Coulomb3D .apply. rho) as tests/gauss_test.F90 computes it."""
     V = coulomb_apply(grid, rho, quad, coda)
     return integrate_cube(grid, rho * V)
+
+
+def matrix_noise_envelope(T: np.ndarray, T1: np.ndarray, band: int = 6) -> np.ndarray:
+    """Per-entry tolerance for comparing operator matrices from two FP64
+    implementations: for each t-point slice and each band of |i - j|
+    (``band`` points wide) the largest |T - T1| inside the band, where T1
+    comes from the +-1 ulp oracle.  The reference's closed-form integrals
+    (exponentials.F90:695-1297) cancel heavily for t*h just above 0.1, so
+    their last bits -- and the matrices -- move by this much with the libm."""
+    no, ni, P = T.shape
+    I, J = np.meshgrid(np.arange(no), np.arange(ni), indexing="ij")
+    bands = np.abs(I - J) // band
+    env = np.zeros_like(T)
+    d = np.abs(T - T1)
+    for p in range(P):
+        dp = d[:, :, p]
+        mx = np.zeros(bands.max() + 1)
+        np.maximum.at(mx, bands.ravel(), dp.ravel())
+        # noise grows with distance: take the running max over nearer bands too
+        env[:, :, p] = np.maximum.accumulate(mx)[bands]
+    return env
+
+
+# ---------------------------------------------------------------------------
+# GBFMM pieces
+# ---------------------------------------------------------------------------
+def solid_harmonics(lmax, xyz) -> np.ndarray:
+    """Racah-normalised real regular solid harmonics, lm = l(l+1)+m."""
+    out = np.zeros((lmax + 1) ** 2)
+    lib().orc_solid_harmonics(lmax, float(xyz[0]), float(xyz[1]), float(xyz[2]), _p(out))
+    return out
+
+
+def interaction_matrix(lmax, d) -> np.ndarray:
+    """M2L matrix T(d) (multipole.F90:81-303): L_i += T(c_j - c_i) q_j."""
+    N = (lmax + 1) ** 2
+    T = np.zeros((N, N), order="F")
+    if lib().orc_interaction_matrix(lmax, _p(_f64(d)), _p(T)):
+        raise ValueError("interaction matrix undefined at d = 0")
+    return T
+
+
+def translation_matrix(lmax, d) -> np.ndarray:
+    """M2M/L2L matrix (multipole.F90:344-515), packed lower triangle."""
+    N = (lmax + 1) ** 2
+    W = np.zeros(N * (N + 1) // 2)
+    lib().orc_translation_matrix(lmax, _p(_f64(d)), _p(W))
+    return W
+
+
+def translate(lmax, q, frm, to) -> np.ndarray:
+    """TranslationMatrix_apply: q expanded about `frm` -> about `to`."""
+    W = translation_matrix(lmax, np.asarray(frm, float) - np.asarray(to, float))
+    x = _f64(q).copy()
+    lib().orc_dtpmv_lower_unit(len(x), _p(W), _p(x))
+    return x
+
+
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+def box_vector(ibox, level):
+    v = (ctypes.c_int * 3)()
+    lib().orc_box_vector(ibox, level, v)
+    return tuple(v)
+
+
+def box_index(v, level):
+    a = (ctypes.c_int * 3)(*v)
+    return lib().orc_box_index(a, level)
+
+
+def nearest_neighbors(ibox, level):
+    out = (ctypes.c_int * 26)()
+    n = lib().orc_nearest_neighbors(ibox, level, out)
+    return list(out[:n])
+
+
+def local_farfield(ibox, level):
+    out = (ctypes.c_int * 1024)()
+    n = lib().orc_local_farfield(ibox, level, out)
+    return list(out[:n])
+
+
+def box_multipoles(lmax, px, wx, py, wy, pz, wz, cube_sub, center):
+    q = np.zeros((lmax + 1) ** 2)
+    c = np.asfortranarray(cube_sub, dtype=np.float64)
+    px, wx, py, wy, pz, wz = (_f64(a) for a in (px, wx, py, wy, pz, wz))
+    lib().orc_box_multipoles(lmax, len(px), _p(px), _p(wx), len(py), _p(py), _p(wy), len(pz),
+                             _p(pz), _p(wz), _p(c), _p(_f64(center)), _p(q))
+    return q
+
+
+def l2p(lmax, L, center, px, py, pz, out):
+    """out += sum_lm L_lm S_lm(r - center) over the product grid."""
+    px, py, pz = (_f64(a) for a in (px, py, pz))
+    assert out.flags.f_contiguous and out.shape == (len(px), len(py), len(pz))
+    lib().orc_l2p(lmax, _p(_f64(L)), _p(_f64(center)), len(px), _p(px), len(py), _p(py),
+                  len(pz), _p(pz), _p(out))
+    return out
+
+
+def subgrid(g1: Grid1D, c0: int, c1: int) -> Grid1D:
+    """Cells c0..c1 (1-based, inclusive) of an axis as a grid of its own
+    (Grid3D_get_subgrid: the same points and cell steps)."""
+    return Grid1D(float(g1.points[(c0 - 1) * (g1.nlip - 1)]), c1 - c0 + 1, g1.nlip,
+                  g1.grid_type, g1.cell_scales[c0 - 1:c1])
+
+
+class GBFMMPlan:
+    """Octree box bookkeeping of GBFMMParallelInfo / GBFMMCoulomb3D for one
+    grid (src/gbfmm/gbfmm_parallel_info.F90, gbfmm_coulomb3d.F90:417-508):
+    boxes at `maxlevel` (2^maxlevel per axis) of ncell // 2^maxlevel cells
+    (integer division, as the reference), near-field cell ranges (box plus
+    its nearest neighbours), local far-field lists and the points each box
+    owns (its last point per axis belongs to the next box unless it is the
+    grid's last point)."""
+
+    def __init__(self, grid: Grid3D, maxlevel: int = 2):
+        self.grid = grid
+        self.level = maxlevel
+        self.nb = 2 ** maxlevel
+        self.nbox = self.nb ** 3
+        self.bs = [a.ncell // self.nb for a in grid.axes]
+        self.ranges = [(a.points[0], a.points[-1]) for a in grid.axes]
+        self.vec = [box_vector(i, maxlevel) for i in range(1, self.nbox + 1)]
+
+    def cells(self, ibox):
+        v = self.vec[ibox - 1]
+        return [(v[d] * self.bs[d] + 1, v[d] * self.bs[d] + self.bs[d]) for d in range(3)]
+
+    def near_cells(self, ibox):
+        lim = self.cells(ibox)
+        for j in nearest_neighbors(ibox, self.level):
+            lj = self.cells(j)
+            lim = [(min(lim[d][0], lj[d][0]), max(lim[d][1], lj[d][1])) for d in range(3)]
+        return lim
+
+    def center(self, ibox):
+        v = self.vec[ibox - 1]
+        return np.array([self.ranges[d][0] + (v[d] + 0.5) * (self.ranges[d][1] - self.ranges[d][0]) / self.nb
+                         for d in range(3)])
+
+    def points(self, ibox):
+        """0-based point index range [p0, p1) per axis of the box's sub-grid."""
+        return [((c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1) + 1)
+                for (c0, c1), a in zip(self.cells(ibox), self.grid.axes)]
+
+    def owned(self, ibox):
+        out = []
+        for (c0, c1), a, (p0, p1) in zip(self.cells(ibox), self.grid.axes, self.points(ibox)):
+            out.append((p0, p1 if c1 == a.ncell else p1 - 1))
+        return out
+
+
+def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
+                return_parts=False):
+    """GBFMMCoulomb3D_calculate_potential along the reference's CUDA path
+    (gbfmm_coulomb3d.F90:650-819, gbfmm_coulomb3d.cu:478-573): multipoles per
+    box, M2L over the local far field, near field by the sub-operator of
+    each box (no coda), L2P of the far field; each grid point takes the near
+    and far contributions of the box that owns it."""
+    plan = GBFMMPlan(grid, maxlevel)
+    rho = np.asfortranarray(rho)
+    N = (lmax + 1) ** 2
+    q = np.zeros((N, plan.nbox))
+    for b in range(1, plan.nbox + 1):
+        (x0, x1), (y0, y1), (z0, z1) = plan.points(b)
+        subs = [subgrid(a, c0, c1) for a, (c0, c1) in zip(grid.axes, plan.cells(b))]
+        q[:, b - 1] = box_multipoles(lmax, subs[0].points, subs[0].weights(), subs[1].points,
+                                     subs[1].weights(), subs[2].points, subs[2].weights(),
+                                     rho[x0:x1, y0:y1, z0:z1], plan.center(b))
+    L = np.zeros((N, plan.nbox))
+    for i in range(1, plan.nbox + 1):
+        ci = plan.center(i)
+        for j in local_farfield(i, maxlevel):
+            L[:, i - 1] += interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
+    tp, tw = gauss_quad(*quad)
+    w = coulomb_weights(tw)
+    V = np.zeros(grid.shape, order="F")
+    Vnear = np.zeros(grid.shape, order="F")
+    for b in range(1, plan.nbox + 1):
+        ncl = plan.near_cells(b)
+        gin = [subgrid(a, c0, c1) for a, (c0, c1) in zip(grid.axes, ncl)]
+        own = plan.owned(b)
+        outs = [grid.axes[d].points[own[d][0]:own[d][1]] for d in range(3)]
+        Ts = [coulomb_matrix(gin[d], outs[d], tp) for d in range(3)]
+        pin = [((c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1) + 1) for a, (c0, c1) in zip(grid.axes, ncl)]
+        sub = np.asfortranarray(rho[pin[0][0]:pin[0][1], pin[1][0]:pin[1][1], pin[2][0]:pin[2][1]])
+        vn = transform_cube(*Ts, w, sub, 0.0)
+        far = np.zeros(vn.shape, order="F")
+        l2p(lmax, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
+        sl = tuple(slice(o0, o1) for o0, o1 in own)
+        V[sl] = vn + far
+        Vnear[sl] = vn
+    if return_parts:
+        return V, q, L, Vnear
+    return V

@@ -8,6 +8,10 @@ tlog=500 (today's GaussQuad default tlog is 1000); with those parameters,
 equidistant 7-point (TEST 3: 5-point) cells and the coda term included, the
 CPU oracle reproduces them to the reference test's tolerance of 1e-14.
 
+multipole_test_kat.json holds the golden errors of the reference's
+multipole test (tests/multipole_test.F90, displaced_monopoles_test), which
+pin the M2L interaction matrix and the M2M translation matrix.
+
 oracle_small.json freezes oracle outputs for a small operator (matrices and
 potential samples) so the GPU tests have committed fixtures to compare with.
 Regenerate with:  python tests/golden/make_golden.py
@@ -44,6 +48,23 @@ KAT = {
 }
 
 
+MULTIPOLE_KAT = {
+    "source": "DAGE tests/multipole_test.F90 displaced_monopoles_test (:185-300)",
+    "note": "|qi . T(boxj - boxi) qj - 1/|ri - rj|| for unit monopoles at ri, rj "
+            "translated to the box centres, truncated at l = 0..15",
+    "rj": [-12.31523266, -2.77677722, -13.87351588],
+    "ri": [-13.80289944, -12.66934534, -8.92620243],
+    "boxj": [-10.625, -2.125, -14.875],
+    "boxi": [-14.875, -10.625, -10.625],
+    "err_ref": [6.4549767744542658e-003, 3.5239702059782635e-003, 3.6472898611333848e-005,
+                3.5551144335181639e-004, 1.2985977061118203e-004, 3.0889425959704231e-005,
+                1.8391214269969369e-006, 2.0053722605550828e-006, 1.0603102051365276e-006,
+                2.9594595833681847e-007, 3.4396637579869882e-008, 1.2534625434823532e-008,
+                9.0637385791181302e-009, 2.9670064183306977e-009, 4.8909977456990106e-010,
+                6.3554106422003542e-011],
+}
+
+
 def small_fixture():
     g = O.Grid3D.cube(-2.4, 4, 0.2)  # 25 points per axis
     tp, tw = O.gauss_quad(6, 6, 0.0, 2.0, 1.0e3)
@@ -68,6 +89,8 @@ def small_fixture():
 if __name__ == "__main__":
     with open(os.path.join(HERE, "gauss_test_kat.json"), "w") as f:
         json.dump(KAT, f, indent=1)
+    with open(os.path.join(HERE, "multipole_test_kat.json"), "w") as f:
+        json.dump(MULTIPOLE_KAT, f, indent=1)
     with open(os.path.join(HERE, "oracle_small.json"), "w") as f:
         json.dump(small_fixture(), f, indent=1)
     print("wrote", HERE)

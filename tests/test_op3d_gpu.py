@@ -1,6 +1,16 @@
 """GPU parity tests of the FP64 cube operator (the drop-in) against the CPU
-oracle, through the C ABI.  Bar: <= 1e-10 relative (max-norm) for the
-potential, matching the reference's own known answers for the energy."""
+oracle, through the C ABI.
+
+Bars (all max-norm relative unless said otherwise):
+- the contraction, coda and energy given the same operator matrices:
+  <= 1e-12 (the GPU arithmetic itself);
+- the operator matrices: within 10x the spread the reference algorithm shows
+  when erf/exp move by +-1 ulp (the oracle's libm_1ulp build) -- the
+  reference's closed-form integrals cancel heavily for t*h just above 0.1,
+  so no other libm can reproduce their last bits;
+- the potential end to end: <= max(1e-10, 10x that same libm spread);
+- energies: <= 1e-12 relative, and the reference's own known answers
+  (tests/gauss_test.F90) to 1e-13 absolute."""
 import json
 import os
 
@@ -18,6 +28,29 @@ def _grids(dage, oracle, qmin, ncell, step, nlip=7, gt=1):
 
 def _relmax(a, b):
     return np.abs(a - b).max() / np.abs(b).max()
+
+
+def _check_apply(oracle, op, go, rho, quad, V, E, coda=True):
+    """V, E from the GPU operator `op` against the oracle."""
+    tp, tw = oracle.gauss_quad(*quad)
+    w = oracle.coulomb_weights(tw)
+    c = oracle.coda_of(quad[4]) if coda else 0.0
+    # 1. the GPU arithmetic: same matrices through the oracle's contraction
+    Tg = [op.matrix(d) for d in range(3)]
+    Vg = oracle.transform_cube(*Tg, w, rho, c)
+    assert _relmax(V, Vg) <= 1e-12
+    Eg = oracle.integrate_cube(go, rho * Vg)
+    assert abs(E - Eg) <= 1e-12 * abs(Eg)
+    # 2. end to end against the oracle, within the reference's libm spread
+    To = oracle.coulomb_operator_matrices(go, go, tp)
+    T1 = oracle.coulomb_operator_matrices(go, go, tp, libm_1ulp=True)
+    Vo = oracle.transform_cube(*To, w, rho, c)
+    V1 = oracle.transform_cube(*T1, w, rho, c)
+    spread = _relmax(V1, Vo)
+    assert _relmax(V, Vo) <= max(1e-10, 10 * spread), (_relmax(V, Vo), spread)
+    Eo = oracle.integrate_cube(go, rho * Vo)
+    assert abs(E - Eo) <= 1e-12 * abs(Eo)
+    return Vo
 
 
 def test_quadrature_matches_oracle(dage, oracle):
@@ -40,8 +73,17 @@ def test_matrices_match_oracle(dage, oracle, ncell, step, nlip, gt):
     tp, _ = oracle.gauss_quad(*quad)
     T = op.matrix(0)
     To = oracle.coulomb_matrix(go.axes[0], go.axes[0].points, tp)
+    T1 = oracle.coulomb_matrix(go.axes[0], go.axes[0].points, tp, libm_1ulp=True)
+    env = oracle.matrix_noise_envelope(To, T1)
     for p in range(T.shape[2]):
-        assert np.abs(T[:, :, p] - To[:, :, p]).max() <= 1e-12 * np.abs(To[:, :, p]).max()
+        tol = 10 * env[:, :, p] + 1e-13 * np.abs(To[:, :, p]).max()
+        assert np.all(np.abs(T[:, :, p] - To[:, :, p]) <= tol), p
+    # where the closed forms are well conditioned (t*h >= 0.5 or the Gauss
+    # rule branch t*h < 0.1) the GPU agrees to 1e-12 of the slice maximum
+    for p in range(T.shape[2]):
+        th = tp[p] * step
+        if th < 0.1 or th >= 0.5:
+            assert np.abs(T[:, :, p] - To[:, :, p]).max() <= 1e-12 * np.abs(To[:, :, p]).max(), p
 
 
 def test_matrices_distinct_grids(dage, oracle):
@@ -57,14 +99,18 @@ def test_matrices_distinct_grids(dage, oracle):
            np.asarray(oracle.Grid1D.equidistant(-1.2, 2, 0.2).points),
            np.asarray(oracle.Grid1D.equidistant(0.0, 3, 0.1).points)]
     Ts = [oracle.coulomb_matrix(oi.axes[d], pts[d], tp) for d in range(3)]
+    Tg = []
     for d in range(3):
         T = op.matrix(d)
         assert T.shape == Ts[d].shape
-        assert np.abs(T - Ts[d]).max() <= 1e-12 * np.abs(Ts[d]).max()
+        T1 = oracle.coulomb_matrix(oi.axes[d], pts[d], tp, libm_1ulp=True)
+        env = oracle.matrix_noise_envelope(Ts[d], T1)
+        assert np.all(np.abs(T - Ts[d]) <= 10 * env + 1e-13 * np.abs(Ts[d]).max())
+        Tg.append(T)
     rho = oracle.gauss_cube(oi, [1.0], [2.0], [[0.1, -0.1, 0.05]])
     V = op.apply(np.asfortranarray(rho))
-    Vo = oracle.transform_cube(*Ts, oracle.coulomb_weights(tw), rho, 0.0)
-    assert _relmax(V, Vo) <= TOL_FP64
+    Vo = oracle.transform_cube(*Tg, oracle.coulomb_weights(tw), rho, 0.0)
+    assert _relmax(V, Vo) <= 1e-12
 
 
 @pytest.mark.parametrize("ncell,step,quad", [(4, 0.2, (6, 6, 0.0, 2.0, 1e3)),
@@ -80,10 +126,7 @@ def test_apply_fp64_matches_oracle(dage, oracle, ncell, step, quad):
     rho = oracle.gauss_cube(go, q, a, c)
     op = dage.Coulomb3D(g, quad=dage.GaussQuad(*quad))
     V, E = op.apply(rho, energy=True)
-    Vo = oracle.coulomb_apply(go, rho, quad=quad)
-    assert _relmax(V, Vo) <= TOL_FP64
-    Eo = oracle.integrate_cube(go, rho * Vo)
-    assert abs(E - Eo) <= 1e-12 * abs(Eo)
+    _check_apply(oracle, op, go, rho, quad, V, E)
 
 
 def test_committed_fixture(dage):
@@ -154,9 +197,12 @@ def test_helmholtz_matches_oracle(dage, oracle):
     hop = dage.Helmholtz3D(cop, E)
     V = hop.apply(rho)
     tp, tw = oracle.gauss_quad(*quad)
-    T = oracle.coulomb_matrix(go.axes[0], go.axes[0].points, tp)
+    T = cop.matrix(0)
     Vo = oracle.transform_cube(T, T, T, oracle.helmholtz_weights(tp, tw, E), rho, oracle.coda_of(1e3))
-    assert _relmax(V, Vo) <= TOL_FP64
+    assert _relmax(V, Vo) <= 1e-12
+    To = oracle.coulomb_matrix(go.axes[0], go.axes[0].points, tp)
+    Vr = oracle.transform_cube(To, To, To, oracle.helmholtz_weights(tp, tw, E), rho, oracle.coda_of(1e3))
+    assert _relmax(V, Vr) <= TOL_FP64
     # the energy is reset to 0 afterwards (helmholtz3d.F90:479)
     np.testing.assert_allclose(cop.weights, oracle.coulomb_weights(tw), rtol=1e-15)
 
@@ -173,8 +219,7 @@ def test_config1_121_cube(dage, oracle):
     quad = (20, 20, 0.0, 2.0, 1e3)
     op = dage.Coulomb3D(g, quad=dage.GaussQuad(*quad))
     V, E = op.apply(rho, energy=True)
-    Vo = oracle.coulomb_apply(go, rho, quad=quad)
-    assert _relmax(V, Vo) <= TOL_FP64
+    _check_apply(oracle, op, go, rho, quad, V, E)
     Va = oracle.gauss_pot_cube(go, q, a, c)
     assert _relmax(V, Va) < 1e-3  # discretisation + quadrature error, reported not pinned
 
