@@ -6,7 +6,9 @@ host-side mirror of the reference's Operator3D/Function3D interface.
 """
 from ._capi import DageError, load  # noqa: F401
 from .operators import (  # noqa: F401
+    Bubbles,
     Coulomb3D,
+    GBFMMCoulomb3D,
     GaussQuad,
     Grid1D,
     Grid3D,
@@ -16,5 +18,5 @@ from .operators import (  # noqa: F401
     integrate,
 )
 
-__all__ = ["Coulomb3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
+__all__ = ["Bubbles", "Coulomb3D", "GBFMMCoulomb3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
            "DageError", "dot", "integrate", "load"]

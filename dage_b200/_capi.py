@@ -62,6 +62,23 @@ SIGNATURES = {
     "dage_op3d_set_timing": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dage_op3d_get_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), _D]),
     "dage_op3d_destroy": (ctypes.c_int, [_VP]),
+    "dage_gbfmm_create": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(DageQuad), ctypes.c_int,
+                                         ctypes.POINTER(_VP)]),
+    "dage_gbfmm_apply": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint, _D]),
+    "dage_gbfmm_multipole_moments": (ctypes.c_int, [_VP, _VP, ctypes.c_uint, _D]),
+    "dage_gbfmm_local_expansions": (ctypes.c_int, [_VP, _D]),
+    "dage_gbfmm_evaluate_le": (ctypes.c_int, [_VP, _D, _VP, ctypes.c_uint]),
+    "dage_gbfmm_box_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
+    "dage_gbfmm_set_stream": (ctypes.c_int, [_VP, _VP]),
+    "dage_gbfmm_last_time_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
+    "dage_gbfmm_destroy": (ctypes.c_int, [_VP]),
+    "dage_bubbles_create": (ctypes.c_int, [ctypes.c_int, _D, ctypes.POINTER(DageGrid1D), ctypes.c_int,
+                                           ctypes.c_int, _D, ctypes.POINTER(_VP)]),
+    "dage_bubbles_inject": (ctypes.c_int, [_VP, ctypes.POINTER(DageGrid1D), ctypes.c_int,
+                                           ctypes.c_double, _VP, ctypes.c_uint]),
+    "dage_bubbles_destroy": (ctypes.c_int, [_VP]),
     "dage_integrate": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, ctypes.c_uint, _D]),
     "dage_last_error": (ctypes.c_char_p, []),
     "dage_abi_version": (ctypes.c_int, []),

@@ -1,0 +1,1027 @@
+// gbfmm.cu -- grid-based fast multipole (GBFMM) Coulomb operator on one B200.
+//
+// The cube is split into an octree level of 2^L boxes per axis (L = maxlevel,
+// default 2: 4x4x4 boxes).  For every box b:
+//   near field  V(b's points) = sub-operator(rho on b + its 26 neighbours):
+//               the tensor-product operator restricted to those input cells
+//               and b's output points, FP64, batched over all boxes in one
+//               launch per contraction stage and t-point;
+//   multipoles  q_lm(b) = sum_{r in b} rho w S_lm(r - c_b)   (FP64);
+//   M2L         L(b) = sum_{j in far(b)} T(c_j - c_b) q(j)    (FP64, the
+//               interaction matrices of the distinct box displacements are
+//               built once on the GPU);
+//   L2P         V(r) += sum_lm L_lm(b) S_lm(r - c_b) over b's points.
+// Each grid point belongs to one box (a box's last point along an axis
+// belongs to the next box unless it is the last grid point), as in the
+// reference's CUDA path (src/gbfmm/gbfmm_coulomb3d.cu:478-573,
+// gbfmm_coulomb3d.F90:1000-1030).  S_lm are Racah-normalised real regular
+// solid harmonics (src/bubbles/harmonics.F90:586-658); the M2L matrices
+// follow src/bubbles/multipole.F90:81-303.
+//
+// Box split.  Boxes get ncell / 2^L cells per axis when that divides; when
+// it does not, the first (ncell mod 2^L) boxes along the axis get one extra
+// cell (the reference's integer division would leave the trailing cells in
+// no box).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "op3d.cuh"
+
+struct dage_gbfmm;
+
+namespace dage {
+
+namespace {
+
+constexpr int kMaxLmax = 15;
+
+// ---------------------------------------------------------------------------
+// Real regular solid harmonics by recursion, visiting every (l, m) once.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int lmi(int l, int m) { return l * (l + 1) + m; }
+
+template <class F>
+__device__ __forceinline__ void solid_harmonics(int lmax, double x, double y, double z, F &&f) {
+  const double r2 = x * x + y * y + z * z;
+  f(0, 1.0);
+  if (lmax == 0) return;
+  {  // m = 0
+    double p2 = 1.0, p1 = z;
+    f(lmi(1, 0), z);
+    for (int l = 2; l <= lmax; ++l) {
+      double cur = (2.0 * l - 1.0) / sqrt((double)(l * l)) * (z * p1);
+      cur = cur - sqrt((double)((l - 1) * (l - 1)) / (double)(l * l)) * (r2 * p2);
+      f(lmi(l, 0), cur);
+      p2 = p1;
+      p1 = cur;
+    }
+  }
+  double top = x, bot = y;  // S_{m,m}, S_{m,-m}
+  for (int mm = 1; mm <= lmax; ++mm) {
+    if (mm >= 2) {
+      const double c = sqrt((2.0 * mm - 1.0) / (2.0 * mm));
+      const double nb = c * (y * top + x * bot);
+      const double nt = c * (x * top - y * bot);
+      top = nt;
+      bot = nb;
+    }
+    f(lmi(mm, mm), top);
+    f(lmi(mm, -mm), bot);
+#pragma unroll 1
+    for (int sgn = 0; sgn < 2; ++sgn) {
+      const int m = sgn ? -mm : mm;
+      double p2 = 0.0, p1 = sgn ? bot : top;
+      for (int l = mm + 1; l <= lmax; ++l) {
+        double cur = (2.0 * l - 1.0) / sqrt((double)((l + m) * (l - m))) * (z * p1);
+        if (l > mm + 1)
+          cur = cur - sqrt((double)((l + m - 1) * (l - m - 1)) / (double)((l + m) * (l - m))) *
+                          (r2 * p2);
+        f(lmi(l, m), cur);
+        p2 = p1;
+        p1 = cur;
+      }
+    }
+  }
+}
+
+struct BoxInfo {
+  int p0[3], np[3];     // box sub-grid points (global index, count)
+  int own[3];           // owned points (from p0) per axis
+  int q0[3], nq[3];     // near-field region points
+  int pos[3];           // box position along each axis
+  double c[3];          // expansion centre
+};
+
+// ---------------------------------------------------------------------------
+// Multipole moments: block (box, slab); each thread accumulates its own
+// column of partial sums in shared memory, then one fixed-order reduction.
+// ---------------------------------------------------------------------------
+__global__ void multipoles_kernel(const double *__restrict__ rho, int Nx, int Ny,
+                                  const BoxInfo *__restrict__ boxes,
+                                  const double *__restrict__ wbox, int wstride, int lmax,
+                                  int nslab, double *partial) {
+  extern __shared__ double part[];  // [N][blockDim.x]
+  const int N = (lmax + 1) * (lmax + 1);
+  const int T = blockDim.x, tid = threadIdx.x;
+  const BoxInfo b = boxes[blockIdx.x];
+  for (int s = 0; s < N; ++s) part[s * T + tid] = 0.0;
+  const double *wx = wbox + (0 * 64 + b.pos[0]) * wstride;
+  const double *wy = wbox + (1 * 64 + b.pos[1]) * wstride;
+  const double *wz = wbox + (2 * 64 + b.pos[2]) * wstride;
+  const long long plane = (long long)b.np[0] * b.np[1];
+  for (int k = blockIdx.y; k < b.np[2]; k += nslab) {
+    for (long long e = tid; e < plane; e += T) {
+      const int i = (int)(e % b.np[0]), j = (int)(e / b.np[0]);
+      const size_t g = (size_t)(b.p0[0] + i) + (size_t)Nx * (b.p0[1] + j) +
+                       (size_t)Nx * Ny * (b.p0[2] + k);
+      const double v = rho[g] * (wx[i] * wy[j] * wz[k]);
+      // coordinates relative to the centre are rebuilt from the box grid
+      // spacing table (xs) by the caller: passed via wbox's tail
+      const double *xs = wbox + (3 * 64) * wstride;
+      const double x = xs[b.p0[0] + i] - b.c[0];
+      const double y = xs[wstride + b.p0[1] + j] - b.c[1];
+      const double z = xs[2 * wstride + b.p0[2] + k] - b.c[2];
+      solid_harmonics(lmax, x, y, z, [&](int lm, double s) { part[lm * T + tid] += v * s; });
+    }
+  }
+  __syncthreads();
+  for (int s = tid; s < N; s += T) {
+    double acc = 0.0;
+    for (int t = 0; t < T; ++t) acc += part[s * T + t];
+    partial[((size_t)blockIdx.x * nslab + blockIdx.y) * N + s] = acc;
+  }
+}
+
+__global__ void reduce_slabs_kernel(const double *partial, int nslab, int N, int nbox,
+                                    double *q) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nbox * N) return;
+  const int b = idx / N, s = idx % N;
+  double acc = 0.0;
+  for (int k = 0; k < nslab; ++k) acc += partial[((size_t)b * nslab + k) * N + s];
+  q[(size_t)b * N + s] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// M2L matrices of the distinct displacements (multipole.F90:265-303):
+//   I_lm(d) = S_lm(d) / |d|^(2l+1), l <= 2 lmax
+//   T(i, s) = c1 I[lm1] + c2 I[lm2] (i >= s),  T(s, i) = (-1)^(l_i - l_s) T(i, s)
+// stored column-major, T[s*N + i], so a warp reading one column is coalesced.
+// ---------------------------------------------------------------------------
+__global__ void m2l_matrices_kernel(const double *__restrict__ disp, int lmax,
+                                    const double *__restrict__ c1, const double *__restrict__ c2,
+                                    const int *__restrict__ lm1, const int *__restrict__ lm2,
+                                    const int *__restrict__ prow, const int *__restrict__ pcol,
+                                    double *Tall) {
+  extern __shared__ double I[];
+  const int L2 = 2 * lmax;
+  const int NI = (L2 + 1) * (L2 + 1);
+  const int N = (lmax + 1) * (lmax + 1);
+  const int M = N * (N + 1) / 2;
+  const double *d = disp + 3 * blockIdx.x;
+  if (threadIdx.x == 0) solid_harmonics(L2, d[0], d[1], d[2], [&](int lm, double s) { I[lm] = s; });
+  __syncthreads();
+  const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  for (int lm = threadIdx.x; lm < NI; lm += blockDim.x) {
+    int l = (int)sqrt((double)lm);
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    while (l * l > lm) --l;
+    double rp = 1.0;
+    for (int e = 0; e < 2 * l + 1; ++e) rp *= r;
+    I[lm] = I[lm] / rp;
+  }
+  __syncthreads();
+  double *T = Tall + (size_t)blockIdx.x * N * N;
+  for (int e = threadIdx.x; e < M; e += blockDim.x) {
+    const int i = prow[e], s = pcol[e];  // 0-based row (l,m) >= column (j,k)
+    const double w = c1[e] * I[lm1[e]] + c2[e] * I[lm2[e]];
+    int li = (int)sqrt((double)i), ls = (int)sqrt((double)s);
+    while ((li + 1) * (li + 1) <= i) ++li;
+    while (li * li > i) --li;
+    while ((ls + 1) * (ls + 1) <= s) ++ls;
+    while (ls * ls > s) --ls;
+    T[(size_t)s * N + i] = w;
+    T[(size_t)i * N + s] = ((li - ls) & 1) ? -w : w;
+  }
+}
+
+// L(b) = sum over the far field of b of T(disp) q(src); one block per box.
+__global__ void m2l_apply_kernel(const double *__restrict__ Tall, const double *__restrict__ q,
+                                 const int *__restrict__ ff_start, const int *__restrict__ ff_src,
+                                 const int *__restrict__ ff_disp, int N, double *Lout) {
+  extern __shared__ double qs[];
+  const int b = blockIdx.x;
+  double acc = 0.0;
+  const int i = threadIdx.x;
+  for (int e = ff_start[b]; e < ff_start[b + 1]; ++e) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < N; k += blockDim.x) qs[k] = q[(size_t)ff_src[e] * N + k];
+    __syncthreads();
+    if (i < N) {
+      const double *T = Tall + (size_t)ff_disp[e] * N * N;
+      for (int k = 0; k < N; ++k) acc += T[(size_t)k * N + i] * qs[k];
+    }
+  }
+  if (i < N) Lout[(size_t)b * N + i] = acc;
+}
+
+// V(r) += sum_lm L_lm S_lm(r - c) over the owned points of every box.
+__global__ void l2p_kernel(const double *__restrict__ L, const BoxInfo *__restrict__ boxes,
+                           const double *__restrict__ xs, int xstride, int lmax, int Nx, int Ny,
+                           double *V) {
+  extern __shared__ double Ls[];
+  const int N = (lmax + 1) * (lmax + 1);
+  const BoxInfo b = boxes[blockIdx.y];
+  for (int k = threadIdx.x; k < N; k += blockDim.x) Ls[k] = L[(size_t)blockIdx.y * N + k];
+  __syncthreads();
+  const long long n = (long long)b.own[0] * b.own[1] * b.own[2];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % b.own[0]);
+    const long long r = e / b.own[0];
+    const int j = (int)(r % b.own[1]), k = (int)(r / b.own[1]);
+    const int gx = b.p0[0] + i, gy = b.p0[1] + j, gz = b.p0[2] + k;
+    double v = 0.0;
+    solid_harmonics(lmax, xs[gx] - b.c[0], xs[xstride + gy] - b.c[1], xs[2 * xstride + gz] - b.c[2],
+                    [&](int lm, double s) { v += Ls[lm] * s; });
+    V[(size_t)gx + (size_t)Nx * gy + (size_t)Nx * Ny * gz] += v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched FP64 contraction stage over boxes (one descriptor per box):
+//   out[o(R, n)] (= or +=) alpha * sum_K X[a(R) + K] * T[n*ldt + K]
+//   a(R) = (R % a_d0) a_s1 + (R / a_d0) a_s2
+//   o(R, n) = (R % o_d0) o_s1 + (R / o_d0) o_s2 + n o_sn
+// ---------------------------------------------------------------------------
+struct StageDesc {
+  const double *X;
+  long long a_d0, a_s1, a_s2;
+  const double *T;
+  long long ldt;
+  double *out;
+  long long o_d0, o_s1, o_s2, o_sn;
+  int M, N, K;
+};
+
+constexpr int BM = 128, BN = 64, BK = 8, PAD = 2;
+
+template <bool ACCUM>
+__global__ void __launch_bounds__(256) stage_fp64_batched_kernel(const StageDesc *__restrict__ descs,
+                                                                 double alpha) {
+  __shared__ __align__(16) double As[2][BK][BM + PAD];
+  __shared__ __align__(16) double Bs[2][BK][BN + PAD];
+  const StageDesc d = descs[blockIdx.z];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (m0 >= d.M || n0 >= d.N) return;
+  const int tid = threadIdx.x;
+  const int tx = tid & 31, ty = tid >> 5;  // tx -> rows (4 each), ty -> columns (8 each)
+  double ra[4], rb[2];
+  auto arow = [&](long long R) { return (R % d.a_d0) * d.a_s1 + (R / d.a_d0) * d.a_s2; };
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
+      const int m = m0 + r, k = k0 + kk;
+      ra[i] = (m < d.M && k < d.K) ? __ldg(d.X + arow(m) + k) : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
+      const int n = n0 + r, k = k0 + kk;
+      rb[i] = (n < d.N && k < d.K) ? __ldg(d.T + (size_t)n * d.ldt + k) : 0.0;
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 256 * i;
+      As[buf][e & 7][e >> 3] = ra[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int e = tid + 256 * i;
+      Bs[buf][e & 7][e >> 3] = rb[i];
+    }
+  };
+  double acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  const int nk = (d.K + BK - 1) / BK;
+  gload(0);
+  sstore(0);
+  __syncthreads();
+  for (int kt = 0; kt < nk; ++kt) {
+    const int cur = kt & 1;
+    if (kt + 1 < nk) gload((kt + 1) * BK);
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      const double2 *ap = reinterpret_cast<const double2 *>(&As[cur][k][0]);
+      const double2 *bp = reinterpret_cast<const double2 *>(&Bs[cur][k][0]);
+      const double2 a0 = ap[tx * 2], a1 = ap[tx * 2 + 1];
+      const double a[4] = {a0.x, a0.y, a1.x, a1.y};
+      double b[8];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 t = bp[ty * 4 + j];
+        b[2 * j] = t.x;
+        b[2 * j + 1] = t.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (kt + 1 < nk) {
+      sstore(cur ^ 1);
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int n = n0 + ty * 8 + j;
+    if (n >= d.N) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const long long m = m0 + tx * 4 + i;
+      if (m >= d.M) continue;
+      double *o = d.out + (m % d.o_d0) * d.o_s1 + (m / d.o_d0) * d.o_s2 + (long long)n * d.o_sn;
+      *o = ACCUM ? *o + alpha * acc[i][j] : alpha * acc[i][j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side M2L coefficient tables (multipole.F90:106-187), built once per
+// lmax: entries of the packed lower triangle of T.
+// ---------------------------------------------------------------------------
+double fprod(int n) {
+  double p = 1.0;
+  for (int i = 1; i <= n; ++i) p = p * (1.0 * i);
+  return p;
+}
+double sg(int k) { return (k & 1) ? -1.0 : 1.0; }
+double Ccf(int l, int m) {
+  if (m == 0) return 1.0 / fprod(l);
+  if (m > 0) return sg(m) / std::sqrt(2.0 * fprod(l - m) * fprod(l + m));
+  return sg(m) * Ccf(l, -m);
+}
+double Csf(int l, int m) {
+  if (m == 0) return 0.0;
+  if (m > 0) return sg(m) / std::sqrt(2.0 * fprod(l - m) * fprod(l + m));
+  return -sg(m) * Csf(l, -m);
+}
+double Cstf(int l, int m) { return fprod(l - m) * fprod(l + m) * Csf(l, m); }
+double Cctf(int l, int m) { return fprod(l - m) * fprod(l + m) * Ccf(l, m); }
+double Df(int l, int m) { return std::sqrt(fprod(l + m) * fprod(l - m) * (2.0 - (m == 0))); }
+
+struct M2LTables {
+  std::vector<double> c1, c2;
+  std::vector<int> lm1, lm2, prow, pcol;
+};
+
+void m2l_tables(int lmax, M2LTables &t) {
+  const int N = (lmax + 1) * (lmax + 1);
+  const double ij[3] = {1.0, 0.5, 0.25};
+  auto lm_of = [](int s, int &l, int &m) {
+    l = 0;
+    while ((l + 1) * (l + 1) <= s) ++l;
+    m = s - l * l - l;
+  };
+  for (int s = 0; s < N; ++s) {
+    int j, k;
+    lm_of(s, j, k);
+    for (int i = s; i < N; ++i) {
+      int l, m;
+      lm_of(i, l, m);
+      const double c = 2 * sg(j) * ij[(m == 0) + (k == 0)];
+      int L1 = l + j, M1, M2;
+      double a, b;
+      if (m >= 0 && k >= 0) {
+        M1 = std::abs(m + k); a = Cctf(L1, m + k);
+        M2 = std::abs(m - k); b = sg(k) * Cctf(L1, m - k);
+      } else if (m >= 0 && k < 0) {
+        M1 = -std::abs(m + k); a = Cstf(L1, m + k);
+        M2 = -std::abs(m - k); b = -sg(k) * Cstf(L1, m - k);
+        a = -a * sg(k); b = -b * sg(k);
+      } else if (m < 0 && k >= 0) {
+        M1 = -std::abs(m + k); a = Cstf(L1, m + k);
+        M2 = -std::abs(m - k); b = sg(k) * Cstf(L1, m - k);
+        a = -a * sg(m); b = -b * sg(m);
+      } else {
+        M1 = std::abs(m + k); a = -Cctf(L1, m + k);
+        M2 = std::abs(m - k); b = sg(k) * Cctf(L1, m - k);
+        a = a * sg(m + k); b = b * sg(m + k);
+      }
+      a = a * c; b = b * c;
+      a = sg(m) * a / Df(l, m); b = sg(m) * b / Df(l, m);
+      a = sg(k) * a / Df(j, k); b = sg(k) * b / Df(j, k);
+      t.c1.push_back(a);
+      t.c2.push_back(b);
+      t.lm1.push_back(L1 * (L1 + 1) + M1);
+      t.lm2.push_back(L1 * (L1 + 1) + M2);
+      t.prow.push_back(i);
+      t.pcol.push_back(s);
+    }
+  }
+}
+
+// octree box index <-> vector (gbfmm_parallel_info.F90:1128-1194)
+void box_vector(int ibox, int level, int v[3]) {
+  int vv[3] = {0, 0, 0}, rem;
+  if (level > 1) {
+    box_vector((ibox - 1) / 8 + 1, level - 1, vv);
+    for (int d = 0; d < 3; ++d) vv[d] *= 2;
+    rem = (ibox - 1) % 8;
+  } else {
+    rem = ibox - 1;
+  }
+  const int iz = rem / 4;
+  rem -= iz * 4;
+  const int iy = rem / 2;
+  rem -= iy * 2;
+  v[0] = vv[0] + rem;
+  v[1] = vv[1] + iy;
+  v[2] = vv[2] + iz;
+}
+int box_index(const int v[3], int level) {
+  int idx, rem[3];
+  if (level > 1) {
+    int pv[3] = {v[0] / 2, v[1] / 2, v[2] / 2};
+    idx = (box_index(pv, level - 1) - 1) * 8 + 1;
+    for (int d = 0; d < 3; ++d) rem[d] = v[d] - pv[d] * 2;
+  } else {
+    idx = 1;
+    for (int d = 0; d < 3; ++d) rem[d] = v[d];
+  }
+  return idx + rem[0] + rem[1] * 2 + rem[2] * 4;
+}
+std::vector<int> neighbours(int ibox, int level) {
+  const int lim = 1 << level;
+  int v[3];
+  box_vector(ibox, level, v);
+  std::vector<int> out;
+  for (int iz = -1; iz <= 1; ++iz)
+    for (int iy = -1; iy <= 1; ++iy)
+      for (int ix = -1; ix <= 1; ++ix) {
+        if (!ix && !iy && !iz) continue;
+        const int w[3] = {v[0] + ix, v[1] + iy, v[2] + iz};
+        if (w[0] < 0 || w[1] < 0 || w[2] < 0 || w[0] >= lim || w[1] >= lim || w[2] >= lim)
+          continue;
+        out.push_back(box_index(w, level));
+      }
+  return out;
+}
+std::vector<int> local_farfield(int ibox, int level) {
+  std::vector<int> out;
+  if (level < 2) return out;
+  const auto pnn = neighbours((ibox - 1) / 8 + 1, level - 1);
+  const auto nn = neighbours(ibox, level);
+  for (int p : pnn)
+    for (int c = 1; c <= 8; ++c) {
+      const int child = (p - 1) * 8 + c;
+      if (std::find(nn.begin(), nn.end(), child) == nn.end()) out.push_back(child);
+    }
+  return out;
+}
+
+}  // namespace
+}  // namespace dage
+
+using namespace dage;
+
+struct dage_gbfmm {
+  int device = 0;
+  int level = 2, lmax = 12, nbox = 0, N = 0, P = 0, precision = DAGE_FP64;
+  Axis ax[3];
+  int npts[3];
+  dage_quad quad{};
+  std::vector<double> tp, tw, w;
+  std::vector<BoxInfo> boxes;
+  int axis_pos_count[3];
+  // per axis, per box position: near-field operator matrix (P x own x near)
+  std::vector<DevBuf> Tnear[3];
+  DevBuf d_boxes, d_wbox, d_q, d_L, d_partial, d_Tm2l, d_ffstart, d_ffsrc, d_ffdisp;
+  int wstride = 0, nslab = 8, ndisp = 0;
+  DevBuf d_U, d_W, d_desc[3];
+  size_t U_per_box = 0, W_per_box = 0;
+  std::vector<StageDesc> desc[3];
+  DevBuf wts[3], partials, d_rho, d_V;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+};
+
+namespace {
+
+int split_axis(int ncell, int nb, int v, int &c0, int &nc) {
+  const int base = ncell / nb, rem = ncell % nb;
+  c0 = v * base + std::min(v, rem);  // 0-based first cell
+  nc = base + (v < rem ? 1 : 0);
+  return 0;
+}
+
+int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, int lmax,
+                      const dage_quad *quad) {
+  if (!grid || !quad) return fail(DAGE_E_INVALID, "null argument");
+  // one octree level: the local far field of a level-2 box covers every box
+  // outside its neighbourhood; deeper levels need M2M/L2L between levels
+  if (maxlevel != 2) return fail(DAGE_E_UNSUPPORTED, "maxlevel must be 2 (4x4x4 boxes)");
+  if (lmax < 0 || lmax > kMaxLmax) return fail(DAGE_E_UNSUPPORTED, "lmax must be 0..%d", kMaxLmax);
+  g->level = maxlevel;
+  g->lmax = lmax;
+  g->N = (lmax + 1) * (lmax + 1);
+  g->quad = *quad;
+  g->P = quad->nlin + quad->nlog;
+  if (g->P < 1) return fail(DAGE_E_INVALID, "quadrature needs t-points");
+  DAGE_CUDA_TRY(cudaGetDevice(&g->device));
+  const int nb = 1 << maxlevel;
+  g->nbox = nb * nb * nb;
+  for (int d = 0; d < 3; ++d) {
+    DAGE_TRY(make_axis(grid[d], g->ax[d]));
+    g->npts[d] = g->ax[d].n();
+    if (g->ax[d].ncell < nb) return fail(DAGE_E_INVALID, "fewer cells than boxes along an axis");
+  }
+  DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
+  g->stream = g->own_stream;
+  DAGE_CUDA_TRY(cudaEventCreate(&g->ev0));
+  DAGE_CUDA_TRY(cudaEventCreate(&g->ev1));
+  cudaStream_t s = g->stream;
+  const int nlip = g->ax[0].nlip;
+
+  // --- boxes ---------------------------------------------------------------
+  g->boxes.resize(g->nbox);
+  std::vector<int> pos_near0[3], pos_nearn[3], pos_p0[3], pos_np[3], pos_own[3];
+  for (int d = 0; d < 3; ++d) {
+    const Axis &a = g->ax[d];
+    for (int v = 0; v < nb; ++v) {
+      int c0, nc;
+      split_axis(a.ncell, nb, v, c0, nc);
+      const int p0 = c0 * (nlip - 1), np = nc * (nlip - 1) + 1;
+      const bool last = (c0 + nc == a.ncell);
+      int nc0, ncn, cc0, ccn;
+      split_axis(a.ncell, nb, std::max(v - 1, 0), nc0, ncn);
+      split_axis(a.ncell, nb, std::min(v + 1, nb - 1), cc0, ccn);
+      const int near_c0 = nc0, near_c1 = cc0 + ccn;  // [near_c0, near_c1)
+      pos_p0[d].push_back(p0);
+      pos_np[d].push_back(np);
+      pos_own[d].push_back(last ? np : np - 1);
+      pos_near0[d].push_back(near_c0 * (nlip - 1));
+      pos_nearn[d].push_back((near_c1 - near_c0) * (nlip - 1) + 1);
+    }
+  }
+  for (int b = 0; b < g->nbox; ++b) {
+    int v[3];
+    box_vector(b + 1, maxlevel, v);
+    BoxInfo &B = g->boxes[b];
+    for (int d = 0; d < 3; ++d) {
+      B.pos[d] = v[d];
+      B.p0[d] = pos_p0[d][v[d]];
+      B.np[d] = pos_np[d][v[d]];
+      B.own[d] = pos_own[d][v[d]];
+      B.q0[d] = pos_near0[d][v[d]];
+      B.nq[d] = pos_nearn[d][v[d]];
+      const Axis &a = g->ax[d];
+      if (a.ncell % nb == 0) {  // the reference's centre (gbfmm_parallel_info.F90:1290-1299)
+        const double qmin = a.points.front(), qmax = a.points.back();
+        B.c[d] = qmin + (v[d] + 0.5) * ((qmax - qmin) / (nb + 0.0));
+      } else {
+        B.c[d] = 0.5 * (a.points[B.p0[d]] + a.points[B.p0[d] + B.np[d] - 1]);
+      }
+    }
+  }
+  DAGE_TRY(g->d_boxes.alloc(sizeof(BoxInfo) * g->nbox));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_boxes.ptr, g->boxes.data(), sizeof(BoxInfo) * g->nbox,
+                                cudaMemcpyHostToDevice, s));
+
+  // --- per-position box weights + point coordinates -------------------------
+  int maxn = 0;
+  for (int d = 0; d < 3; ++d) maxn = std::max(maxn, g->npts[d]);
+  g->wstride = maxn;
+  if (nb > 64) return fail(DAGE_E_UNSUPPORTED, "too many boxes per axis");
+  std::vector<double> wbox((size_t)(3 * 64 + 3) * maxn, 0.0);
+  for (int d = 0; d < 3; ++d) {
+    LipBasis L;
+    DAGE_TRY(make_lip_basis(nlip, g->ax[d].grid_type, L));
+    for (int v = 0; v < nb; ++v) {
+      int c0, nc;
+      split_axis(g->ax[d].ncell, nb, v, c0, nc);
+      double *w = wbox.data() + (size_t)(d * 64 + v) * maxn;
+      for (int c = 0; c < nc; ++c)
+        for (int i = 0; i < nlip; ++i) w[c * (nlip - 1) + i] += L.integrals[i] * g->ax[d].h[c0 + c];
+    }
+    std::copy(g->ax[d].points.begin(), g->ax[d].points.end(),
+              wbox.begin() + (size_t)(3 * 64 + d) * maxn);
+  }
+  DAGE_TRY(g->d_wbox.alloc(sizeof(double) * wbox.size()));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_wbox.ptr, wbox.data(), sizeof(double) * wbox.size(),
+                                cudaMemcpyHostToDevice, s));
+
+  // --- far-field lists grouped by displacement -------------------------------
+  // displacements keyed by integer box-vector differences on a regular box
+  // lattice (all axes divide evenly), else by the exact centre differences
+  bool regular = true;
+  for (int d = 0; d < 3; ++d) regular = regular && (g->ax[d].ncell % nb == 0);
+  std::map<std::vector<long long>, int> disp_index;
+  std::vector<double> disp;
+  std::vector<int> ffstart(1, 0), ffsrc, ffdisp;
+  for (int b = 1; b <= g->nbox; ++b) {
+    for (int j : local_farfield(b, maxlevel)) {
+      double dv[3];
+      std::vector<long long> key(3);
+      for (int d = 0; d < 3; ++d) {
+        dv[d] = g->boxes[j - 1].c[d] - g->boxes[b - 1].c[d];
+        if (regular)
+          key[d] = g->boxes[j - 1].pos[d] - g->boxes[b - 1].pos[d];
+        else
+          std::memcpy(&key[d], &dv[d], 8);
+      }
+      auto it = disp_index.find(key);
+      int di;
+      if (it == disp_index.end()) {
+        di = (int)disp_index.size();
+        disp_index[key] = di;
+        disp.insert(disp.end(), dv, dv + 3);
+      } else {
+        di = it->second;
+      }
+      ffsrc.push_back(j - 1);
+      ffdisp.push_back(di);
+    }
+    ffstart.push_back((int)ffsrc.size());
+  }
+  g->ndisp = (int)disp_index.size();
+  DAGE_TRY(g->d_ffstart.alloc(sizeof(int) * ffstart.size()));
+  DAGE_TRY(g->d_ffsrc.alloc(sizeof(int) * std::max<size_t>(1, ffsrc.size())));
+  DAGE_TRY(g->d_ffdisp.alloc(sizeof(int) * std::max<size_t>(1, ffdisp.size())));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_ffstart.ptr, ffstart.data(), sizeof(int) * ffstart.size(),
+                                cudaMemcpyHostToDevice, s));
+  if (!ffsrc.empty()) {
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_ffsrc.ptr, ffsrc.data(), sizeof(int) * ffsrc.size(),
+                                  cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_ffdisp.ptr, ffdisp.data(), sizeof(int) * ffdisp.size(),
+                                  cudaMemcpyHostToDevice, s));
+  }
+  // M2L matrices on the GPU
+  if (g->ndisp > 0) {
+    M2LTables t;
+    m2l_tables(lmax, t);
+    DevBuf dd, c1, c2, l1, l2, pr, pc;
+    const size_t M = t.c1.size();
+    DAGE_TRY(dd.alloc(sizeof(double) * disp.size()));
+    DAGE_TRY(c1.alloc(sizeof(double) * M));
+    DAGE_TRY(c2.alloc(sizeof(double) * M));
+    DAGE_TRY(l1.alloc(sizeof(int) * M));
+    DAGE_TRY(l2.alloc(sizeof(int) * M));
+    DAGE_TRY(pr.alloc(sizeof(int) * M));
+    DAGE_TRY(pc.alloc(sizeof(int) * M));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(dd.ptr, disp.data(), sizeof(double) * disp.size(), cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(c1.ptr, t.c1.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(c2.ptr, t.c2.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(l1.ptr, t.lm1.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(l2.ptr, t.lm2.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(pr.ptr, t.prow.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(pc.ptr, t.pcol.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+    DAGE_TRY(g->d_Tm2l.alloc(sizeof(double) * (size_t)g->ndisp * g->N * g->N));
+    const int NI = (2 * lmax + 1) * (2 * lmax + 1);
+    m2l_matrices_kernel<<<g->ndisp, 256, sizeof(double) * NI, s>>>(
+        dd.as<double>(), lmax, c1.as<double>(), c2.as<double>(), l1.as<int>(), l2.as<int>(),
+        pr.as<int>(), pc.as<int>(), g->d_Tm2l.as<double>());
+    DAGE_CUDA_TRY(cudaGetLastError());
+    DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  DAGE_TRY(g->d_q.alloc(sizeof(double) * g->nbox * g->N));
+  DAGE_TRY(g->d_L.alloc(sizeof(double) * g->nbox * g->N));
+  DAGE_TRY(g->d_partial.alloc(sizeof(double) * (size_t)g->nbox * g->nslab * g->N));
+
+  // --- near-field sub-operator matrices per axis position --------------------
+  DevBuf d_tp;
+  DAGE_TRY(build_quadrature(g->quad, g->tp, g->tw, d_tp, s));
+  const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
+  g->w.resize(g->P);
+  for (int p = 0; p < g->P; ++p) g->w[p] = two_over_sqrtpi * g->tw[p];
+  for (int d = 0; d < 3; ++d) {
+    g->Tnear[d].resize(nb);
+    for (int v = 0; v < nb; ++v) {
+      const int q0 = pos_near0[d][v], nq = pos_nearn[d][v];
+      dage_grid1d sub;
+      sub.ncell = (nq - 1) / (nlip - 1);
+      sub.nlip = nlip;
+      sub.grid_type = g->ax[d].grid_type;
+      sub.qmin = g->ax[d].points[q0];
+      sub.cell_scales = g->ax[d].h.data() + q0 / (nlip - 1);
+      Axis ain;
+      DAGE_TRY(make_axis(sub, ain));
+      // identical coordinates to the global grid's points: copy them over
+      for (int i = 0; i < nq; ++i) ain.points[i] = g->ax[d].points[q0 + i];
+      for (int c = 0; c < ain.ncell; ++c) ain.celld[c] = g->ax[d].celld[q0 / (nlip - 1) + c];
+      const int own = pos_own[d][v];
+      DAGE_TRY(g->Tnear[d][v].alloc(sizeof(double) * (size_t)g->P * own * nq));
+      DAGE_TRY(build_axis_matrix(ain, g->ax[d].points.data() + pos_p0[d][v], own,
+                                 d_tp.as<double>(), g->P, g->Tnear[d][v].as<double>(), s));
+    }
+  }
+  // intermediates and stage descriptors
+  size_t maxU = 0, maxW = 0;
+  for (const auto &B : g->boxes) {
+    maxU = std::max(maxU, (size_t)B.nq[1] * B.nq[2] * B.own[0]);
+    maxW = std::max(maxW, (size_t)B.nq[2] * B.own[0] * B.own[1]);
+  }
+  g->U_per_box = maxU;
+  g->W_per_box = maxW;
+  DAGE_TRY(g->d_U.alloc(sizeof(double) * maxU * g->nbox));
+  DAGE_TRY(g->d_W.alloc(sizeof(double) * maxW * g->nbox));
+  for (int d = 0; d < 3; ++d) {
+    DAGE_TRY(g->wts[d].alloc(sizeof(double) * g->npts[d]));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->wts[d].ptr, g->ax[d].weights.data(),
+                                  sizeof(double) * g->npts[d], cudaMemcpyHostToDevice, s));
+    DAGE_TRY(g->d_desc[d].alloc(sizeof(StageDesc) * g->nbox * g->P));
+  }
+  DAGE_TRY(g->partials.alloc(sizeof(double) * (finalize_partials_count() + 1)));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// Fills the three stage descriptor arrays (for all t-points) for the given
+// device rho and V.
+int gbfmm_descriptors(dage_gbfmm *g, const double *rho, double *V) {
+  const int Nx = g->npts[0], Ny = g->npts[1];
+  std::vector<StageDesc> ds[3];
+  for (int p = 0; p < g->P; ++p)
+    for (int b = 0; b < g->nbox; ++b) {
+      const BoxInfo &B = g->boxes[b];
+      double *U = g->d_U.as<double>() + g->U_per_box * b;
+      double *W = g->d_W.as<double>() + g->W_per_box * b;
+      StageDesc x{}, y{}, z{};
+      // stage x: rho near region (a: x, rows (b: y, c: z)) -> U(R=(y,z), n=x_own)
+      x.M = B.nq[1] * B.nq[2];
+      x.N = B.own[0];
+      x.K = B.nq[0];
+      x.X = rho + B.q0[0] + (size_t)Nx * B.q0[1] + (size_t)Nx * Ny * B.q0[2];
+      x.a_d0 = B.nq[1];
+      x.a_s1 = Nx;
+      x.a_s2 = (long long)Nx * Ny;
+      x.T = g->Tnear[0][B.pos[0]].as<double>() + (size_t)p * B.own[0] * B.nq[0];
+      x.ldt = B.nq[0];
+      x.out = U;
+      x.o_d0 = x.M;
+      x.o_s1 = 1;
+      x.o_s2 = 0;
+      x.o_sn = x.M;
+      // stage y: U (K = y near, rows (z near, x own)) -> W(R=(z, x), n=y_own)
+      y.M = B.nq[2] * B.own[0];
+      y.N = B.own[1];
+      y.K = B.nq[1];
+      y.X = U;
+      y.a_d0 = y.M;
+      y.a_s1 = B.nq[1];
+      y.a_s2 = 0;
+      y.T = g->Tnear[1][B.pos[1]].as<double>() + (size_t)p * B.own[1] * B.nq[1];
+      y.ldt = B.nq[1];
+      y.out = W;
+      y.o_d0 = y.M;
+      y.o_s1 = 1;
+      y.o_s2 = 0;
+      y.o_sn = y.M;
+      // stage z: W (K = z near, rows (x own, y own)) -> V box (owned points)
+      z.M = B.own[0] * B.own[1];
+      z.N = B.own[2];
+      z.K = B.nq[2];
+      z.X = W;
+      z.a_d0 = z.M;
+      z.a_s1 = B.nq[2];
+      z.a_s2 = 0;
+      z.T = g->Tnear[2][B.pos[2]].as<double>() + (size_t)p * B.own[2] * B.nq[2];
+      z.ldt = B.nq[2];
+      z.out = V + B.p0[0] + (size_t)Nx * B.p0[1] + (size_t)Nx * Ny * B.p0[2];
+      z.o_d0 = B.own[0];
+      z.o_s1 = 1;
+      z.o_s2 = Nx;
+      z.o_sn = (long long)Nx * Ny;
+      ds[0].push_back(x);
+      ds[1].push_back(y);
+      ds[2].push_back(z);
+    }
+  for (int d = 0; d < 3; ++d)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_desc[d].ptr, ds[d].data(), sizeof(StageDesc) * ds[d].size(),
+                                  cudaMemcpyHostToDevice, g->stream));
+  return 0;
+}
+
+int gbfmm_multipoles(dage_gbfmm *g, const double *rho) {
+  cudaStream_t s = g->stream;
+  int threads = 128;
+  size_t smem = sizeof(double) * g->N * threads;
+  while (smem > 200 * 1024 && threads > 32) {
+    threads -= 32;
+    smem = sizeof(double) * g->N * threads;
+  }
+  DAGE_CUDA_TRY(cudaFuncSetAttribute(multipoles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+  multipoles_kernel<<<dim3(g->nbox, g->nslab), threads, smem, s>>>(
+      rho, g->npts[0], g->npts[1], g->d_boxes.as<BoxInfo>(), g->d_wbox.as<double>(), g->wstride,
+      g->lmax, g->nslab, g->d_partial.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  const int n = g->nbox * g->N;
+  reduce_slabs_kernel<<<(n + 255) / 256, 256, 0, s>>>(g->d_partial.as<double>(), g->nslab, g->N,
+                                                      g->nbox, g->d_q.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int gbfmm_m2l(dage_gbfmm *g) {
+  const int threads = ((g->N + 31) / 32) * 32;
+  m2l_apply_kernel<<<g->nbox, threads, sizeof(double) * g->N, g->stream>>>(
+      g->d_Tm2l.as<double>(), g->d_q.as<double>(), g->d_ffstart.as<int>(), g->d_ffsrc.as<int>(),
+      g->d_ffdisp.as<int>(), g->N, g->d_L.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int gbfmm_l2p(dage_gbfmm *g, const double *d_L, double *V) {
+  int maxown = 0;
+  for (const auto &B : g->boxes) maxown = std::max(maxown, B.own[0] * B.own[1] * B.own[2]);
+  const int bx = std::min((maxown + 127) / 128, 64);
+  l2p_kernel<<<dim3(bx, g->nbox), 128, sizeof(double) * g->N, g->stream>>>(
+      d_L, g->d_boxes.as<BoxInfo>(), g->d_wbox.as<double>() + (size_t)3 * 64 * g->wstride,
+      g->wstride, g->lmax, g->npts[0], g->npts[1], V);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int gbfmm_nearfield(dage_gbfmm *g) {
+  cudaStream_t s = g->stream;
+  int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
+  for (const auto &B : g->boxes) {
+    mt[0] = std::max(mt[0], ceil_div((long long)B.nq[1] * B.nq[2], BM));
+    nt[0] = std::max(nt[0], ceil_div(B.own[0], BN));
+    mt[1] = std::max(mt[1], ceil_div((long long)B.nq[2] * B.own[0], BM));
+    nt[1] = std::max(nt[1], ceil_div(B.own[1], BN));
+    mt[2] = std::max(mt[2], ceil_div((long long)B.own[0] * B.own[1], BM));
+    nt[2] = std::max(nt[2], ceil_div(B.own[2], BN));
+  }
+  for (int p = 0; p < g->P; ++p) {
+    for (int st = 0; st < 3; ++st) {
+      const StageDesc *d = g->d_desc[st].as<StageDesc>() + (size_t)p * g->nbox;
+      dim3 grid(mt[st], nt[st], g->nbox);
+      if (st < 2)
+        stage_fp64_batched_kernel<false><<<grid, 256, 0, s>>>(d, 1.0);
+      else if (p == 0)
+        stage_fp64_batched_kernel<false><<<grid, 256, 0, s>>>(d, g->w[p]);
+      else
+        stage_fp64_batched_kernel<true><<<grid, 256, 0, s>>>(d, g->w[p]);
+      DAGE_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  return 0;
+}
+
+void gbfmm_destroy_impl(dage_gbfmm *g) {
+  if (!g) return;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  for (int d = 0; d < 3; ++d) {
+    for (auto &b : g->Tnear[d]) b.release();
+    g->d_desc[d].release();
+    g->wts[d].release();
+  }
+  for (DevBuf *b : {&g->d_boxes, &g->d_wbox, &g->d_q, &g->d_L, &g->d_partial, &g->d_Tm2l,
+                    &g->d_ffstart, &g->d_ffsrc, &g->d_ffdisp, &g->d_U, &g->d_W, &g->partials,
+                    &g->d_rho, &g->d_V})
+    b->release();
+  if (g->ev0) cudaEventDestroy(g->ev0);
+  if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->own_stream) cudaStreamDestroy(g->own_stream);
+  delete g;
+}
+
+// device pointers for rho / V (staging host buffers when needed)
+int stage_io(dage_gbfmm *g, const double *rho, double *V, unsigned flags, const double **d_rho,
+             double **d_V) {
+  const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
+  if (flags & DAGE_DEVICE_PTRS) {
+    *d_rho = rho;
+    *d_V = V;
+    return 0;
+  }
+  DAGE_TRY(g->d_rho.alloc(sizeof(double) * n));
+  DAGE_TRY(g->d_V.alloc(sizeof(double) * n));
+  if (rho)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_rho.ptr, rho, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                  g->stream));
+  *d_rho = g->d_rho.as<double>();
+  *d_V = g->d_V.as<double>();
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const dage_quad *quad,
+                      int precision, dage_gbfmm **out) {
+  clear_error();
+  if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
+  *out = nullptr;
+  if (precision != DAGE_FP64)
+    return fail(DAGE_E_UNSUPPORTED, "the GBFMM operator runs in FP64 (DAGE_FP64)");
+  auto *g = new dage_gbfmm();
+  g->precision = precision;
+  int rc = gbfmm_create_impl(g, grid, maxlevel, lmax, quad);
+  if (rc) {
+    gbfmm_destroy_impl(g);
+    return rc;
+  }
+  *out = g;
+  return 0;
+}
+
+int dage_gbfmm_destroy(dage_gbfmm *g) {
+  clear_error();
+  gbfmm_destroy_impl(g);
+  return 0;
+}
+
+int dage_gbfmm_set_stream(dage_gbfmm *g, void *stream) {
+  if (!g) return fail(DAGE_E_INVALID, "null handle");
+  g->stream = stream ? (cudaStream_t)stream : g->own_stream;
+  return 0;
+}
+
+int dage_gbfmm_box_count(const dage_gbfmm *g, int *nbox, int *nlm) {
+  if (!g) return fail(DAGE_E_INVALID, "null handle");
+  if (nbox) *nbox = g->nbox;
+  if (nlm) *nlm = g->N;
+  return 0;
+}
+
+int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags,
+                     double *energy) {
+  clear_error();
+  if (!g || !rho || !V) return fail(DAGE_E_INVALID, "null argument");
+  if ((flags & DAGE_ENERGY) && !energy) return fail(DAGE_E_INVALID, "energy pointer is null");
+  DAGE_CUDA_TRY(cudaSetDevice(g->device));
+  cudaStream_t s = g->stream;
+  const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
+  DAGE_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  const double *d_rho;
+  double *d_V;
+  DAGE_TRY(stage_io(g, rho, V, flags, &d_rho, &d_V));
+  DAGE_CUDA_TRY(cudaMemsetAsync(d_V, 0, sizeof(double) * n, s));
+  DAGE_TRY(gbfmm_descriptors(g, d_rho, d_V));
+  DAGE_TRY(gbfmm_multipoles(g, d_rho));
+  DAGE_TRY(gbfmm_m2l(g));
+  DAGE_TRY(gbfmm_nearfield(g));
+  DAGE_TRY(gbfmm_l2p(g, g->d_L.as<double>(), d_V));
+  double *d_res = (flags & DAGE_ENERGY) ? g->partials.as<double>() + finalize_partials_count()
+                                        : nullptr;
+  DAGE_TRY(launch_finalize(d_rho, d_V, nullptr, 0.0, g->wts[0].as<double>(),
+                           g->wts[1].as<double>(), g->wts[2].as<double>(), g->npts[0],
+                           g->npts[1], g->npts[2], g->partials.as<double>(),
+                           finalize_partials_count(), d_res, s));
+  if (!(flags & DAGE_DEVICE_PTRS))
+    DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  if (d_res) DAGE_CUDA_TRY(cudaMemcpyAsync(energy, d_res, sizeof(double), cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  DAGE_CUDA_TRY(cudaEventElapsedTime(&g->last_ms, g->ev0, g->ev1));
+  return 0;
+}
+
+int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flags,
+                                 double *moments) {
+  clear_error();
+  if (!g || !rho || !moments) return fail(DAGE_E_INVALID, "null argument");
+  DAGE_CUDA_TRY(cudaSetDevice(g->device));
+  const double *d_rho;
+  double *d_V;
+  DAGE_TRY(stage_io(g, rho, nullptr, flags & DAGE_DEVICE_PTRS, &d_rho, &d_V));
+  DAGE_TRY(gbfmm_multipoles(g, d_rho));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(moments, g->d_q.ptr, sizeof(double) * g->nbox * g->N,
+                                cudaMemcpyDeviceToHost, g->stream));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return 0;
+}
+
+int dage_gbfmm_local_expansions(dage_gbfmm *g, double *L) {
+  clear_error();
+  if (!g || !L) return fail(DAGE_E_INVALID, "null argument");
+  DAGE_CUDA_TRY(cudaMemcpy(L, g->d_L.ptr, sizeof(double) * g->nbox * g->N, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double *V,
+                           unsigned flags) {
+  clear_error();
+  if (!g || !local_expansions || !V) return fail(DAGE_E_INVALID, "null argument");
+  DAGE_CUDA_TRY(cudaSetDevice(g->device));
+  cudaStream_t s = g->stream;
+  const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
+  DevBuf dL;
+  DAGE_TRY(dL.alloc(sizeof(double) * g->nbox * g->N));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(dL.ptr, local_expansions, sizeof(double) * g->nbox * g->N,
+                                cudaMemcpyHostToDevice, s));
+  double *d_V = V;
+  if (!(flags & DAGE_DEVICE_PTRS)) {
+    DAGE_TRY(g->d_V.alloc(sizeof(double) * n));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_V.ptr, V, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    d_V = g->d_V.as<double>();
+  }
+  DAGE_TRY(gbfmm_l2p(g, dL.as<double>(), d_V));
+  if (!(flags & DAGE_DEVICE_PTRS))
+    DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int dage_gbfmm_last_time_ms(const dage_gbfmm *g, float *ms) {
+  if (!g || !ms) return fail(DAGE_E_INVALID, "null argument");
+  *ms = g->last_ms;
+  return 0;
+}
+
+}  // extern "C"

@@ -322,21 +322,64 @@ int launch_finalize(const double *f1, double *f2_or_V, const double *rho_for_cod
 // ---------------------------------------------------------------------------
 // Operator construction
 // ---------------------------------------------------------------------------
+int build_quadrature(const dage_quad &q, std::vector<double> &tp, std::vector<double> &tw,
+                     DevBuf &d_tp, cudaStream_t s) {
+  const int P = q.nlin + q.nlog;
+  DevBuf d_tw;
+  DAGE_TRY(d_tp.alloc(sizeof(double) * P));
+  DAGE_TRY(d_tw.alloc(sizeof(double) * P));
+  quad_kernel<<<2, 128, 0, s>>>(q.nlin, q.nlog, q.tstart, q.tlin, q.tlog, d_tp.as<double>(),
+                                d_tw.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  tp.resize(P);
+  tw.resize(P);
+  DAGE_CUDA_TRY(cudaMemcpyAsync(tp.data(), d_tp.ptr, sizeof(double) * P, cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(tw.data(), d_tw.ptr, sizeof(double) * P, cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int build_axis_matrix(const Axis &ai, const double *out_points, int n_out, const double *d_tp,
+                      int P, double *d_T, cudaStream_t s) {
+  LipBasis L;
+  DAGE_TRY(make_lip_basis(ai.nlip, ai.grid_type, L));
+  const size_t nT = (size_t)P * n_out * ai.n();
+  DAGE_CUDA_TRY(cudaMemsetAsync(d_T, 0, sizeof(double) * nT, s));
+  DevBuf d_celld, d_h, d_x, d_c;
+  DAGE_TRY(d_celld.alloc(sizeof(double) * ai.ncell));
+  DAGE_TRY(d_h.alloc(sizeof(double) * ai.ncell));
+  DAGE_TRY(d_x.alloc(sizeof(double) * n_out));
+  DAGE_TRY(d_c.alloc(sizeof(double) * L.coeff.size()));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(d_celld.ptr, ai.celld.data(), sizeof(double) * ai.ncell,
+                                cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(d_h.ptr, ai.h.data(), sizeof(double) * ai.ncell,
+                                cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(d_x.ptr, out_points, sizeof(double) * n_out,
+                                cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(d_c.ptr, L.coeff.data(), sizeof(double) * L.coeff.size(),
+                                cudaMemcpyHostToDevice, s));
+  TmatArgs a;
+  a.tp = d_tp;
+  a.celld = d_celld.as<double>();
+  a.h = d_h.as<double>();
+  a.xout = d_x.as<double>();
+  a.coeff = d_c.as<double>();
+  a.first = L.first;
+  a.last = L.last;
+  a.P = P;
+  a.ncell = ai.ncell;
+  a.n_in = ai.n();
+  a.n_out = n_out;
+  a.T = d_T;
+  DAGE_TRY(launch_tmatrix(a, ai.nlip, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));  // before the small buffers go
+  return 0;
+}
+
 static int build_matrices(dage_op3d *op) {
   cudaStream_t s = op->stream;
-  DevBuf d_tp, d_tw;
-  DAGE_TRY(d_tp.alloc(sizeof(double) * op->P));
-  DAGE_TRY(d_tw.alloc(sizeof(double) * op->P));
-  quad_kernel<<<2, 128, 0, s>>>(op->quad.nlin, op->quad.nlog, op->quad.tstart, op->quad.tlin,
-                                op->quad.tlog, d_tp.as<double>(), d_tw.as<double>());
-  DAGE_CUDA_TRY(cudaGetLastError());
-  op->tp.resize(op->P);
-  op->tw.resize(op->P);
-  DAGE_CUDA_TRY(cudaMemcpyAsync(op->tp.data(), d_tp.ptr, sizeof(double) * op->P,
-                                cudaMemcpyDeviceToHost, s));
-  DAGE_CUDA_TRY(cudaMemcpyAsync(op->tw.data(), d_tw.ptr, sizeof(double) * op->P,
-                                cudaMemcpyDeviceToHost, s));
-  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  DevBuf d_tp;
+  DAGE_TRY(build_quadrature(op->quad, op->tp, op->tw, d_tp, s));
   const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
   op->w.resize(op->P);
   for (int p = 0; p < op->P; ++p) op->w[p] = two_over_sqrtpi * op->tw[p];
@@ -352,46 +395,12 @@ static int build_matrices(dage_op3d *op) {
     if (op->Towner[d] != d) continue;
     const Axis &ai = op->in[d];
     const Axis &ao = op->out[d];
-    LipBasis L;
-    DAGE_TRY(make_lip_basis(ai.nlip, ai.grid_type, L));
     const size_t nT = (size_t)op->P * ao.n() * ai.n();
     DAGE_TRY(op->Tbuf[d].alloc(sizeof(double) * nT));
-    DAGE_CUDA_TRY(cudaMemsetAsync(op->Tbuf[d].ptr, 0, sizeof(double) * nT, s));
-    DevBuf d_celld, d_h, d_x, d_c;
-    DAGE_TRY(d_celld.alloc(sizeof(double) * ai.ncell));
-    DAGE_TRY(d_h.alloc(sizeof(double) * ai.ncell));
-    DAGE_TRY(d_x.alloc(sizeof(double) * ao.n()));
-    DAGE_TRY(d_c.alloc(sizeof(double) * L.coeff.size()));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(d_celld.ptr, ai.celld.data(), sizeof(double) * ai.ncell,
-                                  cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(d_h.ptr, ai.h.data(), sizeof(double) * ai.ncell,
-                                  cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(d_x.ptr, ao.points.data(), sizeof(double) * ao.n(),
-                                  cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(d_c.ptr, L.coeff.data(), sizeof(double) * L.coeff.size(),
-                                  cudaMemcpyHostToDevice, s));
-    TmatArgs a;
-    a.tp = d_tp.as<double>();
-    a.celld = d_celld.as<double>();
-    a.h = d_h.as<double>();
-    a.xout = d_x.as<double>();
-    a.coeff = d_c.as<double>();
-    a.first = L.first;
-    a.last = L.last;
-    a.P = op->P;
-    a.ncell = ai.ncell;
-    a.n_in = ai.n();
-    a.n_out = ao.n();
-    a.T = op->Tbuf[d].as<double>();
-    DAGE_TRY(launch_tmatrix(a, ai.nlip, s));
-    DAGE_CUDA_TRY(cudaStreamSynchronize(s));  // before the small buffers go
-    d_celld.release();
-    d_h.release();
-    d_x.release();
-    d_c.release();
+    DAGE_TRY(build_axis_matrix(ai, ao.points.data(), ao.n(), d_tp.as<double>(), op->P,
+                               op->Tbuf[d].as<double>(), s));
   }
   d_tp.release();
-  d_tw.release();
   return 0;
 }
 

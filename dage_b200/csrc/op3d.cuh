@@ -71,6 +71,14 @@ int launch_finalize(const double *f1, double *f2_or_V, const double *rho_for_cod
 
 int finalize_partials_count();
 
+// Gauss-Legendre t-points/weights on the GPU (host copies + device tp).
+int build_quadrature(const dage_quad &q, std::vector<double> &tp, std::vector<double> &tw,
+                     DevBuf &d_tp, cudaStream_t s);
+// FP64 operator matrix of one axis, T[p][i_out][j_in], for an input axis and
+// arbitrary output coordinates (host array of n_out values).
+int build_axis_matrix(const Axis &in, const double *out_points, int n_out, const double *d_tp,
+                      int P, double *d_T, cudaStream_t s);
+
 // mixed-precision path (op3d_mixed.cu)
 int mixed_setup(dage_op3d *op);
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s);

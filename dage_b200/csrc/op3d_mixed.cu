@@ -192,7 +192,8 @@ struct StageArgs {
   double *V;
   int accumulate;
   int *err;
-  long long wait_limit;
+  long long wait_limit;   // normal waits (dage_set_wait_limit)
+  long long drain_limit;  // waits for in-flight copies/MMAs after a timeout
 };
 
 template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (*abort_flag) {
         // let every copy that was issued land before the CTA goes away
         for (int i = 0; i < NS; ++i)
-          if (issued[i]) mbar_wait(full(i), issued_ph[i], a.wait_limit);
+          if (issued[i]) mbar_wait(full(i), issued_ph[i], a.drain_limit);
       }
     }
   } else if (warp == 1) {
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       // every MMA this thread issued has completed once `drain` fires
       umma_commit(drain);
-      mbar_wait(drain, 0, a.wait_limit);
+      mbar_wait(drain, 0, a.drain_limit);
     }
   } else {
     // ------------------------------------------------------------ epilogue
@@ -582,6 +583,7 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
   StageArgs base{};
   base.err = st.err.as<int>();
   base.wait_limit = g_wait_limit;
+  base.drain_limit = 4000000000LL;  // ~2 s: copies and MMAs in flight always finish
   const int ni[3] = {nix, niy, niz}, no[3] = {nox, noy, noz};
   const long long M[3] = {(long long)niy * niz, (long long)niz * nox, (long long)nox * noy};
   const int d0[3] = {niy, niz, 0}, d1[3] = {niz, nox, 0};

@@ -291,3 +291,126 @@ def integrate(grid: Grid3D, f1, f2=None) -> float:
 
 
 dot = integrate
+
+
+class GBFMMCoulomb3D:
+    """GBFMMCoulomb3D (src/gbfmm/gbfmm_coulomb3d.F90:331-819), FP64: near
+    field by per-box sub-operators, far field by multipoles (lmax) and M2L,
+    2^maxlevel boxes per axis.  The near-field quadrature defaults to the
+    reference's GaussQuad(25, 25)."""
+
+    def __init__(self, grid: Grid3D, lmax: int = 12, maxlevel: int = 2,
+                 quad: GaussQuad | None = None):
+        lib = load()
+        self.grid = grid
+        self.lmax = lmax
+        self.maxlevel = maxlevel
+        self.quad = quad if quad is not None else GaussQuad(25, 25)
+        self._keep = (grid.c(), self.quad.c())
+        h = ctypes.c_void_p()
+        check(lib.dage_gbfmm_create(self._keep[0], maxlevel, lmax, ctypes.byref(self._keep[1]),
+                                    _capi.DAGE_FP64, ctypes.byref(h)))
+        self._h = h
+        nb, nlm = ctypes.c_int(), ctypes.c_int()
+        check(lib.dage_gbfmm_box_count(h, ctypes.byref(nb), ctypes.byref(nlm)))
+        self.nbox, self.nlm = nb.value, nlm.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                load().dage_gbfmm_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def apply(self, rho, out=None, energy: bool = False):
+        n = int(np.prod(self.grid.shape))
+        rp, rdev = _ptr(rho, n)
+        if out is None:
+            if rdev:
+                import torch
+
+                out = torch.zeros(self.grid.shape[::-1], dtype=torch.float64, device=rho.device)
+            else:
+                out = np.zeros(self.grid.shape, order="F")
+        vp, vdev = _ptr(out, n)
+        if rdev != vdev:
+            raise ValueError("rho and out must both be host or both be device cubes")
+        flags = (_capi.DAGE_DEVICE_PTRS if rdev else 0) | (_capi.DAGE_ENERGY if energy else 0)
+        e = ctypes.c_double(0.0)
+        check(load().dage_gbfmm_apply(self._h, rp, vp, flags, ctypes.byref(e)))
+        return (out, e.value) if energy else out
+
+    __call__ = apply
+
+    def multipole_moments(self, rho) -> np.ndarray:
+        """(N_lm, nbox) moments, boxes in the reference's octree order."""
+        n = int(np.prod(self.grid.shape))
+        rp, rdev = _ptr(rho, n)
+        q = np.zeros((self.nlm, self.nbox), order="F")
+        check(load().dage_gbfmm_multipole_moments(
+            self._h, rp, _capi.DAGE_DEVICE_PTRS if rdev else 0,
+            q.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return q
+
+    def local_expansions(self) -> np.ndarray:
+        L = np.zeros((self.nlm, self.nbox), order="F")
+        check(load().dage_gbfmm_local_expansions(self._h,
+                                                 L.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return L
+
+    def evaluate_local_expansions(self, L, V):
+        """V += far-field potential of the local expansions L (N_lm, nbox)."""
+        L = np.asfortranarray(L, dtype=np.float64)
+        n = int(np.prod(self.grid.shape))
+        vp, vdev = _ptr(V, n)
+        check(load().dage_gbfmm_evaluate_le(self._h, L.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            vp, _capi.DAGE_DEVICE_PTRS if vdev else 0))
+        return V
+
+    @property
+    def last_time_ms(self) -> float:
+        v = ctypes.c_float()
+        check(load().dage_gbfmm_last_time_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+
+class Bubbles:
+    """Atom-centred radial functions times real spherical harmonics
+    (Bubbles, src/bubbles/bubbles.F90), uploaded once for GPU injection into
+    cubes (Function3D_inject_bubbles, function3d.F90:1757-1787)."""
+
+    def __init__(self, centers, radial_grids, f, lmax: int, k: int = 0):
+        lib = load()
+        c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+        self.natom = len(c)
+        self.lmax = lmax
+        self._grids = list(radial_grids)
+        arr = (DageGrid1D * self.natom)(*[gr.c() for gr in self._grids])
+        ff = np.ascontiguousarray(np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1) for a in f]))
+        h = ctypes.c_void_p()
+        dp = ctypes.POINTER(ctypes.c_double)
+        check(lib.dage_bubbles_create(self.natom, c.ctypes.data_as(dp), arr, lmax, k,
+                                      ff.ctypes.data_as(dp), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                load().dage_bubbles_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def inject(self, grid: Grid3D, cube=None, lmin: int = 0, factor: float = 1.0):
+        """cube += factor * bubbles at the grid points; returns the cube."""
+        n = int(np.prod(grid.shape))
+        if cube is None:
+            cube = np.zeros(grid.shape, order="F")
+        p, dev = _ptr(cube, n)
+        g = grid.c()
+        check(load().dage_bubbles_inject(self._h, g, lmin, float(factor), p,
+                                         _capi.DAGE_DEVICE_PTRS if dev else 0))
+        return cube

@@ -130,6 +130,77 @@ int dage_op3d_get_timing(const dage_op3d *op, int kind, long long *launches, dou
 int dage_op3d_destroy(dage_op3d *op);
 
 /* ---------------------------------------------------------------------------
+ * GBFMM Coulomb operator (GBFMMCoulomb3D, FP64)
+ * ------------------------------------------------------------------------ */
+typedef struct dage_gbfmm dage_gbfmm;
+
+/* Builds the operator for a grid split into 2^maxlevel boxes per axis:
+ * near-field sub-operator matrices (quadrature `quad`, the reference's
+ * default for the near field is GaussQuad(25, 25)), box geometry, local
+ * far-field lists and the M2L matrices of all box displacements, on the GPU.
+ * maxlevel must be 2 (the reference default: 4x4x4 boxes, whose local far
+ * field needs no M2M/L2L); lmax <= 15; precision must be DAGE_FP64.  Boxes take ncell/2^maxlevel
+ * cells per axis; when that does not divide, the first ncell mod 2^maxlevel
+ * boxes along the axis take one cell more.
+ * Replaces GBFMMCoulomb3D_init + init_nearfield + init_interaction_matrices
+ * and gbfmmcoulomb3d_init_cuda (src/gbfmm/gbfmm_coulomb3d.F90:331-508,
+ * 1313-1438; src/gbfmm/gbfmm_coulomb3d.cu:583-600). */
+int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const dage_quad *quad,
+                      int precision, dage_gbfmm **g);
+
+/* V = near field + far field (multipoles -> M2L -> L2P), every point taking
+ * the contributions of the box that owns it; optional LIP-weighted energy.
+ * Replaces GBFMMCoulomb3D_calculate_potential's CUDA path
+ * (src/gbfmm/gbfmm_coulomb3d.F90:650-819). */
+int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags,
+                     double *energy);
+
+/* Multipole moments of every box, host array (N_lm, nbox) column-major with
+ * lm = l(l+1)+m and boxes in the reference's octree order.  Replaces
+ * gbfmmcoulomb3d_calculate_multipole_moments_cuda + _download_multipole_
+ * moments_cuda (src/gbfmm/gbfmm_coulomb3d.cu:620-640). */
+int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flags,
+                                 double *moments);
+
+/* Local expansions (N_lm, nbox) of the last apply (the far-field potential
+ * coefficients, GBFMMFunction3D%farfield_potential). */
+int dage_gbfmm_local_expansions(dage_gbfmm *g, double *L);
+
+/* V += sum_lm L_lm S_lm(r - c_box) over every box's points for host local
+ * expansions (N_lm, nbox).  Replaces gbfmmcoulomb3d_evaluate_potential_le_cuda
+ * (src/gbfmm/gbfmm_coulomb3d.cu:641-660). */
+int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double *V,
+                           unsigned flags);
+
+int dage_gbfmm_box_count(const dage_gbfmm *g, int *nbox, int *nlm);
+int dage_gbfmm_set_stream(dage_gbfmm *g, void *stream);
+int dage_gbfmm_last_time_ms(const dage_gbfmm *g, float *ms);
+int dage_gbfmm_destroy(dage_gbfmm *g);
+
+/* ---------------------------------------------------------------------------
+ * Bubbles -> cube injection
+ * ------------------------------------------------------------------------ */
+typedef struct dage_bubbles dage_bubbles;
+
+/* Uploads a bubble set: natom centres (3*natom), one radial LIP grid per atom
+ * (equidistant-point cells starting at r = 0; any cell steps), lmax <= 12,
+ * the r^k exponent k >= 0, and the radial values f: per atom (lmax+1)^2 rows
+ * (lm = l(l+1)+m) of that atom's grid points, atoms concatenated.  The LIP
+ * values are turned into per-cell monomial coefficients on the GPU.
+ * Replaces bubbles_init_cuda / bubble_init_cuda / bubble_upload_all_cuda
+ * (src/bubbles/bubbles_cuda.cu:3716-3770). */
+int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *radial, int lmax,
+                        int k, const double *f, dage_bubbles **b);
+
+/* cube += factor * sum_atoms sum_{l >= lmin} [r^k f_lm](|r-R|) Y_lm(r-R) at
+ * every point of `grid` (Y_lm: Racah-normalised real spherical harmonics).
+ * Replaces bubbles_inject_cuda / Bubbles::inject
+ * (src/bubbles/bubbles_cuda.cu:3090-3350, 3774-3776). */
+int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, double factor,
+                        double *cube, unsigned flags);
+int dage_bubbles_destroy(dage_bubbles *b);
+
+/* ---------------------------------------------------------------------------
  * Integration (Function3D_integrate / Function3D_dot_product cube part)
  * ------------------------------------------------------------------------ */
 

@@ -126,6 +126,16 @@ int orc_box_multipoles(int lmax, int nx, const double *px, const double *wx, int
 int orc_l2p(int lmax, const double *L, const double *center, int nx, const double *px, int ny,
             const double *py, int nz, const double *pz, double *out);
 
+/* ---- bubbles -> cube injection (src/bubbles/bubbles.F90:1904-1975) ------ */
+/* cube += factor * sum_atoms sum_{l >= lmin} [r^k f_lm](|r - R|) Y_lm.
+ * Atom a: radial grid of ncell[a] equidistant-LIP cells starting at r = 0
+ * (cell_scales concatenated over atoms); f: per atom (lmax+1)^2 rows of the
+ * radial grid's points, atoms concatenated. */
+int orc_bubbles_inject(int natom, const double *centers, const int *ncell,
+                       const double *cell_scales, int nlip, int lmax, int lmin, int k,
+                       const double *f, int nx, const double *x, int ny, const double *y,
+                       int nz, const double *z, double factor, double *cube);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,8 @@ def lib(libm_1ulp: bool = False):
             "orc_local_farfield": (_I, [_I, _I, ctypes.POINTER(_I)]),
             "orc_box_multipoles": (_I, [_I, _I, _D, _D, _I, _D, _D, _I, _D, _D, _D, _D, _D]),
             "orc_l2p": (_I, [_I, _D, _D, _I, _D, _I, _D, _I, _D, _D]),
+            "orc_bubbles_inject": (_I, [_I, _D, ctypes.POINTER(_I), _D, _I, _I, _I, _I, _D, _I, _D,
+                                        _I, _D, _I, _D, _F, _D]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -453,36 +455,53 @@ def subgrid(g1: Grid1D, c0: int, c1: int) -> Grid1D:
 class GBFMMPlan:
     """Octree box bookkeeping of GBFMMParallelInfo / GBFMMCoulomb3D for one
     grid (src/gbfmm/gbfmm_parallel_info.F90, gbfmm_coulomb3d.F90:417-508):
-    boxes at `maxlevel` (2^maxlevel per axis) of ncell // 2^maxlevel cells
-    (integer division, as the reference), near-field cell ranges (box plus
-    its nearest neighbours), local far-field lists and the points each box
-    owns (its last point per axis belongs to the next box unless it is the
-    grid's last point)."""
+    boxes at `maxlevel` (2^maxlevel per axis), near-field cell ranges (box
+    plus its nearest neighbours), local far-field lists and the points each
+    box owns (its last point per axis belongs to the next box unless it is
+    the grid's last point).
+
+    Cells per box: ncell // 2^maxlevel, as the reference's integer division
+    (gbfmm_parallel_info.F90:1072-1084) when it divides evenly.  When it does
+    not, the reference leaves the trailing cells in no box; the policy shared
+    by this oracle and the GPU code gives the first (ncell mod 2^maxlevel)
+    boxes along the axis one extra cell and centres each box on the midpoint
+    of its points."""
 
     def __init__(self, grid: Grid3D, maxlevel: int = 2):
         self.grid = grid
         self.level = maxlevel
         self.nb = 2 ** maxlevel
         self.nbox = self.nb ** 3
-        self.bs = [a.ncell // self.nb for a in grid.axes]
         self.ranges = [(a.points[0], a.points[-1]) for a in grid.axes]
         self.vec = [box_vector(i, maxlevel) for i in range(1, self.nbox + 1)]
 
+    def _axis_cells(self, d, v):
+        """1-based (first, last) cell of box position v along axis d."""
+        nc = self.grid.axes[d].ncell
+        base, rem = divmod(nc, self.nb)
+        c0 = v * base + min(v, rem)
+        return c0 + 1, c0 + base + (1 if v < rem else 0)
+
     def cells(self, ibox):
         v = self.vec[ibox - 1]
-        return [(v[d] * self.bs[d] + 1, v[d] * self.bs[d] + self.bs[d]) for d in range(3)]
+        return [self._axis_cells(d, v[d]) for d in range(3)]
 
     def near_cells(self, ibox):
-        lim = self.cells(ibox)
-        for j in nearest_neighbors(ibox, self.level):
-            lj = self.cells(j)
-            lim = [(min(lim[d][0], lj[d][0]), max(lim[d][1], lj[d][1])) for d in range(3)]
-        return lim
+        v = self.vec[ibox - 1]
+        return [(self._axis_cells(d, max(v[d] - 1, 0))[0],
+                 self._axis_cells(d, min(v[d] + 1, self.nb - 1))[1]) for d in range(3)]
 
     def center(self, ibox):
         v = self.vec[ibox - 1]
-        return np.array([self.ranges[d][0] + (v[d] + 0.5) * (self.ranges[d][1] - self.ranges[d][0]) / self.nb
-                         for d in range(3)])
+        c = np.zeros(3)
+        for d in range(3):
+            a = self.grid.axes[d]
+            if a.ncell % self.nb == 0:  # gbfmm_parallel_info.F90:1290-1299
+                c[d] = self.ranges[d][0] + (v[d] + 0.5) * ((self.ranges[d][1] - self.ranges[d][0]) / self.nb)
+            else:
+                (p0, p1) = self.points(ibox)[d]
+                c[d] = 0.5 * (a.points[p0] + a.points[p1 - 1])
+        return c
 
     def points(self, ibox):
         """0-based point index range [p0, p1) per axis of the box's sub-grid."""
@@ -497,7 +516,7 @@ class GBFMMPlan:
 
 
 def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
-                return_parts=False):
+                return_parts=False, libm_1ulp=False):
     """GBFMMCoulomb3D_calculate_potential along the reference's CUDA path
     (gbfmm_coulomb3d.F90:650-819, gbfmm_coulomb3d.cu:478-573): multipoles per
     box, M2L over the local far field, near field by the sub-operator of
@@ -527,7 +546,7 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
         gin = [subgrid(a, c0, c1) for a, (c0, c1) in zip(grid.axes, ncl)]
         own = plan.owned(b)
         outs = [grid.axes[d].points[own[d][0]:own[d][1]] for d in range(3)]
-        Ts = [coulomb_matrix(gin[d], outs[d], tp) for d in range(3)]
+        Ts = [coulomb_matrix(gin[d], outs[d], tp, libm_1ulp=libm_1ulp) for d in range(3)]
         pin = [((c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1) + 1) for a, (c0, c1) in zip(grid.axes, ncl)]
         sub = np.asfortranarray(rho[pin[0][0]:pin[0][1], pin[1][0]:pin[1][1], pin[2][0]:pin[2][1]])
         vn = transform_cube(*Ts, w, sub, 0.0)
@@ -539,3 +558,32 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
     if return_parts:
         return V, q, L, Vnear
     return V
+
+
+# ---------------------------------------------------------------------------
+# Bubbles
+# ---------------------------------------------------------------------------
+def bubbles_inject(centers, ncells, cell_scales, lmax, f, grid: Grid3D, lmin=0, k=0,
+                   factor=1.0, cube=None, nlip=7):
+    """cube += factor * sum of the atom-centred bubbles (Bubbles_eval_pick,
+    bubbles.F90:1904-1975).  f: list over atoms of ((lmax+1)^2, npoints)."""
+    centers = _f64(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+    nc = (ctypes.c_int * len(ncells))(*ncells)
+    cs = _f64(np.concatenate([np.asarray(c, dtype=np.float64) for c in cell_scales]))
+    ff = _f64(np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1) for a in f]))
+    if cube is None:
+        cube = np.zeros(grid.shape, order="F")
+    gx, gy, gz = grid.axes
+    rc = lib().orc_bubbles_inject(len(ncells), _p(centers), nc, _p(cs), nlip, lmax, lmin, k,
+                                  _p(ff), gx.n, _p(gx.points), gy.n, _p(gy.points), gz.n,
+                                  _p(gz.points), float(factor), _p(cube))
+    if rc:
+        raise ValueError("bad bubbles input")
+    return cube
+
+
+def log_radial_grid(ncell=33, r0=1e-5, r1=15.0, nlip=7):
+    """Cell steps of a radial LIP grid from r = 0 whose cell ends are
+    log-spaced on [r0, r1] (ncell cells, ncell*(nlip-1)+1 points)."""
+    edges = np.concatenate([[0.0], r0 * (r1 / r0) ** (np.arange(ncell) / (ncell - 1))])
+    return np.diff(edges) / (nlip - 1)

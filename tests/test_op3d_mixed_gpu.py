@@ -85,4 +85,4 @@ def test_mixed_device_pointers(dage, oracle):
     op = dage.Coulomb3D(g, quad=q, precision="bf16x6")
     Vh = op.apply(rho)
     Vd = op.apply(torch.from_numpy(rho.reshape(-1, order="F").copy()).cuda())
-    np.testing.assert_array_equal(Vd.cpu().numpy(), Vh.reshape(-1, order="F"))
+    np.testing.assert_array_equal(Vd.cpu().numpy().reshape(-1), Vh.reshape(-1, order="F"))
