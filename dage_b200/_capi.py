@@ -80,6 +80,8 @@ SIGNATURES = {
                                            ctypes.c_double, _VP, ctypes.c_uint]),
     "dage_bubbles_destroy": (ctypes.c_int, [_VP]),
     "dage_integrate": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, ctypes.c_uint, _D]),
+    "dage_op3d_apply_fp64_noalloc": (ctypes.c_int, [ctypes.c_int] * 7 + [_VP, _VP, _VP, _D, _VP,
+                                                                       _VP, _VP]),
     "dage_last_error": (ctypes.c_char_p, []),
     "dage_abi_version": (ctypes.c_int, []),
     "dage_set_wait_limit": (ctypes.c_int, [ctypes.c_longlong]),

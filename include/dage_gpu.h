@@ -212,6 +212,29 @@ int dage_integrate(const dage_grid1d grid[3], const double *f1, const double *f2
                    unsigned flags, double *out);
 
 /* ---------------------------------------------------------------------------
+ * Allocation-free FP64 apply
+ * ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory around an operator call (a caching allocator or fixed pool owns the
+ * free memory, or the loop must not hit cudaFree, which synchronises the
+ * device): V = sum_p w[p] (Tx_p (x) Ty_p (x) Tz_p) rho in FP64 (no coda),
+ * allocating nothing.  All pointers except w are device pointers on the
+ * current device: Tx/Ty/Tz hold P matrices laid out T[p][i_out][j_in]
+ * (j_in fastest), rho is nix*niy*niz and V nox*noy*noz (x fastest); w holds
+ * P host weights; stream may be NULL.  The two intermediate cubes live in one
+ * fixed device array of 4 Mi doubles (32 MiB) that every GPU loading the
+ * library keeps until exit: niy*niz*nox + niz*nox*noy must not exceed it, or
+ * the call fails with DAGE_E_INVALID.  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress), so make it before any
+ * stream capture.  Every call shares the array: calls that overlap on the
+ * GPU race.  The array needs no clearing (each call overwrites what it
+ * reads), and V is overwritten. */
+int dage_op3d_apply_fp64_noalloc(int nix, int niy, int niz, int nox, int noy, int noz, int P,
+                                 const double *Tx, const double *Ty, const double *Tz,
+                                 const double *w, const double *rho, double *V, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Library
  * ------------------------------------------------------------------------ */
 const char *dage_last_error(void);
