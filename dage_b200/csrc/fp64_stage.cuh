@@ -1,0 +1,67 @@
+// fp64_stage.cuh -- FP64 contraction stage on the FP64 tensor path (DMMA,
+// mma.sync m8n8k4 f64), shared by the cube operator and the GBFMM near field.
+//
+//   out[o(R, n)] (= or +=) alpha * sum_K X[a(R) + K] * T[n * ldt + K]
+//   a(R)    = (R % a_d0) a_s1 + (R / a_d0) a_s2
+//   o(R, n) = (R % o_d0) o_s1 + (R / o_d0) o_s2 + n o_sn
+//
+// One descriptor describes one independent contraction (a whole cube stage,
+// or one GBFMM box); a launch covers any number of them (grid.z).  Tiles are
+// 128 x 128 per 256-thread block, 64 x 32 per warp (8 x 4 MMA tiles of
+// 8 x 8), K in steps of 16 through a 3-deep cp.async ring.  Rows of both
+// operands are K-contiguous but only 8-byte aligned, so the copies are
+// 8 bytes wide; shared rows are padded to 20 doubles, which keeps the
+// fragment loads free of bank conflicts.  An optional per-n-tile K range
+// (first, last index) limits the K loop to the band of the matrix (entries
+// outside it are below 2^-64 of their row's scale).  With accumulation each
+// output element gets one correctly rounded FP64 add (an L2 reduction; one
+// writer per element per launch).
+#pragma once
+
+#include "common.cuh"
+
+namespace dage {
+
+struct StageDesc {
+  const double *X;
+  long long a_d0, a_s1, a_s2;
+  const double *T;
+  long long ldt;
+  double *out;
+  long long o_d0, o_s1, o_s2, o_sn;
+  int M, N, K;
+  const int2 *krange;  // per 128-column tile: K band [first, last], or null
+};
+
+constexpr int kFp64TileM = 128, kFp64TileN = 128;
+
+// Contiguous cube stage: X[R * ldx + K], out[R + n * M].
+inline StageDesc cube_stage(const double *X, long long ldx, int M, int N, int K, const double *T,
+                            long long ldt, double *out, const int2 *krange) {
+  StageDesc d{};
+  d.X = X;
+  d.a_d0 = M;
+  d.a_s1 = ldx;
+  d.a_s2 = 0;
+  d.T = T;
+  d.ldt = ldt;
+  d.out = out;
+  d.o_d0 = M;
+  d.o_s1 = 1;
+  d.o_s2 = 0;
+  d.o_sn = M;
+  d.M = M;
+  d.N = N;
+  d.K = K;
+  d.krange = krange;
+  return d;
+}
+
+// One contraction given by value.
+int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s);
+// ndesc contractions from a device array; mtiles/ntiles bound the tile
+// counts of every descriptor.
+int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ntiles, double alpha,
+                       bool accumulate, cudaStream_t s);
+
+}  // namespace dage

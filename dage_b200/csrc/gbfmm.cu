@@ -28,6 +28,7 @@
 #include <map>
 #include <vector>
 
+#include "fp64_stage.cuh"
 #include "op3d.cuh"
 
 struct dage_gbfmm;
@@ -228,111 +229,6 @@ __global__ void l2p_kernel(const double *__restrict__ L, const BoxInfo *__restri
     solid_harmonics(lmax, xs[gx] - b.c[0], xs[xstride + gy] - b.c[1], xs[2 * xstride + gz] - b.c[2],
                     [&](int lm, double s) { v += Ls[lm] * s; });
     V[(size_t)gx + (size_t)Nx * gy + (size_t)Nx * Ny * gz] += v;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Batched FP64 contraction stage over boxes (one descriptor per box):
-//   out[o(R, n)] (= or +=) alpha * sum_K X[a(R) + K] * T[n*ldt + K]
-//   a(R) = (R % a_d0) a_s1 + (R / a_d0) a_s2
-//   o(R, n) = (R % o_d0) o_s1 + (R / o_d0) o_s2 + n o_sn
-// ---------------------------------------------------------------------------
-struct StageDesc {
-  const double *X;
-  long long a_d0, a_s1, a_s2;
-  const double *T;
-  long long ldt;
-  double *out;
-  long long o_d0, o_s1, o_s2, o_sn;
-  int M, N, K;
-};
-
-constexpr int BM = 128, BN = 64, BK = 8, PAD = 2;
-
-template <bool ACCUM>
-__global__ void __launch_bounds__(256) stage_fp64_batched_kernel(const StageDesc *__restrict__ descs,
-                                                                 double alpha) {
-  __shared__ __align__(16) double As[2][BK][BM + PAD];
-  __shared__ __align__(16) double Bs[2][BK][BN + PAD];
-  const StageDesc d = descs[blockIdx.z];
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  if (m0 >= d.M || n0 >= d.N) return;
-  const int tid = threadIdx.x;
-  const int tx = tid & 31, ty = tid >> 5;  // tx -> rows (4 each), ty -> columns (8 each)
-  double ra[4], rb[2];
-  auto arow = [&](long long R) { return (R % d.a_d0) * d.a_s1 + (R / d.a_d0) * d.a_s2; };
-  auto gload = [&](int k0) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
-      const int m = m0 + r, k = k0 + kk;
-      ra[i] = (m < d.M && k < d.K) ? __ldg(d.X + arow(m) + k) : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
-      const int n = n0 + r, k = k0 + kk;
-      rb[i] = (n < d.N && k < d.K) ? __ldg(d.T + (size_t)n * d.ldt + k) : 0.0;
-    }
-  };
-  auto sstore = [&](int buf) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int e = tid + 256 * i;
-      As[buf][e & 7][e >> 3] = ra[i];
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int e = tid + 256 * i;
-      Bs[buf][e & 7][e >> 3] = rb[i];
-    }
-  };
-  double acc[4][8];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-  const int nk = (d.K + BK - 1) / BK;
-  gload(0);
-  sstore(0);
-  __syncthreads();
-  for (int kt = 0; kt < nk; ++kt) {
-    const int cur = kt & 1;
-    if (kt + 1 < nk) gload((kt + 1) * BK);
-#pragma unroll
-    for (int k = 0; k < BK; ++k) {
-      const double2 *ap = reinterpret_cast<const double2 *>(&As[cur][k][0]);
-      const double2 *bp = reinterpret_cast<const double2 *>(&Bs[cur][k][0]);
-      const double2 a0 = ap[tx * 2], a1 = ap[tx * 2 + 1];
-      const double a[4] = {a0.x, a0.y, a1.x, a1.y};
-      double b[8];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const double2 t = bp[ty * 4 + j];
-        b[2 * j] = t.x;
-        b[2 * j + 1] = t.y;
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    if (kt + 1 < nk) {
-      sstore(cur ^ 1);
-      __syncthreads();
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int n = n0 + ty * 8 + j;
-    if (n >= d.N) continue;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const long long m = m0 + tx * 4 + i;
-      if (m >= d.M) continue;
-      double *o = d.out + (m % d.o_d0) * d.o_s1 + (m / d.o_d0) * d.o_s2 + (long long)n * d.o_sn;
-      *o = ACCUM ? *o + alpha * acc[i][j] : alpha * acc[i][j];
-    }
   }
 }
 
@@ -837,27 +733,21 @@ int gbfmm_l2p(dage_gbfmm *g, const double *d_L, double *V) {
 int gbfmm_nearfield(dage_gbfmm *g) {
   cudaStream_t s = g->stream;
   int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
+  const int TM = kFp64TileM, TN = kFp64TileN;
   for (const auto &B : g->boxes) {
-    mt[0] = std::max(mt[0], ceil_div((long long)B.nq[1] * B.nq[2], BM));
-    nt[0] = std::max(nt[0], ceil_div(B.own[0], BN));
-    mt[1] = std::max(mt[1], ceil_div((long long)B.nq[2] * B.own[0], BM));
-    nt[1] = std::max(nt[1], ceil_div(B.own[1], BN));
-    mt[2] = std::max(mt[2], ceil_div((long long)B.own[0] * B.own[1], BM));
-    nt[2] = std::max(nt[2], ceil_div(B.own[2], BN));
+    mt[0] = std::max(mt[0], ceil_div((long long)B.nq[1] * B.nq[2], TM));
+    nt[0] = std::max(nt[0], ceil_div(B.own[0], TN));
+    mt[1] = std::max(mt[1], ceil_div((long long)B.nq[2] * B.own[0], TM));
+    nt[1] = std::max(nt[1], ceil_div(B.own[1], TN));
+    mt[2] = std::max(mt[2], ceil_div((long long)B.own[0] * B.own[1], TM));
+    nt[2] = std::max(nt[2], ceil_div(B.own[2], TN));
   }
-  for (int p = 0; p < g->P; ++p) {
+  for (int p = 0; p < g->P; ++p)
     for (int st = 0; st < 3; ++st) {
       const StageDesc *d = g->d_desc[st].as<StageDesc>() + (size_t)p * g->nbox;
-      dim3 grid(mt[st], nt[st], g->nbox);
-      if (st < 2)
-        stage_fp64_batched_kernel<false><<<grid, 256, 0, s>>>(d, 1.0);
-      else if (p == 0)
-        stage_fp64_batched_kernel<false><<<grid, 256, 0, s>>>(d, g->w[p]);
-      else
-        stage_fp64_batched_kernel<true><<<grid, 256, 0, s>>>(d, g->w[p]);
-      DAGE_CUDA_TRY(cudaGetLastError());
+      const double alpha = st < 2 ? 1.0 : g->w[p];
+      DAGE_TRY(launch_fp64_stages(d, g->nbox, mt[st], nt[st], alpha, st == 2 && p > 0, s));
     }
-  }
   return 0;
 }
 

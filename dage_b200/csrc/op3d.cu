@@ -18,6 +18,7 @@
 #include <cstring>
 
 #include "expo.cuh"
+#include "fp64_stage.cuh"
 #include "op3d.cuh"
 
 namespace dage {
@@ -137,93 +138,173 @@ int launch_tmatrix(const TmatArgs &a, int nlip, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------
-// FP64 stage GEMM: 128x128 output tile per 256-thread block, 8x8 register
-// micro-tile per thread, K in steps of 8 with register-staged double
-// buffering through shared memory.
+// FP64 contraction stage (fp64_stage.cuh) on DMMA
 // ---------------------------------------------------------------------------
-constexpr int BM = 128, BN = 128, BK = 8, PAD = 2;
+constexpr int BM = kFp64TileM, BN = kFp64TileN, BK = 16, SROW = BK + 4, NST = 3;
+constexpr int kStageSmem = NST * (BM + BN) * SROW * (int)sizeof(double);
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gmem),
+               "r"(pred ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// D(8x8) += A(8x4, row) B(4x8, col); lane l holds A[l/4][l%4], B[l%4][l/4]
+// and D[l/4][2(l%4) + {0,1}]
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
 
 template <bool ACCUM>
-__global__ void __launch_bounds__(256) stage_fp64_kernel(const double *__restrict__ X,
-                                                         long long ldx, int M, int N, int K,
-                                                         const double *__restrict__ T,
-                                                         long long ldt, double *__restrict__ out,
-                                                         double alpha) {
-  __shared__ __align__(16) double As[2][BK][BM + PAD];
-  __shared__ __align__(16) double Bs[2][BK][BN + PAD];
-  const int tid = threadIdx.x;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int tx = tid & 15, ty = tid >> 4;  // tx -> rows (R), ty -> columns (n)
+__device__ __forceinline__ void stage_tile(const StageDesc &d, double alpha, int m0, int n0) {
+  extern __shared__ double fsm[];
+  double *As = fsm;                    // [NST][BM][SROW]
+  double *Bs = fsm + NST * BM * SROW;  // [NST][BN][SROW]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  int kt0 = 0, kt1 = (d.K + BK - 1) / BK - 1;
+  if (d.krange) {
+    const int2 r = d.krange[n0 / BN];
+    kt0 = r.x / BK;
+    kt1 = r.y / BK;
+  }
+  const int nk = kt1 - kt0 + 1;
 
-  double ra[4], rb[4];
-  auto gload = [&](int k0) {
+  // this thread copies rows (tid >> 4) + 16 i at K offset tid & 15
+  const int kk = tid & 15;
+  const double *arow[8];
+  const double *brow[8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
-      const int m = m0 + r, n = n0 + r, k = k0 + kk;
-      ra[i] = (m < M && k < K) ? __ldg(X + (size_t)m * ldx + k) : 0.0;
-      rb[i] = (n < N && k < K) ? __ldg(T + (size_t)n * ldt + k) : 0.0;
+  for (int i = 0; i < 8; ++i) {
+    const long long m = m0 + (tid >> 4) + 16 * i;
+    const int n = n0 + (tid >> 4) + 16 * i;
+    arow[i] = m < d.M ? d.X + (m % d.a_d0) * d.a_s1 + (m / d.a_d0) * d.a_s2 : nullptr;
+    brow[i] = n < d.N ? d.T + (size_t)n * d.ldt : nullptr;
+  }
+  auto load = [&](int slot, int kt) {
+    const int k = kt * BK + kk;
+    double *as = As + slot * BM * SROW + (tid >> 4) * SROW + kk;
+    double *bs = Bs + slot * BN * SROW + (tid >> 4) * SROW + kk;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const bool pa = arow[i] && k < d.K, pb = brow[i] && k < d.K;
+      cp_async8(as + 16 * i * SROW, pa ? arow[i] + k : d.X, pa);
+      cp_async8(bs + 16 * i * SROW, pb ? brow[i] + k : d.T, pb);
     }
   };
-  auto sstore = [&](int buf) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int e = tid + 256 * i, r = e >> 3, kk = e & 7;
-      As[buf][kk][r] = ra[i];
-      Bs[buf][kk][r] = rb[i];
-    }
-  };
 
-  double acc[8][8];
+  double acc[8][4][2];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  const int nk = (K + BK - 1) / BK;
-  gload(0);
-  sstore(0);
+#pragma unroll
+  for (int st = 0; st < NST - 1; ++st) {
+    if (st < nk) load(st, kt0 + st);
+    cp_async_commit();
+  }
+  for (int i = 0; i < nk; ++i) {
+    cp_async_wait<NST - 2>();
+    __syncthreads();  // slot i landed for all threads; slot i-1 is free
+    if (i + NST - 1 < nk) load((i + NST - 1) % NST, kt0 + i + NST - 1);
+    cp_async_commit();
+    const double *as = As + (i % NST) * BM * SROW + (wm + (lane >> 2)) * SROW + (lane & 3);
+    const double *bs = Bs + (i % NST) * BN * SROW + (wn + (lane >> 2)) * SROW + (lane & 3);
+#pragma unroll
+    for (int ks = 0; ks < BK / 4; ++ks) {
+      double fa[8], fb[4];
+#pragma unroll
+      for (int mb = 0; mb < 8; ++mb) fa[mb] = as[mb * 8 * SROW + ks * 4];
+#pragma unroll
+      for (int nb = 0; nb < 4; ++nb) fb[nb] = bs[nb * 8 * SROW + ks * 4];
+#pragma unroll
+      for (int mb = 0; mb < 8; ++mb)
+#pragma unroll
+        for (int nb = 0; nb < 4; ++nb) dmma(acc[mb][nb], fa[mb], fb[nb]);
+    }
+  }
+  cp_async_wait<0>();
+
+#pragma unroll
+  for (int mb = 0; mb < 8; ++mb) {
+    const long long m = m0 + wm + mb * 8 + (lane >> 2);
+    if (m >= d.M) continue;
+    double *orow = d.out + (m % d.o_d0) * d.o_s1 + (m / d.o_d0) * d.o_s2;
+#pragma unroll
+    for (int nb = 0; nb < 4; ++nb)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int n = n0 + wn + nb * 8 + 2 * (lane & 3) + h;
+        if (n >= d.N) continue;
+        double *dst = orow + (long long)n * d.o_sn;
+        if (ACCUM)
+          atomicAdd(dst, alpha * acc[mb][nb][h]);
+        else
+          *dst = alpha * acc[mb][nb][h];
+      }
+  }
+}
+
+template <bool ACCUM>
+__global__ void __launch_bounds__(256, 1)
+    stage_fp64_kernel(const __grid_constant__ StageDesc d, double alpha) {
+  stage_tile<ACCUM>(d, alpha, blockIdx.x * BM, blockIdx.y * BN);
+}
+
+template <bool ACCUM>
+__global__ void __launch_bounds__(256, 1)
+    stage_fp64_batched_kernel(const StageDesc *__restrict__ descs, double alpha) {
+  const StageDesc d = descs[blockIdx.z];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (m0 >= d.M || n0 >= d.N) return;  // uniform across the block
+  stage_tile<ACCUM>(d, alpha, m0, n0);
+}
+
+// Band of each (t-point, 128-row tile) of an axis matrix T[p][n][K]: the
+// first and last K index holding an entry above 2^-64 of its row's scale
+// 2^ceil(log2 max_K |T(n, :)|).  One block per (p, tile), one warp per row.
+// Tiles of all-zero rows get [0, 0].
+__global__ void band_kernel(const double *__restrict__ T, int K, int N, int ntiles,
+                            int2 *range) {
+  const int p = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ int lo, hi;
+  if (threadIdx.x == 0) {
+    lo = K;
+    hi = -1;
+  }
   __syncthreads();
-  for (int kt = 0; kt < nk; ++kt) {
-    const int cur = kt & 1;
-    if (kt + 1 < nk) gload((kt + 1) * BK);
+  for (int rr = warp; rr < BN; rr += blockDim.x >> 5) {
+    const int n = tile * BN + rr;
+    if (n >= N) break;
+    const double *row = T + ((size_t)p * N + n) * K;
+    double m = 0.0;
+    for (int k = lane; k < K; k += 32) m = fmax(m, fabs(row[k]));
 #pragma unroll
-    for (int k = 0; k < BK; ++k) {
-      double a[8], b[8];
-      const double2 *ap = reinterpret_cast<const double2 *>(&As[cur][k][0]);
-      const double2 *bp = reinterpret_cast<const double2 *>(&Bs[cur][k][0]);
-      double2 t0 = ap[tx * 2], t1 = ap[tx * 2 + 1], t2 = ap[32 + tx * 2], t3 = ap[32 + tx * 2 + 1];
-      a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
-      a[4] = t2.x; a[5] = t2.y; a[6] = t3.x; a[7] = t3.y;
-      double2 u0 = bp[ty * 2], u1 = bp[ty * 2 + 1], u2 = bp[32 + ty * 2], u3 = bp[32 + ty * 2 + 1];
-      b[0] = u0.x; b[1] = u0.y; b[2] = u1.x; b[3] = u1.y;
-      b[4] = u2.x; b[5] = u2.y; b[6] = u3.x; b[7] = u3.y;
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    if (kt + 1 < nk) {
-      sstore(cur ^ 1);
-      __syncthreads();
-    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (m == 0.0) continue;
+    const double thr = ldexp(exp2(ceil(log2(m))), -64);
+    int mylo = K, myhi = -1;
+    for (int k = lane; k < K; k += 32)
+      if (fabs(row[k]) > thr) {
+        mylo = min(mylo, k);
+        myhi = max(myhi, k);
+      }
+    atomicMin(&lo, mylo);
+    atomicMax(&hi, myhi);
   }
-
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int n = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
-    if (n >= N) continue;
-    double *col = out + (size_t)n * M;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int m = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-      if (m >= M) continue;
-      if (ACCUM)
-        col[m] = col[m] + alpha * acc[i][j];
-      else
-        col[m] = alpha * acc[i][j];
-    }
-  }
+  __syncthreads();
+  if (threadIdx.x == 0) range[blockIdx.x] = hi < 0 ? make_int2(0, 0) : make_int2(lo, hi);
 }
 
 // ---------------------------------------------------------------------------
@@ -287,15 +368,57 @@ __global__ void sum_partials_kernel(const double *partials, int n, double *resul
 
 }  // namespace
 
+template <class Kern>
+int smem_attr(Kern kern, bool &done) {
+  if (!done) {
+    DAGE_CUDA_TRY(
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem));
+    done = true;
+  }
+  return 0;
+}
+
+int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s) {
+  dim3 grid(ceil_div(d.M, BM), ceil_div(d.N, BN));
+  if (grid.y > 65535) return fail(DAGE_E_UNSUPPORTED, "N=%d too large", d.N);
+  static bool done[2] = {false, false};
+  if (accumulate) {
+    DAGE_TRY(smem_attr(stage_fp64_kernel<true>, done[1]));
+    stage_fp64_kernel<true><<<grid, 256, kStageSmem, s>>>(d, alpha);
+  } else {
+    DAGE_TRY(smem_attr(stage_fp64_kernel<false>, done[0]));
+    stage_fp64_kernel<false><<<grid, 256, kStageSmem, s>>>(d, alpha);
+  }
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ntiles, double alpha,
+                       bool accumulate, cudaStream_t s) {
+  if (ndesc <= 0) return 0;
+  if (ntiles > 65535 || ndesc > 65535) return fail(DAGE_E_UNSUPPORTED, "batch too large");
+  dim3 grid(mtiles, ntiles, ndesc);
+  static bool done[2] = {false, false};
+  if (accumulate) {
+    DAGE_TRY(smem_attr(stage_fp64_batched_kernel<true>, done[1]));
+    stage_fp64_batched_kernel<true><<<grid, 256, kStageSmem, s>>>(d_descs, alpha);
+  } else {
+    DAGE_TRY(smem_attr(stage_fp64_batched_kernel<false>, done[0]));
+    stage_fp64_batched_kernel<false><<<grid, 256, kStageSmem, s>>>(d_descs, alpha);
+  }
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,
                       long long ldt, double *out, double alpha, bool accumulate,
-                      cudaStream_t s) {
-  dim3 grid(ceil_div(M, BM), ceil_div(N, BN));
-  if (grid.y > 65535) return fail(DAGE_E_UNSUPPORTED, "N=%d too large", N);
-  if (accumulate)
-    stage_fp64_kernel<true><<<grid, 256, 0, s>>>(X, ldx, M, N, K, T, ldt, out, alpha);
-  else
-    stage_fp64_kernel<false><<<grid, 256, 0, s>>>(X, ldx, M, N, K, T, ldt, out, alpha);
+                      cudaStream_t s, const int2 *krange) {
+  return launch_fp64_stage(cube_stage(X, ldx, M, N, K, T, ldt, out, krange), alpha, accumulate, s);
+}
+
+int launch_band(const double *T, int K, int N, int P, int2 *range, cudaStream_t s) {
+  const int ntiles = ceil_div(N, BN);
+  band_kernel<<<P * ntiles, 256, 0, s>>>(T, K, N, ntiles, range);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -399,6 +522,9 @@ static int build_matrices(dage_op3d *op) {
     DAGE_TRY(op->Tbuf[d].alloc(sizeof(double) * nT));
     DAGE_TRY(build_axis_matrix(ai, ao.points.data(), ao.n(), d_tp.as<double>(), op->P,
                                op->Tbuf[d].as<double>(), s));
+    DAGE_TRY(op->band[d].alloc(sizeof(int2) * (size_t)op->P * ceil_div(ao.n(), BN)));
+    DAGE_TRY(launch_band(op->Tbuf[d].as<double>(), ai.n(), ao.n(), op->P,
+                         op->band[d].as<int2>(), s));
   }
   d_tp.release();
   return 0;
@@ -461,6 +587,7 @@ static void destroy_impl(dage_op3d *op) {
   mixed_destroy(op);
   for (int d = 0; d < 3; ++d) {
     op->Tbuf[d].release();
+    op->band[d].release();
     op->wts[d].release();
   }
   op->d_w.release();
@@ -484,18 +611,21 @@ static int apply_fp64(dage_op3d *op, const double *rho, double *V, bool accumula
   DAGE_TRY(op->tmp2.alloc(sizeof(double) * (size_t)niz * nox * noy));
   double *U = op->tmp1.as<double>(), *W = op->tmp2.as<double>();
   const size_t sx = (size_t)nox * nix, sy = (size_t)noy * niy, sz = (size_t)noz * niz;
+  auto band = [&](int d, int p) {
+    return op->band[op->Towner[d]].as<int2>() + (size_t)p * ceil_div(op->nout[d], BN);
+  };
   for (int p = 0; p < op->P; ++p) {
     int t = op->tmark_begin(0);
     DAGE_TRY(launch_stage_fp64(rho, nix, niy * niz, nox, nix, op->T(0) + sx * p, nix, U, 1.0,
-                               false, s));
+                               false, s, band(0, p)));
     op->tmark_end(t);
     t = op->tmark_begin(0);
     DAGE_TRY(launch_stage_fp64(U, niy, niz * nox, noy, niy, op->T(1) + sy * p, niy, W, 1.0,
-                               false, s));
+                               false, s, band(1, p)));
     op->tmark_end(t);
     t = op->tmark_begin(0);
     DAGE_TRY(launch_stage_fp64(W, niz, nox * noy, noz, niz, op->T(2) + sz * p, niz, V,
-                               op->w[p], accumulate || p > 0, s));
+                               op->w[p], accumulate || p > 0, s, band(2, p)));
     op->tmark_end(t);
   }
   return 0;

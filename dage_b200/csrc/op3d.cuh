@@ -24,6 +24,9 @@ struct dage_op3d {
   // with identical input/output grids share one buffer (owner index).
   dage::DevBuf Tbuf[3];
   int Towner[3] = {0, 1, 2};
+  // per axis owner: K band (first, last index, inclusive) of each t-point's
+  // 128-row tiles, int2[P][ceil(n_out / 128)]
+  dage::DevBuf band[3];
   const double *T(int axis) const { return Tbuf[Towner[axis]].as<double>(); }
 
   // per-point LIP integration weights of the output grid (energy)
@@ -57,9 +60,14 @@ namespace dage {
 
 // FP64 "contract the fastest index and rotate" stage:
 //   out[R + n*M] (= or +=) alpha * sum_K X[R*ldx + K] * T[n*ldt + K]
+// krange (optional): per 128-column tile of out, the K band [first, last].
 int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,
                       long long ldt, double *out, double alpha, bool accumulate,
-                      cudaStream_t s);
+                      cudaStream_t s, const int2 *krange = nullptr);
+
+// K band of every (t-point, 128-row tile) of an axis matrix T[p][n][K]: the
+// first and last K index holding an entry above 2^-64 of its row's scale.
+int launch_band(const double *T, int K, int N, int P, int2 *range, cudaStream_t s);
 
 // V += coda * rho (when coda != 0) and the LIP-weighted integral of
 // f1 * f2 (f2 may be null: integral of f1).  The result lands in *d_result

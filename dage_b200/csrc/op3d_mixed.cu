@@ -3,22 +3,50 @@
 // Each "contract the fastest index and rotate" stage (see op3d.cu)
 //     D(R, n) = sum_K X(K, R) T(n, K)
 // runs on the 5th-generation tensor cores (tcgen05.mma kind::f16, BF16 in,
-// FP32 accumulate in TMEM).  FP64 operands are represented as sums of BF16
-// parts: X = X0 + X1 [+ X2], T_p(n, :) / s_n = T0 + T1 [+ T2] with s_n the
-// row maximum of |T_p(n, :)| (the matrix entries span many decades as t
-// grows).  "bf16x3" uses two parts and the three products (0,0) (0,1) (1,0);
-// "bf16x6" uses three parts and the six products with part-index sum <= 2.
-// The epilogue rescales by s_n and writes the next stage's input already
-// split into BF16 parts; the last stage multiplies by w_p s_n and
-// accumulates V in FP64.  The sum over t-points is FP64.
+// FP32 accumulate in TMEM).  Every operand is a sum of BF16 parts,
+// X = X0 + X1 [+ X2] and T_p(n, :) / s_n = T0 + T1 [+ T2], s_n the power of
+// two at or above the row maximum of |T_p(n, :)| (the entries span many
+// decades as t grows).  "bf16x3" uses two parts and the products (0,0)
+// (0,1) (1,0); "bf16x6" three parts and the six products with part-index
+// sum <= 2.
 //
-// Kernel structure (one persistent CTA per SM, 6 warps):
+// In bf16x6 the leading parts are fixed point: X0 is a multiple of one
+// quantum q = 2^(E-7) shared by each run of 32 consecutive K (2^E >= the
+// run's largest |X|), and T0 a multiple of 2^-7 along the whole row, so
+// |X0 / q|, |T0 * 2^7| <= 128.  The trailing parts are the BF16 roundings
+// of what is left.  A K=32 slice of the main product X0 T0 is then an
+// integer below 2^19 times q 2^-7: it is exact in FP32, and the tensor
+// core, which rounds its FP32 sums toward zero, never has to round it.  The
+// kernel gives every such slice a fresh TMEM partial and adds the partials
+// in FP32 registers (round to nearest), so the dominant product carries no
+// directed rounding at all.  The correction products (~2^-8 of the main
+// one and below) accumulate in TMEM over the whole K range, where the
+// rounding direction no longer matters at the 1e-7 level.  bf16x3 keeps
+// floating leading parts (the BF16 rounding of each value): with a single
+// trailing part a fixed-point lead would leave small elements only 8 bits.
+// Its main-product partials therefore carry the tensor core's directed
+// rounding (~1e-7 relative), far below that mode's 2^-17 representation
+// error.
+//
+// The epilogue rescales by s_n and writes the next stage's input already
+// split.  For that it needs the largest |value| of each 32-run of the next
+// stage's K index, which is the current row index R modulo d0: the M tiles
+// of an intermediate stage are therefore laid out two-dimensionally, 128
+// consecutive values of R mod d0 for one R / d0, so that every warp holds
+// exactly one 32-run and a warp-wide max reduction gives its quantum.  The
+// last stage multiplies by w_p s_n and adds into V (FP64) with L2
+// reductions; the sum over t-points is FP64.  K blocks outside the band of
+// the matrix tile (entries below 2^-64 of their row's scale) are skipped.
+//
+// Kernel structure (one persistent CTA per SM, 10 warps):
 //   warp 0      TMA producer: X and T tiles -> shared-memory ring (SW128)
 //   warp 1      TMEM allocator + single-thread MMA issuer
-//   warps 2-5   epilogue: tcgen05.ld -> scale -> split -> global stores
-// Two TMEM accumulators let the epilogue of tile i overlap the MMAs of tile
-// i+1.  Every mbarrier wait is bounded (clock64 budget); on timeout the CTA
-// records DAGE_E_TIMEOUT in a device flag, drains its in-flight copies and
+//   warps 2-9   epilogue, two warps per scheduler (64 columns each):
+//               partial sums -> scale -> split -> global stores
+// TMEM holds three 128-column partial buffers (the MMAs of the next slices
+// overlap the epilogue's reads) and the 128-column correction accumulator.
+// Every mbarrier wait is bounded (clock64 budget); on timeout the CTA
+// records the failure in a device flag, drains its in-flight copies and
 // MMAs, frees TMEM and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -36,7 +64,11 @@ extern long long g_wait_limit;
 namespace {
 
 constexpr int BM = 128;           // tile rows (TMEM lanes)
-constexpr int kThreads = 192;     // 6 warps
+constexpr int BN = 128;           // tile columns
+constexpr int BK = 64;            // K extent of one shared-memory stage (128-byte rows)
+constexpr int kGroup = 32;        // K extent sharing one quantum in a leading part
+constexpr int kThreads = 320;     // 10 warps
+constexpr int kEpiThreads = 256;  // warps 2-9
 
 // ---------------------------------------------------------------------------
 // PTX wrappers
@@ -110,37 +142,40 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
-// 32 lanes x 16 consecutive 32-bit columns; the wait takes the registers as
+// 32 lanes x 32 consecutive 32-bit columns; the wait takes the registers as
 // operands so no use of them can be scheduled before the load completes.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%32];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
                  "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
-                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31])
                :
                : "memory");
 }
 
-// Shared-memory matrix descriptor of a K-major tile written by TMA with a
-// 128-byte (BK = 64) or 64-byte (BK = 32) swizzle: rows of BK bf16, 8-row
-// swizzle atoms stacked at SBO = 8 * row bytes.
-template <int BK>
+// Shared-memory matrix descriptor of a K-major tile written by TMA with the
+// 128-byte swizzle: rows of 64 bf16 (128 bytes), 8-row swizzle atoms stacked
+// at SBO = 1024 bytes.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-  constexpr uint32_t row_bytes = BK * 2;
-  constexpr uint64_t layout = (BK == 64) ? 2 : 4;  // SWIZZLE_128B : SWIZZLE_64B
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)1 << 16;                         // LBO (unused for swizzled K-major)
-  d |= (uint64_t)((8 * row_bytes) >> 4) << 32;    // SBO
-  d |= (uint64_t)1 << 46;                         // descriptor version
-  d |= layout << 61;
+  d |= (uint64_t)1 << 16;            // LBO (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;  // SBO
+  d |= (uint64_t)1 << 46;            // descriptor version
+  d |= (uint64_t)2 << 61;            // SWIZZLE_128B
   return d;
 }
 
@@ -151,22 +186,47 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 }
 
 // ---------------------------------------------------------------------------
-// Split helpers
+// Splitting into BF16 parts
 // ---------------------------------------------------------------------------
+// v = lead + rest with lead = j 2^(E-7), |j| <= 128 and 2^E >= m >= |v|, the
+// smallest such E.  lead is exact in BF16 (8-bit integer times a power of
+// two); v - lead is exact in the working precision.  Runs whose largest
+// value is below 2^-119 keep everything in the trailing parts.
+__device__ __forceinline__ float lead_f32(float v, float m) {
+  const uint32_t mb = __float_as_uint(m);
+  const int E = (int)((mb >> 23) & 0xff) - 127 + ((mb & 0x7fffff) != 0);
+  if (m == 0.0f || E < -119) return 0.0f;
+  const float up = __uint_as_float((uint32_t)(127 + 7 - E) << 23);    // 2^(7-E)
+  const float down = __uint_as_float((uint32_t)(127 - 7 + E) << 23);  // 2^(E-7)
+  return rintf(v * up) * down;
+}
+__device__ __forceinline__ double lead_f64(double v, double m) {
+  if (m == 0.0) return 0.0;
+  int E = ilogb(m);
+  if (ldexp(1.0, E) != m) ++E;
+  if (E < -119) return 0.0;
+  return ldexp(rint(ldexp(v, 7 - E)), E - 7);
+}
+// NS == 2 (bf16x3) keeps a floating leading part: with a single trailing
+// part, a fixed-point lead would give small elements only 8 bits.
 template <int NS>
-__device__ __forceinline__ void split_f32(float v, __nv_bfloat16 (&o)[NS]) {
-  float r = v;
+__device__ __forceinline__ void split_lead_f32(float v, float m, __nv_bfloat16 (&o)[NS]) {
+  const float l = NS == 2 ? __bfloat162float(__float2bfloat16_rn(v)) : lead_f32(v, m);
+  o[0] = __float2bfloat16_rn(l);
+  float r = v - l;
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
+  for (int s = 1; s < NS; ++s) {
     o[s] = __float2bfloat16_rn(r);
     r = r - __bfloat162float(o[s]);
   }
 }
 template <int NS>
-__device__ __forceinline__ void split_f64(double v, __nv_bfloat16 (&o)[NS]) {
-  double r = v;
+__device__ __forceinline__ void split_lead_f64(double v, double m, __nv_bfloat16 (&o)[NS]) {
+  const double l = NS == 2 ? (double)__bfloat162float(__double2bfloat16(v)) : lead_f64(v, m);
+  o[0] = __double2bfloat16(l);
+  double r = v - l;
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
+  for (int s = 1; s < NS; ++s) {
     o[s] = __double2bfloat16(r);
     r = r - (double)__bfloat162float(o[s]);
   }
@@ -180,6 +240,10 @@ struct StageArgs {
   int n_ntiles, ntiles;  // tiles: m-tile major, n-tile minor
   int nkb, last_k16;     // K blocks; MMAs of K=16 in the last block
   int brow0;             // first row of this t-point in the T-part maps
+  // M tiling: nrb == 0: tile mt covers rows [128 mt, 128 mt + 128);
+  // nrb > 0 (intermediate stages): tile mt covers R = r1 d0 + r0 with
+  // r1 = mt / nrb and r0 in [128 (mt % nrb), +128) intersected with [0, d0)
+  int nrb;
   const float *scale;    // s_n of this t-point (intermediate stages)
   const double *scale64; // s_n of this t-point (final stage)
   double wcoef;          // w_p (final stage)
@@ -191,37 +255,52 @@ struct StageArgs {
   // final output V[R + M * n] (FP64)
   double *V;
   int accumulate;
+  // per n-tile of this t-point: first and last K index holding a matrix
+  // entry above 2^-64 of its row's scale (the matrices are banded for large
+  // t; K blocks outside the band add nothing and are skipped)
+  const int2 *k_range;
   int *err;
   long long wait_limit;   // normal waits (dage_set_wait_limit)
   long long drain_limit;  // waits for in-flight copies/MMAs after a timeout
 };
 
-template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
+template <int NSX, int NS>
 struct StageCfg {
-  static constexpr int kAParts = NSX;
-  static constexpr int kBParts = NSX;  // the same number of parts for T
   static constexpr int kRowBytes = BK * 2;
-  static constexpr int kABytes = BM * kRowBytes;       // one part of the A tile
-  static constexpr int kBBytes = BN * kRowBytes;       // one part of the B tile
+  static constexpr int kABytes = BM * kRowBytes;  // one part of the A tile
+  static constexpr int kBBytes = BN * kRowBytes;  // one part of the B tile
   static constexpr int kStageBytes = NSX * kABytes + NSX * kBBytes;
-  static constexpr int kTmemCols = 2 * BN;             // two accumulators
+  static constexpr int kNP = 3;                   // partial buffers
+  static constexpr int kTmemCols = 512;           // 3 partials + correction
   static constexpr int kSmem = NS * kStageBytes + 1024 + 256;
 };
 
-// products (a-part, b-part), smallest terms first
-__device__ __forceinline__ void product(int nprod, int i, int &a, int &b) {
-  if (nprod == 3) {
-    const int pa[3] = {1, 0, 0}, pb[3] = {0, 1, 0};
+// correction products (a-part, b-part): all pairs with 1 <= a + b <= NSX - 1
+__device__ __forceinline__ void corr_product(int nsx, int i, int &a, int &b) {
+  if (nsx == 2) {
+    const int pa[2] = {1, 0}, pb[2] = {0, 1};
     a = pa[i];
     b = pb[i];
   } else {
-    const int pa[6] = {2, 1, 0, 1, 0, 0}, pb[6] = {0, 1, 2, 0, 1, 0};
+    const int pa[5] = {2, 1, 0, 1, 0}, pb[5] = {0, 1, 2, 0, 1};
     a = pa[i];
     b = pb[i];
   }
 }
 
-template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
+// K blocks [first, last] of the band of n-tile nt
+__device__ __forceinline__ int2 kblocks(const StageArgs &a, int nt) {
+  const int2 r = a.k_range[nt];
+  return make_int2(r.x / BK, r.y / BK);
+}
+
+__device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
+  return a.nrb ? (mt / a.nrb) * a.d0 + (mt % a.nrb) * BM : mt * BM;
+}
+
+// NSX parts per operand; NS shared-memory stages; the main product starts a
+// fresh partial every kGroup / 16 MMAs (one 32-run of K).
+template <int NSX, int NS, bool FINAL>
 __global__ void __launch_bounds__(kThreads, 1)
     stage_bf16_kernel(const __grid_constant__ CUtensorMap mapA0,
                       const __grid_constant__ CUtensorMap mapA1,
@@ -229,7 +308,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                       const __grid_constant__ CUtensorMap mapB0,
                       const __grid_constant__ CUtensorMap mapB1,
                       const __grid_constant__ CUtensorMap mapB2, const StageArgs a) {
-  using C = StageCfg<NSX, NPROD, BN, BK, NS, FINAL>;
+  using C = StageCfg<NSX, NS>;
+  constexpr int NCORR = NSX == 2 ? 2 : 5;
+  constexpr int GRAN = kGroup / 16;
   // an earlier launch of this apply timed out: do nothing
   if (*reinterpret_cast<volatile int *>(a.err)) return;
   extern __shared__ uint8_t smem_raw[];
@@ -237,26 +318,28 @@ __global__ void __launch_bounds__(kThreads, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *tiles = smem;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + NS * C::kStageBytes);
-  // bars: full[NS], empty[NS], tfull[2], tempty[2], drain[1]
-  uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * NS + 5);
+  // bars: full[NS], empty[NS], pfull[3], pempty[3], cfull, cempty, drain
+  uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * NS + 9);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
-
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  auto full = [&](int s) { return smem_u32(bars + s); };
-  auto empty = [&](int s) { return smem_u32(bars + NS + s); };
-  auto tfull = [&](int i) { return smem_u32(bars + 2 * NS + i); };
-  auto tempty = [&](int i) { return smem_u32(bars + 2 * NS + 2 + i); };
-  const uint32_t drain = smem_u32(bars + 2 * NS + 4);
+  auto full = [&](int i) { return smem_u32(bars + i); };
+  auto empty = [&](int i) { return smem_u32(bars + NS + i); };
+  auto pfull = [&](int i) { return smem_u32(bars + 2 * NS + i); };
+  auto pempty = [&](int i) { return smem_u32(bars + 2 * NS + 3 + i); };
+  const uint32_t cfull = smem_u32(bars + 2 * NS + 6), cempty = smem_u32(bars + 2 * NS + 7);
+  const uint32_t drain = smem_u32(bars + 2 * NS + 8);
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NS; ++s) {
-      mbar_init(full(s), 1);
-      mbar_init(empty(s), 1);
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(full(i), 1);
+      mbar_init(empty(i), 1);
     }
-    for (int i = 0; i < 2; ++i) {
-      mbar_init(tfull(i), 1);
-      mbar_init(tempty(i), 128);
+    for (int i = 0; i < C::kNP; ++i) {
+      mbar_init(pfull(i), 1);
+      mbar_init(pempty(i), kEpiThreads);
     }
+    mbar_init(cfull, 1);
+    mbar_init(cempty, kEpiThreads);
     mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -266,10 +349,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_holder;
-
+  const uint32_t tmem_corr = tmem_base + C::kNP * BN;
   auto on_timeout = [&]() {
     *abort_flag = 1;
     atomicCAS(a.err, 0, 1);
+  };
+  // K=16 steps of a tile with K blocks [lo, hi]
+  auto tile_steps = [&](int2 r) {
+    return (r.y - r.x) * (BK / 16) + (r.y == a.nkb - 1 ? a.last_k16 : BK / 16);
   };
 
   if (warp == 0) {
@@ -283,8 +370,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t issued_ph[NS];
       for (int i = 0; i < NS; ++i) issued[i] = 0, issued_ph[i] = 0;
       for (int tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x) {
-        const int m0 = (tile / a.n_ntiles) * BM, n0 = (tile % a.n_ntiles) * BN;
-        for (int kb = 0; kb < a.nkb; ++kb) {
+        const int row0 = tile_row0(a, tile / a.n_ntiles), n0 = (tile % a.n_ntiles) * BN;
+        const int2 r = kblocks(a, tile % a.n_ntiles);
+        for (int kb = r.x; kb <= r.y; ++kb) {
           if (!mbar_wait(empty(s), ph ^ 1, a.wait_limit)) {
             on_timeout();
             break;
@@ -293,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_expect_tx(full(s), C::kStageBytes);
 #pragma unroll
           for (int i = 0; i < NSX; ++i)
-            tma_load_2d(smem_u32(st + i * C::kABytes), mA[i], full(s), kb * BK, m0);
+            tma_load_2d(smem_u32(st + i * C::kABytes), mA[i], full(s), kb * BK, row0);
 #pragma unroll
           for (int j = 0; j < NSX; ++j)
             tma_load_2d(smem_u32(st + NSX * C::kABytes + j * C::kBBytes), mB[j], full(s),
@@ -303,33 +391,28 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (++s == NS) s = 0, ph ^= 1;
         }
       }
-      if (*abort_flag) {
-        // let every copy that was issued land before the CTA goes away
+      if (*abort_flag)  // let every copy that was issued land first
         for (int i = 0; i < NS; ++i)
           if (issued[i]) mbar_wait(full(i), issued_ph[i], a.drain_limit);
-      }
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
+      int g = 0;  // partial counter over all tiles
       int t = 0;
-      for (int tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x, ++t) {
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < a.ntiles && ok && !*abort_flag; tile += gridDim.x, ++t) {
         const int n0 = (tile % a.n_ntiles) * BN;
         int nt = a.N - n0;
         if (nt > BN) nt = BN;
         nt = (nt + 15) & ~15;
         const uint32_t idesc = idesc_bf16(BM, nt);
-        const int acc = t & 1;
-        if (!mbar_wait(tempty(acc), ((t >> 1) & 1) ^ 1, a.wait_limit)) {
-          on_timeout();
-          break;
-        }
-        tc_fence_after();
-        const uint32_t d = tmem_base + acc * BN;
-        bool ok = true;
-        for (int kb = 0; kb < a.nkb; ++kb) {
+        const int2 r = kblocks(a, tile % a.n_ntiles);
+        const int nsteps = tile_steps(r);
+        int step = 0;  // K=16 step within the tile; K blocks start on a 32-run
+        for (int kb = r.x; kb <= r.y && ok; ++kb) {
           if (!mbar_wait(full(s), ph, a.wait_limit)) {
             on_timeout();
             ok = false;
@@ -338,21 +421,43 @@ __global__ void __launch_bounds__(kThreads, 1)
           tc_fence_after();
           const uint32_t st = smem_u32(tiles + s * C::kStageBytes);
           const int nk16 = (kb == a.nkb - 1) ? a.last_k16 : BK / 16;
-          for (int k = 0; k < nk16; ++k) {
+          for (int k = 0; k < nk16; ++k, ++step) {
+            const int b = g % C::kNP;
+            if (step % GRAN == 0) {
+              if (!mbar_wait(pempty(b), ((g / C::kNP) & 1) ^ 1, a.wait_limit)) {
+                on_timeout();
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+            }
+            umma_bf16(tmem_base + b * BN, sdesc(st + k * 32), sdesc(st + NSX * C::kABytes + k * 32),
+                      idesc, step % GRAN != 0);
+            if (step % GRAN == GRAN - 1 || step == nsteps - 1) {
+              umma_commit(pfull(b));
+              ++g;
+            }
+            if (step == 0) {
+              if (!mbar_wait(cempty, (t & 1) ^ 1, a.wait_limit)) {
+                on_timeout();
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+            }
 #pragma unroll
-            for (int pr = 0; pr < NPROD; ++pr) {
+            for (int pr = 0; pr < NCORR; ++pr) {
               int ia, ib;
-              product(NPROD, pr, ia, ib);
-              const uint64_t ad = sdesc<BK>(st + ia * C::kABytes + k * 32);
-              const uint64_t bd = sdesc<BK>(st + NSX * C::kABytes + ib * C::kBBytes + k * 32);
-              umma_bf16(d, ad, bd, idesc, (kb | k | pr) != 0);
+              corr_product(NSX, pr, ia, ib);
+              const uint64_t ad = sdesc(st + ia * C::kABytes + k * 32);
+              const uint64_t bd = sdesc(st + NSX * C::kABytes + ib * C::kBBytes + k * 32);
+              umma_bf16(tmem_corr, ad, bd, idesc, (step | pr) != 0);
             }
           }
           umma_commit(empty(s));
           if (++s == NS) s = 0, ph ^= 1;
         }
-        if (!ok) break;
-        umma_commit(tfull(acc));
+        if (ok) umma_commit(cfull);
       }
       // every MMA this thread issued has completed once `drain` fires
       umma_commit(drain);
@@ -360,56 +465,102 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    const int q = warp & 3;  // TMEM lane quarter this warp may access
-    int t = 0;
+    // 8 warps, two per scheduler: warp w reads TMEM lanes 32 (w % 4) .. +31
+    // (the hardware's lane quarter) and the column half (w - 2) / 4.
+    constexpr int HC = BN / 2;
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+    const uint32_t col0 = half * HC;
+    int g = 0, t = 0;
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++t) {
-      const int acc = t & 1;
-      const bool got = mbar_wait(tfull(acc), (t >> 1) & 1, a.wait_limit);
+      float acc[HC];
+#pragma unroll
+      for (int j = 0; j < HC; ++j) acc[j] = 0.0f;
+      bool ok = true;
+      const int nparts = (tile_steps(kblocks(a, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
+      for (int pi = 0; pi < nparts; ++pi, ++g) {
+        const int b = g % C::kNP;
+        const bool got = mbar_wait(pfull(b), (g / C::kNP) & 1, a.wait_limit);
+        __syncwarp();
+        if (!got) {
+          on_timeout();
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int c = 0; c < HC / 32; ++c) {
+          uint32_t r[32];
+          tmem_ld32(tmem_base + lane_off + b * BN + col0 + c * 32, r);
+#pragma unroll
+          for (int j = 0; j < 32; ++j) acc[c * 32 + j] += __uint_as_float(r[j]);
+        }
+        tc_fence_before();
+        mbar_arrive(pempty(b));
+      }
+      if (!ok) break;
+      const bool got = mbar_wait(cfull, t & 1, a.wait_limit);
       __syncwarp();
       if (!got) {
         on_timeout();
         break;
       }
       tc_fence_after();
-      const int m0 = (tile / a.n_ntiles) * BM, n0 = (tile % a.n_ntiles) * BN;
-      const int R = m0 + 32 * q + lane;
-      const bool row_ok = R < a.M;
-      int nvalid = a.N - n0;
-      if (nvalid > BN) nvalid = BN;
-      const int nchunks = (nvalid + 15) >> 4;
-      long long r0 = 0, r1 = 0;
-      if (!FINAL) {
-        r0 = R % a.d0;
-        r1 = R / a.d0;
-      }
-      for (int c = 0; c < nchunks; ++c) {
-        uint32_t r[16];
-        __syncwarp();  // tcgen05.ld is warp-collective
-        tmem_ld16(tmem_base + ((uint32_t)(32 * q) << 16) + acc * BN + c * 16, r);
-        if (row_ok) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int n = n0 + c * 16 + j;
-          if (n >= a.N) break;
-          const float v = __uint_as_float(r[j]);
-          if (FINAL) {
-            double *dst = a.V + (size_t)R + (size_t)a.M * n;
-            const double add = a.wcoef * a.scale64[n] * (double)v;
-            *dst = a.accumulate ? *dst + add : add;
-          } else {
-            __nv_bfloat16 parts[NSX];
-            split_f32<NSX>(v * a.scale[n], parts);
-            const size_t off = (size_t)(r1 + (long long)a.d1 * n) * a.ldn + r0;
-            a.out0[off] = parts[0];
-            a.out1[off] = parts[1];
-            if (NSX > 2) a.out2[off] = parts[NSX > 2 ? 2 : 0];
+      for (int c = 0; c < HC / 32; ++c) {
+        uint32_t r[32];
+        tmem_ld32(tmem_corr + lane_off + col0 + c * 32, r);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[c * 32 + j] += __uint_as_float(r[j]);
+      }
+      tc_fence_before();
+      mbar_arrive(cempty);
+      const int mt = tile / a.n_ntiles, n0 = (tile % a.n_ntiles) * BN + col0;
+      if (FINAL) {
+        // V[R + M n] (+)= w_p s_n acc.  Additions are L2 reductions: each
+        // element gets exactly one correctly rounded FP64 add per t-point,
+        // and the warp does not wait for the old values.
+        const int R = mt * BM + 32 * q + lane;
+        if (R < a.M) {
+          double *col = a.V + (size_t)R;
+#pragma unroll
+          for (int j = 0; j < HC; ++j) {
+            const int n = n0 + j;
+            if (n < a.N) {
+              const double add = a.wcoef * a.scale64[n] * (double)acc[j];
+              double *dst = col + (size_t)a.M * n;
+              if (a.accumulate)
+                atomicAdd(dst, add);
+              else
+                __stcs(dst, add);
+            }
           }
         }
+      } else {
+        // next stage: row R / d0 + d1 n, K index R mod d0; this warp holds
+        // one aligned 32-run of that K index
+        const int r1 = mt / a.nrb;
+        const int r0 = (mt % a.nrb) * BM + 32 * q + lane;
+        const bool valid = r0 < a.d0;
+#pragma unroll
+        for (int j = 0; j < HC; ++j) {
+          const int n = n0 + j;
+          if (n < a.N) {  // uniform across the warp
+            const float v = valid ? acc[j] * a.scale[n] : 0.0f;
+            float m = 0.0f;
+            if (NSX > 2)
+              m = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v))));
+            __nv_bfloat16 parts[NSX];
+            split_lead_f32<NSX>(v, m, parts);
+            if (valid) {
+              const size_t off = (size_t)(r1 + (long long)a.d1 * n) * a.ldn + r0;
+              a.out0[off] = parts[0];
+              a.out1[off] = parts[1];
+              if (NSX > 2) a.out2[off] = parts[NSX > 2 ? 2 : 0];
+            }
+          }
         }
       }
-      __syncwarp();
-      tc_fence_before();
-      mbar_arrive(tempty(acc));
     }
   }
 
@@ -424,25 +575,38 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------------------
 // Input and matrix preparation
 // ---------------------------------------------------------------------------
-// rho (FP64, x fastest) -> NSX BF16 parts, rows of ld elements.
+// rho (FP64, x fastest, rows of K) -> NSX BF16 parts, rows of ld elements.
+// One warp per 32-run of a row; the run's largest |rho| sets the quantum of
+// the leading part.  Elements K..ld-1 are written as zeros.
 template <int NSX>
 __global__ void split_input_kernel(const double *__restrict__ rho, int K, long long rows,
                                    long long ld, __nv_bfloat16 *o0, __nv_bfloat16 *o1,
                                    __nv_bfloat16 *o2) {
-  const long long n = (long long)K * rows;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long r = i / K, k = i % K;
+  const int runs = (int)((ld + kGroup - 1) / kGroup);
+  const long long nwork = rows * runs;
+  const int lane = threadIdx.x & 31;
+  const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < nwork;
+       w += wstride) {
+    const long long r = w / runs;
+    const int k = (int)(w % runs) * kGroup + lane;
+    const double v = k < K ? rho[r * K + k] : 0.0;
+    double m = fabs(v);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     __nv_bfloat16 p[NSX];
-    split_f64<NSX>(rho[i], p);
-    const size_t off = (size_t)r * ld + k;
-    o0[off] = p[0];
-    o1[off] = p[1];
-    if (NSX > 2) o2[off] = p[NSX > 2 ? 2 : 0];
+    split_lead_f64<NSX>(v, m, p);
+    if (k < ld) {
+      const size_t off = (size_t)r * ld + k;
+      o0[off] = p[0];
+      o1[off] = p[1];
+      if (NSX > 2) o2[off] = p[NSX > 2 ? 2 : 0];
+    }
   }
 }
 
-// One block per matrix row (p, n): s = max_K |T|, parts of T/s.
+// One block per matrix row (p, n): s = 2^ceil(log2 max_K |T|), parts of
+// T / s with the leading part on the quantum 2^-7.
 template <int NSX>
 __global__ void split_matrix_kernel(const double *__restrict__ T, int K, long long ld,
                                     float *scale, double *scale64, __nv_bfloat16 *o0,
@@ -462,14 +626,14 @@ __global__ void split_matrix_kernel(const double *__restrict__ T, int K, long lo
   }
   __syncthreads();
   // power-of-two scale: the division is exact
-  double s = red[0] > 0.0 ? exp2(ceil(log2(red[0]))) : 1.0;
+  const double s = red[0] > 0.0 ? exp2(ceil(log2(red[0]))) : 1.0;
   if (threadIdx.x == 0) {
     scale[row] = (float)s;
     scale64[row] = s;
   }
   for (int k = threadIdx.x; k < (int)ld; k += blockDim.x) {
     __nv_bfloat16 p[NSX];
-    split_f64<NSX>(k < K ? src[k] / s : 0.0, p);
+    split_lead_f64<NSX>(k < K ? src[k] / s : 0.0, 1.0, p);
     const size_t off = (size_t)row * ld + k;
     o0[off] = p[0];
     o1[off] = p[1];
@@ -516,8 +680,6 @@ int make_map(CUtensorMap *m, const void *base, long long inner, long long rows, 
 
 struct MixedState {
   int nparts = 2;   // BF16 parts per operand
-  int nprod = 3;
-  int bn = 256, bk = 64;
   long long ld[3];  // padded K extent of each stage's input rows
   long long rows[3];
   DevBuf X[3];      // stage inputs: nparts planes of rows x ld BF16
@@ -534,11 +696,13 @@ __nv_bfloat16 *plane(DevBuf &b, int part, long long plane_elems) {
   return b.as<__nv_bfloat16>() + (size_t)part * plane_elems;
 }
 
-template <int NSX, int NPROD, int BN, int BK, int NS, bool FINAL>
-int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, const StageArgs &base,
-                 cudaStream_t s) {
-  using C = StageCfg<NSX, NPROD, BN, BK, NS, FINAL>;
-  auto kern = stage_bf16_kernel<NSX, NPROD, BN, BK, NS, FINAL>;
+// One stage launch.  nrb > 0 selects the two-dimensional M tiling of the
+// intermediate stages (see StageArgs).
+template <int NSX, int NS, bool FINAL>
+int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, int nrb,
+                 const StageArgs &base, cudaStream_t s) {
+  using C = StageCfg<NSX, NS>;
+  auto kern = stage_bf16_kernel<NSX, NS, FINAL>;
   static bool attr_set = false;
   if (!attr_set) {
     DAGE_CUDA_TRY(
@@ -549,22 +713,23 @@ int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, const St
   a.M = M;
   a.N = N;
   a.K = K;
+  a.nrb = nrb;
   a.n_ntiles = ceil_div(N, BN);
-  a.ntiles = ceil_div(M, BM) * a.n_ntiles;
+  const long long nmt = nrb ? (long long)(M / a.d0) * nrb : ceil_div(M, BM);
+  a.ntiles = (int)(nmt * a.n_ntiles);
   a.nkb = ceil_div(K, BK);
   a.last_k16 = ceil_div(K - (a.nkb - 1) * BK, 16);
   a.brow0 = p * N;
-  const int ax = stage;
   const int grid = std::min(a.ntiles, sm_count());
   const CUtensorMap *mA = st.mapA[stage];
-  const CUtensorMap *mB = st.mapB[st.towner[ax]];
+  const CUtensorMap *mB = st.mapB[st.towner[stage]];
   kern<<<grid, kThreads, C::kSmem, s>>>(mA[0], mA[1], mA[NSX > 2 ? 2 : 1], mB[0], mB[1],
                                         mB[NSX > 2 ? 2 : 1], a);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
 
-template <int NSX, int NPROD, int BN, int BK, int NS>
+template <int NSX, int NS>
 int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, cudaStream_t s) {
   const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
   const int nox = op->nout[0], noy = op->nout[1], noz = op->nout[2];
@@ -572,8 +737,8 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
   // input split
   {
     const int t = op->tmark_begin(1);
-    const long long n = (long long)nix * st.rows[0];
-    const int blocks = (int)std::min<long long>((n + 255) / 256, sm_count() * 8LL);
+    const long long nwarps = st.rows[0] * ((st.ld[0] + kGroup - 1) / kGroup);
+    const int blocks = (int)std::min<long long>((nwarps + 7) / 8, sm_count() * 16LL);
     split_input_kernel<NSX><<<blocks, 256, 0, s>>>(
         d_rho, nix, st.rows[0], st.ld[0], plane(st.X[0], 0, pe[0]), plane(st.X[0], 1, pe[0]),
         plane(st.X[0], NSX > 2 ? 2 : 1, pe[0]));
@@ -593,6 +758,7 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
       const int ow = st.towner[stage];
       a.scale = st.sc[ow].as<float>() + (size_t)p * no[stage];
       a.scale64 = st.sc64[ow].as<double>() + (size_t)p * no[stage];
+      a.k_range = op->band[ow].as<int2>() + (size_t)p * ceil_div(no[stage], BN);
       const int t = op->tmark_begin(0);
       if (stage < 2) {
         a.out0 = plane(st.X[stage + 1], 0, pe[stage + 1]);
@@ -601,14 +767,14 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
         a.d0 = d0[stage];
         a.d1 = d1[stage];
         a.ldn = st.ld[stage + 1];
-        DAGE_TRY((launch_stage<NSX, NPROD, BN, BK, NS, false>(st, stage, (int)M[stage],
-                                                               no[stage], ni[stage], p, a, s)));
+        DAGE_TRY((launch_stage<NSX, NS, false>(st, stage, (int)M[stage], no[stage], ni[stage], p,
+                                               ceil_div(d0[stage], BM), a, s)));
       } else {
         a.V = d_V;
         a.wcoef = op->w[p];
         a.accumulate = p > 0;
-        DAGE_TRY((launch_stage<NSX, NPROD, BN, BK, NS, true>(st, stage, (int)M[stage], no[stage],
-                                                              ni[stage], p, a, s)));
+        DAGE_TRY((launch_stage<NSX, NS, true>(st, stage, (int)M[stage], no[stage], ni[stage], p,
+                                              0, a, s)));
       }
       op->tmark_end(t);
     }
@@ -621,16 +787,7 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
 int mixed_setup(dage_op3d *op) {
   auto *st = new MixedState();
   op->mixed = st;
-  if (op->precision == DAGE_MIXED_BF16X3) {
-    st->nparts = 2;
-    st->nprod = 3;
-    st->bn = 256;
-  } else {
-    st->nparts = 3;
-    st->nprod = 6;
-    st->bn = 128;
-  }
-  st->bk = 64;
+  st->nparts = op->precision == DAGE_MIXED_BF16X3 ? 2 : 3;
   const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
   const int nox = op->nout[0], noy = op->nout[1];
   const int ni[3] = {nix, niy, niz};
@@ -644,7 +801,7 @@ int mixed_setup(dage_op3d *op) {
     DAGE_CUDA_TRY(cudaMemsetAsync(st->X[s].ptr, 0, st->X[s].bytes, op->stream));
     for (int i = 0; i < st->nparts; ++i)
       DAGE_TRY(make_map(&st->mapA[s][i], plane(st->X[s], i, pe), ni[s], st->rows[s], st->ld[s],
-                        st->bk, BM));
+                        BK, BM));
   }
   DAGE_TRY(st->err.alloc(sizeof(int)));
   DAGE_CUDA_TRY(cudaMemsetAsync(st->err.ptr, 0, sizeof(int), op->stream));
@@ -668,11 +825,8 @@ int mixed_setup(dage_op3d *op) {
           op->T(ax), K, ld, st->sc[ax].as<float>(), st->sc64[ax].as<double>(), o0, o1, o2);
     DAGE_CUDA_TRY(cudaGetLastError());
     for (int i = 0; i < st->nparts; ++i)
-      DAGE_TRY(make_map(&st->mapB[ax][i], plane(st->Tp[ax], i, pe), K, nrows, ld, st->bk,
-                        st->bn));
+      DAGE_TRY(make_map(&st->mapB[ax][i], plane(st->Tp[ax], i, pe), K, nrows, ld, BK, BN));
   }
-  // the A maps of stage s must describe the stage's input extent; ld must
-  // match the padded extent the previous stage writes
   return 0;
 }
 
@@ -681,11 +835,8 @@ int mixed_set_weights(dage_op3d *) { return 0; }
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
   auto *st = static_cast<MixedState *>(op->mixed);
   if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
-  int rc;
-  if (st->nparts == 2)
-    rc = run_stages<2, 3, 256, 64, 2>(op, *st, d_rho, d_V, s);
-  else
-    rc = run_stages<3, 6, 128, 64, 2>(op, *st, d_rho, d_V, s);
+  const int rc = st->nparts == 2 ? run_stages<2, 3>(op, *st, d_rho, d_V, s)
+                                 : run_stages<3, 2>(op, *st, d_rho, d_V, s);
   if (rc) return rc;
   int herr = 0;
   DAGE_CUDA_TRY(cudaMemcpyAsync(&herr, st->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));

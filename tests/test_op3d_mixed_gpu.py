@@ -1,14 +1,16 @@
 """GPU tests of the split-precision tensor-core operator (tcgen05, BF16
 parts, FP32 accumulation) against the FP64 GPU operator and the oracle.
 
-Bars: bf16x6 <= 2e-6 max-norm relative potential and <= 2e-7 relative
-energy; bf16x3 <= 2e-5 / 2e-6 (two BF16 parts carry ~16 bits)."""
+Bars: bf16x6 <= 1e-6 max-norm relative potential and <= 1e-7 relative
+energy (the targets); bf16x3 <= 1e-5 / 1e-5 (two BF16 parts carry ~16
+bits, a 2^-17 ~ 7.6e-6 relative representation error per element, so it
+cannot reach them)."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-BARS = {"bf16x6": (2e-6, 2e-7), "bf16x3": (2e-5, 2e-6)}
+BARS = {"bf16x6": (1e-6, 1e-7), "bf16x3": (1e-5, 1e-5)}
 
 
 def _case(dage, oracle, axes, quad, ng=3, seed=0):
