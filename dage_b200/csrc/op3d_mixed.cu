@@ -38,10 +38,10 @@
 // reductions; the sum over t-points is FP64.  K blocks outside the band of
 // the matrix tile (entries below 2^-64 of their row's scale) are skipped.
 //
-// Kernel structure (one persistent CTA per SM, 10 warps):
+// Kernel structure (one persistent CTA per SM, 18 warps):
 //   warp 0      TMA producer: X and T tiles -> shared-memory ring (SW128)
 //   warp 1      TMEM allocator + single-thread MMA issuer
-//   warps 2-9   epilogue, two warps per scheduler (64 columns each):
+//   warps 2-17  epilogue, four warps per scheduler (32 columns each):
 //               partial sums -> scale -> split -> global stores
 // TMEM holds three 128-column partial buffers (the MMAs of the next slices
 // overlap the epilogue's reads) and the 128-column correction accumulator.
@@ -67,8 +67,8 @@ constexpr int BM = 128;           // tile rows (TMEM lanes)
 constexpr int BN = 128;           // tile columns
 constexpr int BK = 64;            // K extent of one shared-memory stage (128-byte rows)
 constexpr int kGroup = 32;        // K extent sharing one quantum in a leading part
-constexpr int kThreads = 320;     // 10 warps
-constexpr int kEpiThreads = 256;  // warps 2-9
+constexpr int kThreads = 576;     // 18 warps
+constexpr int kEpiThreads = 512;  // warps 2-17
 
 // ---------------------------------------------------------------------------
 // PTX wrappers
@@ -465,17 +465,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    // 8 warps, two per scheduler: warp w reads TMEM lanes 32 (w % 4) .. +31
-    // (the hardware's lane quarter) and the column half (w - 2) / 4.
-    constexpr int HC = BN / 2;
-    const int q = warp & 3, half = (warp - 2) >> 2;
+    // 16 warps, four per scheduler: warp w reads TMEM lanes 32 (w % 4) ..
+    // +31 (the hardware's lane quarter) and the 32 columns (w - 2) / 4.
+    constexpr int CW = BN / 4;
+    const int q = warp & 3;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
-    const uint32_t col0 = half * HC;
+    const uint32_t col0 = ((warp - 2) >> 2) * CW;
     int g = 0, t = 0;
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++t) {
-      float acc[HC];
+      float acc[CW];
 #pragma unroll
-      for (int j = 0; j < HC; ++j) acc[j] = 0.0f;
+      for (int j = 0; j < CW; ++j) acc[j] = 0.0f;
       bool ok = true;
       const int nparts = (tile_steps(kblocks(a, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
       for (int pi = 0; pi < nparts; ++pi, ++g) {
@@ -488,15 +488,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-#pragma unroll
-        for (int c = 0; c < HC / 32; ++c) {
-          uint32_t r[32];
-          tmem_ld32(tmem_base + lane_off + b * BN + col0 + c * 32, r);
-#pragma unroll
-          for (int j = 0; j < 32; ++j) acc[c * 32 + j] += __uint_as_float(r[j]);
-        }
+        uint32_t r[32];
+        tmem_ld32(tmem_base + lane_off + b * BN + col0, r);
         tc_fence_before();
         mbar_arrive(pempty(b));
+#pragma unroll
+        for (int j = 0; j < CW; ++j) acc[j] += __uint_as_float(r[j]);
       }
       if (!ok) break;
       const bool got = mbar_wait(cfull, t & 1, a.wait_limit);
@@ -506,15 +503,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         break;
       }
       tc_fence_after();
-#pragma unroll
-      for (int c = 0; c < HC / 32; ++c) {
+      {
         uint32_t r[32];
-        tmem_ld32(tmem_corr + lane_off + col0 + c * 32, r);
+        tmem_ld32(tmem_corr + lane_off + col0, r);
+        tc_fence_before();
+        mbar_arrive(cempty);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[c * 32 + j] += __uint_as_float(r[j]);
+        for (int j = 0; j < CW; ++j) acc[j] += __uint_as_float(r[j]);
       }
-      tc_fence_before();
-      mbar_arrive(cempty);
       const int mt = tile / a.n_ntiles, n0 = (tile % a.n_ntiles) * BN + col0;
       if (FINAL) {
         // V[R + M n] (+)= w_p s_n acc.  Additions are L2 reductions: each
@@ -524,7 +520,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (R < a.M) {
           double *col = a.V + (size_t)R;
 #pragma unroll
-          for (int j = 0; j < HC; ++j) {
+          for (int j = 0; j < CW; ++j) {
             const int n = n0 + j;
             if (n < a.N) {
               const double add = a.wcoef * a.scale64[n] * (double)acc[j];
@@ -538,25 +534,45 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       } else {
         // next stage: row R / d0 + d1 n, K index R mod d0; this warp holds
-        // one aligned 32-run of that K index
+        // one aligned 32-run of that K index.  Columns go in pairs: the two
+        // lanes of a pair swap one value so that the even lane holds K
+        // indices (r0, r0 + 1) of column j and the odd lane those of column
+        // j + 1; each stores its two elements as one packed BF16 pair per
+        // part.  (ld is even; index d0 < ld is padding and receives zeros.)
         const int r1 = mt / a.nrb;
         const int r0 = (mt % a.nrb) * BM + 32 * q + lane;
         const bool valid = r0 < a.d0;
+        const bool odd = lane & 1;
+        const int rpair = r0 & ~1;
 #pragma unroll
-        for (int j = 0; j < HC; ++j) {
+        for (int j = 0; j < CW; j += 2) {
           const int n = n0 + j;
           if (n < a.N) {  // uniform across the warp
-            const float v = valid ? acc[j] * a.scale[n] : 0.0f;
+            const bool has1 = n + 1 < a.N;
+            const float v0 = valid ? acc[j] * a.scale[n] : 0.0f;
+            const float v1 = valid && has1 ? acc[j + 1] * a.scale[n + 1] : 0.0f;
             float m = 0.0f;
-            if (NSX > 2)
-              m = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v))));
-            __nv_bfloat16 parts[NSX];
-            split_lead_f32<NSX>(v, m, parts);
-            if (valid) {
-              const size_t off = (size_t)(r1 + (long long)a.d1 * n) * a.ldn + r0;
-              a.out0[off] = parts[0];
-              a.out1[off] = parts[1];
-              if (NSX > 2) a.out2[off] = parts[NSX > 2 ? 2 : 0];
+            if (NSX > 2) {
+              const float m0 =
+                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v0))));
+              const float m1 =
+                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v1))));
+              m = odd ? m1 : m0;
+            }
+            const float recv = __shfl_xor_sync(0xffffffffu, odd ? v0 : v1, 1);
+            const float mine = odd ? v1 : v0;
+            const float lo = odd ? recv : mine, hi = odd ? mine : recv;
+            __nv_bfloat16 pl[NSX], ph[NSX];
+            split_lead_f32<NSX>(lo, m, pl);
+            split_lead_f32<NSX>(hi, m, ph);
+            if (rpair < a.d0 && (!odd || has1)) {
+              const size_t off =
+                  (size_t)(r1 + (long long)a.d1 * (n + (odd ? 1 : 0))) * a.ldn + rpair;
+              *reinterpret_cast<__nv_bfloat162 *>(a.out0 + off) = __halves2bfloat162(pl[0], ph[0]);
+              *reinterpret_cast<__nv_bfloat162 *>(a.out1 + off) = __halves2bfloat162(pl[1], ph[1]);
+              if (NSX > 2)
+                *reinterpret_cast<__nv_bfloat162 *>(a.out2 + off) =
+                    __halves2bfloat162(pl[NSX > 2 ? 2 : 0], ph[NSX > 2 ? 2 : 0]);
             }
           }
         }
