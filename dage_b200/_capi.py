@@ -69,6 +69,7 @@ SIGNATURES = {
     "dage_gbfmm_multipole_moments": (ctypes.c_int, [_VP, _VP, ctypes.c_uint, _D]),
     "dage_gbfmm_local_expansions": (ctypes.c_int, [_VP, _D]),
     "dage_gbfmm_evaluate_le": (ctypes.c_int, [_VP, _D, _VP, ctypes.c_uint]),
+    "dage_gbfmm_tiles": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "dage_gbfmm_box_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),
     "dage_gbfmm_set_stream": (ctypes.c_int, [_VP, _VP]),

@@ -7,8 +7,9 @@
 //
 // One descriptor describes one independent contraction (a whole cube stage,
 // or one GBFMM box); a launch covers any number of them (grid.z).  Tiles are
-// 128 x 128 per 256-thread block, 64 x 32 per warp (8 x 4 MMA tiles of
-// 8 x 8), K in steps of 16 through a 3-deep cp.async ring.  Rows of both
+// 128 x TN per 256-thread block (TN = 32, 64 or 128), 64 x TN/4 per warp
+// (8 x TN/32 MMA tiles of 8 x 8), K in steps of 16 through a 3-deep
+// cp.async ring.  Rows of both
 // operands are K-contiguous but only 8-byte aligned, so the copies are
 // 8 bytes wide; shared rows are padded to 20 doubles, which keeps the
 // fragment loads free of bank conflicts.  An optional per-n-tile K range
@@ -57,11 +58,12 @@ inline StageDesc cube_stage(const double *X, long long ldx, int M, int N, int K,
   return d;
 }
 
-// One contraction given by value.
-int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s);
-// ndesc contractions from a device array; mtiles/ntiles bound the tile
-// counts of every descriptor.
-int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ntiles, double alpha,
-                       bool accumulate, cudaStream_t s);
+// One contraction given by value; tn = tile width in n (32, 64 or 128).
+int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s,
+                      int tn = kFp64TileN);
+// ndesc contractions from a device array; mtiles bounds the 128-row tile
+// count and ncols the N of every descriptor.
+int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, double alpha,
+                       bool accumulate, cudaStream_t s, int tn = kFp64TileN);
 
 }  // namespace dage

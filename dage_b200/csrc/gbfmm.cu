@@ -25,7 +25,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <array>
+#include <limits>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "fp64_stage.cuh"
@@ -387,6 +390,7 @@ struct dage_gbfmm {
   DevBuf d_U, d_W, d_desc[3];
   size_t U_per_box = 0, W_per_box = 0;
   std::vector<StageDesc> desc[3];
+  int tile_n[3] = {64, 64, 64};  // near-field stage tile widths (autotuned)
   DevBuf wts[3], partials, d_rho, d_V;
   cudaStream_t own_stream = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -730,23 +734,92 @@ int gbfmm_l2p(dage_gbfmm *g, const double *d_L, double *V) {
   return 0;
 }
 
-int gbfmm_nearfield(dage_gbfmm *g) {
-  cudaStream_t s = g->stream;
-  int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
-  const int TM = kFp64TileM, TN = kFp64TileN;
+// Largest 128-row tile count and column count of each near-field stage over
+// the boxes (the batched launch's grid bounds).
+void near_bounds(const dage_gbfmm *g, int mt[3], int nt[3]) {
+  const int TM = kFp64TileM;
+  for (int d = 0; d < 3; ++d) mt[d] = nt[d] = 0;
   for (const auto &B : g->boxes) {
     mt[0] = std::max(mt[0], ceil_div((long long)B.nq[1] * B.nq[2], TM));
-    nt[0] = std::max(nt[0], ceil_div(B.own[0], TN));
+    nt[0] = std::max(nt[0], B.own[0]);
     mt[1] = std::max(mt[1], ceil_div((long long)B.nq[2] * B.own[0], TM));
-    nt[1] = std::max(nt[1], ceil_div(B.own[1], TN));
+    nt[1] = std::max(nt[1], B.own[1]);
     mt[2] = std::max(mt[2], ceil_div((long long)B.own[0] * B.own[1], TM));
-    nt[2] = std::max(nt[2], ceil_div(B.own[2], TN));
+    nt[2] = std::max(nt[2], B.own[2]);
   }
+}
+
+// Autotuner: the tile width (32, 64 or 128 columns) of each near-field
+// stage, chosen by timing every candidate on this plan's own batched launch
+// (scratch input and output cubes, three timed launches after one warm-up)
+// and cached per (points per axis, t-points, boxes) for the process.
+std::mutex g_tune_mutex;
+std::map<std::array<int, 5>, std::array<int, 3>> g_tune_cache;
+
+int gbfmm_autotune(dage_gbfmm *g) {
+  const std::array<int, 5> key = {g->npts[0], g->npts[1], g->npts[2], g->P, g->nbox};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      for (int d = 0; d < 3; ++d) g->tile_n[d] = it->second[d];
+      return 0;
+    }
+  }
+  cudaStream_t s = g->stream;
+  const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
+  DevBuf rho, V;
+  DAGE_TRY(rho.alloc(sizeof(double) * n));
+  DAGE_TRY(V.alloc(sizeof(double) * n));
+  DAGE_CUDA_TRY(cudaMemsetAsync(rho.ptr, 0, sizeof(double) * n, s));
+  DAGE_TRY(gbfmm_descriptors(g, rho.as<double>(), V.as<double>()));
+  int mt[3], nt[3];
+  near_bounds(g, mt, nt);
+  cudaEvent_t e0, e1;
+  DAGE_CUDA_TRY(cudaEventCreate(&e0));
+  DAGE_CUDA_TRY(cudaEventCreate(&e1));
+  const int cand[3] = {32, 64, 128};
+  int rc = 0;
+  for (int st = 0; st < 3 && !rc; ++st) {
+    const StageDesc *d = g->d_desc[st].as<StageDesc>();
+    float best = std::numeric_limits<float>::max();
+    for (int tn : cand) {
+      for (int r = 0; r < 4 && !rc; ++r) {
+        if (r == 1) cudaEventRecord(e0, s);
+        rc = launch_fp64_stages(d, g->nbox, mt[st], nt[st], 1.0, false, s, tn);
+      }
+      if (rc) break;
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        g->tile_n[st] = tn;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  rho.release();
+  V.release();
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_cache[key] = {g->tile_n[0], g->tile_n[1], g->tile_n[2]};
+  return 0;
+}
+
+int gbfmm_nearfield(dage_gbfmm *g) {
+  cudaStream_t s = g->stream;
+  int mt[3], nt[3];
+  near_bounds(g, mt, nt);
   for (int p = 0; p < g->P; ++p)
     for (int st = 0; st < 3; ++st) {
       const StageDesc *d = g->d_desc[st].as<StageDesc>() + (size_t)p * g->nbox;
       const double alpha = st < 2 ? 1.0 : g->w[p];
-      DAGE_TRY(launch_fp64_stages(d, g->nbox, mt[st], nt[st], alpha, st == 2 && p > 0, s));
+      DAGE_TRY(launch_fp64_stages(d, g->nbox, mt[st], nt[st], alpha, st == 2 && p > 0, s,
+                                  g->tile_n[st]));
     }
   return 0;
 }
@@ -802,6 +875,7 @@ int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const d
   auto *g = new dage_gbfmm();
   g->precision = precision;
   int rc = gbfmm_create_impl(g, grid, maxlevel, lmax, quad);
+  if (!rc) rc = gbfmm_autotune(g);
   if (rc) {
     gbfmm_destroy_impl(g);
     return rc;
@@ -819,6 +893,12 @@ int dage_gbfmm_destroy(dage_gbfmm *g) {
 int dage_gbfmm_set_stream(dage_gbfmm *g, void *stream) {
   if (!g) return fail(DAGE_E_INVALID, "null handle");
   g->stream = stream ? (cudaStream_t)stream : g->own_stream;
+  return 0;
+}
+
+int dage_gbfmm_tiles(const dage_gbfmm *g, int tile_n[3]) {
+  if (!g || !tile_n) return fail(DAGE_E_INVALID, "null argument");
+  for (int d = 0; d < 3; ++d) tile_n[d] = g->tile_n[d];
   return 0;
 }
 

@@ -141,7 +141,6 @@ int launch_tmatrix(const TmatArgs &a, int nlip, cudaStream_t s) {
 // FP64 contraction stage (fp64_stage.cuh) on DMMA
 // ---------------------------------------------------------------------------
 constexpr int BM = kFp64TileM, BN = kFp64TileN, BK = 16, SROW = BK + 4, NST = 3;
-constexpr int kStageSmem = NST * (BM + BN) * SROW * (int)sizeof(double);
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
   const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
@@ -164,16 +163,24 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-template <bool ACCUM>
+// TN: tile width in n (32, 64 or 128); warps 2 (M) x 4 (N), each 64 x TN/4.
+template <int TN>
+constexpr int stage_smem() {
+  return NST * (BM + TN) * SROW * (int)sizeof(double);
+}
+
+template <bool ACCUM, int TN>
 __device__ __forceinline__ void stage_tile(const StageDesc &d, double alpha, int m0, int n0) {
+  constexpr int NB = TN / 32;   // 8-column MMA tiles per warp
+  constexpr int BR = TN / 16;   // B rows copied per thread per K step
   extern __shared__ double fsm[];
   double *As = fsm;                    // [NST][BM][SROW]
-  double *Bs = fsm + NST * BM * SROW;  // [NST][BN][SROW]
+  double *Bs = fsm + NST * BM * SROW;  // [NST][TN][SROW]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * (TN / 4);
   int kt0 = 0, kt1 = (d.K + BK - 1) / BK - 1;
-  if (d.krange) {
-    const int2 r = d.krange[n0 / BN];
+  if (d.krange) {  // bands are kept per 128 columns
+    const int2 r = d.krange[n0 / kFp64TileN];
     kt0 = r.x / BK;
     kt1 = r.y / BK;
   }
@@ -182,31 +189,38 @@ __device__ __forceinline__ void stage_tile(const StageDesc &d, double alpha, int
   // this thread copies rows (tid >> 4) + 16 i at K offset tid & 15
   const int kk = tid & 15;
   const double *arow[8];
-  const double *brow[8];
+  const double *brow[BR];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const long long m = m0 + (tid >> 4) + 16 * i;
-    const int n = n0 + (tid >> 4) + 16 * i;
     arow[i] = m < d.M ? d.X + (m % d.a_d0) * d.a_s1 + (m / d.a_d0) * d.a_s2 : nullptr;
+  }
+#pragma unroll
+  for (int i = 0; i < BR; ++i) {
+    const int n = n0 + (tid >> 4) + 16 * i;
     brow[i] = n < d.N ? d.T + (size_t)n * d.ldt : nullptr;
   }
   auto load = [&](int slot, int kt) {
     const int k = kt * BK + kk;
     double *as = As + slot * BM * SROW + (tid >> 4) * SROW + kk;
-    double *bs = Bs + slot * BN * SROW + (tid >> 4) * SROW + kk;
+    double *bs = Bs + slot * TN * SROW + (tid >> 4) * SROW + kk;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const bool pa = arow[i] && k < d.K, pb = brow[i] && k < d.K;
+      const bool pa = arow[i] && k < d.K;
       cp_async8(as + 16 * i * SROW, pa ? arow[i] + k : d.X, pa);
+    }
+#pragma unroll
+    for (int i = 0; i < BR; ++i) {
+      const bool pb = brow[i] && k < d.K;
       cp_async8(bs + 16 * i * SROW, pb ? brow[i] + k : d.T, pb);
     }
   };
 
-  double acc[8][4][2];
+  double acc[8][NB][2];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < NB; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
 #pragma unroll
   for (int st = 0; st < NST - 1; ++st) {
@@ -219,18 +233,18 @@ __device__ __forceinline__ void stage_tile(const StageDesc &d, double alpha, int
     if (i + NST - 1 < nk) load((i + NST - 1) % NST, kt0 + i + NST - 1);
     cp_async_commit();
     const double *as = As + (i % NST) * BM * SROW + (wm + (lane >> 2)) * SROW + (lane & 3);
-    const double *bs = Bs + (i % NST) * BN * SROW + (wn + (lane >> 2)) * SROW + (lane & 3);
+    const double *bs = Bs + (i % NST) * TN * SROW + (wn + (lane >> 2)) * SROW + (lane & 3);
 #pragma unroll
     for (int ks = 0; ks < BK / 4; ++ks) {
-      double fa[8], fb[4];
+      double fa[8], fb[NB];
 #pragma unroll
       for (int mb = 0; mb < 8; ++mb) fa[mb] = as[mb * 8 * SROW + ks * 4];
 #pragma unroll
-      for (int nb = 0; nb < 4; ++nb) fb[nb] = bs[nb * 8 * SROW + ks * 4];
+      for (int nb = 0; nb < NB; ++nb) fb[nb] = bs[nb * 8 * SROW + ks * 4];
 #pragma unroll
       for (int mb = 0; mb < 8; ++mb)
 #pragma unroll
-        for (int nb = 0; nb < 4; ++nb) dmma(acc[mb][nb], fa[mb], fb[nb]);
+        for (int nb = 0; nb < NB; ++nb) dmma(acc[mb][nb], fa[mb], fb[nb]);
     }
   }
   cp_async_wait<0>();
@@ -241,7 +255,7 @@ __device__ __forceinline__ void stage_tile(const StageDesc &d, double alpha, int
     if (m >= d.M) continue;
     double *orow = d.out + (m % d.o_d0) * d.o_s1 + (m / d.o_d0) * d.o_s2;
 #pragma unroll
-    for (int nb = 0; nb < 4; ++nb)
+    for (int nb = 0; nb < NB; ++nb)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int n = n0 + wn + nb * 8 + 2 * (lane & 3) + h;
@@ -255,19 +269,19 @@ __device__ __forceinline__ void stage_tile(const StageDesc &d, double alpha, int
   }
 }
 
-template <bool ACCUM>
+template <bool ACCUM, int TN>
 __global__ void __launch_bounds__(256, 1)
     stage_fp64_kernel(const __grid_constant__ StageDesc d, double alpha) {
-  stage_tile<ACCUM>(d, alpha, blockIdx.x * BM, blockIdx.y * BN);
+  stage_tile<ACCUM, TN>(d, alpha, blockIdx.x * BM, blockIdx.y * TN);
 }
 
-template <bool ACCUM>
+template <bool ACCUM, int TN>
 __global__ void __launch_bounds__(256, 1)
     stage_fp64_batched_kernel(const StageDesc *__restrict__ descs, double alpha) {
   const StageDesc d = descs[blockIdx.z];
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * TN;
   if (m0 >= d.M || n0 >= d.N) return;  // uniform across the block
-  stage_tile<ACCUM>(d, alpha, m0, n0);
+  stage_tile<ACCUM, TN>(d, alpha, m0, n0);
 }
 
 // Band of each (t-point, 128-row tile) of an axis matrix T[p][n][K]: the
@@ -368,46 +382,60 @@ __global__ void sum_partials_kernel(const double *partials, int n, double *resul
 
 }  // namespace
 
-template <class Kern>
-int smem_attr(Kern kern, bool &done) {
+template <bool ACCUM, int TN>
+int launch_single(const StageDesc &d, double alpha, cudaStream_t s) {
+  auto kern = stage_fp64_kernel<ACCUM, TN>;
+  static bool done = false;
   if (!done) {
     DAGE_CUDA_TRY(
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem));
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<TN>()));
     done = true;
   }
-  return 0;
-}
-
-int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s) {
-  dim3 grid(ceil_div(d.M, BM), ceil_div(d.N, BN));
+  dim3 grid(ceil_div(d.M, BM), ceil_div(d.N, TN));
   if (grid.y > 65535) return fail(DAGE_E_UNSUPPORTED, "N=%d too large", d.N);
-  static bool done[2] = {false, false};
-  if (accumulate) {
-    DAGE_TRY(smem_attr(stage_fp64_kernel<true>, done[1]));
-    stage_fp64_kernel<true><<<grid, 256, kStageSmem, s>>>(d, alpha);
-  } else {
-    DAGE_TRY(smem_attr(stage_fp64_kernel<false>, done[0]));
-    stage_fp64_kernel<false><<<grid, 256, kStageSmem, s>>>(d, alpha);
-  }
+  kern<<<grid, 256, stage_smem<TN>(), s>>>(d, alpha);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
 
-int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ntiles, double alpha,
-                       bool accumulate, cudaStream_t s) {
-  if (ndesc <= 0) return 0;
-  if (ntiles > 65535 || ndesc > 65535) return fail(DAGE_E_UNSUPPORTED, "batch too large");
-  dim3 grid(mtiles, ntiles, ndesc);
-  static bool done[2] = {false, false};
-  if (accumulate) {
-    DAGE_TRY(smem_attr(stage_fp64_batched_kernel<true>, done[1]));
-    stage_fp64_batched_kernel<true><<<grid, 256, kStageSmem, s>>>(d_descs, alpha);
-  } else {
-    DAGE_TRY(smem_attr(stage_fp64_batched_kernel<false>, done[0]));
-    stage_fp64_batched_kernel<false><<<grid, 256, kStageSmem, s>>>(d_descs, alpha);
+template <bool ACCUM, int TN>
+int launch_batched(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, double alpha,
+                   cudaStream_t s) {
+  auto kern = stage_fp64_batched_kernel<ACCUM, TN>;
+  static bool done = false;
+  if (!done) {
+    DAGE_CUDA_TRY(
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<TN>()));
+    done = true;
   }
+  dim3 grid(mtiles, ceil_div(ncols, TN), ndesc);
+  if (grid.y > 65535 || ndesc > 65535) return fail(DAGE_E_UNSUPPORTED, "batch too large");
+  kern<<<grid, 256, stage_smem<TN>(), s>>>(d_descs, alpha);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
+}
+
+int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s, int tn) {
+  switch (tn) {
+    case 32: return accumulate ? launch_single<true, 32>(d, alpha, s) : launch_single<false, 32>(d, alpha, s);
+    case 64: return accumulate ? launch_single<true, 64>(d, alpha, s) : launch_single<false, 64>(d, alpha, s);
+    case 128: return accumulate ? launch_single<true, 128>(d, alpha, s) : launch_single<false, 128>(d, alpha, s);
+  }
+  return fail(DAGE_E_INVALID, "tile width %d", tn);
+}
+
+int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, double alpha,
+                       bool accumulate, cudaStream_t s, int tn) {
+  if (ndesc <= 0) return 0;
+  switch (tn) {
+    case 32: return accumulate ? launch_batched<true, 32>(d_descs, ndesc, mtiles, ncols, alpha, s)
+                               : launch_batched<false, 32>(d_descs, ndesc, mtiles, ncols, alpha, s);
+    case 64: return accumulate ? launch_batched<true, 64>(d_descs, ndesc, mtiles, ncols, alpha, s)
+                               : launch_batched<false, 64>(d_descs, ndesc, mtiles, ncols, alpha, s);
+    case 128: return accumulate ? launch_batched<true, 128>(d_descs, ndesc, mtiles, ncols, alpha, s)
+                                : launch_batched<false, 128>(d_descs, ndesc, mtiles, ncols, alpha, s);
+  }
+  return fail(DAGE_E_INVALID, "tile width %d", tn);
 }
 
 int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,

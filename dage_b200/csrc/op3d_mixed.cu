@@ -192,14 +192,6 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 // smallest such E.  lead is exact in BF16 (8-bit integer times a power of
 // two); v - lead is exact in the working precision.  Runs whose largest
 // value is below 2^-119 keep everything in the trailing parts.
-__device__ __forceinline__ float lead_f32(float v, float m) {
-  const uint32_t mb = __float_as_uint(m);
-  const int E = (int)((mb >> 23) & 0xff) - 127 + ((mb & 0x7fffff) != 0);
-  if (m == 0.0f || E < -119) return 0.0f;
-  const float up = __uint_as_float((uint32_t)(127 + 7 - E) << 23);    // 2^(7-E)
-  const float down = __uint_as_float((uint32_t)(127 - 7 + E) << 23);  // 2^(E-7)
-  return rintf(v * up) * down;
-}
 __device__ __forceinline__ double lead_f64(double v, double m) {
   if (m == 0.0) return 0.0;
   int E = ilogb(m);
@@ -210,17 +202,6 @@ __device__ __forceinline__ double lead_f64(double v, double m) {
 // NS == 2 (bf16x3) keeps a floating leading part: with a single trailing
 // part, a fixed-point lead would give small elements only 8 bits.
 template <int NS>
-__device__ __forceinline__ void split_lead_f32(float v, float m, __nv_bfloat16 (&o)[NS]) {
-  const float l = NS == 2 ? __bfloat162float(__float2bfloat16_rn(v)) : lead_f32(v, m);
-  o[0] = __float2bfloat16_rn(l);
-  float r = v - l;
-#pragma unroll
-  for (int s = 1; s < NS; ++s) {
-    o[s] = __float2bfloat16_rn(r);
-    r = r - __bfloat162float(o[s]);
-  }
-}
-template <int NS>
 __device__ __forceinline__ void split_lead_f64(double v, double m, __nv_bfloat16 (&o)[NS]) {
   const double l = NS == 2 ? (double)__bfloat162float(__double2bfloat16(v)) : lead_f64(v, m);
   o[0] = __double2bfloat16(l);
@@ -229,6 +210,36 @@ __device__ __forceinline__ void split_lead_f64(double v, double m, __nv_bfloat16
   for (int s = 1; s < NS; ++s) {
     o[s] = __double2bfloat16(r);
     r = r - (double)__bfloat162float(o[s]);
+  }
+}
+
+// The same split for two values sharing one run maximum m, on packed FP32x2
+// arithmetic; part s of (v.x, v.y) lands in o[s] as a BF16 pair.
+template <int NS>
+__device__ __forceinline__ void split_pair_f32(float2 v, float m, __nv_bfloat162 (&o)[NS]) {
+  const float2 neg1 = make_float2(-1.0f, -1.0f);
+  float2 l;
+  if (NS == 2) {
+    o[0] = __floats2bfloat162_rn(v.x, v.y);
+    l = __bfloat1622float2(o[0]);
+  } else {
+    const uint32_t mb = __float_as_uint(m);
+    const int E = (int)((mb >> 23) & 0xff) - 127 + ((mb & 0x7fffff) != 0);
+    if (m == 0.0f || E < -119) {
+      l = make_float2(0.0f, 0.0f);
+    } else {
+      const float up = __uint_as_float((uint32_t)(127 + 7 - E) << 23);    // 2^(7-E)
+      const float down = __uint_as_float((uint32_t)(127 - 7 + E) << 23);  // 2^(E-7)
+      const float2 t = __fmul2_rn(v, make_float2(up, up));
+      l = __fmul2_rn(make_float2(rintf(t.x), rintf(t.y)), make_float2(down, down));
+    }
+    o[0] = __floats2bfloat162_rn(l.x, l.y);
+  }
+  float2 r = __ffma2_rn(l, neg1, v);  // v - lead, exact
+#pragma unroll
+  for (int s = 1; s < NS; ++s) {
+    o[s] = __floats2bfloat162_rn(r.x, r.y);
+    r = __ffma2_rn(__bfloat1622float2(o[s]), neg1, r);
   }
 }
 
@@ -473,9 +484,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t col0 = ((warp - 2) >> 2) * CW;
     int g = 0, t = 0;
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++t) {
-      float acc[CW];
+      float2 acc[CW / 2];  // columns (2j, 2j + 1)
 #pragma unroll
-      for (int j = 0; j < CW; ++j) acc[j] = 0.0f;
+      for (int j = 0; j < CW / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
       bool ok = true;
       const int nparts = (tile_steps(kblocks(a, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
       for (int pi = 0; pi < nparts; ++pi, ++g) {
@@ -493,7 +504,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_before();
         mbar_arrive(pempty(b));
 #pragma unroll
-        for (int j = 0; j < CW; ++j) acc[j] += __uint_as_float(r[j]);
+        for (int j = 0; j < CW / 2; ++j)
+          acc[j] = __fadd2_rn(acc[j], make_float2(__uint_as_float(r[2 * j]),
+                                                  __uint_as_float(r[2 * j + 1])));
       }
       if (!ok) break;
       const bool got = mbar_wait(cfull, t & 1, a.wait_limit);
@@ -509,7 +522,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_before();
         mbar_arrive(cempty);
 #pragma unroll
-        for (int j = 0; j < CW; ++j) acc[j] += __uint_as_float(r[j]);
+        for (int j = 0; j < CW / 2; ++j)
+          acc[j] = __fadd2_rn(acc[j], make_float2(__uint_as_float(r[2 * j]),
+                                                  __uint_as_float(r[2 * j + 1])));
       }
       const int mt = tile / a.n_ntiles, n0 = (tile % a.n_ntiles) * BN + col0;
       if (FINAL) {
@@ -523,7 +538,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int j = 0; j < CW; ++j) {
             const int n = n0 + j;
             if (n < a.N) {
-              const double add = a.wcoef * a.scale64[n] * (double)acc[j];
+              const double add =
+                  a.wcoef * a.scale64[n] * (double)((j & 1) ? acc[j >> 1].y : acc[j >> 1].x);
               double *dst = col + (size_t)a.M * n;
               if (a.accumulate)
                 atomicAdd(dst, add);
@@ -549,30 +565,26 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int n = n0 + j;
           if (n < a.N) {  // uniform across the warp
             const bool has1 = n + 1 < a.N;
-            const float v0 = valid ? acc[j] * a.scale[n] : 0.0f;
-            const float v1 = valid && has1 ? acc[j + 1] * a.scale[n + 1] : 0.0f;
+            const float2 sc = make_float2(a.scale[n], has1 ? a.scale[n + 1] : 0.0f);
+            const float2 v = valid ? __fmul2_rn(acc[j >> 1], sc) : make_float2(0.0f, 0.0f);
             float m = 0.0f;
             if (NSX > 2) {
               const float m0 =
-                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v0))));
+                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v.x))));
               const float m1 =
-                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v1))));
+                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v.y))));
               m = odd ? m1 : m0;
             }
-            const float recv = __shfl_xor_sync(0xffffffffu, odd ? v0 : v1, 1);
-            const float mine = odd ? v1 : v0;
-            const float lo = odd ? recv : mine, hi = odd ? mine : recv;
-            __nv_bfloat16 pl[NSX], ph[NSX];
-            split_lead_f32<NSX>(lo, m, pl);
-            split_lead_f32<NSX>(hi, m, ph);
+            const float recv = __shfl_xor_sync(0xffffffffu, odd ? v.x : v.y, 1);
+            const float mine = odd ? v.y : v.x;
+            __nv_bfloat162 pp[NSX];
+            split_pair_f32<NSX>(odd ? make_float2(recv, mine) : make_float2(mine, recv), m, pp);
             if (rpair < a.d0 && (!odd || has1)) {
               const size_t off =
                   (size_t)(r1 + (long long)a.d1 * (n + (odd ? 1 : 0))) * a.ldn + rpair;
-              *reinterpret_cast<__nv_bfloat162 *>(a.out0 + off) = __halves2bfloat162(pl[0], ph[0]);
-              *reinterpret_cast<__nv_bfloat162 *>(a.out1 + off) = __halves2bfloat162(pl[1], ph[1]);
-              if (NSX > 2)
-                *reinterpret_cast<__nv_bfloat162 *>(a.out2 + off) =
-                    __halves2bfloat162(pl[NSX > 2 ? 2 : 0], ph[NSX > 2 ? 2 : 0]);
+              *reinterpret_cast<__nv_bfloat162 *>(a.out0 + off) = pp[0];
+              *reinterpret_cast<__nv_bfloat162 *>(a.out1 + off) = pp[1];
+              if (NSX > 2) *reinterpret_cast<__nv_bfloat162 *>(a.out2 + off) = pp[NSX > 2 ? 2 : 0];
             }
           }
         }

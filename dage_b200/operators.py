@@ -315,6 +315,13 @@ class GBFMMCoulomb3D:
         check(lib.dage_gbfmm_box_count(h, ctypes.byref(nb), ctypes.byref(nlm)))
         self.nbox, self.nlm = nb.value, nlm.value
 
+    @property
+    def tiles(self):
+        """Near-field stage tile widths chosen by the autotuner (x, y, z)."""
+        t = (ctypes.c_int * 3)()
+        check(load().dage_gbfmm_tiles(self._h, t))
+        return tuple(t)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

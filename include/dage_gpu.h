@@ -173,6 +173,10 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
                            unsigned flags);
 
 int dage_gbfmm_box_count(const dage_gbfmm *g, int *nbox, int *nlm);
+/* Tile widths (32, 64 or 128 columns) the plan's autotuner chose for the
+ * three near-field contraction stages (no reference counterpart: the
+ * reference issues one cuBLAS call per box). */
+int dage_gbfmm_tiles(const dage_gbfmm *g, int tile_n[3]);
 int dage_gbfmm_set_stream(dage_gbfmm *g, void *stream);
 int dage_gbfmm_last_time_ms(const dage_gbfmm *g, float *ms);
 int dage_gbfmm_destroy(dage_gbfmm *g);

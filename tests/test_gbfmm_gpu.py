@@ -54,6 +54,7 @@ def test_gbfmm_apply_matches_oracle(dage, oracle, ncell, lmax):
     g, go, rho = _setup(dage, oracle, ncell, 0.2)
     quad = (8, 8, 0.0, 2.0, 1e3)
     op = dage.GBFMMCoulomb3D(g, lmax=lmax, quad=dage.GaussQuad(*quad))
+    assert set(op.tiles) <= {32, 64, 128}  # near-field tile widths from the autotuner
     V, E = op.apply(rho, energy=True)
     Vo = oracle.gbfmm_apply(go, rho, lmax=lmax, quad=quad)
     V1 = oracle.gbfmm_apply(go, rho, lmax=lmax, quad=quad, libm_1ulp=True)
