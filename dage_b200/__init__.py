@@ -8,6 +8,7 @@ from ._capi import DageError, load  # noqa: F401
 from .operators import (  # noqa: F401
     Bubbles,
     Coulomb3D,
+    GBFMMBatch,
     GBFMMCoulomb3D,
     GaussQuad,
     Grid1D,
@@ -18,5 +19,5 @@ from .operators import (  # noqa: F401
     integrate,
 )
 
-__all__ = ["Bubbles", "Coulomb3D", "GBFMMCoulomb3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
+__all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
            "DageError", "dot", "integrate", "load"]

@@ -11,6 +11,7 @@ DAGE_DEVICE_PTRS = 1
 DAGE_ENERGY = 2
 DAGE_NO_CODA = 4
 DAGE_ACCUMULATE = 8
+DAGE_NO_GRAPH = 16
 
 DAGE_FP64 = 0
 DAGE_MIXED_BF16X3 = 1
@@ -69,6 +70,16 @@ SIGNATURES = {
     "dage_gbfmm_multipole_moments": (ctypes.c_int, [_VP, _VP, ctypes.c_uint, _D]),
     "dage_gbfmm_local_expansions": (ctypes.c_int, [_VP, _D]),
     "dage_gbfmm_evaluate_le": (ctypes.c_int, [_VP, _D, _VP, ctypes.c_uint]),
+    "dage_gbfmm_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(DageGrid1D), ctypes.c_int,
+                                               ctypes.c_int, _VP, ctypes.c_size_t, _VP]),
+    "dage_gbfmm_batch_apply": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint, _D]),
+    "dage_gbfmm_batch_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_longlong)]),
+    "dage_gbfmm_batch_set_stream": (ctypes.c_int, [_VP, _VP]),
+    "dage_gbfmm_batch_last_time_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
+    "dage_gbfmm_batch_destroy": (ctypes.c_int, [_VP]),
     "dage_gbfmm_tiles": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "dage_gbfmm_box_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),

@@ -32,6 +32,7 @@ struct StageDesc {
   long long o_d0, o_s1, o_s2, o_sn;
   int M, N, K;
   const int2 *krange;  // per 128-column tile: K band [first, last], or null
+  long long t_ps;      // batched launches: T of t-point p is T + p * t_ps
 };
 
 constexpr int kFp64TileM = 128, kFp64TileN = 128;
@@ -61,9 +62,9 @@ inline StageDesc cube_stage(const double *X, long long ldx, int M, int N, int K,
 // One contraction given by value; tn = tile width in n (32, 64 or 128).
 int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStream_t s,
                       int tn = kFp64TileN);
-// ndesc contractions from a device array; mtiles bounds the 128-row tile
-// count and ncols the N of every descriptor.
-int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, double alpha,
-                       bool accumulate, cudaStream_t s, int tn = kFp64TileN);
+// ndesc contractions from a device array, with the matrices of t-point p;
+// mtiles bounds the 128-row tile count and ncols the N of every descriptor.
+int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, int p,
+                       double alpha, bool accumulate, cudaStream_t s, int tn = kFp64TileN);
 
 }  // namespace dage

@@ -99,35 +99,51 @@ struct BoxInfo {
   double c[3];          // expansion centre
 };
 
+// One density of a batch (a batch of one for dage_gbfmm_apply): its cubes,
+// its expansion buffers, and the tables of the plan (grid geometry) it
+// shares with every density on the same grid.
+struct GInst {
+  const double *rho;
+  double *V;
+  double *q, *L, *partial;  // moments, local expansions (nbox x N), slab sums
+  double *epart;            // energy partial sums [kEnergyBlocks]
+  const BoxInfo *boxes;     // plan: nbox boxes
+  const double *wbox;       // plan: per-position box weights, then coordinates
+  int wstride, Nx, Ny, Nz;
+  const double *Tm2l;       // plan: M2L matrix per displacement
+  const int *ffstart, *ffsrc, *ffdisp;  // plan: far-field lists
+  const double *wx, *wy, *wz;           // plan: full-grid integration weights
+};
+
+constexpr int kEnergyBlocks = 256;
+
 // ---------------------------------------------------------------------------
-// Multipole moments: block (box, slab); each thread accumulates its own
-// column of partial sums in shared memory, then one fixed-order reduction.
+// Multipole moments: block (box, slab, density); each thread accumulates its
+// own column of partial sums in shared memory, then one fixed-order
+// reduction.
 // ---------------------------------------------------------------------------
-__global__ void multipoles_kernel(const double *__restrict__ rho, int Nx, int Ny,
-                                  const BoxInfo *__restrict__ boxes,
-                                  const double *__restrict__ wbox, int wstride, int lmax,
-                                  int nslab, double *partial) {
+__global__ void multipoles_kernel(const GInst *__restrict__ insts, int lmax, int nslab) {
   extern __shared__ double part[];  // [N][blockDim.x]
+  const GInst I = insts[blockIdx.z];
   const int N = (lmax + 1) * (lmax + 1);
   const int T = blockDim.x, tid = threadIdx.x;
-  const BoxInfo b = boxes[blockIdx.x];
+  const BoxInfo b = I.boxes[blockIdx.x];
   for (int s = 0; s < N; ++s) part[s * T + tid] = 0.0;
-  const double *wx = wbox + (0 * 64 + b.pos[0]) * wstride;
-  const double *wy = wbox + (1 * 64 + b.pos[1]) * wstride;
-  const double *wz = wbox + (2 * 64 + b.pos[2]) * wstride;
+  const int ws = I.wstride;
+  const double *wx = I.wbox + (0 * 64 + b.pos[0]) * ws;
+  const double *wy = I.wbox + (1 * 64 + b.pos[1]) * ws;
+  const double *wz = I.wbox + (2 * 64 + b.pos[2]) * ws;
+  const double *xs = I.wbox + (3 * 64) * ws;  // point coordinates per axis
   const long long plane = (long long)b.np[0] * b.np[1];
   for (int k = blockIdx.y; k < b.np[2]; k += nslab) {
     for (long long e = tid; e < plane; e += T) {
       const int i = (int)(e % b.np[0]), j = (int)(e / b.np[0]);
-      const size_t g = (size_t)(b.p0[0] + i) + (size_t)Nx * (b.p0[1] + j) +
-                       (size_t)Nx * Ny * (b.p0[2] + k);
-      const double v = rho[g] * (wx[i] * wy[j] * wz[k]);
-      // coordinates relative to the centre are rebuilt from the box grid
-      // spacing table (xs) by the caller: passed via wbox's tail
-      const double *xs = wbox + (3 * 64) * wstride;
+      const size_t g = (size_t)(b.p0[0] + i) + (size_t)I.Nx * (b.p0[1] + j) +
+                       (size_t)I.Nx * I.Ny * (b.p0[2] + k);
+      const double v = I.rho[g] * (wx[i] * wy[j] * wz[k]);
       const double x = xs[b.p0[0] + i] - b.c[0];
-      const double y = xs[wstride + b.p0[1] + j] - b.c[1];
-      const double z = xs[2 * wstride + b.p0[2] + k] - b.c[2];
+      const double y = xs[ws + b.p0[1] + j] - b.c[1];
+      const double z = xs[2 * ws + b.p0[2] + k] - b.c[2];
       solid_harmonics(lmax, x, y, z, [&](int lm, double s) { part[lm * T + tid] += v * s; });
     }
   }
@@ -135,18 +151,19 @@ __global__ void multipoles_kernel(const double *__restrict__ rho, int Nx, int Ny
   for (int s = tid; s < N; s += T) {
     double acc = 0.0;
     for (int t = 0; t < T; ++t) acc += part[s * T + t];
-    partial[((size_t)blockIdx.x * nslab + blockIdx.y) * N + s] = acc;
+    I.partial[((size_t)blockIdx.x * nslab + blockIdx.y) * N + s] = acc;
   }
 }
 
-__global__ void reduce_slabs_kernel(const double *partial, int nslab, int N, int nbox,
-                                    double *q) {
+// q(box, lm) = sum over slabs, fixed order; grid (., density)
+__global__ void reduce_slabs_kernel(const GInst *__restrict__ insts, int nslab, int N, int nbox) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nbox * N) return;
+  const GInst &I = insts[blockIdx.y];
   const int b = idx / N, s = idx % N;
   double acc = 0.0;
-  for (int k = 0; k < nslab; ++k) acc += partial[((size_t)b * nslab + k) * N + s];
-  q[(size_t)b * N + s] = acc;
+  for (int k = 0; k < nslab; ++k) acc += I.partial[((size_t)b * nslab + k) * N + s];
+  I.q[(size_t)b * N + s] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -192,35 +209,39 @@ __global__ void m2l_matrices_kernel(const double *__restrict__ disp, int lmax,
   }
 }
 
-// L(b) = sum over the far field of b of T(disp) q(src); one block per box.
-__global__ void m2l_apply_kernel(const double *__restrict__ Tall, const double *__restrict__ q,
-                                 const int *__restrict__ ff_start, const int *__restrict__ ff_src,
-                                 const int *__restrict__ ff_disp, int N, double *Lout) {
+// L(b) = sum over the far field of b of T(disp) q(src); block (box, density).
+__global__ void m2l_apply_kernel(const GInst *__restrict__ insts, int N) {
   extern __shared__ double qs[];
+  const GInst &I = insts[blockIdx.y];
   const int b = blockIdx.x;
   double acc = 0.0;
   const int i = threadIdx.x;
-  for (int e = ff_start[b]; e < ff_start[b + 1]; ++e) {
+  for (int e = I.ffstart[b]; e < I.ffstart[b + 1]; ++e) {
     __syncthreads();
-    for (int k = threadIdx.x; k < N; k += blockDim.x) qs[k] = q[(size_t)ff_src[e] * N + k];
+    for (int k = threadIdx.x; k < N; k += blockDim.x) qs[k] = I.q[(size_t)I.ffsrc[e] * N + k];
     __syncthreads();
     if (i < N) {
-      const double *T = Tall + (size_t)ff_disp[e] * N * N;
+      const double *T = I.Tm2l + (size_t)I.ffdisp[e] * N * N;
       for (int k = 0; k < N; ++k) acc += T[(size_t)k * N + i] * qs[k];
     }
   }
-  if (i < N) Lout[(size_t)b * N + i] = acc;
+  if (i < N) I.L[(size_t)b * N + i] = acc;
 }
 
-// V(r) += sum_lm L_lm S_lm(r - c) over the owned points of every box.
-__global__ void l2p_kernel(const double *__restrict__ L, const BoxInfo *__restrict__ boxes,
-                           const double *__restrict__ xs, int xstride, int lmax, int Nx, int Ny,
-                           double *V) {
+// V(r) += sum_lm L_lm S_lm(r - c) over the owned points of every box; block
+// (chunk, box, density).  L = the density's own local expansions unless
+// Lext is given (evaluation of caller-supplied expansions).
+__global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__restrict__ Lext,
+                           int lmax) {
   extern __shared__ double Ls[];
+  const GInst &I = insts[blockIdx.z];
   const int N = (lmax + 1) * (lmax + 1);
-  const BoxInfo b = boxes[blockIdx.y];
+  const BoxInfo b = I.boxes[blockIdx.y];
+  const double *L = Lext ? Lext : I.L;
   for (int k = threadIdx.x; k < N; k += blockDim.x) Ls[k] = L[(size_t)blockIdx.y * N + k];
   __syncthreads();
+  const double *xs = I.wbox + (3 * 64) * I.wstride;
+  const int ws = I.wstride;
   const long long n = (long long)b.own[0] * b.own[1] * b.own[2];
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
@@ -229,10 +250,43 @@ __global__ void l2p_kernel(const double *__restrict__ L, const BoxInfo *__restri
     const int j = (int)(r % b.own[1]), k = (int)(r / b.own[1]);
     const int gx = b.p0[0] + i, gy = b.p0[1] + j, gz = b.p0[2] + k;
     double v = 0.0;
-    solid_harmonics(lmax, xs[gx] - b.c[0], xs[xstride + gy] - b.c[1], xs[2 * xstride + gz] - b.c[2],
+    solid_harmonics(lmax, xs[gx] - b.c[0], xs[ws + gy] - b.c[1], xs[2 * ws + gz] - b.c[2],
                     [&](int lm, double s) { v += Ls[lm] * s; });
-    V[(size_t)gx + (size_t)Nx * gy + (size_t)Nx * Ny * gz] += v;
+    I.V[(size_t)gx + (size_t)I.Nx * gy + (size_t)I.Nx * I.Ny * gz] += v;
   }
+}
+
+// Energy int rho V with the LIP weights: kEnergyBlocks fixed blocks per
+// density, then one fixed-order sum per density (deterministic).
+__global__ void energy_kernel(const GInst *__restrict__ insts) {
+  __shared__ double sh[32];
+  const GInst &I = insts[blockIdx.y];
+  const long long n = (long long)I.Nx * I.Ny * I.Nz;
+  double acc = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(e % I.Nx);
+    const long long r = e / I.Nx;
+    const int y = (int)(r % I.Ny), z = (int)(r / I.Ny);
+    acc += I.rho[e] * I.V[e] * (I.wx[x] * I.wy[y] * I.wz[z]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    I.epart[blockIdx.x] = t;
+  }
+}
+
+__global__ void energy_sum_kernel(const GInst *__restrict__ insts, double *out) {
+  if (threadIdx.x != 0) return;
+  const GInst &I = insts[blockIdx.x];
+  double t = 0.0;
+  for (int k = 0; k < kEnergyBlocks; ++k) t += I.epart[k];
+  out[blockIdx.x] = t;
 }
 
 // ---------------------------------------------------------------------------
@@ -391,7 +445,7 @@ struct dage_gbfmm {
   size_t U_per_box = 0, W_per_box = 0;
   std::vector<StageDesc> desc[3];
   int tile_n[3] = {64, 64, 64};  // near-field stage tile widths (autotuned)
-  DevBuf wts[3], partials, d_rho, d_V;
+  DevBuf wts[3], d_epart, d_energy, d_inst, d_rho, d_V;
   cudaStream_t own_stream = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
@@ -620,125 +674,113 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
     DAGE_TRY(g->wts[d].alloc(sizeof(double) * g->npts[d]));
     DAGE_CUDA_TRY(cudaMemcpyAsync(g->wts[d].ptr, g->ax[d].weights.data(),
                                   sizeof(double) * g->npts[d], cudaMemcpyHostToDevice, s));
-    DAGE_TRY(g->d_desc[d].alloc(sizeof(StageDesc) * g->nbox * g->P));
+    DAGE_TRY(g->d_desc[d].alloc(sizeof(StageDesc) * g->nbox));
   }
-  DAGE_TRY(g->partials.alloc(sizeof(double) * (finalize_partials_count() + 1)));
+  DAGE_TRY(g->d_epart.alloc(sizeof(double) * kEnergyBlocks));
+  DAGE_TRY(g->d_energy.alloc(sizeof(double)));
+  DAGE_TRY(g->d_inst.alloc(sizeof(GInst)));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   return 0;
 }
 
-// Fills the three stage descriptor arrays (for all t-points) for the given
-// device rho and V.
-int gbfmm_descriptors(dage_gbfmm *g, const double *rho, double *V) {
+
+// ---------------------------------------------------------------------------
+// Pipeline pieces shared by the single-density and batched applies
+// ---------------------------------------------------------------------------
+GInst plan_inst(const dage_gbfmm *g, const double *rho, double *V, double *q, double *L,
+                double *partial, double *epart) {
+  GInst I{};
+  I.rho = rho;
+  I.V = V;
+  I.q = q;
+  I.L = L;
+  I.partial = partial;
+  I.epart = epart;
+  I.boxes = g->d_boxes.as<BoxInfo>();
+  I.wbox = g->d_wbox.as<double>();
+  I.wstride = g->wstride;
+  I.Nx = g->npts[0];
+  I.Ny = g->npts[1];
+  I.Nz = g->npts[2];
+  I.Tm2l = g->d_Tm2l.as<double>();
+  I.ffstart = g->d_ffstart.as<int>();
+  I.ffsrc = g->d_ffsrc.as<int>();
+  I.ffdisp = g->d_ffdisp.as<int>();
+  I.wx = g->wts[0].as<double>();
+  I.wy = g->wts[1].as<double>();
+  I.wz = g->wts[2].as<double>();
+  return I;
+}
+
+// Appends the near-field stage descriptors of one density (one per box and
+// stage; t-point p reads its matrices at T + p * t_ps) with intermediates
+// U (U_per_box per box) and W (W_per_box per box).
+void near_descs(const dage_gbfmm *g, const double *rho, double *V, double *U0, double *W0,
+                std::vector<StageDesc> ds[3]) {
   const int Nx = g->npts[0], Ny = g->npts[1];
-  std::vector<StageDesc> ds[3];
-  for (int p = 0; p < g->P; ++p)
-    for (int b = 0; b < g->nbox; ++b) {
-      const BoxInfo &B = g->boxes[b];
-      double *U = g->d_U.as<double>() + g->U_per_box * b;
-      double *W = g->d_W.as<double>() + g->W_per_box * b;
-      StageDesc x{}, y{}, z{};
-      // stage x: rho near region (a: x, rows (b: y, c: z)) -> U(R=(y,z), n=x_own)
-      x.M = B.nq[1] * B.nq[2];
-      x.N = B.own[0];
-      x.K = B.nq[0];
-      x.X = rho + B.q0[0] + (size_t)Nx * B.q0[1] + (size_t)Nx * Ny * B.q0[2];
-      x.a_d0 = B.nq[1];
-      x.a_s1 = Nx;
-      x.a_s2 = (long long)Nx * Ny;
-      x.T = g->Tnear[0][B.pos[0]].as<double>() + (size_t)p * B.own[0] * B.nq[0];
-      x.ldt = B.nq[0];
-      x.out = U;
-      x.o_d0 = x.M;
-      x.o_s1 = 1;
-      x.o_s2 = 0;
-      x.o_sn = x.M;
-      // stage y: U (K = y near, rows (z near, x own)) -> W(R=(z, x), n=y_own)
-      y.M = B.nq[2] * B.own[0];
-      y.N = B.own[1];
-      y.K = B.nq[1];
-      y.X = U;
-      y.a_d0 = y.M;
-      y.a_s1 = B.nq[1];
-      y.a_s2 = 0;
-      y.T = g->Tnear[1][B.pos[1]].as<double>() + (size_t)p * B.own[1] * B.nq[1];
-      y.ldt = B.nq[1];
-      y.out = W;
-      y.o_d0 = y.M;
-      y.o_s1 = 1;
-      y.o_s2 = 0;
-      y.o_sn = y.M;
-      // stage z: W (K = z near, rows (x own, y own)) -> V box (owned points)
-      z.M = B.own[0] * B.own[1];
-      z.N = B.own[2];
-      z.K = B.nq[2];
-      z.X = W;
-      z.a_d0 = z.M;
-      z.a_s1 = B.nq[2];
-      z.a_s2 = 0;
-      z.T = g->Tnear[2][B.pos[2]].as<double>() + (size_t)p * B.own[2] * B.nq[2];
-      z.ldt = B.nq[2];
-      z.out = V + B.p0[0] + (size_t)Nx * B.p0[1] + (size_t)Nx * Ny * B.p0[2];
-      z.o_d0 = B.own[0];
-      z.o_s1 = 1;
-      z.o_s2 = Nx;
-      z.o_sn = (long long)Nx * Ny;
-      ds[0].push_back(x);
-      ds[1].push_back(y);
-      ds[2].push_back(z);
-    }
-  for (int d = 0; d < 3; ++d)
-    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_desc[d].ptr, ds[d].data(), sizeof(StageDesc) * ds[d].size(),
-                                  cudaMemcpyHostToDevice, g->stream));
-  return 0;
-}
-
-int gbfmm_multipoles(dage_gbfmm *g, const double *rho) {
-  cudaStream_t s = g->stream;
-  int threads = 128;
-  size_t smem = sizeof(double) * g->N * threads;
-  while (smem > 200 * 1024 && threads > 32) {
-    threads -= 32;
-    smem = sizeof(double) * g->N * threads;
+  for (int b = 0; b < g->nbox; ++b) {
+    const BoxInfo &B = g->boxes[b];
+    double *U = U0 + g->U_per_box * b;
+    double *W = W0 + g->W_per_box * b;
+    StageDesc x{}, y{}, z{};
+    // stage x: rho near region (a: x, rows (b: y, c: z)) -> U(R=(y,z), n=x_own)
+    x.M = B.nq[1] * B.nq[2];
+    x.N = B.own[0];
+    x.K = B.nq[0];
+    x.X = rho + B.q0[0] + (size_t)Nx * B.q0[1] + (size_t)Nx * Ny * B.q0[2];
+    x.a_d0 = B.nq[1];
+    x.a_s1 = Nx;
+    x.a_s2 = (long long)Nx * Ny;
+    x.T = g->Tnear[0][B.pos[0]].as<double>();
+    x.t_ps = (long long)B.own[0] * B.nq[0];
+    x.ldt = B.nq[0];
+    x.out = U;
+    x.o_d0 = x.M;
+    x.o_s1 = 1;
+    x.o_s2 = 0;
+    x.o_sn = x.M;
+    // stage y: U (K = y near, rows (z near, x own)) -> W(R=(z, x), n=y_own)
+    y.M = B.nq[2] * B.own[0];
+    y.N = B.own[1];
+    y.K = B.nq[1];
+    y.X = U;
+    y.a_d0 = y.M;
+    y.a_s1 = B.nq[1];
+    y.a_s2 = 0;
+    y.T = g->Tnear[1][B.pos[1]].as<double>();
+    y.t_ps = (long long)B.own[1] * B.nq[1];
+    y.ldt = B.nq[1];
+    y.out = W;
+    y.o_d0 = y.M;
+    y.o_s1 = 1;
+    y.o_s2 = 0;
+    y.o_sn = y.M;
+    // stage z: W (K = z near, rows (x own, y own)) -> V box (owned points)
+    z.M = B.own[0] * B.own[1];
+    z.N = B.own[2];
+    z.K = B.nq[2];
+    z.X = W;
+    z.a_d0 = z.M;
+    z.a_s1 = B.nq[2];
+    z.a_s2 = 0;
+    z.T = g->Tnear[2][B.pos[2]].as<double>();
+    z.t_ps = (long long)B.own[2] * B.nq[2];
+    z.ldt = B.nq[2];
+    z.out = V + B.p0[0] + (size_t)Nx * B.p0[1] + (size_t)Nx * Ny * B.p0[2];
+    z.o_d0 = B.own[0];
+    z.o_s1 = 1;
+    z.o_s2 = Nx;
+    z.o_sn = (long long)Nx * Ny;
+    ds[0].push_back(x);
+    ds[1].push_back(y);
+    ds[2].push_back(z);
   }
-  DAGE_CUDA_TRY(cudaFuncSetAttribute(multipoles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-  multipoles_kernel<<<dim3(g->nbox, g->nslab), threads, smem, s>>>(
-      rho, g->npts[0], g->npts[1], g->d_boxes.as<BoxInfo>(), g->d_wbox.as<double>(), g->wstride,
-      g->lmax, g->nslab, g->d_partial.as<double>());
-  DAGE_CUDA_TRY(cudaGetLastError());
-  const int n = g->nbox * g->N;
-  reduce_slabs_kernel<<<(n + 255) / 256, 256, 0, s>>>(g->d_partial.as<double>(), g->nslab, g->N,
-                                                      g->nbox, g->d_q.as<double>());
-  DAGE_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-int gbfmm_m2l(dage_gbfmm *g) {
-  const int threads = ((g->N + 31) / 32) * 32;
-  m2l_apply_kernel<<<g->nbox, threads, sizeof(double) * g->N, g->stream>>>(
-      g->d_Tm2l.as<double>(), g->d_q.as<double>(), g->d_ffstart.as<int>(), g->d_ffsrc.as<int>(),
-      g->d_ffdisp.as<int>(), g->N, g->d_L.as<double>());
-  DAGE_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-int gbfmm_l2p(dage_gbfmm *g, const double *d_L, double *V) {
-  int maxown = 0;
-  for (const auto &B : g->boxes) maxown = std::max(maxown, B.own[0] * B.own[1] * B.own[2]);
-  const int bx = std::min((maxown + 127) / 128, 64);
-  l2p_kernel<<<dim3(bx, g->nbox), 128, sizeof(double) * g->N, g->stream>>>(
-      d_L, g->d_boxes.as<BoxInfo>(), g->d_wbox.as<double>() + (size_t)3 * 64 * g->wstride,
-      g->wstride, g->lmax, g->npts[0], g->npts[1], V);
-  DAGE_CUDA_TRY(cudaGetLastError());
-  return 0;
 }
 
 // Largest 128-row tile count and column count of each near-field stage over
-// the boxes (the batched launch's grid bounds).
+// the boxes of a plan (a batched launch's grid bounds).
 void near_bounds(const dage_gbfmm *g, int mt[3], int nt[3]) {
   const int TM = kFp64TileM;
-  for (int d = 0; d < 3; ++d) mt[d] = nt[d] = 0;
   for (const auto &B : g->boxes) {
     mt[0] = std::max(mt[0], ceil_div((long long)B.nq[1] * B.nq[2], TM));
     nt[0] = std::max(nt[0], B.own[0]);
@@ -749,10 +791,103 @@ void near_bounds(const dage_gbfmm *g, int mt[3], int nt[3]) {
   }
 }
 
+int max_owned(const dage_gbfmm *g) {
+  int m = 0;
+  for (const auto &B : g->boxes) m = std::max(m, B.own[0] * B.own[1] * B.own[2]);
+  return m;
+}
+
+int multipoles_smem(int N, int *threads) {
+  int t = 128;
+  while ((size_t)sizeof(double) * N * t > 200 * 1024 && t > 32) t -= 32;
+  *threads = t;
+  const int smem = (int)(sizeof(double) * N * t);
+  DAGE_CUDA_TRY(
+      cudaFuncSetAttribute(multipoles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  return 0;
+}
+
+int run_multipoles(const GInst *d_inst, int ninst, int nbox, int lmax, int nslab, cudaStream_t s) {
+  const int N = (lmax + 1) * (lmax + 1);
+  int threads;
+  DAGE_TRY(multipoles_smem(N, &threads));
+  multipoles_kernel<<<dim3(nbox, nslab, ninst), threads, sizeof(double) * N * threads, s>>>(
+      d_inst, lmax, nslab);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  reduce_slabs_kernel<<<dim3((nbox * N + 255) / 256, ninst), 256, 0, s>>>(d_inst, nslab, N, nbox);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int run_m2l(const GInst *d_inst, int ninst, int nbox, int N, cudaStream_t s) {
+  const int threads = ((N + 31) / 32) * 32;
+  m2l_apply_kernel<<<dim3(nbox, ninst), threads, sizeof(double) * N, s>>>(d_inst, N);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int run_l2p(const GInst *d_inst, int ninst, int nbox, int lmax, int maxown, const double *Lext,
+            cudaStream_t s) {
+  const int N = (lmax + 1) * (lmax + 1);
+  const int bx = std::min((maxown + 127) / 128, 64);
+  l2p_kernel<<<dim3(bx, nbox, ninst), 128, sizeof(double) * N, s>>>(d_inst, Lext, lmax);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int run_near(const StageDesc *const d_desc[3], int njobs, const int mt[3], const int nt[3], int P,
+             const std::vector<double> &w, const int tile_n[3], cudaStream_t s) {
+  for (int p = 0; p < P; ++p)
+    for (int st = 0; st < 3; ++st)
+      DAGE_TRY(launch_fp64_stages(d_desc[st], njobs, mt[st], nt[st], p, st < 2 ? 1.0 : w[p],
+                                  st == 2 && p > 0, s, tile_n[st]));
+  return 0;
+}
+
+int run_energy(const GInst *d_inst, int ninst, double *d_out, cudaStream_t s) {
+  energy_kernel<<<dim3(kEnergyBlocks, ninst), 256, 0, s>>>(d_inst);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  energy_sum_kernel<<<ninst, 32, 0, s>>>(d_inst, d_out);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 // Autotuner: the tile width (32, 64 or 128 columns) of each near-field
-// stage, chosen by timing every candidate on this plan's own batched launch
-// (scratch input and output cubes, three timed launches after one warm-up)
-// and cached per (points per axis, t-points, boxes) for the process.
+// stage, chosen by timing every candidate on a batched launch of t-point 0
+// (one warm-up, three timed launches; the launches write the intermediates
+// and the output cubes of the descriptors, which the caller overwrites).
+int autotune_tiles(const StageDesc *const d_desc[3], int njobs, const int mt[3], const int nt[3],
+                   cudaStream_t s, int tile_n[3]) {
+  cudaEvent_t e0, e1;
+  DAGE_CUDA_TRY(cudaEventCreate(&e0));
+  DAGE_CUDA_TRY(cudaEventCreate(&e1));
+  const int cand[3] = {32, 64, 128};
+  int rc = 0;
+  for (int st = 0; st < 3 && !rc; ++st) {
+    float best = std::numeric_limits<float>::max();
+    for (int tn : cand) {
+      for (int r = 0; r < 4 && !rc; ++r) {
+        if (r == 1) cudaEventRecord(e0, s);
+        rc = launch_fp64_stages(d_desc[st], njobs, mt[st], nt[st], 0, 1.0, false, s, tn);
+      }
+      if (rc) break;
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        tile_n[st] = tn;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+// The plan's own tiles, cached per (points per axis, t-points, boxes) for
+// the process; tuned on scratch input and output cubes.
 std::mutex g_tune_mutex;
 std::map<std::array<int, 5>, std::array<int, 3>> g_tune_cache;
 
@@ -772,35 +907,16 @@ int gbfmm_autotune(dage_gbfmm *g) {
   DAGE_TRY(rho.alloc(sizeof(double) * n));
   DAGE_TRY(V.alloc(sizeof(double) * n));
   DAGE_CUDA_TRY(cudaMemsetAsync(rho.ptr, 0, sizeof(double) * n, s));
-  DAGE_TRY(gbfmm_descriptors(g, rho.as<double>(), V.as<double>()));
-  int mt[3], nt[3];
+  std::vector<StageDesc> ds[3];
+  near_descs(g, rho.as<double>(), V.as<double>(), g->d_U.as<double>(), g->d_W.as<double>(), ds);
+  for (int d = 0; d < 3; ++d)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_desc[d].ptr, ds[d].data(), sizeof(StageDesc) * g->nbox,
+                                  cudaMemcpyHostToDevice, s));
+  int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
   near_bounds(g, mt, nt);
-  cudaEvent_t e0, e1;
-  DAGE_CUDA_TRY(cudaEventCreate(&e0));
-  DAGE_CUDA_TRY(cudaEventCreate(&e1));
-  const int cand[3] = {32, 64, 128};
-  int rc = 0;
-  for (int st = 0; st < 3 && !rc; ++st) {
-    const StageDesc *d = g->d_desc[st].as<StageDesc>();
-    float best = std::numeric_limits<float>::max();
-    for (int tn : cand) {
-      for (int r = 0; r < 4 && !rc; ++r) {
-        if (r == 1) cudaEventRecord(e0, s);
-        rc = launch_fp64_stages(d, g->nbox, mt[st], nt[st], 1.0, false, s, tn);
-      }
-      if (rc) break;
-      cudaEventRecord(e1, s);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) {
-        best = ms;
-        g->tile_n[st] = tn;
-      }
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  const StageDesc *dd[3] = {g->d_desc[0].as<StageDesc>(), g->d_desc[1].as<StageDesc>(),
+                            g->d_desc[2].as<StageDesc>()};
+  const int rc = autotune_tiles(dd, g->nbox, mt, nt, s, g->tile_n);
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   rho.release();
   V.release();
@@ -810,17 +926,20 @@ int gbfmm_autotune(dage_gbfmm *g) {
   return 0;
 }
 
-int gbfmm_nearfield(dage_gbfmm *g) {
-  cudaStream_t s = g->stream;
-  int mt[3], nt[3];
-  near_bounds(g, mt, nt);
-  for (int p = 0; p < g->P; ++p)
-    for (int st = 0; st < 3; ++st) {
-      const StageDesc *d = g->d_desc[st].as<StageDesc>() + (size_t)p * g->nbox;
-      const double alpha = st < 2 ? 1.0 : g->w[p];
-      DAGE_TRY(launch_fp64_stages(d, g->nbox, mt[st], nt[st], alpha, st == 2 && p > 0, s,
-                                  g->tile_n[st]));
-    }
+// Uploads the single-density instance table and near-field descriptors.
+int single_setup(dage_gbfmm *g, const double *rho, double *V) {
+  const GInst I = plan_inst(g, rho, V, g->d_q.as<double>(), g->d_L.as<double>(),
+                            g->d_partial.as<double>(), g->d_epart.as<double>());
+  DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_inst.ptr, &I, sizeof(GInst), cudaMemcpyHostToDevice, g->stream));
+  if (V) {
+    std::vector<StageDesc> ds[3];
+    near_descs(g, rho, V, g->d_U.as<double>(), g->d_W.as<double>(), ds);
+    for (int d = 0; d < 3; ++d)
+      DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_desc[d].ptr, ds[d].data(), sizeof(StageDesc) * g->nbox,
+                                    cudaMemcpyHostToDevice, g->stream));
+  }
+  // the host copies above are pageable: finish them before the vectors go
+  DAGE_CUDA_TRY(cudaStreamSynchronize(g->stream));
   return 0;
 }
 
@@ -833,8 +952,8 @@ void gbfmm_destroy_impl(dage_gbfmm *g) {
     g->wts[d].release();
   }
   for (DevBuf *b : {&g->d_boxes, &g->d_wbox, &g->d_q, &g->d_L, &g->d_partial, &g->d_Tm2l,
-                    &g->d_ffstart, &g->d_ffsrc, &g->d_ffdisp, &g->d_U, &g->d_W, &g->partials,
-                    &g->d_rho, &g->d_V})
+                    &g->d_ffstart, &g->d_ffsrc, &g->d_ffdisp, &g->d_U, &g->d_W, &g->d_epart,
+                    &g->d_energy, &g->d_inst, &g->d_rho, &g->d_V})
     b->release();
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
@@ -862,6 +981,198 @@ int stage_io(dage_gbfmm *g, const double *rho, double *V, unsigned flags, const 
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Batch of independent densities (grids of any sizes): densities on equal
+// grids share one plan; every pipeline stage is one launch over all of them,
+// except the near field, whose intermediates are processed in chunks of
+// densities that fit a memory budget.
+// ---------------------------------------------------------------------------
+struct dage_gbfmm_batch {
+  int device = 0, n = 0, lmax = 0, N = 0, P = 0, nbox = 0, nslab = 8;
+  std::vector<dage_gbfmm *> plans;
+  std::vector<int> plan_of;
+  std::vector<size_t> npts;   // points of each density
+  std::vector<double> w;      // t-point weights (shared quadrature)
+  DevBuf q, L, partial, epart, energy, inst;
+  struct Chunk {
+    int i0 = 0, i1 = 0, njobs = 0;
+    DevBuf desc[3];
+    std::vector<size_t> uoff, woff;  // per density: offsets into U, W
+  };
+  std::vector<Chunk> chunks;
+  DevBuf U, W;
+  int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0}, maxown = 0;
+  int tile_n[3] = {64, 64, 64};
+  bool tuned = false;
+  DevBuf stage_rho, stage_V;  // host-pointer mode
+  std::vector<size_t> stage_off;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  size_t graph_nodes = 0;
+  std::vector<const void *> graph_key;  // rho/V pointers the graph was captured for
+};
+
+namespace dage {
+namespace {
+
+bool same_grid(const dage_gbfmm *g, const dage_grid1d grid[3]) {
+  for (int d = 0; d < 3; ++d) {
+    Axis a;
+    if (make_axis(grid[d], a)) return false;
+    if (!same_axis(a, g->ax[d])) return false;
+  }
+  return true;
+}
+
+void batch_destroy_impl(dage_gbfmm_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto *g : b->plans) gbfmm_destroy_impl(g);
+  for (auto &c : b->chunks)
+    for (auto &d : c.desc) d.release();
+  for (DevBuf *d : {&b->q, &b->L, &b->partial, &b->epart, &b->energy, &b->inst, &b->U, &b->W,
+                    &b->stage_rho, &b->stage_V})
+    d->release();
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  delete b;
+}
+
+int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int maxlevel, int lmax,
+                      const dage_quad *quad, size_t budget) {
+  DAGE_CUDA_TRY(cudaGetDevice(&b->device));
+  DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking));
+  b->stream = b->own_stream;
+  DAGE_CUDA_TRY(cudaEventCreate(&b->ev0));
+  DAGE_CUDA_TRY(cudaEventCreate(&b->ev1));
+  b->n = n;
+  b->plan_of.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const dage_grid1d *gi = grids + 3 * i;
+    int found = -1;
+    for (size_t k = 0; k < b->plans.size() && found < 0; ++k)
+      if (same_grid(b->plans[k], gi)) found = (int)k;
+    if (found < 0) {
+      auto *g = new dage_gbfmm();
+      const int rc = gbfmm_create_impl(g, gi, maxlevel, lmax, quad);
+      if (rc) {
+        gbfmm_destroy_impl(g);
+        return rc;
+      }
+      b->plans.push_back(g);
+      found = (int)b->plans.size() - 1;
+    }
+    b->plan_of[i] = found;
+    const dage_gbfmm *g = b->plans[found];
+    b->npts.push_back((size_t)g->npts[0] * g->npts[1] * g->npts[2]);
+  }
+  const dage_gbfmm *g0 = b->plans[0];
+  b->lmax = lmax;
+  b->N = g0->N;
+  b->P = g0->P;
+  b->nbox = g0->nbox;
+  b->nslab = g0->nslab;
+  b->w = g0->w;
+  for (const auto *g : b->plans) {
+    near_bounds(g, b->mt, b->nt);
+    b->maxown = std::max(b->maxown, max_owned(g));
+  }
+  const size_t per = (size_t)b->nbox * b->N;
+  DAGE_TRY(b->q.alloc(sizeof(double) * per * n));
+  DAGE_TRY(b->L.alloc(sizeof(double) * per * n));
+  DAGE_TRY(b->partial.alloc(sizeof(double) * per * b->nslab * n));
+  DAGE_TRY(b->epart.alloc(sizeof(double) * kEnergyBlocks * n));
+  DAGE_TRY(b->energy.alloc(sizeof(double) * n));
+  DAGE_TRY(b->inst.alloc(sizeof(GInst) * n));
+  // near-field chunks: consecutive densities while their intermediates fit
+  size_t umax = 0, wmax = 0, ucur = 0, wcur = 0;
+  dage_gbfmm_batch::Chunk cur;
+  for (int i = 0; i < n; ++i) {
+    const dage_gbfmm *g = b->plans[b->plan_of[i]];
+    const size_t ui = g->U_per_box * b->nbox, wi = g->W_per_box * b->nbox;
+    const bool full = cur.i1 > cur.i0 &&
+                      ((ucur + ui + wcur + wi) * sizeof(double) > budget ||
+                       (long long)(cur.i1 - cur.i0 + 1) * b->nbox > 65535);
+    if (full) {
+      b->chunks.push_back(std::move(cur));
+      cur = dage_gbfmm_batch::Chunk();
+      cur.i0 = cur.i1 = i;
+      ucur = wcur = 0;
+    }
+    cur.uoff.push_back(ucur);
+    cur.woff.push_back(wcur);
+    ucur += ui;
+    wcur += wi;
+    cur.i1 = i + 1;
+    umax = std::max(umax, ucur);
+    wmax = std::max(wmax, wcur);
+  }
+  b->chunks.push_back(std::move(cur));
+  DAGE_TRY(b->U.alloc(sizeof(double) * std::max<size_t>(umax, 1)));
+  DAGE_TRY(b->W.alloc(sizeof(double) * std::max<size_t>(wmax, 1)));
+  for (auto &c : b->chunks) {
+    c.njobs = (c.i1 - c.i0) * b->nbox;
+    for (auto &d : c.desc) DAGE_TRY(d.alloc(sizeof(StageDesc) * c.njobs));
+  }
+  // plans share the batch's stream
+  for (auto *g : b->plans) g->stream = b->stream;
+  return 0;
+}
+
+// Instance tables and near-field descriptors for a set of device cubes.
+int batch_tables(dage_gbfmm_batch *b, const double *const *rho, double *const *V) {
+  const size_t per = (size_t)b->nbox * b->N;
+  std::vector<GInst> ins(b->n);
+  for (int i = 0; i < b->n; ++i)
+    ins[i] = plan_inst(b->plans[b->plan_of[i]], rho[i], V[i], b->q.as<double>() + per * i,
+                       b->L.as<double>() + per * i, b->partial.as<double>() + per * b->nslab * i,
+                       b->epart.as<double>() + (size_t)kEnergyBlocks * i);
+  DAGE_CUDA_TRY(cudaMemcpyAsync(b->inst.ptr, ins.data(), sizeof(GInst) * b->n,
+                                cudaMemcpyHostToDevice, b->stream));
+  std::vector<std::vector<StageDesc>> keep;
+  for (auto &c : b->chunks) {
+    std::vector<StageDesc> ds[3];
+    for (int i = c.i0; i < c.i1; ++i)
+      near_descs(b->plans[b->plan_of[i]], rho[i], V[i], b->U.as<double>() + c.uoff[i - c.i0],
+                 b->W.as<double>() + c.woff[i - c.i0], ds);
+    for (int d = 0; d < 3; ++d)
+      DAGE_CUDA_TRY(cudaMemcpyAsync(c.desc[d].ptr, ds[d].data(), sizeof(StageDesc) * c.njobs,
+                                    cudaMemcpyHostToDevice, b->stream));
+    for (int d = 0; d < 3; ++d) keep.push_back(std::move(ds[d]));
+  }
+  // the host copies are pageable: finish them before the vectors go
+  DAGE_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+// The whole pipeline for the current tables, as stream work (captured into
+// the graph or launched directly).
+int batch_launch(dage_gbfmm_batch *b, double *const *V) {
+  cudaStream_t s = b->stream;
+  const GInst *d_inst = b->inst.as<GInst>();
+  for (int i = 0; i < b->n; ++i)
+    DAGE_CUDA_TRY(cudaMemsetAsync(V[i], 0, sizeof(double) * b->npts[i], s));
+  DAGE_TRY(run_multipoles(d_inst, b->n, b->nbox, b->lmax, b->nslab, s));
+  DAGE_TRY(run_m2l(d_inst, b->n, b->nbox, b->N, s));
+  for (auto &c : b->chunks) {
+    const StageDesc *dd[3] = {c.desc[0].as<StageDesc>(), c.desc[1].as<StageDesc>(),
+                              c.desc[2].as<StageDesc>()};
+    DAGE_TRY(run_near(dd, c.njobs, b->mt, b->nt, b->P, b->w, b->tile_n, s));
+  }
+  DAGE_TRY(run_l2p(d_inst, b->n, b->nbox, b->lmax, b->maxown, nullptr, s));
+  DAGE_TRY(run_energy(d_inst, b->n, b->energy.as<double>(), s));
+  return 0;
+}
+
+}  // namespace
+}  // namespace dage
 
 extern "C" {
 
@@ -921,21 +1232,22 @@ int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags
   const double *d_rho;
   double *d_V;
   DAGE_TRY(stage_io(g, rho, V, flags, &d_rho, &d_V));
+  DAGE_TRY(single_setup(g, d_rho, d_V));
+  const GInst *d_inst = g->d_inst.as<GInst>();
   DAGE_CUDA_TRY(cudaMemsetAsync(d_V, 0, sizeof(double) * n, s));
-  DAGE_TRY(gbfmm_descriptors(g, d_rho, d_V));
-  DAGE_TRY(gbfmm_multipoles(g, d_rho));
-  DAGE_TRY(gbfmm_m2l(g));
-  DAGE_TRY(gbfmm_nearfield(g));
-  DAGE_TRY(gbfmm_l2p(g, g->d_L.as<double>(), d_V));
-  double *d_res = (flags & DAGE_ENERGY) ? g->partials.as<double>() + finalize_partials_count()
-                                        : nullptr;
-  DAGE_TRY(launch_finalize(d_rho, d_V, nullptr, 0.0, g->wts[0].as<double>(),
-                           g->wts[1].as<double>(), g->wts[2].as<double>(), g->npts[0],
-                           g->npts[1], g->npts[2], g->partials.as<double>(),
-                           finalize_partials_count(), d_res, s));
+  DAGE_TRY(run_multipoles(d_inst, 1, g->nbox, g->lmax, g->nslab, s));
+  DAGE_TRY(run_m2l(d_inst, 1, g->nbox, g->N, s));
+  int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
+  near_bounds(g, mt, nt);
+  const StageDesc *dd[3] = {g->d_desc[0].as<StageDesc>(), g->d_desc[1].as<StageDesc>(),
+                            g->d_desc[2].as<StageDesc>()};
+  DAGE_TRY(run_near(dd, g->nbox, mt, nt, g->P, g->w, g->tile_n, s));
+  DAGE_TRY(run_l2p(d_inst, 1, g->nbox, g->lmax, max_owned(g), nullptr, s));
+  if (flags & DAGE_ENERGY) DAGE_TRY(run_energy(d_inst, 1, g->d_energy.as<double>(), s));
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-  if (d_res) DAGE_CUDA_TRY(cudaMemcpyAsync(energy, d_res, sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (flags & DAGE_ENERGY)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(energy, g->d_energy.ptr, sizeof(double), cudaMemcpyDeviceToHost, s));
   DAGE_CUDA_TRY(cudaEventRecord(g->ev1, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   DAGE_CUDA_TRY(cudaEventElapsedTime(&g->last_ms, g->ev0, g->ev1));
@@ -950,7 +1262,8 @@ int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flag
   const double *d_rho;
   double *d_V;
   DAGE_TRY(stage_io(g, rho, nullptr, flags & DAGE_DEVICE_PTRS, &d_rho, &d_V));
-  DAGE_TRY(gbfmm_multipoles(g, d_rho));
+  DAGE_TRY(single_setup(g, d_rho, nullptr));
+  DAGE_TRY(run_multipoles(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, g->nslab, g->stream));
   DAGE_CUDA_TRY(cudaMemcpyAsync(moments, g->d_q.ptr, sizeof(double) * g->nbox * g->N,
                                 cudaMemcpyDeviceToHost, g->stream));
   DAGE_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -981,7 +1294,8 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
     DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_V.ptr, V, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     d_V = g->d_V.as<double>();
   }
-  DAGE_TRY(gbfmm_l2p(g, dL.as<double>(), d_V));
+  DAGE_TRY(single_setup(g, nullptr, d_V));
+  DAGE_TRY(run_l2p(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, max_owned(g), dL.as<double>(), s));
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
@@ -991,6 +1305,147 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
 int dage_gbfmm_last_time_ms(const dage_gbfmm *g, float *ms) {
   if (!g || !ms) return fail(DAGE_E_INVALID, "null argument");
   *ms = g->last_ms;
+  return 0;
+}
+
+// ----------------------------------------------------------------- batch
+int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int lmax,
+                            const dage_quad *quad, size_t near_budget_bytes,
+                            dage_gbfmm_batch **out) {
+  clear_error();
+  if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
+  *out = nullptr;
+  if (n < 1 || n > 65535 || !grids || !quad)
+    return fail(DAGE_E_INVALID, "need 1..65535 densities, grids and a quadrature");
+  auto *b = new dage_gbfmm_batch();
+  const size_t budget = near_budget_bytes ? near_budget_bytes : ((size_t)8 << 30);
+  const int rc = batch_create_impl(b, n, grids, maxlevel, lmax, quad, budget);
+  if (rc) {
+    batch_destroy_impl(b);
+    return rc;
+  }
+  *out = b;
+  return 0;
+}
+
+int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double *const *V,
+                           unsigned flags, double *energies) {
+  clear_error();
+  if (!b || !rho || !V) return fail(DAGE_E_INVALID, "null argument");
+  if ((flags & DAGE_ENERGY) && !energies) return fail(DAGE_E_INVALID, "energies pointer is null");
+  for (int i = 0; i < b->n; ++i)
+    if (!rho[i] || !V[i]) return fail(DAGE_E_INVALID, "null cube for density %d", i);
+  DAGE_CUDA_TRY(cudaSetDevice(b->device));
+  cudaStream_t s = b->stream;
+  DAGE_CUDA_TRY(cudaEventRecord(b->ev0, s));
+  // device cubes
+  std::vector<const double *> dr(b->n);
+  std::vector<double *> dv(b->n);
+  if (flags & DAGE_DEVICE_PTRS) {
+    for (int i = 0; i < b->n; ++i) {
+      dr[i] = rho[i];
+      dv[i] = V[i];
+    }
+  } else {
+    if (b->stage_off.empty()) {
+      size_t off = 0;
+      for (int i = 0; i < b->n; ++i) {
+        b->stage_off.push_back(off);
+        off += b->npts[i];
+      }
+      DAGE_TRY(b->stage_rho.alloc(sizeof(double) * off));
+      DAGE_TRY(b->stage_V.alloc(sizeof(double) * off));
+    }
+    for (int i = 0; i < b->n; ++i) {
+      dr[i] = b->stage_rho.as<double>() + b->stage_off[i];
+      dv[i] = b->stage_V.as<double>() + b->stage_off[i];
+      DAGE_CUDA_TRY(cudaMemcpyAsync(const_cast<double *>(dr[i]), rho[i],
+                                    sizeof(double) * b->npts[i], cudaMemcpyHostToDevice, s));
+    }
+  }
+  std::vector<const void *> key;
+  for (int i = 0; i < b->n; ++i) {
+    key.push_back(dr[i]);
+    key.push_back(dv[i]);
+  }
+  const bool use_graph = !(flags & DAGE_NO_GRAPH);
+  if (!use_graph || key != b->graph_key || !b->exec) {
+    DAGE_TRY(batch_tables(b, dr.data(), dv.data()));
+    if (!b->tuned) {
+      const auto &c = b->chunks[0];
+      const StageDesc *dd[3] = {c.desc[0].as<StageDesc>(), c.desc[1].as<StageDesc>(),
+                                c.desc[2].as<StageDesc>()};
+      DAGE_TRY(autotune_tiles(dd, c.njobs, b->mt, b->nt, s, b->tile_n));
+      b->tuned = true;
+    }
+    if (use_graph) {
+      if (b->exec) cudaGraphExecDestroy(b->exec);
+      if (b->graph) cudaGraphDestroy(b->graph);
+      b->exec = nullptr;
+      b->graph = nullptr;
+      b->graph_key.clear();
+      // kernel attributes are set before capture
+      int threads;
+      DAGE_TRY(multipoles_smem(b->N, &threads));
+      DAGE_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int rc = batch_launch(b, dv.data());
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ce != cudaSuccess) return fail(DAGE_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+      b->graph = graph;
+      DAGE_CUDA_TRY(cudaGraphGetNodes(graph, nullptr, &b->graph_nodes));
+      DAGE_CUDA_TRY(cudaGraphInstantiate(&b->exec, graph, 0));
+      b->graph_key = key;
+    }
+  }
+  if (use_graph)
+    DAGE_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+  else
+    DAGE_TRY(batch_launch(b, dv.data()));
+  if (!(flags & DAGE_DEVICE_PTRS))
+    for (int i = 0; i < b->n; ++i)
+      DAGE_CUDA_TRY(cudaMemcpyAsync(V[i], dv[i], sizeof(double) * b->npts[i],
+                                    cudaMemcpyDeviceToHost, s));
+  if (flags & DAGE_ENERGY)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(energies, b->energy.ptr, sizeof(double) * b->n,
+                                  cudaMemcpyDeviceToHost, s));
+  DAGE_CUDA_TRY(cudaEventRecord(b->ev1, s));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  DAGE_CUDA_TRY(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  return 0;
+}
+
+int dage_gbfmm_batch_info(const dage_gbfmm_batch *b, int *nplans, int *nchunks, int tile_n[3],
+                          long long *graph_nodes) {
+  if (!b) return fail(DAGE_E_INVALID, "null handle");
+  if (nplans) *nplans = (int)b->plans.size();
+  if (nchunks) *nchunks = (int)b->chunks.size();
+  if (tile_n)
+    for (int d = 0; d < 3; ++d) tile_n[d] = b->tile_n[d];
+  if (graph_nodes) *graph_nodes = (long long)b->graph_nodes;
+  return 0;
+}
+
+int dage_gbfmm_batch_set_stream(dage_gbfmm_batch *b, void *stream) {
+  if (!b) return fail(DAGE_E_INVALID, "null handle");
+  b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+  for (auto *g : b->plans) g->stream = b->stream;
+  return 0;
+}
+
+int dage_gbfmm_batch_last_time_ms(const dage_gbfmm_batch *b, float *ms) {
+  if (!b || !ms) return fail(DAGE_E_INVALID, "null argument");
+  *ms = b->last_ms;
+  return 0;
+}
+
+int dage_gbfmm_batch_destroy(dage_gbfmm_batch *b) {
+  clear_error();
+  batch_destroy_impl(b);
   return 0;
 }
 

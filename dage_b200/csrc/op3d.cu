@@ -277,8 +277,9 @@ __global__ void __launch_bounds__(256, 1)
 
 template <bool ACCUM, int TN>
 __global__ void __launch_bounds__(256, 1)
-    stage_fp64_batched_kernel(const StageDesc *__restrict__ descs, double alpha) {
-  const StageDesc d = descs[blockIdx.z];
+    stage_fp64_batched_kernel(const StageDesc *__restrict__ descs, int p, double alpha) {
+  StageDesc d = descs[blockIdx.z];
+  d.T += p * d.t_ps;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * TN;
   if (m0 >= d.M || n0 >= d.N) return;  // uniform across the block
   stage_tile<ACCUM, TN>(d, alpha, m0, n0);
@@ -399,8 +400,8 @@ int launch_single(const StageDesc &d, double alpha, cudaStream_t s) {
 }
 
 template <bool ACCUM, int TN>
-int launch_batched(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, double alpha,
-                   cudaStream_t s) {
+int launch_batched(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, int p,
+                   double alpha, cudaStream_t s) {
   auto kern = stage_fp64_batched_kernel<ACCUM, TN>;
   static bool done = false;
   if (!done) {
@@ -410,7 +411,7 @@ int launch_batched(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, d
   }
   dim3 grid(mtiles, ceil_div(ncols, TN), ndesc);
   if (grid.y > 65535 || ndesc > 65535) return fail(DAGE_E_UNSUPPORTED, "batch too large");
-  kern<<<grid, 256, stage_smem<TN>(), s>>>(d_descs, alpha);
+  kern<<<grid, 256, stage_smem<TN>(), s>>>(d_descs, p, alpha);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -424,17 +425,18 @@ int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStr
   return fail(DAGE_E_INVALID, "tile width %d", tn);
 }
 
-int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, double alpha,
-                       bool accumulate, cudaStream_t s, int tn) {
+int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, int p,
+                       double alpha, bool accumulate, cudaStream_t s, int tn) {
   if (ndesc <= 0) return 0;
+#define DAGE_BATCHED(TNV)                                                                  \
+  return accumulate ? launch_batched<true, TNV>(d_descs, ndesc, mtiles, ncols, p, alpha, s) \
+                    : launch_batched<false, TNV>(d_descs, ndesc, mtiles, ncols, p, alpha, s)
   switch (tn) {
-    case 32: return accumulate ? launch_batched<true, 32>(d_descs, ndesc, mtiles, ncols, alpha, s)
-                               : launch_batched<false, 32>(d_descs, ndesc, mtiles, ncols, alpha, s);
-    case 64: return accumulate ? launch_batched<true, 64>(d_descs, ndesc, mtiles, ncols, alpha, s)
-                               : launch_batched<false, 64>(d_descs, ndesc, mtiles, ncols, alpha, s);
-    case 128: return accumulate ? launch_batched<true, 128>(d_descs, ndesc, mtiles, ncols, alpha, s)
-                                : launch_batched<false, 128>(d_descs, ndesc, mtiles, ncols, alpha, s);
+    case 32: DAGE_BATCHED(32);
+    case 64: DAGE_BATCHED(64);
+    case 128: DAGE_BATCHED(128);
   }
+#undef DAGE_BATCHED
   return fail(DAGE_E_INVALID, "tile width %d", tn);
 }
 

@@ -383,6 +383,76 @@ class GBFMMCoulomb3D:
         return v.value
 
 
+
+class GBFMMBatch:
+    """Many independent densities through the GBFMM Coulomb operator at once
+    (config: hundreds of orbitals of uneven grid sizes in one SCF step).
+    Densities on equal grids share one plan; each pipeline stage is one
+    launch over all densities, and the pipeline runs as a CUDA graph
+    captured for the set of device cubes it is given."""
+
+    def __init__(self, grids, lmax: int = 12, maxlevel: int = 2,
+                 quad: GaussQuad | None = None, near_budget_bytes: int = 0):
+        lib = load()
+        self.grids = list(grids)
+        self.lmax = lmax
+        self.quad = quad if quad is not None else GaussQuad(25, 25)
+        axes = [a.c() for g in self.grids for a in g.axes]
+        arr = (DageGrid1D * len(axes))(*axes)
+        self._keep = (arr, self.grids, self.quad.c())
+        h = ctypes.c_void_p()
+        check(lib.dage_gbfmm_batch_create(len(self.grids), arr, maxlevel, lmax,
+                                          ctypes.byref(self._keep[2]), near_budget_bytes,
+                                          ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                load().dage_gbfmm_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def info(self):
+        """(plans, near-field chunks, tile widths, nodes of the captured graph)."""
+        npl, nch, nodes = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        t = (ctypes.c_int * 3)()
+        check(load().dage_gbfmm_batch_info(self._h, ctypes.byref(npl), ctypes.byref(nch), t,
+                                           ctypes.byref(nodes)))
+        return npl.value, nch.value, tuple(t), nodes.value
+
+    @property
+    def last_time_ms(self) -> float:
+        v = ctypes.c_float()
+        check(load().dage_gbfmm_batch_last_time_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+    def apply(self, rhos, outs, energy: bool = False, graph: bool = True):
+        """outs[i] = GBFMM potential of rhos[i] (all host numpy or all device
+        torch cubes); returns the per-density energies with energy=True."""
+        n = len(self.grids)
+        if len(rhos) != n or len(outs) != n:
+            raise ValueError(f"need {n} input and output cubes")
+        rp = (ctypes.c_void_p * n)()
+        vp = (ctypes.c_void_p * n)()
+        devs = set()
+        for i, g in enumerate(self.grids):
+            m = int(np.prod(g.shape))
+            rp[i], d1 = _ptr(rhos[i], m)
+            vp[i], d2 = _ptr(outs[i], m)
+            devs.update((d1, d2))
+        if len(devs) != 1:
+            raise ValueError("cubes must all be host or all be device cubes")
+        flags = (_capi.DAGE_DEVICE_PTRS if devs.pop() else 0) | (_capi.DAGE_ENERGY if energy else 0)
+        if not graph:
+            flags |= _capi.DAGE_NO_GRAPH
+        e = np.zeros(n)
+        check(load().dage_gbfmm_batch_apply(self._h, rp, vp, flags,
+                                            e.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return e if energy else None
+
 class Bubbles:
     """Atom-centred radial functions times real spherical harmonics
     (Bubbles, src/bubbles/bubbles.F90), uploaded once for GPU injection into

@@ -41,6 +41,7 @@ extern "C" {
 #define DAGE_ENERGY 2u        /* also return the integral of rho * V */
 #define DAGE_NO_CODA 4u       /* skip the coda term for this call */
 #define DAGE_ACCUMULATE 8u    /* V += result instead of V = result */
+#define DAGE_NO_GRAPH 16u     /* batch apply: launch the pipeline directly, no CUDA graph */
 
 /* operator precisions */
 #define DAGE_FP64 0            /* FP64 everywhere: the drop-in */
@@ -180,6 +181,35 @@ int dage_gbfmm_tiles(const dage_gbfmm *g, int tile_n[3]);
 int dage_gbfmm_set_stream(dage_gbfmm *g, void *stream);
 int dage_gbfmm_last_time_ms(const dage_gbfmm *g, float *ms);
 int dage_gbfmm_destroy(dage_gbfmm *g);
+
+/* ---------------------------------------------------------------------------
+ * Batched GBFMM: many independent densities of any grid sizes
+ * ------------------------------------------------------------------------ */
+/* Replaces the reference's per-density loop over GBFMMCoulomb3D_calculate_potential
+ * (src/gbfmm/gbfmm_coulomb3d.F90:650-819) when many orbitals/densities are
+ * operated on in one SCF step.  Densities on equal grids share one plan
+ * (boxes, near-field matrices, M2L matrices); every pipeline stage
+ * (moments, M2L, near field per t-point and contraction stage, L2P, energy)
+ * is one launch over all densities.  The near field's intermediates are
+ * processed in chunks of densities that fit near_budget_bytes (0 = 8 GiB).
+ * grids holds 3 axes per density; maxlevel must be 2. */
+typedef struct dage_gbfmm_batch dage_gbfmm_batch;
+int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int lmax,
+                            const dage_quad *quad, size_t near_budget_bytes,
+                            dage_gbfmm_batch **out);
+/* rho[i], V[i]: cube i (host arrays, or device pointers with DAGE_DEVICE_PTRS);
+ * energies[n] receives each int rho V with DAGE_ENERGY.  The pipeline is
+ * captured into a CUDA graph for the set of device cubes it runs on and
+ * replayed while later calls use the same cubes (host-array calls always
+ * use the batch's own device cubes); DAGE_NO_GRAPH launches it directly.
+ * The near-field tile widths are autotuned on the first call. */
+int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double *const *V,
+                           unsigned flags, double *energies);
+int dage_gbfmm_batch_info(const dage_gbfmm_batch *b, int *nplans, int *nchunks, int tile_n[3],
+                          long long *graph_nodes);
+int dage_gbfmm_batch_set_stream(dage_gbfmm_batch *b, void *stream);
+int dage_gbfmm_batch_last_time_ms(const dage_gbfmm_batch *b, float *ms);
+int dage_gbfmm_batch_destroy(dage_gbfmm_batch *b);
 
 /* ---------------------------------------------------------------------------
  * Bubbles -> cube injection
