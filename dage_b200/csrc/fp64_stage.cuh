@@ -67,4 +67,8 @@ int launch_fp64_stage(const StageDesc &d, double alpha, bool accumulate, cudaStr
 int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, int p,
                        double alpha, bool accumulate, cudaStream_t s, int tn = kFp64TileN);
 
+// Sets the shared-memory limits of every stage kernel variant (done lazily by
+// the launchers; call it before capturing launches into a CUDA graph).
+int prepare_fp64_stages();
+
 }  // namespace dage

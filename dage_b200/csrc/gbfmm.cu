@@ -797,13 +797,22 @@ int max_owned(const dage_gbfmm *g) {
   return m;
 }
 
+// Threads per multipole block and its shared memory; raises the kernel's
+// shared-memory limit only when a larger size is first needed (so a call
+// inside a stream capture changes no attribute once set up).
 int multipoles_smem(int N, int *threads) {
+  static int limit = 0;
+  static std::mutex mu;
   int t = 128;
   while ((size_t)sizeof(double) * N * t > 200 * 1024 && t > 32) t -= 32;
   *threads = t;
   const int smem = (int)(sizeof(double) * N * t);
-  DAGE_CUDA_TRY(
-      cudaFuncSetAttribute(multipoles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  std::lock_guard<std::mutex> lock(mu);
+  if (smem > limit) {
+    DAGE_CUDA_TRY(
+        cudaFuncSetAttribute(multipoles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    limit = smem;
+  }
   return 0;
 }
 
@@ -926,12 +935,13 @@ int gbfmm_autotune(dage_gbfmm *g) {
   return 0;
 }
 
-// Uploads the single-density instance table and near-field descriptors.
-int single_setup(dage_gbfmm *g, const double *rho, double *V) {
+// Uploads the single-density instance table and, for a full apply, the
+// near-field descriptors.
+int single_setup(dage_gbfmm *g, const double *rho, double *V, bool near) {
   const GInst I = plan_inst(g, rho, V, g->d_q.as<double>(), g->d_L.as<double>(),
                             g->d_partial.as<double>(), g->d_epart.as<double>());
   DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_inst.ptr, &I, sizeof(GInst), cudaMemcpyHostToDevice, g->stream));
-  if (V) {
+  if (near) {
     std::vector<StageDesc> ds[3];
     near_descs(g, rho, V, g->d_U.as<double>(), g->d_W.as<double>(), ds);
     for (int d = 0; d < 3; ++d)
@@ -1232,7 +1242,7 @@ int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags
   const double *d_rho;
   double *d_V;
   DAGE_TRY(stage_io(g, rho, V, flags, &d_rho, &d_V));
-  DAGE_TRY(single_setup(g, d_rho, d_V));
+  DAGE_TRY(single_setup(g, d_rho, d_V, true));
   const GInst *d_inst = g->d_inst.as<GInst>();
   DAGE_CUDA_TRY(cudaMemsetAsync(d_V, 0, sizeof(double) * n, s));
   DAGE_TRY(run_multipoles(d_inst, 1, g->nbox, g->lmax, g->nslab, s));
@@ -1262,7 +1272,7 @@ int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flag
   const double *d_rho;
   double *d_V;
   DAGE_TRY(stage_io(g, rho, nullptr, flags & DAGE_DEVICE_PTRS, &d_rho, &d_V));
-  DAGE_TRY(single_setup(g, d_rho, nullptr));
+  DAGE_TRY(single_setup(g, d_rho, nullptr, false));
   DAGE_TRY(run_multipoles(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, g->nslab, g->stream));
   DAGE_CUDA_TRY(cudaMemcpyAsync(moments, g->d_q.ptr, sizeof(double) * g->nbox * g->N,
                                 cudaMemcpyDeviceToHost, g->stream));
@@ -1294,7 +1304,7 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
     DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_V.ptr, V, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     d_V = g->d_V.as<double>();
   }
-  DAGE_TRY(single_setup(g, nullptr, d_V));
+  DAGE_TRY(single_setup(g, nullptr, d_V, false));
   DAGE_TRY(run_l2p(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, max_owned(g), dL.as<double>(), s));
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -1387,6 +1397,7 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
       // kernel attributes are set before capture
       int threads;
       DAGE_TRY(multipoles_smem(b->N, &threads));
+      DAGE_TRY(prepare_fp64_stages());
       DAGE_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       const int rc = batch_launch(b, dv.data());
       cudaGraph_t graph = nullptr;

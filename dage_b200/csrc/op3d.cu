@@ -15,6 +15,7 @@
 // the same arithmetic as the reference's per-slice DGEMMs
 // (src/bubbles/function3d.F90:4296-4332), reordered for coalescing.
 #include <cmath>
+#include <mutex>
 #include <cstring>
 
 #include "expo.cuh"
@@ -384,14 +385,34 @@ __global__ void sum_partials_kernel(const double *partials, int n, double *resul
 }  // namespace
 
 template <bool ACCUM, int TN>
+int attr_variants() {
+  DAGE_CUDA_TRY(cudaFuncSetAttribute(stage_fp64_kernel<ACCUM, TN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<TN>()));
+  DAGE_CUDA_TRY(cudaFuncSetAttribute(stage_fp64_batched_kernel<ACCUM, TN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<TN>()));
+  return 0;
+}
+
+int prepare_fp64_stages() {
+  // once per process
+  static std::mutex mu;
+  static bool done = false;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done) return 0;
+  DAGE_TRY((attr_variants<false, 32>()));
+  DAGE_TRY((attr_variants<true, 32>()));
+  DAGE_TRY((attr_variants<false, 64>()));
+  DAGE_TRY((attr_variants<true, 64>()));
+  DAGE_TRY((attr_variants<false, 128>()));
+  DAGE_TRY((attr_variants<true, 128>()));
+  done = true;
+  return 0;
+}
+
+template <bool ACCUM, int TN>
 int launch_single(const StageDesc &d, double alpha, cudaStream_t s) {
   auto kern = stage_fp64_kernel<ACCUM, TN>;
-  static bool done = false;
-  if (!done) {
-    DAGE_CUDA_TRY(
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<TN>()));
-    done = true;
-  }
+  DAGE_TRY(prepare_fp64_stages());
   dim3 grid(ceil_div(d.M, BM), ceil_div(d.N, TN));
   if (grid.y > 65535) return fail(DAGE_E_UNSUPPORTED, "N=%d too large", d.N);
   kern<<<grid, 256, stage_smem<TN>(), s>>>(d, alpha);
@@ -403,12 +424,7 @@ template <bool ACCUM, int TN>
 int launch_batched(const StageDesc *d_descs, int ndesc, int mtiles, int ncols, int p,
                    double alpha, cudaStream_t s) {
   auto kern = stage_fp64_batched_kernel<ACCUM, TN>;
-  static bool done = false;
-  if (!done) {
-    DAGE_CUDA_TRY(
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<TN>()));
-    done = true;
-  }
+  DAGE_TRY(prepare_fp64_stages());
   dim3 grid(mtiles, ceil_div(ncols, TN), ndesc);
   if (grid.y > 65535 || ndesc > 65535) return fail(DAGE_E_UNSUPPORTED, "batch too large");
   kern<<<grid, 256, stage_smem<TN>(), s>>>(d_descs, p, alpha);
