@@ -439,6 +439,7 @@ struct dage_gbfmm {
   int axis_pos_count[3];
   // per axis, per box position: near-field operator matrix (P x own x near)
   std::vector<DevBuf> Tnear[3];
+  std::vector<DevBuf> band_near[3];  // K band per (t-point, 128-row tile) of Tnear
   DevBuf d_boxes, d_wbox, d_q, d_L, d_partial, d_Tm2l, d_ffstart, d_ffsrc, d_ffdisp;
   int wstride = 0, nslab = 8, ndisp = 0;
   DevBuf d_U, d_W, d_desc[3];
@@ -641,6 +642,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   for (int p = 0; p < g->P; ++p) g->w[p] = two_over_sqrtpi * g->tw[p];
   for (int d = 0; d < 3; ++d) {
     g->Tnear[d].resize(nb);
+    g->band_near[d].resize(nb);
     for (int v = 0; v < nb; ++v) {
       const int q0 = pos_near0[d][v], nq = pos_nearn[d][v];
       dage_grid1d sub;
@@ -658,6 +660,9 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
       DAGE_TRY(g->Tnear[d][v].alloc(sizeof(double) * (size_t)g->P * own * nq));
       DAGE_TRY(build_axis_matrix(ain, g->ax[d].points.data() + pos_p0[d][v], own,
                                  d_tp.as<double>(), g->P, g->Tnear[d][v].as<double>(), s));
+      DAGE_TRY(g->band_near[d][v].alloc(sizeof(int2) * (size_t)g->P * ceil_div(own, kFp64TileN)));
+      DAGE_TRY(launch_band(g->Tnear[d][v].as<double>(), nq, own, g->P,
+                           g->band_near[d][v].as<int2>(), s));
     }
   }
   // intermediates and stage descriptors
@@ -732,6 +737,8 @@ void near_descs(const dage_gbfmm *g, const double *rho, double *V, double *U0, d
     x.a_s1 = Nx;
     x.a_s2 = (long long)Nx * Ny;
     x.T = g->Tnear[0][B.pos[0]].as<double>();
+    x.krange = g->band_near[0][B.pos[0]].as<int2>();
+    x.kr_ps = ceil_div(B.own[0], kFp64TileN);
     x.t_ps = (long long)B.own[0] * B.nq[0];
     x.ldt = B.nq[0];
     x.out = U;
@@ -748,6 +755,8 @@ void near_descs(const dage_gbfmm *g, const double *rho, double *V, double *U0, d
     y.a_s1 = B.nq[1];
     y.a_s2 = 0;
     y.T = g->Tnear[1][B.pos[1]].as<double>();
+    y.krange = g->band_near[1][B.pos[1]].as<int2>();
+    y.kr_ps = ceil_div(B.own[1], kFp64TileN);
     y.t_ps = (long long)B.own[1] * B.nq[1];
     y.ldt = B.nq[1];
     y.out = W;
@@ -764,6 +773,8 @@ void near_descs(const dage_gbfmm *g, const double *rho, double *V, double *U0, d
     z.a_s1 = B.nq[2];
     z.a_s2 = 0;
     z.T = g->Tnear[2][B.pos[2]].as<double>();
+    z.krange = g->band_near[2][B.pos[2]].as<int2>();
+    z.kr_ps = ceil_div(B.own[2], kFp64TileN);
     z.t_ps = (long long)B.own[2] * B.nq[2];
     z.ldt = B.nq[2];
     z.out = V + B.p0[0] + (size_t)Nx * B.p0[1] + (size_t)Nx * Ny * B.p0[2];
@@ -958,6 +969,7 @@ void gbfmm_destroy_impl(dage_gbfmm *g) {
   if (g->stream) cudaStreamSynchronize(g->stream);
   for (int d = 0; d < 3; ++d) {
     for (auto &b : g->Tnear[d]) b.release();
+    for (auto &b : g->band_near[d]) b.release();
     g->d_desc[d].release();
     g->wts[d].release();
   }

@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(256, 1)
     stage_fp64_batched_kernel(const StageDesc *__restrict__ descs, int p, double alpha) {
   StageDesc d = descs[blockIdx.z];
   d.T += p * d.t_ps;
+  if (d.krange) d.krange += p * d.kr_ps;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * TN;
   if (m0 >= d.M || n0 >= d.N) return;  // uniform across the block
   stage_tile<ACCUM, TN>(d, alpha, m0, n0);
