@@ -54,6 +54,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "op3d.cuh"
 
@@ -69,6 +70,7 @@ constexpr int BK = 64;            // K extent of one shared-memory stage (128-by
 constexpr int kGroup = 32;        // K extent sharing one quantum in a leading part
 constexpr int kThreads = 576;     // 18 warps
 constexpr int kEpiThreads = 512;  // warps 2-17
+constexpr int kMaxGroup = 8;      // t-points summed per pass of the last stage
 
 // ---------------------------------------------------------------------------
 // PTX wrappers
@@ -142,26 +144,20 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
-// 32 lanes x 32 consecutive 32-bit columns; the wait takes the registers as
+// 32 lanes x 16 consecutive 32-bit columns; the wait takes the registers as
 // operands so no use of them can be scheduled before the load completes.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-      "%28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
                  "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
-                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
-                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
-                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
-                 "+r"(r[30]), "+r"(r[31])
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
                :
                : "memory");
 }
@@ -255,9 +251,13 @@ struct StageArgs {
   // nrb > 0 (intermediate stages): tile mt covers R = r1 d0 + r0 with
   // r1 = mt / nrb and r0 in [128 (mt % nrb), +128) intersected with [0, d0)
   int nrb;
-  const float *scale;    // s_n of this t-point (intermediate stages)
-  const double *scale64; // s_n of this t-point (final stage)
-  double wcoef;          // w_p (final stage)
+  // Sub-problems per tile: the last stage sums ng t-points p0 .. p0+ng-1 in
+  // one pass over V; sub-problem g reads A rows from g * gM, matrix rows
+  // from brow0 + g * N, bands k_range[g * n_ntiles + nt], scales
+  // scale[g * N + n] and weight wcoef[g].  Intermediate stages: ng = 1.
+  int ng, gM;
+  const float *scale;    // s_n, row scales of the t-points
+  const float *wcoef;    // w_p of the t-points (device)
   // intermediate output: part s of element (R, n) at
   //   out[s][(R / d0 + d1 * n) * ldn + R % d0]
   __nv_bfloat16 *out0, *out1, *out2;
@@ -266,9 +266,9 @@ struct StageArgs {
   // final output V[R + M * n] (FP64)
   double *V;
   int accumulate;
-  // per n-tile of this t-point: first and last K index holding a matrix
-  // entry above 2^-64 of its row's scale (the matrices are banded for large
-  // t; K blocks outside the band add nothing and are skipped)
+  // per t-point and n-tile: first and last K index holding a matrix entry
+  // above 2^-64 of its row's scale (the matrices are banded for large t; K
+  // blocks outside the band add nothing and are skipped)
   const int2 *k_range;
   int *err;
   long long wait_limit;   // normal waits (dage_set_wait_limit)
@@ -299,9 +299,9 @@ __device__ __forceinline__ void corr_product(int nsx, int i, int &a, int &b) {
   }
 }
 
-// K blocks [first, last] of the band of n-tile nt
-__device__ __forceinline__ int2 kblocks(const StageArgs &a, int nt) {
-  const int2 r = a.k_range[nt];
+// K blocks [first, last] of the band of sub-problem gi, n-tile nt
+__device__ __forceinline__ int2 kblocks(const StageArgs &a, int gi, int nt) {
+  const int2 r = a.k_range[gi * a.n_ntiles + nt];
   return make_int2(r.x / BK, r.y / BK);
 }
 
@@ -311,8 +311,9 @@ __device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
 
 // NSX parts per operand; NS shared-memory stages; the main product starts a
 // fresh partial every kGroup / 16 MMAs (one 32-run of K).
+// 18 warps x 32 threads x 112 registers = 64512 <= 65536: one CTA per SM.
 template <int NSX, int NS, bool FINAL>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __maxnreg__(112)
     stage_bf16_kernel(const __grid_constant__ CUtensorMap mapA0,
                       const __grid_constant__ CUtensorMap mapA1,
                       const __grid_constant__ CUtensorMap mapA2,
@@ -380,9 +381,12 @@ __global__ void __launch_bounds__(kThreads, 1)
       int issued[NS];
       uint32_t issued_ph[NS];
       for (int i = 0; i < NS; ++i) issued[i] = 0, issued_ph[i] = 0;
-      for (int tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x) {
-        const int row0 = tile_row0(a, tile / a.n_ntiles), n0 = (tile % a.n_ntiles) * BN;
-        const int2 r = kblocks(a, tile % a.n_ntiles);
+      for (int u = blockIdx.x * a.ng; u < a.ntiles * a.ng && !*abort_flag;
+           u += (u % a.ng == a.ng - 1) ? (gridDim.x - 1) * a.ng + 1 : 1) {
+        const int tile = u / a.ng, gi = u % a.ng;
+        const int row0 = tile_row0(a, tile / a.n_ntiles) + gi * a.gM;
+        const int n0 = (tile % a.n_ntiles) * BN + gi * a.N;
+        const int2 r = kblocks(a, gi, tile % a.n_ntiles);
         for (int kb = r.x; kb <= r.y; ++kb) {
           if (!mbar_wait(empty(s), ph ^ 1, a.wait_limit)) {
             on_timeout();
@@ -414,13 +418,15 @@ __global__ void __launch_bounds__(kThreads, 1)
       int g = 0;  // partial counter over all tiles
       int t = 0;
       bool ok = true;
-      for (int tile = blockIdx.x; tile < a.ntiles && ok && !*abort_flag; tile += gridDim.x, ++t) {
+      for (int u = blockIdx.x * a.ng; u < a.ntiles * a.ng && ok && !*abort_flag;
+           u += (u % a.ng == a.ng - 1) ? (gridDim.x - 1) * a.ng + 1 : 1, ++t) {
+        const int tile = u / a.ng, gi = u % a.ng;
         const int n0 = (tile % a.n_ntiles) * BN;
         int nt = a.N - n0;
         if (nt > BN) nt = BN;
         nt = (nt + 15) & ~15;
         const uint32_t idesc = idesc_bf16(BM, nt);
-        const int2 r = kblocks(a, tile % a.n_ntiles);
+        const int2 r = kblocks(a, gi, tile % a.n_ntiles);
         const int nsteps = tile_steps(r);
         int step = 0;  // K=16 step within the tile; K blocks start on a 32-run
         for (int kb = r.x; kb <= r.y && ok; ++kb) {
@@ -483,15 +489,42 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
     const uint32_t col0 = ((warp - 2) >> 2) * CW;
     int g = 0, t = 0;
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++t) {
-      float2 acc[CW / 2];  // columns (2j, 2j + 1)
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+      float2 acc[CW / 2];   // one t-point, columns (2j, 2j + 1)
+      float2 accg[CW / 2];  // last stage: sum over the group of w_p s_n D_p
 #pragma unroll
-      for (int j = 0; j < CW / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
+      for (int j = 0; j < CW / 2; ++j) accg[j] = make_float2(0.0f, 0.0f);
       bool ok = true;
-      const int nparts = (tile_steps(kblocks(a, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
-      for (int pi = 0; pi < nparts; ++pi, ++g) {
-        const int b = g % C::kNP;
-        const bool got = mbar_wait(pfull(b), (g / C::kNP) & 1, a.wait_limit);
+      for (int gi = 0; gi < a.ng && ok; ++gi, ++t) {
+#pragma unroll
+        for (int j = 0; j < CW / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
+        const int nparts =
+            (tile_steps(kblocks(a, gi, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
+        for (int pi = 0; pi < nparts; ++pi, ++g) {
+          const int b = g % C::kNP;
+          const bool got = mbar_wait(pfull(b), (g / C::kNP) & 1, a.wait_limit);
+          __syncwarp();
+          if (!got) {
+            on_timeout();
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {  // 16 columns at a time: fewer live registers
+            uint32_t r[16];
+            tmem_ld16(tmem_base + lane_off + b * BN + col0 + hh * 16, r);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              acc[hh * 8 + j] = __fadd2_rn(acc[hh * 8 + j],
+                                           make_float2(__uint_as_float(r[2 * j]),
+                                                       __uint_as_float(r[2 * j + 1])));
+          }
+          tc_fence_before();
+          mbar_arrive(pempty(b));
+        }
+        if (!ok) break;
+        const bool got = mbar_wait(cfull, t & 1, a.wait_limit);
         __syncwarp();
         if (!got) {
           on_timeout();
@@ -499,37 +532,37 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        uint32_t r[32];
-        tmem_ld32(tmem_base + lane_off + b * BN + col0, r);
-        tc_fence_before();
-        mbar_arrive(pempty(b));
 #pragma unroll
-        for (int j = 0; j < CW / 2; ++j)
-          acc[j] = __fadd2_rn(acc[j], make_float2(__uint_as_float(r[2 * j]),
-                                                  __uint_as_float(r[2 * j + 1])));
-      }
-      if (!ok) break;
-      const bool got = mbar_wait(cfull, t & 1, a.wait_limit);
-      __syncwarp();
-      if (!got) {
-        on_timeout();
-        break;
-      }
-      tc_fence_after();
-      {
-        uint32_t r[32];
-        tmem_ld32(tmem_corr + lane_off + col0, r);
+        for (int hh = 0; hh < 2; ++hh) {
+          uint32_t r[16];
+          tmem_ld16(tmem_corr + lane_off + col0 + hh * 16, r);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            acc[hh * 8 + j] = __fadd2_rn(acc[hh * 8 + j],
+                                         make_float2(__uint_as_float(r[2 * j]),
+                                                     __uint_as_float(r[2 * j + 1])));
+        }
         tc_fence_before();
         mbar_arrive(cempty);
+        if (FINAL) {
+          const int n0 = (tile % a.n_ntiles) * BN + col0;
+          const float *sc = a.scale + (size_t)gi * a.N;
+          const float wg = a.wcoef[gi];
 #pragma unroll
-        for (int j = 0; j < CW / 2; ++j)
-          acc[j] = __fadd2_rn(acc[j], make_float2(__uint_as_float(r[2 * j]),
-                                                  __uint_as_float(r[2 * j + 1])));
+          for (int j = 0; j < CW / 2; ++j) {
+            const int n = n0 + 2 * j;
+            const float2 f = make_float2(n < a.N ? wg * sc[n] : 0.0f,
+                                         n + 1 < a.N ? wg * sc[n + 1] : 0.0f);
+            accg[j] = __ffma2_rn(f, acc[j], accg[j]);
+          }
+        }
       }
+      if (!ok) break;
       const int mt = tile / a.n_ntiles, n0 = (tile % a.n_ntiles) * BN + col0;
       if (FINAL) {
-        // V[R + M n] (+)= w_p s_n acc.  Additions are L2 reductions: each
-        // element gets exactly one correctly rounded FP64 add per t-point,
+        // V[R + M n] (+)= sum over the group of w_p s_n D_p (FP32 sum of the
+        // group's terms, round to nearest).  Additions are L2 reductions:
+        // each element gets exactly one correctly rounded FP64 add per group,
         // and the warp does not wait for the old values.
         const int R = mt * BM + 32 * q + lane;
         if (R < a.M) {
@@ -538,8 +571,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int j = 0; j < CW; ++j) {
             const int n = n0 + j;
             if (n < a.N) {
-              const double add =
-                  a.wcoef * a.scale64[n] * (double)((j & 1) ? acc[j >> 1].y : acc[j >> 1].x);
+              const double add = (double)((j & 1) ? accg[j >> 1].y : accg[j >> 1].x);
               double *dst = col + (size_t)a.M * n;
               if (a.accumulate)
                 atomicAdd(dst, add);
@@ -708,6 +740,8 @@ int make_map(CUtensorMap *m, const void *base, long long inner, long long rows, 
 
 struct MixedState {
   int nparts = 2;   // BF16 parts per operand
+  int G = 1;        // t-points per pass of the last stage (slots of X[2])
+  DevBuf wdev;      // w_p as FP32 on the device
   long long ld[3];  // padded K extent of each stage's input rows
   long long rows[3];
   DevBuf X[3];      // stage inputs: nparts planes of rows x ld BF16
@@ -727,7 +761,7 @@ __nv_bfloat16 *plane(DevBuf &b, int part, long long plane_elems) {
 // One stage launch.  nrb > 0 selects the two-dimensional M tiling of the
 // intermediate stages (see StageArgs).
 template <int NSX, int NS, bool FINAL>
-int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, int nrb,
+int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, int nrb, int ng,
                  const StageArgs &base, cudaStream_t s) {
   using C = StageCfg<NSX, NS>;
   auto kern = stage_bf16_kernel<NSX, NS, FINAL>;
@@ -742,6 +776,8 @@ int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, int nrb,
   a.N = N;
   a.K = K;
   a.nrb = nrb;
+  a.ng = ng;
+  a.gM = M;
   a.n_ntiles = ceil_div(N, BN);
   const long long nmt = nrb ? (long long)(M / a.d0) * nrb : ceil_div(M, BM);
   a.ntiles = (int)(nmt * a.n_ntiles);
@@ -780,31 +816,43 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
   const int ni[3] = {nix, niy, niz}, no[3] = {nox, noy, noz};
   const long long M[3] = {(long long)niy * niz, (long long)niz * nox, (long long)nox * noy};
   const int d0[3] = {niy, niz, 0}, d1[3] = {niz, nox, 0};
+  auto common = [&](StageArgs &a, int stage, int p) {
+    const int ow = st.towner[stage];
+    a.scale = st.sc[ow].as<float>() + (size_t)p * no[stage];
+    a.k_range = op->band[ow].as<int2>() + (size_t)p * ceil_div(no[stage], BN);
+  };
+  // last-stage input: slot p % G of X[2], parts stored [part][slot][rows][ld]
+  auto slot_plane = [&](int part, int slot) {
+    return plane(st.X[2], part, pe[2] * st.G) + (size_t)slot * pe[2];
+  };
+  int p0 = 0;  // first t-point of the open group
   for (int p = 0; p < op->P; ++p) {
-    for (int stage = 0; stage < 3; ++stage) {
+    for (int stage = 0; stage < 2; ++stage) {
       StageArgs a = base;
-      const int ow = st.towner[stage];
-      a.scale = st.sc[ow].as<float>() + (size_t)p * no[stage];
-      a.scale64 = st.sc64[ow].as<double>() + (size_t)p * no[stage];
-      a.k_range = op->band[ow].as<int2>() + (size_t)p * ceil_div(no[stage], BN);
+      common(a, stage, p);
+      const int slot = p % st.G;
+      a.out0 = stage == 0 ? plane(st.X[1], 0, pe[1]) : slot_plane(0, slot);
+      a.out1 = stage == 0 ? plane(st.X[1], 1, pe[1]) : slot_plane(1, slot);
+      a.out2 = stage == 0 ? plane(st.X[1], NSX > 2 ? 2 : 1, pe[1]) : slot_plane(NSX > 2 ? 2 : 1, slot);
+      a.d0 = d0[stage];
+      a.d1 = d1[stage];
+      a.ldn = st.ld[stage + 1];
       const int t = op->tmark_begin(0);
-      if (stage < 2) {
-        a.out0 = plane(st.X[stage + 1], 0, pe[stage + 1]);
-        a.out1 = plane(st.X[stage + 1], 1, pe[stage + 1]);
-        a.out2 = plane(st.X[stage + 1], NSX > 2 ? 2 : 1, pe[stage + 1]);
-        a.d0 = d0[stage];
-        a.d1 = d1[stage];
-        a.ldn = st.ld[stage + 1];
-        DAGE_TRY((launch_stage<NSX, NS, false>(st, stage, (int)M[stage], no[stage], ni[stage], p,
-                                               ceil_div(d0[stage], BM), a, s)));
-      } else {
-        a.V = d_V;
-        a.wcoef = op->w[p];
-        a.accumulate = p > 0;
-        DAGE_TRY((launch_stage<NSX, NS, true>(st, stage, (int)M[stage], no[stage], ni[stage], p,
-                                              0, a, s)));
-      }
+      DAGE_TRY((launch_stage<NSX, NS, false>(st, stage, (int)M[stage], no[stage], ni[stage], p,
+                                             ceil_div(d0[stage], BM), 1, a, s)));
       op->tmark_end(t);
+    }
+    if (p - p0 + 1 == st.G || p == op->P - 1) {
+      StageArgs a = base;
+      common(a, 2, p0);
+      const int ng = p - p0 + 1;
+      a.wcoef = st.wdev.as<float>() + p0;
+      a.V = d_V;
+      a.accumulate = p0 > 0;
+      const int t = op->tmark_begin(0);
+      DAGE_TRY((launch_stage<NSX, NS, true>(st, 2, (int)M[2], no[2], ni[2], p0, 0, ng, a, s)));
+      op->tmark_end(t);
+      p0 = p + 1;
     }
   }
   return 0;
@@ -822,14 +870,16 @@ int mixed_setup(dage_op3d *op) {
   st->rows[0] = (long long)niy * niz;
   st->rows[1] = (long long)niz * nox;
   st->rows[2] = (long long)nox * noy;
+  st->G = std::min(op->P, kMaxGroup);
   for (int s = 0; s < 3; ++s) {
     st->ld[s] = round_up(ni[s], 8);
-    const long long pe = st->rows[s] * st->ld[s];
+    const int slots = s == 2 ? st->G : 1;
+    const long long pe = st->rows[s] * st->ld[s] * slots;
     DAGE_TRY(st->X[s].alloc(sizeof(__nv_bfloat16) * pe * st->nparts));
     DAGE_CUDA_TRY(cudaMemsetAsync(st->X[s].ptr, 0, st->X[s].bytes, op->stream));
     for (int i = 0; i < st->nparts; ++i)
-      DAGE_TRY(make_map(&st->mapA[s][i], plane(st->X[s], i, pe), ni[s], st->rows[s], st->ld[s],
-                        BK, BM));
+      DAGE_TRY(make_map(&st->mapA[s][i], plane(st->X[s], i, pe), ni[s], st->rows[s] * slots,
+                        st->ld[s], BK, BM));
   }
   DAGE_TRY(st->err.alloc(sizeof(int)));
   DAGE_CUDA_TRY(cudaMemsetAsync(st->err.ptr, 0, sizeof(int), op->stream));
@@ -855,10 +905,18 @@ int mixed_setup(dage_op3d *op) {
     for (int i = 0; i < st->nparts; ++i)
       DAGE_TRY(make_map(&st->mapB[ax][i], plane(st->Tp[ax], i, pe), K, nrows, ld, BK, BN));
   }
-  return 0;
+  return mixed_set_weights(op);
 }
 
-int mixed_set_weights(dage_op3d *) { return 0; }
+int mixed_set_weights(dage_op3d *op) {
+  auto *st = static_cast<MixedState *>(op->mixed);
+  if (!st) return 0;
+  std::vector<float> w(op->w.begin(), op->w.end());
+  DAGE_TRY(st->wdev.alloc(sizeof(float) * w.size()));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(st->wdev.ptr, w.data(), sizeof(float) * w.size(),
+                                cudaMemcpyHostToDevice, op->stream));
+  return cudaStreamSynchronize(op->stream) == cudaSuccess ? 0 : fail(DAGE_E_CUDA, "weights upload");
+}
 
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
   auto *st = static_cast<MixedState *>(op->mixed);
@@ -886,6 +944,7 @@ void mixed_destroy(dage_op3d *op) {
     st->sc64[i].release();
   }
   st->err.release();
+  st->wdev.release();
   delete st;
   op->mixed = nullptr;
 }
