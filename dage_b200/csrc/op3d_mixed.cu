@@ -311,9 +311,9 @@ __device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
 
 // NSX parts per operand; NS shared-memory stages; the main product starts a
 // fresh partial every kGroup / 16 MMAs (one 32-run of K).
-// 18 warps x 32 threads x 112 registers = 64512 <= 65536: one CTA per SM.
+// 576 threads, one CTA per SM (the launch bound leaves 96 registers a thread).
 template <int NSX, int NS, bool FINAL>
-__global__ void __maxnreg__(112)
+__global__ void __launch_bounds__(kThreads, 1)
     stage_bf16_kernel(const __grid_constant__ CUtensorMap mapA0,
                       const __grid_constant__ CUtensorMap mapA1,
                       const __grid_constant__ CUtensorMap mapA2,
