@@ -311,9 +311,9 @@ __device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
 
 // NSX parts per operand; NS shared-memory stages; the main product starts a
 // fresh partial every kGroup / 16 MMAs (one 32-run of K).
-// 576 threads, one CTA per SM (the launch bound leaves 96 registers a thread).
+// 576 threads x 96 registers (55296 of the SM's 65536): one CTA per SM.
 template <int NSX, int NS, bool FINAL>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __maxnreg__(96)
     stage_bf16_kernel(const __grid_constant__ CUtensorMap mapA0,
                       const __grid_constant__ CUtensorMap mapA1,
                       const __grid_constant__ CUtensorMap mapA2,
