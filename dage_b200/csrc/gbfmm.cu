@@ -45,10 +45,11 @@ constexpr int kMaxLmax = 15;
 // ---------------------------------------------------------------------------
 // Real regular solid harmonics by recursion, visiting every (l, m) once.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int lmi(int l, int m) { return l * (l + 1) + m; }
+__host__ __device__ __forceinline__ int lmi(int l, int m) { return l * (l + 1) + m; }
 
 template <class F>
-__device__ __forceinline__ void solid_harmonics(int lmax, double x, double y, double z, F &&f) {
+__host__ __device__ __forceinline__ void solid_harmonics(int lmax, double x, double y, double z,
+                                                         F &&f) {
   const double r2 = x * x + y * y + z * z;
   f(0, 1.0);
   if (lmax == 0) return;
@@ -113,9 +114,37 @@ struct GInst {
   const double *Tm2l;       // plan: M2L matrix per displacement
   const int *ffstart, *ffsrc, *ffdisp;  // plan: far-field lists
   const double *wx, *wy, *wz;           // plan: full-grid integration weights
+  double kappa;  // 0: Coulomb; > 0: Helmholtz kernel e^(-kappa r)/r
 };
 
 constexpr int kEnergyBlocks = 256;
+
+// ---------------------------------------------------------------------------
+// Modified spherical Bessel functions of the first kind, as the ratios
+// f_l(x) = i_l(x) / x^l (finite at x = 0, f_l(0) = 1/(2l+1)!!), l = 0..L:
+// the series sum_k (x^2/2)^k / (k! (2l+3)(2l+5)..(2l+2k+1)) / (2l+1)!! for
+// l = L and L-1 (positive terms, no cancellation) and the downward
+// recursion f_l = (2l+3) f_{l+1} + x^2 f_{l+2} (from i_l = (2l+3)/x i_{l+1}
+// + i_{l+2}, src/bubbles/helmholtz3d.F90:879-971; all terms positive).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double bessel_ratio_series(double x2h, int n) {
+  double df = 1.0;  // (2n+1)!!
+  for (int i = 3; i <= 2 * n + 1; i += 2) df *= i;
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 400; ++k) {
+    term *= x2h / (k * (2.0 * n + 2 * k + 1));
+    sum += term;
+    if (term < 1e-17 * sum) break;
+  }
+  return sum / df;
+}
+
+__device__ __forceinline__ void bessel_ratios(double x, int L, double *f) {
+  const double x2 = x * x;
+  f[L] = bessel_ratio_series(0.5 * x2, L);
+  if (L >= 1) f[L - 1] = bessel_ratio_series(0.5 * x2, L - 1);
+  for (int l = L - 2; l >= 0; --l) f[l] = (2 * l + 3) * f[l + 1] + x2 * f[l + 2];
+}
 
 // ---------------------------------------------------------------------------
 // Multipole moments: block (box, slab, density); each thread accumulates its
@@ -144,7 +173,18 @@ __global__ void multipoles_kernel(const GInst *__restrict__ insts, int lmax, int
       const double x = xs[b.p0[0] + i] - b.c[0];
       const double y = xs[ws + b.p0[1] + j] - b.c[1];
       const double z = xs[2 * ws + b.p0[2] + k] - b.c[2];
-      solid_harmonics(lmax, x, y, z, [&](int lm, double s) { part[lm * T + tid] += v * s; });
+      if (I.kappa > 0.0) {
+        // i_l(kappa r) Y_lm(rhat) = kappa^l f_l(kappa r) S_lm(r)
+        double g[kMaxLmax + 1];
+        bessel_ratios(I.kappa * sqrt(x * x + y * y + z * z), lmax, g);
+        double kp = 1.0;
+        for (int l = 0; l <= lmax; ++l, kp *= I.kappa) g[l] *= v * kp;
+        solid_harmonics(lmax, x, y, z, [&](int lm, double s) {
+          part[lm * T + tid] += g[(int)sqrtf((float)lm + 0.5f)] * s;
+        });
+      } else {
+        solid_harmonics(lmax, x, y, z, [&](int lm, double s) { part[lm * T + tid] += v * s; });
+      }
     }
   }
   __syncthreads();
@@ -209,6 +249,35 @@ __global__ void m2l_matrices_kernel(const double *__restrict__ disp, int lmax,
   }
 }
 
+// Helmholtz M2L matrices (src/bubbles/helmholtz_multipole_tools.F90:172-278:
+// Racah -> orthonormal scaling, rotation to the translation axis, coaxial
+// translation, rotation back, orthonormal -> Racah):
+//   T[(n,m') -> (l,m)] = s_out(l) sum_mu R_l[mu][m] C(l, n, |mu|) R_n[mu][m'] s_in(n)
+// with per-displacement rotation blocks R (rblk doubles each, block l at
+// roff(l)) and coaxial coefficients C[(l (L+1) + n) (L+1) + m].  Stored like
+// the Coulomb matrices, T[k N + i] (column k = input (n,m')).
+__global__ void helm_m2l_matrices_kernel(const double *__restrict__ R, int rblk,
+                                         const double *__restrict__ C, int L, double *Tall) {
+  const int N = (L + 1) * (L + 1);
+  const double *Rd = R + (size_t)blockIdx.x * rblk;
+  const double *Cd = C + (size_t)blockIdx.x * (L + 1) * (L + 1) * (L + 1);
+  double *T = Tall + (size_t)blockIdx.x * N * N;
+  const double four_pi = 4.0 * 3.141592653589793238;
+  for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+    const int k = e / N, i = e % N;
+    int l = (int)sqrtf((float)i + 0.5f), n = (int)sqrtf((float)k + 0.5f);
+    const int m = i - l * (l + 1), mp = k - n * (n + 1);
+    const int roff_l = (2 * l - 1) * l * (2 * l + 1) / 3, roff_n = (2 * n - 1) * n * (2 * n + 1) / 3;
+    const int wl = 2 * l + 1, wn = 2 * n + 1;
+    const int mu_max = l < n ? l : n;
+    double acc = 0.0;
+    for (int mu = -mu_max; mu <= mu_max; ++mu)
+      acc += Rd[roff_l + (mu + l) * wl + (m + l)] * Cd[((size_t)l * (L + 1) + n) * (L + 1) + abs(mu)] *
+             Rd[roff_n + (mu + n) * wn + (mp + n)];
+    T[(size_t)k * N + i] = sqrt(four_pi / (2 * l + 1)) * acc * sqrt((2 * n + 1) / four_pi);
+  }
+}
+
 // L(b) = sum over the far field of b of T(disp) q(src); block (box, density).
 __global__ void m2l_apply_kernel(const GInst *__restrict__ insts, int N) {
   extern __shared__ double qs[];
@@ -250,8 +319,20 @@ __global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__rest
     const int j = (int)(r % b.own[1]), k = (int)(r / b.own[1]);
     const int gx = b.p0[0] + i, gy = b.p0[1] + j, gz = b.p0[2] + k;
     double v = 0.0;
-    solid_harmonics(lmax, xs[gx] - b.c[0], xs[ws + gy] - b.c[1], xs[2 * ws + gz] - b.c[2],
-                    [&](int lm, double s) { v += Ls[lm] * s; });
+    const double x = xs[gx] - b.c[0], y = xs[ws + gy] - b.c[1], z = xs[2 * ws + gz] - b.c[2];
+    if (I.kappa > 0.0) {
+      // 8 kappa sum (2l+1)/(4 pi) i_l(kappa r) Y_lm L_lm
+      // (src/gbfmm/gbfmm_helmholtz3d.F90:1019-1105)
+      double g[kMaxLmax + 1];
+      bessel_ratios(I.kappa * sqrt(x * x + y * y + z * z), lmax, g);
+      double kp = 8.0 * I.kappa / (4.0 * 3.141592653589793238);
+      for (int l = 0; l <= lmax; ++l, kp *= I.kappa) g[l] *= (2 * l + 1) * kp;
+      solid_harmonics(lmax, x, y, z, [&](int lm, double s) {
+        v += g[(int)sqrtf((float)lm + 0.5f)] * Ls[lm] * s;
+      });
+    } else {
+      solid_harmonics(lmax, x, y, z, [&](int lm, double s) { v += Ls[lm] * s; });
+    }
     I.V[(size_t)gx + (size_t)I.Nx * gy + (size_t)I.Nx * I.Ny * gz] += v;
   }
 }
@@ -430,6 +511,8 @@ using namespace dage;
 
 struct dage_gbfmm {
   int device = 0;
+  double energy = 0.0, kappa = 0.0;  // kernel: Coulomb (energy 0) or e^(-kappa r)/r
+  std::vector<double> disp;          // distinct far-field displacements (x, y, z)
   int level = 2, lmax = 12, nbox = 0, N = 0, P = 0, precision = DAGE_FP64;
   Axis ax[3];
   int npts[3];
@@ -459,6 +542,197 @@ int split_axis(int ncell, int nb, int v, int &c0, int &nc) {
   c0 = v * base + std::min(v, rem);  // 0-based first cell
   nc = base + (v < rem ? 1 : 0);
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Helmholtz M2L coefficient tables (host; assembled into matrices on the GPU)
+// ---------------------------------------------------------------------------
+// k_0..k_L(x), k_0 = (pi/2) e^-x / x, upward recursion
+// (src/bubbles/helmholtz3d.F90:1133-1174; long double as the reference's
+// REAL128 evaluation is closer to it than double).
+void bessel_k_host(double x, int L, std::vector<double> &out) {
+  typedef long double ext;
+  const ext X = x, pi = 3.14159265358979323846264338327950288L;
+  std::vector<ext> k(L + 2, 0.0L);
+  k[0] = std::exp(-X) / X * pi / 2;
+  if (L >= 1) k[1] = std::exp(-X) * (X + 1) / (X * X) * pi / 2;
+  for (int l = 2; l <= L; ++l) k[l] = (2 * l - 1) * k[l - 1] / X + k[l - 2];
+  out.assign(k.begin(), k.begin() + L + 1);
+}
+
+// Coaxial multipole-to-local coefficients C(l, n, m), l, n, m <= L, from
+// k_0..k_{L+1}(kappa d): the recurrence of src/bubbles/
+// helmholtz_multipole_tools.F90:428-511 (a/b coefficients :591-607, zero for
+// n < 0), which seeds (l, 0, 0) and (0, n, 0) up to L+1 and leaves the
+// entries it never fills at zero, exactly as the reference does.
+void coaxial_ml(const std::vector<double> &k, int L, std::vector<double> &out) {
+  const int D = L + 3;  // indices -1 .. L+1
+  std::vector<double> C((size_t)D * D * D, 0.0);
+  auto c = [&](int l, int n, int m) -> double & {
+    return C[((size_t)(l + 1) * D + (n + 1)) * D + (m + 1)];
+  };
+  auto A = [](int n, int m) {
+    if (n < 0) return 0.0;
+    const int am = std::abs(m);
+    return std::sqrt((double)((n + 1 + am) * (n + 1 - am)) / ((2 * n + 1) * (2 * n + 3)));
+  };
+  auto B = [](int n, int m) {
+    if (n < 0 || std::abs(m) > n) return 0.0;
+    const double b = std::sqrt((double)((n - m - 1) * (n - m)) / ((2 * n - 1) * (2 * n + 1)));
+    return m < 0 ? -b : b;
+  };
+  c(0, 0, 0) = k[0];
+  for (int n = 1; n <= L + 1; ++n) {
+    c(n, 0, 0) = ((n & 1) ? -1.0 : 1.0) * std::sqrt(2.0 * n + 1) * k[n];
+    c(0, n, 0) = std::sqrt(2.0 * n + 1) * k[n];
+  }
+  for (int n = 1; n <= L; ++n) {
+    c(1, n, 0) = (-A(n, 0) * c(0, n + 1, 0) - A(n - 1, 0) * c(0, n - 1, 0)) / A(0, 0);
+    c(n, 1, 0) = (((1 + n) & 1) ? -1.0 : 1.0) * c(1, n, 0);
+  }
+  for (int m = 0; m <= L; ++m) {
+    for (int n = m; n <= L; ++n)
+      for (int l = m; l <= L; ++l)
+        c(l, n + 1, m) = (-A(l, m) * c(l + 1, n, m) - A(l - 1, m) * c(l - 1, n, m) -
+                          A(n - 1, m) * c(l, n - 1, m)) /
+                         A(n, m);
+    for (int l = m; l <= L; ++l)
+      c(l, m + 1, m + 1) = (-B(l, -m - 1) * c(l - 1, m, m) - B(l + 1, m) * c(l + 1, m, m)) /
+                           B(m + 1, -m - 1);
+  }
+  out.resize((size_t)(L + 1) * (L + 1) * (L + 1));
+  for (int l = 0; l <= L; ++l)
+    for (int n = 0; n <= L; ++n)
+      for (int m = 0; m <= L; ++m) out[((size_t)l * (L + 1) + n) * (L + 1) + m] = c(l, n, m);
+}
+
+// Rotation blocks R_l[m'][m] (l = 0..L, block l at (2l-1)l(2l+1)/3) taking
+// real-harmonic expansions to the frame whose z axis is dhat: the unique
+// matrices with S_lm(Q^T r') = sum_m' R_l[m'][m] S_lm'(r'), solved from
+// 3(2l+1) sample directions by the normal equations.
+void rotation_blocks(const double *dhat, int L, std::vector<double> &out) {
+  double z[3] = {dhat[0], dhat[1], dhat[2]};
+  const double nz = std::sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2]);
+  for (double &v : z) v /= nz;
+  const double t[3] = {std::fabs(z[0]) > 0.9 ? 0.0 : 1.0, std::fabs(z[0]) > 0.9 ? 1.0 : 0.0, 0.0};
+  double x[3] = {t[1] * z[2] - t[2] * z[1], t[2] * z[0] - t[0] * z[2], t[0] * z[1] - t[1] * z[0]};
+  const double nx = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  for (double &v : x) v /= nx;
+  const double y[3] = {z[1] * x[2] - z[2] * x[1], z[2] * x[0] - z[0] * x[2],
+                       z[0] * x[1] - z[1] * x[0]};
+  out.assign((size_t)(2 * L + 1) * L * (2 * L + 3) / 3 + (2 * L + 1) * (2 * L + 1), 0.0);
+  for (int l = 0; l <= L; ++l) {
+    const int w = 2 * l + 1, np = 3 * w;
+    std::vector<double> Bm((size_t)np * w), Gm((size_t)np * w);
+    for (int q = 0; q < np; ++q) {
+      const double u = 1.0 - 2.0 * (q + 0.5) / np, ph = 2.399963229728653 * q;
+      const double sr = std::sqrt(1.0 - u * u);
+      const double rp[3] = {sr * std::cos(ph), sr * std::sin(ph), u};
+      const double ro[3] = {x[0] * rp[0] + y[0] * rp[1] + z[0] * rp[2],
+                            x[1] * rp[0] + y[1] * rp[1] + z[1] * rp[2],
+                            x[2] * rp[0] + y[2] * rp[1] + z[2] * rp[2]};
+      solid_harmonics(l, rp[0], rp[1], rp[2], [&](int lm, double v) {
+        if (lm >= l * l) Bm[(size_t)q * w + lm - l * l] = v;
+      });
+      solid_harmonics(l, ro[0], ro[1], ro[2], [&](int lm, double v) {
+        if (lm >= l * l) Gm[(size_t)q * w + lm - l * l] = v;
+      });
+    }
+    std::vector<double> M((size_t)w * 2 * w, 0.0);
+    for (int i = 0; i < w; ++i)
+      for (int j = 0; j < w; ++j)
+        for (int q = 0; q < np; ++q) {
+          M[(size_t)i * 2 * w + j] += Bm[(size_t)q * w + i] * Bm[(size_t)q * w + j];
+          M[(size_t)i * 2 * w + w + j] += Bm[(size_t)q * w + i] * Gm[(size_t)q * w + j];
+        }
+    for (int cc = 0; cc < w; ++cc) {
+      int pv = cc;
+      for (int r = cc + 1; r < w; ++r)
+        if (std::fabs(M[(size_t)r * 2 * w + cc]) > std::fabs(M[(size_t)pv * 2 * w + cc])) pv = r;
+      for (int j = 0; j < 2 * w; ++j) std::swap(M[(size_t)cc * 2 * w + j], M[(size_t)pv * 2 * w + j]);
+      const double dv = M[(size_t)cc * 2 * w + cc];
+      for (int j = 0; j < 2 * w; ++j) M[(size_t)cc * 2 * w + j] /= dv;
+      for (int r = 0; r < w; ++r)
+        if (r != cc) {
+          const double f = M[(size_t)r * 2 * w + cc];
+          for (int j = 0; j < 2 * w; ++j) M[(size_t)r * 2 * w + j] -= f * M[(size_t)cc * 2 * w + j];
+        }
+    }
+    const size_t off = (size_t)(2 * l - 1) * l * (2 * l + 1) / 3;
+    for (int i = 0; i < w; ++i)
+      for (int j = 0; j < w; ++j) out[off + (size_t)i * w + j] = M[(size_t)i * 2 * w + w + j];
+  }
+}
+
+// M2L matrix of every distinct displacement for the plan's kernel.
+int build_m2l(dage_gbfmm *g) {
+  if (g->ndisp == 0) return 0;
+  cudaStream_t s = g->stream;
+  const int lmax = g->lmax;
+  DAGE_TRY(g->d_Tm2l.alloc(sizeof(double) * (size_t)g->ndisp * g->N * g->N));
+  if (g->kappa > 0.0) {
+    const int rblk = (2 * lmax + 1) * lmax * (2 * lmax + 3) / 3 + (2 * lmax + 1) * (2 * lmax + 1);
+    const size_t cblk = (size_t)(lmax + 1) * (lmax + 1) * (lmax + 1);
+    std::vector<double> R((size_t)g->ndisp * rblk), C(g->ndisp * cblk), r, c, k;
+    for (int d = 0; d < g->ndisp; ++d) {
+      // translation from the source box to the target box: target - source
+      const double *dv = &g->disp[3 * d];  // source - target
+      const double dir[3] = {-dv[0], -dv[1], -dv[2]};
+      rotation_blocks(dir, lmax, r);
+      std::copy(r.begin(), r.begin() + rblk, R.begin() + (size_t)d * rblk);
+      bessel_k_host(g->kappa * std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]),
+                    lmax + 1, k);
+      coaxial_ml(k, lmax, c);
+      std::copy(c.begin(), c.end(), C.begin() + (size_t)d * cblk);
+    }
+    DevBuf dR, dC;
+    DAGE_TRY(dR.alloc(sizeof(double) * R.size()));
+    DAGE_TRY(dC.alloc(sizeof(double) * C.size()));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(dR.ptr, R.data(), sizeof(double) * R.size(), cudaMemcpyHostToDevice, s));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(dC.ptr, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, s));
+    helm_m2l_matrices_kernel<<<g->ndisp, 256, 0, s>>>(dR.as<double>(), rblk, dC.as<double>(), lmax,
+                                                       g->d_Tm2l.as<double>());
+    DAGE_CUDA_TRY(cudaGetLastError());
+    DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  }
+  M2LTables t;
+  m2l_tables(lmax, t);
+  DevBuf dd, c1, c2, l1, l2, pr, pc;
+  const size_t M = t.c1.size();
+  DAGE_TRY(dd.alloc(sizeof(double) * g->disp.size()));
+  DAGE_TRY(c1.alloc(sizeof(double) * M));
+  DAGE_TRY(c2.alloc(sizeof(double) * M));
+  DAGE_TRY(l1.alloc(sizeof(int) * M));
+  DAGE_TRY(l2.alloc(sizeof(int) * M));
+  DAGE_TRY(pr.alloc(sizeof(int) * M));
+  DAGE_TRY(pc.alloc(sizeof(int) * M));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(dd.ptr, g->disp.data(), sizeof(double) * g->disp.size(), cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(c1.ptr, t.c1.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(c2.ptr, t.c2.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(l1.ptr, t.lm1.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(l2.ptr, t.lm2.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(pr.ptr, t.prow.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(pc.ptr, t.pcol.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+  const int NI = (2 * lmax + 1) * (2 * lmax + 1);
+  m2l_matrices_kernel<<<g->ndisp, 256, sizeof(double) * NI, s>>>(
+      dd.as<double>(), lmax, c1.as<double>(), c2.as<double>(), l1.as<int>(), l2.as<int>(),
+      pr.as<int>(), pc.as<int>(), g->d_Tm2l.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// Near-field weights w_p = 2/sqrt(pi) tw_p, times e^(2E/(4 t_p^2)) for the
+// Helmholtz kernel when E < -0.005 (src/gbfmm/gbfmm_helmholtz3d.F90:478-516).
+void set_weights(dage_gbfmm *g) {
+  const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
+  g->w.resize(g->P);
+  for (int p = 0; p < g->P; ++p) {
+    double tw = g->tw[p];
+    if (g->energy < -0.005) tw *= std::exp(2.0 * g->energy / (4.0 * g->tp[p] * g->tp[p]));
+    g->w[p] = two_over_sqrtpi * tw;
+  }
 }
 
 int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, int lmax,
@@ -563,7 +837,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   bool regular = true;
   for (int d = 0; d < 3; ++d) regular = regular && (g->ax[d].ncell % nb == 0);
   std::map<std::vector<long long>, int> disp_index;
-  std::vector<double> disp;
+  std::vector<double> &disp = g->disp;
   std::vector<int> ffstart(1, 0), ffsrc, ffdisp;
   for (int b = 1; b <= g->nbox; ++b) {
     for (int j : local_farfield(b, maxlevel)) {
@@ -602,34 +876,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
     DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_ffdisp.ptr, ffdisp.data(), sizeof(int) * ffdisp.size(),
                                   cudaMemcpyHostToDevice, s));
   }
-  // M2L matrices on the GPU
-  if (g->ndisp > 0) {
-    M2LTables t;
-    m2l_tables(lmax, t);
-    DevBuf dd, c1, c2, l1, l2, pr, pc;
-    const size_t M = t.c1.size();
-    DAGE_TRY(dd.alloc(sizeof(double) * disp.size()));
-    DAGE_TRY(c1.alloc(sizeof(double) * M));
-    DAGE_TRY(c2.alloc(sizeof(double) * M));
-    DAGE_TRY(l1.alloc(sizeof(int) * M));
-    DAGE_TRY(l2.alloc(sizeof(int) * M));
-    DAGE_TRY(pr.alloc(sizeof(int) * M));
-    DAGE_TRY(pc.alloc(sizeof(int) * M));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(dd.ptr, disp.data(), sizeof(double) * disp.size(), cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(c1.ptr, t.c1.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(c2.ptr, t.c2.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(l1.ptr, t.lm1.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(l2.ptr, t.lm2.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(pr.ptr, t.prow.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
-    DAGE_CUDA_TRY(cudaMemcpyAsync(pc.ptr, t.pcol.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
-    DAGE_TRY(g->d_Tm2l.alloc(sizeof(double) * (size_t)g->ndisp * g->N * g->N));
-    const int NI = (2 * lmax + 1) * (2 * lmax + 1);
-    m2l_matrices_kernel<<<g->ndisp, 256, sizeof(double) * NI, s>>>(
-        dd.as<double>(), lmax, c1.as<double>(), c2.as<double>(), l1.as<int>(), l2.as<int>(),
-        pr.as<int>(), pc.as<int>(), g->d_Tm2l.as<double>());
-    DAGE_CUDA_TRY(cudaGetLastError());
-    DAGE_CUDA_TRY(cudaStreamSynchronize(s));
-  }
+  DAGE_TRY(build_m2l(g));
   DAGE_TRY(g->d_q.alloc(sizeof(double) * g->nbox * g->N));
   DAGE_TRY(g->d_L.alloc(sizeof(double) * g->nbox * g->N));
   DAGE_TRY(g->d_partial.alloc(sizeof(double) * (size_t)g->nbox * g->nslab * g->N));
@@ -637,9 +884,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   // --- near-field sub-operator matrices per axis position --------------------
   DevBuf d_tp;
   DAGE_TRY(build_quadrature(g->quad, g->tp, g->tw, d_tp, s));
-  const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
-  g->w.resize(g->P);
-  for (int p = 0; p < g->P; ++p) g->w[p] = two_over_sqrtpi * g->tw[p];
+  set_weights(g);
   for (int d = 0; d < 3; ++d) {
     g->Tnear[d].resize(nb);
     g->band_near[d].resize(nb);

@@ -136,6 +136,19 @@ int orc_bubbles_inject(int natom, const double *centers, const int *ncell,
                        const double *f, int nx, const double *x, int ny, const double *y,
                        int nz, const double *z, double factor, double *cube);
 
+/* Helmholtz (Yukawa) far field (helmholtz_ref.cpp) */
+void orc_bessel_i(double x, int lmax, double *out);
+void orc_bessel_k(double x, int lmax, double *out);
+void orc_aligned_ml(const double *bessel, int lmax, int lin, double *out);
+void orc_rotation(const double *dhat, int lmax, double *out);
+int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double *src,
+                 const double *dst, double *L);
+int orc_helm_box_multipoles(int lmax, double kappa, int nx, const double *px, const double *wx,
+                            int ny, const double *py, const double *wy, int nz, const double *pz,
+                            const double *wz, const double *rho, const double *center, double *q);
+int orc_helm_l2p(int lmax, double kappa, const double *L, const double *center, int nx,
+                 const double *px, int ny, const double *py, int nz, const double *pz, double *V);
+
 #ifdef __cplusplus
 }
 #endif

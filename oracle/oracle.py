@@ -44,6 +44,14 @@ def lib(libm_1ulp: bool = False):
         L = ctypes.CDLL(path)
         sig = {
             "orc_gauss_quad": (None, [_I, _I, _F, _F, _F, _D, _D]),
+            "orc_bessel_i": (None, [_F, _I, _D]),
+            "orc_bessel_k": (None, [_F, _I, _D]),
+            "orc_aligned_ml": (None, [_D, _I, _I, _D]),
+            "orc_rotation": (None, [_D, _I, _D]),
+            "orc_helm_m2l": (_I, [_I, _I, _F, _D, _D, _D, _D]),
+            "orc_helm_box_multipoles": (_I, [_I, _F, _I, _D, _D, _I, _D, _D, _I, _D, _D, _D, _D,
+                                             _D]),
+            "orc_helm_l2p": (_I, [_I, _F, _D, _D, _I, _D, _I, _D, _I, _D, _D]),
             "orc_gauleg": (None, [_I, _D, _D]),
             "orc_lip_coeffs": (_I, [_I, _I, _D, _D, _D]),
             "orc_lip_integrals": (_I, [_I, _I, _D]),
@@ -445,6 +453,52 @@ def l2p(lmax, L, center, px, py, pz, out):
     return out
 
 
+def bessel_i(x, lmax):
+    """i_0..i_lmax(x) (helmholtz3d.F90:879-971)."""
+    out = np.zeros(lmax + 1)
+    lib().orc_bessel_i(float(x), lmax, _p(out))
+    return out
+
+
+def bessel_k(x, lmax):
+    """k_0..k_lmax(x), k_0 = (pi/2) e^-x / x (helmholtz3d.F90:1133-1174)."""
+    out = np.zeros(lmax + 1)
+    lib().orc_bessel_k(float(x), lmax, _p(out))
+    return out
+
+
+def helm_box_multipoles(lmax, kappa, px, wx, py, wy, pz, wz, cube_sub, center):
+    """Helmholtz box moments sum rho w i_l(kappa r) Y_lm (gbfmm_helmholtz3d.F90:1491-1577)."""
+    q = np.zeros((lmax + 1) ** 2)
+    c = np.asfortranarray(cube_sub, dtype=np.float64)
+    px, wx, py, wy, pz, wz = (_f64(a) for a in (px, wx, py, wy, pz, wz))
+    lib().orc_helm_box_multipoles(lmax, float(kappa), len(px), _p(px), _p(wx), len(py), _p(py),
+                                  _p(wy), len(pz), _p(pz), _p(wz), _p(c), _p(_f64(center)), _p(q))
+    return q
+
+
+def helm_m2l(lmax, kappa, M, src, dst, lin=None):
+    """Local expansion at dst of the Helmholtz multipoles M at src
+    (HelmholtzMultipoleConverter, helmholtz_multipole_tools.F90:172-511)."""
+    lin = lmax if lin is None else lin
+    L = np.zeros((lmax + 1) ** 2)
+    rc = lib().orc_helm_m2l(lmax, lin, float(kappa), _p(_f64(M)), _p(_f64(src)), _p(_f64(dst)),
+                            _p(L))
+    if rc:
+        raise ValueError("zero translation distance")
+    return L
+
+
+def helm_l2p(lmax, kappa, L, center, px, py, pz, out):
+    """out += 8 kappa sum (2l+1)/(4 pi) i_l(kappa r) Y_lm L_lm
+    (gbfmm_helmholtz3d.F90:1019-1105)."""
+    px, py, pz = (_f64(a) for a in (px, py, pz))
+    assert out.flags.f_contiguous and out.shape == (len(px), len(py), len(pz))
+    lib().orc_helm_l2p(lmax, float(kappa), _p(_f64(L)), _p(_f64(center)), len(px), _p(px),
+                       len(py), _p(py), len(pz), _p(pz), _p(out))
+    return out
+
+
 def subgrid(g1: Grid1D, c0: int, c1: int) -> Grid1D:
     """Cells c0..c1 (1-based, inclusive) of an axis as a grid of its own
     (Grid3D_get_subgrid: the same points and cell steps)."""
@@ -516,29 +570,38 @@ class GBFMMPlan:
 
 
 def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
-                return_parts=False, libm_1ulp=False):
+                return_parts=False, libm_1ulp=False, energy=0.0):
     """GBFMMCoulomb3D_calculate_potential along the reference's CUDA path
     (gbfmm_coulomb3d.F90:650-819, gbfmm_coulomb3d.cu:478-573): multipoles per
     box, M2L over the local far field, near field by the sub-operator of
     each box (no coda), L2P of the far field; each grid point takes the near
-    and far contributions of the box that owns it."""
+    and far contributions of the box that owns it.  energy < 0: the
+    GBFMMHelmholtz3D kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)
+    (gbfmm_helmholtz3d.F90:478-1105): Helmholtz near-field weights, Bessel
+    multipoles, the Helmholtz multipole-to-local converter and L2P."""
     plan = GBFMMPlan(grid, maxlevel)
     rho = np.asfortranarray(rho)
     N = (lmax + 1) ** 2
+    helm = energy < 0.0
+    kappa = np.sqrt(-2.0 * energy) if helm else 0.0
     q = np.zeros((N, plan.nbox))
     for b in range(1, plan.nbox + 1):
         (x0, x1), (y0, y1), (z0, z1) = plan.points(b)
         subs = [subgrid(a, c0, c1) for a, (c0, c1) in zip(grid.axes, plan.cells(b))]
-        q[:, b - 1] = box_multipoles(lmax, subs[0].points, subs[0].weights(), subs[1].points,
-                                     subs[1].weights(), subs[2].points, subs[2].weights(),
-                                     rho[x0:x1, y0:y1, z0:z1], plan.center(b))
+        args = (subs[0].points, subs[0].weights(), subs[1].points, subs[1].weights(),
+                subs[2].points, subs[2].weights(), rho[x0:x1, y0:y1, z0:z1], plan.center(b))
+        q[:, b - 1] = (helm_box_multipoles(lmax, kappa, *args) if helm
+                       else box_multipoles(lmax, *args))
     L = np.zeros((N, plan.nbox))
     for i in range(1, plan.nbox + 1):
         ci = plan.center(i)
         for j in local_farfield(i, maxlevel):
-            L[:, i - 1] += interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
+            if helm:
+                L[:, i - 1] += helm_m2l(lmax, kappa, q[:, j - 1], plan.center(j), ci)
+            else:
+                L[:, i - 1] += interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
     tp, tw = gauss_quad(*quad)
-    w = coulomb_weights(tw)
+    w = helmholtz_weights(tp, tw, energy) if helm else coulomb_weights(tw)
     V = np.zeros(grid.shape, order="F")
     Vnear = np.zeros(grid.shape, order="F")
     for b in range(1, plan.nbox + 1):
@@ -551,7 +614,10 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
         sub = np.asfortranarray(rho[pin[0][0]:pin[0][1], pin[1][0]:pin[1][1], pin[2][0]:pin[2][1]])
         vn = transform_cube(*Ts, w, sub, 0.0)
         far = np.zeros(vn.shape, order="F")
-        l2p(lmax, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
+        if helm:
+            helm_l2p(lmax, kappa, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
+        else:
+            l2p(lmax, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
         sl = tuple(slice(o0, o1) for o0, o1 in own)
         V[sl] = vn + far
         Vnear[sl] = vn
