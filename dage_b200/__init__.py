@@ -10,6 +10,7 @@ from .operators import (  # noqa: F401
     Coulomb3D,
     GBFMMBatch,
     GBFMMCoulomb3D,
+    GBFMMHelmholtz3D,
     GaussQuad,
     Grid1D,
     Grid3D,
@@ -19,5 +20,5 @@ from .operators import (  # noqa: F401
     integrate,
 )
 
-__all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
+__all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GBFMMHelmholtz3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
            "DageError", "dot", "integrate", "load"]

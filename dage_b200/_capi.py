@@ -80,6 +80,7 @@ SIGNATURES = {
     "dage_gbfmm_batch_set_stream": (ctypes.c_int, [_VP, _VP]),
     "dage_gbfmm_batch_last_time_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
     "dage_gbfmm_batch_destroy": (ctypes.c_int, [_VP]),
+    "dage_gbfmm_set_energy": (ctypes.c_int, [_VP, ctypes.c_double]),
     "dage_gbfmm_tiles": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "dage_gbfmm_box_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),

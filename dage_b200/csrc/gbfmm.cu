@@ -959,6 +959,7 @@ GInst plan_inst(const dage_gbfmm *g, const double *rho, double *V, double *q, do
   I.wx = g->wts[0].as<double>();
   I.wy = g->wts[1].as<double>();
   I.wz = g->wts[2].as<double>();
+  I.kappa = g->kappa;
   return I;
 }
 
@@ -1472,6 +1473,17 @@ int dage_gbfmm_set_stream(dage_gbfmm *g, void *stream) {
   if (!g) return fail(DAGE_E_INVALID, "null handle");
   g->stream = stream ? (cudaStream_t)stream : g->own_stream;
   return 0;
+}
+
+int dage_gbfmm_set_energy(dage_gbfmm *g, double energy) {
+  clear_error();
+  if (!g) return fail(DAGE_E_INVALID, "null handle");
+  if (!(energy <= 0.0)) return fail(DAGE_E_INVALID, "energy must be <= 0 (got %g)", energy);
+  DAGE_CUDA_TRY(cudaSetDevice(g->device));
+  g->energy = energy;
+  g->kappa = energy < 0.0 ? std::sqrt(-2.0 * energy) : 0.0;
+  set_weights(g);
+  return build_m2l(g);
 }
 
 int dage_gbfmm_tiles(const dage_gbfmm *g, int tile_n[3]) {

@@ -384,6 +384,20 @@ class GBFMMCoulomb3D:
 
 
 
+
+class GBFMMHelmholtz3D(GBFMMCoulomb3D):
+    """GBFMMHelmholtz3D (src/gbfmm/gbfmm_helmholtz3d.F90:241-1105): the GBFMM
+    operator with the kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)."""
+
+    def __init__(self, grid: Grid3D, energy: float, lmax: int = 12, maxlevel: int = 2,
+                 quad: GaussQuad | None = None):
+        super().__init__(grid, lmax=lmax, maxlevel=maxlevel, quad=quad)
+        self.set_energy(energy)
+
+    def set_energy(self, energy: float) -> None:
+        check(load().dage_gbfmm_set_energy(self._h, float(energy)))
+        self.energy = float(energy)
+
 class GBFMMBatch:
     """Many independent densities through the GBFMM Coulomb operator at once
     (config: hundreds of orbitals of uneven grid sizes in one SCF step).

@@ -174,6 +174,13 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
                            unsigned flags);
 
 int dage_gbfmm_box_count(const dage_gbfmm *g, int *nbox, int *nlm);
+/* GBFMMHelmholtz3D_set_energy (src/gbfmm/gbfmm_helmholtz3d.F90:478-516): energy < 0
+ * switches the operator to the Helmholtz kernel e^(-kappa r)/r, kappa = sqrt(-2 energy):
+ * near-field weights times e^(2E/(4 t_p^2)) (when E < -0.005), multipoles and local
+ * expansions with modified spherical Bessel functions, the Helmholtz
+ * multipole-to-local converter (src/bubbles/helmholtz_multipole_tools.F90:172-511).
+ * energy = 0 returns to the Coulomb kernel. */
+int dage_gbfmm_set_energy(dage_gbfmm *g, double energy);
 /* Tile widths (32, 64 or 128 columns) the plan's autotuner chose for the
  * three near-field contraction stages (no reference counterpart: the
  * reference issues one cuBLAS call per box). */

@@ -1,0 +1,75 @@
+"""GPU tests of the GBFMM Helmholtz operator (kernel e^(-kappa r)/r) against
+the oracle: Bessel multipoles, the Helmholtz multipole-to-local converter,
+the full potential and energy, and against the direct Helmholtz cube
+operator within the multipole truncation error."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(dage, oracle, ncell, step=0.2, ng=6, seed=3):
+    half = 0.5 * ncell * 6 * step
+    g = dage.Grid3D.cube(-half, ncell, step)
+    go = oracle.Grid3D.cube(-half, ncell, step)
+    rng = np.random.default_rng(seed)
+    q = rng.uniform(-1, 2, ng)
+    a = rng.uniform(0.8, 6, ng)
+    c = rng.uniform(-0.7 * half, 0.7 * half, (ng, 3))
+    return g, go, oracle.gauss_cube(go, q, a, c)
+
+
+@pytest.mark.parametrize("ncell,energy", [(16, -0.5), (15, -1.2)])  # 15 cells: uneven split
+def test_helmholtz_moments_and_local_expansions(dage, oracle, ncell, energy):
+    lmax = 8
+    kappa = np.sqrt(-2 * energy)
+    g, go, rho = _setup(dage, oracle, ncell)
+    op = dage.GBFMMHelmholtz3D(g, energy, lmax=lmax, quad=dage.GaussQuad(6, 6))
+    Qg = op.multipole_moments(rho)
+    plan = oracle.GBFMMPlan(go, 2)
+    Qo = np.zeros_like(Qg)
+    for b in range(1, plan.nbox + 1):
+        (x0, x1), (y0, y1), (z0, z1) = plan.points(b)
+        subs = [oracle.subgrid(a, c0, c1) for a, (c0, c1) in zip(go.axes, plan.cells(b))]
+        Qo[:, b - 1] = oracle.helm_box_multipoles(lmax, kappa, subs[0].points, subs[0].weights(),
+                                                  subs[1].points, subs[1].weights(),
+                                                  subs[2].points, subs[2].weights(),
+                                                  rho[x0:x1, y0:y1, z0:z1], plan.center(b))
+    assert np.abs(Qg - Qo).max() <= 1e-12 * np.abs(Qo).max()
+    op.apply(rho)
+    Lg = op.local_expansions()
+    Lo = np.zeros_like(Lg)
+    for i in range(1, plan.nbox + 1):
+        for j in oracle.local_farfield(i, 2):
+            Lo[:, i - 1] += oracle.helm_m2l(lmax, kappa, Qo[:, j - 1], plan.center(j),
+                                            plan.center(i))
+    assert np.abs(Lg - Lo).max() <= 1e-11 * np.abs(Lo).max()
+
+
+def test_helmholtz_apply_matches_oracle(dage, oracle):
+    g, go, rho = _setup(dage, oracle, 16)
+    quad, lmax, energy = (8, 8, 0.0, 2.0, 1e3), 8, -0.5
+    op = dage.GBFMMHelmholtz3D(g, energy, lmax=lmax, quad=dage.GaussQuad(*quad))
+    V, E = op.apply(rho, energy=True)
+    Vo = oracle.gbfmm_apply(go, rho, lmax=lmax, quad=quad, energy=energy)
+    V1 = oracle.gbfmm_apply(go, rho, lmax=lmax, quad=quad, energy=energy, libm_1ulp=True)
+    spread = np.abs(V1 - Vo).max() / np.abs(Vo).max()
+    err = np.abs(V - Vo).max() / np.abs(Vo).max()
+    assert err <= max(1e-10, 10 * spread), (err, spread)
+    Eo = oracle.integrate_cube(go, rho * Vo)
+    assert abs(E - Eo) <= 1e-11 * abs(Eo)
+
+
+def test_helmholtz_close_to_direct_operator_and_back_to_coulomb(dage, oracle):
+    g, go, rho = _setup(dage, oracle, 20, ng=8)
+    quad = dage.GaussQuad(12, 12)
+    op = dage.GBFMMHelmholtz3D(g, -0.8, lmax=12, quad=quad)
+    V, E = op.apply(rho, energy=True)
+    direct = dage.Helmholtz3D(dage.Coulomb3D(g, quad=quad), -0.8)
+    Vd, Ed = direct.apply(rho, energy=True, coda=False)
+    assert np.abs(V - Vd).max() / np.abs(Vd).max() < 5e-3
+    assert abs(E - Ed) / abs(Ed) < 1e-3
+    op.set_energy(0.0)  # the Coulomb operator again
+    Vc = op.apply(rho)
+    V0 = dage.GBFMMCoulomb3D(g, lmax=12, quad=quad).apply(rho)
+    assert np.abs(Vc - V0).max() <= 1e-14 * np.abs(V0).max()
