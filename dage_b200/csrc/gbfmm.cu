@@ -620,7 +620,7 @@ void rotation_blocks(const double *dhat, int L, std::vector<double> &out) {
   for (double &v : x) v /= nx;
   const double y[3] = {z[1] * x[2] - z[2] * x[1], z[2] * x[0] - z[0] * x[2],
                        z[0] * x[1] - z[1] * x[0]};
-  out.assign((size_t)(2 * L + 1) * L * (2 * L + 3) / 3 + (2 * L + 1) * (2 * L + 1), 0.0);
+  out.assign((size_t)(L + 1) * (2 * L + 1) * (2 * L + 3) / 3, 0.0);  // sum of (2l+1)^2
   for (int l = 0; l <= L; ++l) {
     const int w = 2 * l + 1, np = 3 * w;
     std::vector<double> Bm((size_t)np * w), Gm((size_t)np * w);
@@ -671,7 +671,7 @@ int build_m2l(dage_gbfmm *g) {
   const int lmax = g->lmax;
   DAGE_TRY(g->d_Tm2l.alloc(sizeof(double) * (size_t)g->ndisp * g->N * g->N));
   if (g->kappa > 0.0) {
-    const int rblk = (2 * lmax + 1) * lmax * (2 * lmax + 3) / 3 + (2 * lmax + 1) * (2 * lmax + 1);
+    const int rblk = (lmax + 1) * (2 * lmax + 1) * (2 * lmax + 3) / 3;
     const size_t cblk = (size_t)(lmax + 1) * (lmax + 1) * (lmax + 1);
     std::vector<double> R((size_t)g->ndisp * rblk), C(g->ndisp * cblk), r, c, k;
     for (int d = 0; d < g->ndisp; ++d) {
