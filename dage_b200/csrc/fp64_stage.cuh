@@ -34,6 +34,7 @@ struct StageDesc {
   const int2 *krange;  // per 128-column tile: K band [first, last], or null
   long long t_ps;      // batched launches: T of t-point p is T + p * t_ps
   int kr_ps;           // ... and its K bands start at krange + p * kr_ps
+  const double *wp;    // batched launches: alpha of t-point p is wp[p] (null: the argument)
 };
 
 constexpr int kFp64TileM = 128, kFp64TileN = 128;

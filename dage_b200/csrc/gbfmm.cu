@@ -665,12 +665,14 @@ void rotation_blocks(const double *dhat, int L, std::vector<double> &out) {
 }
 
 // M2L matrix of every distinct displacement for the plan's kernel.
-int build_m2l(dage_gbfmm *g) {
+// M2L matrix of every distinct displacement of a plan for the kernel with
+// parameter kappa (0: Coulomb), into T.
+int build_m2l_into(const dage_gbfmm *g, double kappa, DevBuf &T) {
   if (g->ndisp == 0) return 0;
   cudaStream_t s = g->stream;
   const int lmax = g->lmax;
-  DAGE_TRY(g->d_Tm2l.alloc(sizeof(double) * (size_t)g->ndisp * g->N * g->N));
-  if (g->kappa > 0.0) {
+  DAGE_TRY(T.alloc(sizeof(double) * (size_t)g->ndisp * g->N * g->N));
+  if (kappa > 0.0) {
     const int rblk = (lmax + 1) * (2 * lmax + 1) * (2 * lmax + 3) / 3;
     const size_t cblk = (size_t)(lmax + 1) * (lmax + 1) * (lmax + 1);
     std::vector<double> R((size_t)g->ndisp * rblk), C(g->ndisp * cblk), r, c, k;
@@ -680,7 +682,7 @@ int build_m2l(dage_gbfmm *g) {
       const double dir[3] = {-dv[0], -dv[1], -dv[2]};
       rotation_blocks(dir, lmax, r);
       std::copy(r.begin(), r.begin() + rblk, R.begin() + (size_t)d * rblk);
-      bessel_k_host(g->kappa * std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]),
+      bessel_k_host(kappa * std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]),
                     lmax + 1, k);
       coaxial_ml(k, lmax, c);
       std::copy(c.begin(), c.end(), C.begin() + (size_t)d * cblk);
@@ -691,7 +693,7 @@ int build_m2l(dage_gbfmm *g) {
     DAGE_CUDA_TRY(cudaMemcpyAsync(dR.ptr, R.data(), sizeof(double) * R.size(), cudaMemcpyHostToDevice, s));
     DAGE_CUDA_TRY(cudaMemcpyAsync(dC.ptr, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, s));
     helm_m2l_matrices_kernel<<<g->ndisp, 256, 0, s>>>(dR.as<double>(), rblk, dC.as<double>(), lmax,
-                                                       g->d_Tm2l.as<double>());
+                                                       T.as<double>());
     DAGE_CUDA_TRY(cudaGetLastError());
     DAGE_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
@@ -717,23 +719,27 @@ int build_m2l(dage_gbfmm *g) {
   const int NI = (2 * lmax + 1) * (2 * lmax + 1);
   m2l_matrices_kernel<<<g->ndisp, 256, sizeof(double) * NI, s>>>(
       dd.as<double>(), lmax, c1.as<double>(), c2.as<double>(), l1.as<int>(), l2.as<int>(),
-      pr.as<int>(), pc.as<int>(), g->d_Tm2l.as<double>());
+      pr.as<int>(), pc.as<int>(), T.as<double>());
   DAGE_CUDA_TRY(cudaGetLastError());
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   return 0;
 }
 
+int build_m2l(dage_gbfmm *g) { return build_m2l_into(g, g->kappa, g->d_Tm2l); }
+
 // Near-field weights w_p = 2/sqrt(pi) tw_p, times e^(2E/(4 t_p^2)) for the
 // Helmholtz kernel when E < -0.005 (src/gbfmm/gbfmm_helmholtz3d.F90:478-516).
-void set_weights(dage_gbfmm *g) {
+void weights_for(const dage_gbfmm *g, double energy, std::vector<double> &w) {
   const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
-  g->w.resize(g->P);
+  w.resize(g->P);
   for (int p = 0; p < g->P; ++p) {
     double tw = g->tw[p];
-    if (g->energy < -0.005) tw *= std::exp(2.0 * g->energy / (4.0 * g->tp[p] * g->tp[p]));
-    g->w[p] = two_over_sqrtpi * tw;
+    if (energy < -0.005) tw *= std::exp(2.0 * energy / (4.0 * g->tp[p] * g->tp[p]));
+    w[p] = two_over_sqrtpi * tw;
   }
 }
+
+void set_weights(dage_gbfmm *g) { weights_for(g, g->energy, g->w); }
 
 int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, int lmax,
                       const dage_quad *quad) {
@@ -1282,6 +1288,15 @@ struct dage_gbfmm_batch {
   cudaGraphExec_t exec = nullptr;
   size_t graph_nodes = 0;
   std::vector<const void *> graph_key;  // rho/V pointers the graph was captured for
+  // Helmholtz kernels: one per distinct (plan, energy < 0); densities with
+  // energy 0 use their plan's Coulomb matrices and the Coulomb weights
+  struct Kern {
+    int plan = 0;
+    double energy = 0.0;
+    DevBuf T, w;  // M2L matrices of the plan's displacements; near-field weights
+  };
+  std::vector<Kern> kerns;
+  std::vector<int> kern_of;  // per density, -1: Coulomb
 };
 
 namespace dage {
@@ -1304,6 +1319,10 @@ void batch_destroy_impl(dage_gbfmm_batch *b) {
   for (auto *g : b->plans) gbfmm_destroy_impl(g);
   for (auto &c : b->chunks)
     for (auto &d : c.desc) d.release();
+  for (auto &k : b->kerns) {
+    k.T.release();
+    k.w.release();
+  }
   for (DevBuf *d : {&b->q, &b->L, &b->partial, &b->epart, &b->energy, &b->inst, &b->U, &b->W,
                     &b->stage_rho, &b->stage_V})
     d->release();
@@ -1322,6 +1341,7 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
   DAGE_CUDA_TRY(cudaEventCreate(&b->ev1));
   b->n = n;
   b->plan_of.resize(n);
+  b->kern_of.assign(n, -1);
   for (int i = 0; i < n; ++i) {
     const dage_grid1d *gi = grids + 3 * i;
     int found = -1;
@@ -1398,18 +1418,28 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
 int batch_tables(dage_gbfmm_batch *b, const double *const *rho, double *const *V) {
   const size_t per = (size_t)b->nbox * b->N;
   std::vector<GInst> ins(b->n);
-  for (int i = 0; i < b->n; ++i)
+  for (int i = 0; i < b->n; ++i) {
     ins[i] = plan_inst(b->plans[b->plan_of[i]], rho[i], V[i], b->q.as<double>() + per * i,
                        b->L.as<double>() + per * i, b->partial.as<double>() + per * b->nslab * i,
                        b->epart.as<double>() + (size_t)kEnergyBlocks * i);
+    if (b->kern_of[i] >= 0) {
+      const auto &k = b->kerns[b->kern_of[i]];
+      ins[i].kappa = std::sqrt(-2.0 * k.energy);
+      ins[i].Tm2l = k.T.as<double>();
+    }
+  }
   DAGE_CUDA_TRY(cudaMemcpyAsync(b->inst.ptr, ins.data(), sizeof(GInst) * b->n,
                                 cudaMemcpyHostToDevice, b->stream));
   std::vector<std::vector<StageDesc>> keep;
   for (auto &c : b->chunks) {
     std::vector<StageDesc> ds[3];
-    for (int i = c.i0; i < c.i1; ++i)
+    for (int i = c.i0; i < c.i1; ++i) {
+      const size_t z0 = ds[2].size();
       near_descs(b->plans[b->plan_of[i]], rho[i], V[i], b->U.as<double>() + c.uoff[i - c.i0],
                  b->W.as<double>() + c.woff[i - c.i0], ds);
+      if (b->kern_of[i] >= 0)  // this density's own t-point weights in the z stage
+        for (size_t e = z0; e < ds[2].size(); ++e) ds[2][e].wp = b->kerns[b->kern_of[i]].w.as<double>();
+    }
     for (int d = 0; d < 3; ++d)
       DAGE_CUDA_TRY(cudaMemcpyAsync(c.desc[d].ptr, ds[d].data(), sizeof(StageDesc) * c.njobs,
                                     cudaMemcpyHostToDevice, b->stream));
@@ -1696,6 +1726,43 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
   DAGE_CUDA_TRY(cudaEventRecord(b->ev1, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   DAGE_CUDA_TRY(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  return 0;
+}
+
+int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies) {
+  clear_error();
+  if (!b || !energies) return fail(DAGE_E_INVALID, "null argument");
+  for (int i = 0; i < b->n; ++i)
+    if (!(energies[i] <= 0.0)) return fail(DAGE_E_INVALID, "energy %d must be <= 0", i);
+  DAGE_CUDA_TRY(cudaSetDevice(b->device));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  for (auto &k : b->kerns) {
+    k.T.release();
+    k.w.release();
+  }
+  b->kerns.clear();
+  for (int i = 0; i < b->n; ++i) {
+    b->kern_of[i] = -1;
+    if (energies[i] == 0.0) continue;
+    for (size_t k = 0; k < b->kerns.size() && b->kern_of[i] < 0; ++k)
+      if (b->kerns[k].plan == b->plan_of[i] && b->kerns[k].energy == energies[i])
+        b->kern_of[i] = (int)k;
+    if (b->kern_of[i] >= 0) continue;
+    b->kerns.emplace_back();
+    auto &k = b->kerns.back();
+    k.plan = b->plan_of[i];
+    k.energy = energies[i];
+    const dage_gbfmm *g = b->plans[k.plan];
+    DAGE_TRY(build_m2l_into(g, std::sqrt(-2.0 * k.energy), k.T));
+    std::vector<double> w;
+    weights_for(g, k.energy, w);
+    DAGE_TRY(k.w.alloc(sizeof(double) * w.size()));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(k.w.ptr, w.data(), sizeof(double) * w.size(),
+                                  cudaMemcpyHostToDevice, b->stream));
+    DAGE_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    b->kern_of[i] = (int)b->kerns.size() - 1;
+  }
+  b->graph_key.clear();  // the tables change: capture again on the next apply
   return 0;
 }
 

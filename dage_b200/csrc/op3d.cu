@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(256, 1)
   if (d.krange) d.krange += p * d.kr_ps;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * TN;
   if (m0 >= d.M || n0 >= d.N) return;  // uniform across the block
-  stage_tile<ACCUM, TN>(d, alpha, m0, n0);
+  stage_tile<ACCUM, TN>(d, d.wp ? d.wp[p] : alpha, m0, n0);
 }
 
 // Band of each (t-point, 128-row tile) of an axis matrix T[p][n][K]: the

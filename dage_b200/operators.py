@@ -429,6 +429,15 @@ class GBFMMBatch:
                 pass
             self._h = None
 
+    def set_energies(self, energies) -> None:
+        """Per-density kernel: energy < 0 gives e^(-kappa r)/r, kappa = sqrt(-2 E);
+        0 the Coulomb kernel."""
+        e = np.ascontiguousarray(energies, dtype=np.float64)
+        if e.size != len(self.grids):
+            raise ValueError("one energy per density")
+        check(load().dage_gbfmm_batch_set_energies(
+            self._h, e.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
     def info(self):
         """(plans, near-field chunks, tile widths, nodes of the captured graph)."""
         npl, nch, nodes = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()

@@ -212,6 +212,10 @@ int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int l
  * The near-field tile widths are autotuned on the first call. */
 int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double *const *V,
                            unsigned flags, double *energies);
+/* Per-density kernel (as dage_gbfmm_set_energy): energies[i] < 0 gives density i
+ * the Helmholtz kernel e^(-kappa r)/r, kappa = sqrt(-2 energies[i]); 0 the Coulomb
+ * kernel (the default).  Densities with equal grids and energies share matrices. */
+int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies);
 int dage_gbfmm_batch_info(const dage_gbfmm_batch *b, int *nplans, int *nchunks, int tile_n[3],
                           long long *graph_nodes);
 int dage_gbfmm_batch_set_stream(dage_gbfmm_batch *b, void *stream);

@@ -74,3 +74,20 @@ def test_batch_graph_replay_and_device_cubes(dage, oracle):
     for a, b in zip(dv, dv2):
         assert torch.equal(a, b)
     np.testing.assert_array_equal(E2, E3)
+
+
+def test_batch_helmholtz_energies(dage, oracle):
+    ncells = [8, 9, 8, 9]
+    lmax = 6
+    energies = [-0.5, -1.1, 0.0, -0.5]  # two shared kernels, one Coulomb density
+    grids, rhos = _densities(dage, oracle, ncells, seed=7)
+    batch = dage.GBFMMBatch(grids, lmax=lmax, quad=dage.GaussQuad(*QUAD))
+    batch.set_energies(energies)
+    outs = [np.zeros(g.shape, order="F") for g in grids]
+    E = batch.apply(rhos, outs, energy=True)
+    for g, rho, V, e, en in zip(grids, rhos, outs, E, energies):
+        op = (dage.GBFMMHelmholtz3D(g, en, lmax=lmax, quad=dage.GaussQuad(*QUAD)) if en < 0
+              else dage.GBFMMCoulomb3D(g, lmax=lmax, quad=dage.GaussQuad(*QUAD)))
+        V1, e1 = op.apply(rho, energy=True)
+        assert np.abs(V - V1).max() <= 1e-13 * np.abs(V1).max()
+        assert abs(e - e1) <= 1e-13 * abs(e1)
