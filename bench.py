@@ -425,6 +425,181 @@ def run_gpu(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# The other configurations of the path (not the headline line): each prints
+# one JSON line of its own (bench.py --workload NAME)
+# ---------------------------------------------------------------------------
+def _timed(fn, steps, warmup, sync):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _line(args, world, metric, value, unit, ms, dtype, config, clocks, launches, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": config, "e2e": None, "roofline": None, "cpu_baseline": None,
+            "clocks": clocks, "gpu_launches": launches}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def _gauss_cube(dev, n_cell, step, q, a, c):
+    return density_torch(axis_points(n_cell, step), q, a, c, dev)
+
+
+def run_workload(args, world, rank, local):
+    import torch
+
+    import dage_b200 as dage
+    from dage_b200 import build as b
+
+    b.build()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sync = torch.cuda.synchronize
+    clk = ClockSampler(local)
+    wl = args.workload
+    if wl == "coulomb_cube_121":
+        # FP64 single box, 121^3 (20 cells, step 0.2), 2 Gaussians, 40 t-points
+        rng = np.random.default_rng(SEED)
+        q, a, c = rng.uniform(0.5, 2, 2), rng.uniform(0.5, 4, 2), rng.uniform(-3, 3, (2, 3))
+        g = dage.Grid3D.cube(-12.0, 20, 0.2)
+        rho = _gauss_cube(dev, 20, 0.2, q, a, c)
+        op = dage.Coulomb3D(g, quad=dage.GaussQuad(20, 20, 0.0, TLIN, TLOG))
+        V = torch.empty_like(rho)
+        clk.start()
+        ms = _timed(lambda: op.apply(rho, out=V, energy=True), args.steps, args.warmup, sync)
+        clocks = clk.stop()
+        # analytic potential sum q erf(sqrt(a) r) / r at the grid points
+        x = torch.tensor(axis_points(20, 0.2), dtype=torch.float64, device=dev)
+        Z, Y, X = torch.meshgrid(x, x, x, indexing="ij")
+        Va = torch.zeros_like(X)
+        for qi, ai, ci in zip(q, a, c):
+            r = torch.sqrt((X - ci[0]) ** 2 + (Y - ci[1]) ** 2 + (Z - ci[2]) ** 2).clamp_min(1e-300)
+            Va += qi * torch.erf(np.sqrt(ai) * r) / r
+        err = float((V - Va.reshape(-1)).abs().max() / Va.abs().max())
+        n = 121 ** 3
+        _line(args, world, "Coulomb-op Mpts/s @121^3 FP64", n / ms / 1e3, "Mpts/s", ms, "f64",
+              {"workload": wl, "points_per_axis": 121, "step_bohr": 0.2, "t_points": 40,
+               "gaussians": 2, "seed": SEED}, clocks, 3 * 40 + 2,
+              {"accuracy": {"vs": "analytic sum q erf(sqrt(a) r)/r", "max_rel": err}})
+    elif wl == "gbfmm_241":
+        # FP64 GBFMM, 241^3 (40 cells, step 0.2), 4^3 boxes, lmax 12, 16 Gaussians
+        rng = np.random.default_rng(SEED)
+        q, a = rng.uniform(-1, 2, 16), rng.uniform(0.3, 6, 16)
+        c = rng.uniform(-24, 24, (16, 3))
+        g = dage.Grid3D.cube(-24.0, 40, 0.2)
+        rho = _gauss_cube(dev, 40, 0.2, q, a, c)
+        quad = dage.GaussQuad(20, 20, 0.0, TLIN, TLOG)
+        op = dage.GBFMMCoulomb3D(g, lmax=12, quad=quad)
+        V = torch.empty_like(rho)
+        clk.start()
+        ms = _timed(lambda: op.apply(rho, out=V, energy=True), args.steps, args.warmup, sync)
+        clocks = clk.stop()
+        _, E = op.apply(rho, out=V, energy=True)
+        Vd = torch.empty_like(rho)
+        _, Ed = dage.Coulomb3D(g, quad=quad).apply(rho, out=Vd, energy=True, coda=False)
+        err = float((V - Vd).abs().max() / Vd.abs().max())
+        n = 241 ** 3
+        _line(args, world, "GBFMM Coulomb Mpts/s @241^3 FP64 (lmax 12, 4^3 boxes)", n / ms / 1e3,
+              "Mpts/s", ms, "f64",
+              {"workload": wl, "points_per_axis": 241, "step_bohr": 0.2, "t_points": 40,
+               "lmax": 12, "boxes": 64, "gaussians": 16, "seed": SEED,
+               "near_field_tiles": list(op.tiles)}, clocks, 3 * 40 + 9,
+              {"accuracy": {"vs": "single-box FP64 operator (no coda)", "max_rel": err,
+                            "energy_rel": abs(E - Ed) / abs(Ed)}})
+    elif wl in ("gbfmm_batch_256", "helmholtz_step_301"):
+        rng = np.random.default_rng(SEED)
+        if wl == "gbfmm_batch_256":
+            nd, lmax = 256, 12
+            cells = rng.choice([10, 15, 20, 25, 30], nd)
+            energies = None
+        else:
+            nd, lmax = 64, 10
+            cells = np.full(nd, 50)  # 301^3, step 0.1
+            energies = -0.5 * rng.uniform(0.5, 2.0, nd) ** 2  # kappa ~ U[0.5, 2]
+        step = 0.2 if wl == "gbfmm_batch_256" else 0.1
+        grids, rhos, outs = [], [], []
+        inject_ms = None
+        if wl == "helmholtz_step_301":
+            # 20 atoms in a 30 bohr box, radial LIP grids of 199 points (33 cells, cell
+            # ends log-spaced on [1e-5, 15]), lmax 2, f_lm = c r^l e^(-zeta r)
+            gcube = dage.Grid3D.cube(-15.0, 50, 0.1)
+            edges = np.concatenate([[0.0], 1e-5 * (15.0 / 1e-5) ** (np.arange(33) / 32)])
+            h = np.diff(edges) / 6
+            rad = dage.Grid1D(0.0, 33, 7, 1, h)
+            r = rad.coordinates()
+            centers = rng.uniform(-15, 15, (20, 3))
+            f = []
+            for _ in range(20):
+                fa = np.zeros((9, len(r)))
+                for l in range(3):
+                    for m in range(-l, l + 1):
+                        fa[l * (l + 1) + m] = rng.uniform(-1, 1) * r ** l * np.exp(-rng.uniform(0.5, 3) * r)
+                f.append(fa)
+            bub = dage.Bubbles(centers, [rad] * 20, f, 2)
+            base = torch.zeros(301 ** 3, dtype=torch.float64, device=dev)
+            inject_ms = _timed(lambda: bub.inject(gcube, cube=base.zero_()), args.steps,
+                               args.warmup, sync)
+        for i in range(nd):
+            nc = int(cells[i])
+            half = 0.5 * nc * 6 * step
+            grids.append(dage.Grid3D.cube(-half, nc, step))
+            ng = int(rng.integers(1, 9))
+            q, a = rng.uniform(-1, 2, ng), rng.uniform(0.3, 6, ng)
+            c = rng.uniform(-0.6 * half, 0.6 * half, (ng, 3))
+            rho = _gauss_cube(dev, nc, step, q, a, c)
+            if wl == "helmholtz_step_301":
+                rho += rng.uniform(0.5, 1.5) * base  # the injected bubbles of the molecule
+            rhos.append(rho)
+            outs.append(torch.empty_like(rho))
+        quad = dage.GaussQuad(20, 20, 0.0, TLIN, TLOG)
+        bt = dage.GBFMMBatch(grids, lmax=lmax, quad=quad)
+        if energies is not None:
+            bt.set_energies(energies)
+        Ebox = {}
+        clk.start()
+        ms = _timed(lambda: Ebox.update(e=bt.apply(rhos, outs, energy=True)), args.steps,
+                    args.warmup, sync)
+        clocks = clk.stop()
+        nplans, nchunks, tiles, nodes = bt.info()
+        # per-density check of a few densities against the single-density operator
+        chk = []
+        for i in range(3):
+            op = (dage.GBFMMHelmholtz3D(grids[i], energies[i], lmax=lmax, quad=quad)
+                  if energies is not None else dage.GBFMMCoulomb3D(grids[i], lmax=lmax, quad=quad))
+            V1 = torch.empty_like(rhos[i])
+            op.apply(rhos[i], out=V1)
+            chk.append(float((outs[i] - V1).abs().max() / V1.abs().max()))
+        pts = float(sum(int(gr.shape[0]) ** 3 for gr in grids))
+        metric = ("GBFMM batch Mpts/s, 256 densities 61^3..181^3, FP64, lmax 12"
+                  if wl == "gbfmm_batch_256" else
+                  "Helmholtz GBFMM batch Mpts/s, 64 orbitals 301^3, FP64, lmax 10")
+        extra = {"per_density_check": {"vs": "single-density operator", "max_rel": max(chk)},
+                 "batch": {"densities": nd, "plans": nplans, "near_chunks": nchunks,
+                           "tiles": list(tiles), "graph_nodes": nodes},
+                 "mixed_precision": "not available for the GBFMM paths (FP64 only)"}
+        if inject_ms is not None:
+            extra["bubbles_inject"] = {"ms": inject_ms, "atoms": 20, "lmax": 2,
+                                       "points": 301 ** 3,
+                                       "Mpts_per_s": 301 ** 3 / inject_ms / 1e3}
+        _line(args, world, metric, pts / ms / 1e3, "Mpts/s", ms, "f64",
+              {"workload": wl, "densities": nd, "step_bohr": step, "t_points": 40,
+               "lmax": lmax, "boxes": 64, "seed": SEED,
+               "sizes": sorted(set(int(6 * x + 1) for x in cells))}, clocks, nodes, extra)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -439,11 +614,18 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--n-cell", type=int, default=N_CELL,
                     help="cells per axis (80 -> 481^3, the headline workload)")
+    ap.add_argument("--workload", default="coulomb_cube_481",
+                    choices=["coulomb_cube_481", "coulomb_cube_121", "gbfmm_241",
+                             "gbfmm_batch_256", "helmholtz_step_301"],
+                    help="coulomb_cube_481 is the headline line; the others time the other "
+                         "configurations of the path")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload != "coulomb_cube_481":
+            run_workload(args, world, rank, local)
         else:
             run_gpu(args, world, rank, local)
     finally:
