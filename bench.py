@@ -348,7 +348,7 @@ def run_gpu(args, world, rank, local):
     # one stage of one t-point: M = n^2, N = K = n; the last stage's launches
     # cover up to 8 t-points, so rates use the total stage time of an apply
     dense_flops = 2.0 * n ** 4 * nprod
-    band = band_fraction(op.matrix(0), bk=16 if prec == "fp64" else 64)
+    band = band_fraction(op.matrix(0), bk=16 if prec == "fp64" else 32)
     stage_flops = dense_flops * band    # work the banded contraction issues
     stage_s = k_ms / args.steps / 1e3   # contraction kernels' time per apply
     apply_flops = 3 * (NLIN + NLOG) * stage_flops

@@ -39,7 +39,7 @@
 // the matrix tile (entries below 2^-64 of their row's scale) are skipped.
 //
 // Kernel structure (one persistent CTA per SM, 18 warps):
-//   warp 0      TMA producer: X and T tiles -> shared-memory ring (SW128)
+//   warp 0      TMA producer: X and T tiles -> shared-memory ring (SW64)
 //   warp 1      TMEM allocator + single-thread MMA issuer
 //   warps 2-17  epilogue, four warps per scheduler (32 columns each):
 //               partial sums -> scale -> split -> global stores
@@ -66,7 +66,7 @@ namespace {
 
 constexpr int BM = 128;           // tile rows (TMEM lanes)
 constexpr int BN = 128;           // tile columns
-constexpr int BK = 64;            // K extent of one shared-memory stage (128-byte rows)
+constexpr int BK = 32;            // K extent of one shared-memory stage (64-byte rows)
 constexpr int kGroup = 32;        // K extent sharing one quantum in a leading part
 constexpr int kThreads = 576;     // 18 warps
 constexpr int kEpiThreads = 512;  // warps 2-17
@@ -163,15 +163,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 // Shared-memory matrix descriptor of a K-major tile written by TMA with the
-// 128-byte swizzle: rows of 64 bf16 (128 bytes), 8-row swizzle atoms stacked
-// at SBO = 1024 bytes.
+// 64-byte swizzle: rows of 32 bf16 (64 bytes), 8-row swizzle atoms stacked
+// at SBO = 512 bytes.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)1 << 16;            // LBO (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;  // SBO
-  d |= (uint64_t)1 << 46;            // descriptor version
-  d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+  d |= (uint64_t)1 << 16;           // LBO (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;  // SBO
+  d |= (uint64_t)1 << 46;           // descriptor version
+  d |= (uint64_t)4 << 61;           // SWIZZLE_64B
   return d;
 }
 
@@ -921,8 +921,8 @@ int mixed_set_weights(dage_op3d *op) {
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
   auto *st = static_cast<MixedState *>(op->mixed);
   if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
-  const int rc = st->nparts == 2 ? run_stages<2, 3>(op, *st, d_rho, d_V, s)
-                                 : run_stages<3, 2>(op, *st, d_rho, d_V, s);
+  const int rc = st->nparts == 2 ? run_stages<2, 6>(op, *st, d_rho, d_V, s)
+                                 : run_stages<3, 4>(op, *st, d_rho, d_V, s);
   if (rc) return rc;
   int herr = 0;
   DAGE_CUDA_TRY(cudaMemcpyAsync(&herr, st->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
