@@ -461,6 +461,26 @@ def _gauss_cube(dev, n_cell, step, q, a, c):
     return density_torch(axis_points(n_cell, step), q, a, c, dev)
 
 
+def _molecule_bubbles(dage, rng):
+    """20 atoms uniform in a 30 bohr box, each a radial LIP grid of 199 points
+    (33 cells, cell ends log-spaced on [1e-5, 15] bohr) with lmax 2 radial
+    functions c r^l e^(-zeta r), c ~ U[-1, 1], zeta ~ U[0.5, 3]; and the
+    301^3 cube (step 0.1) they are injected into."""
+    gcube = dage.Grid3D.cube(-15.0, 50, 0.1)
+    edges = np.concatenate([[0.0], 1e-5 * (15.0 / 1e-5) ** (np.arange(33) / 32)])
+    rad = dage.Grid1D(0.0, 33, 7, 1, np.diff(edges) / 6)
+    r = rad.coordinates()
+    centers = rng.uniform(-15, 15, (20, 3))
+    f = []
+    for _ in range(20):
+        fa = np.zeros((9, len(r)))
+        for l in range(3):
+            for m in range(-l, l + 1):
+                fa[l * (l + 1) + m] = rng.uniform(-1, 1) * r ** l * np.exp(-rng.uniform(0.5, 3) * r)
+        f.append(fa)
+    return dage.Bubbles(centers, [rad] * 20, f, 2), gcube
+
+
 def run_workload(args, world, rank, local):
     import torch
 
@@ -522,6 +542,19 @@ def run_workload(args, world, rank, local):
                "near_field_tiles": list(op.tiles)}, clocks, 3 * 40 + 9,
               {"accuracy": {"vs": "single-box FP64 operator (no coda)", "max_rel": err,
                             "energy_rel": abs(E - Ed) / abs(Ed)}})
+    elif wl == "bubbles_inject_301":
+        rng = np.random.default_rng(SEED)
+        bub, gcube = _molecule_bubbles(dage, rng)
+        cube = torch.zeros(301 ** 3, dtype=torch.float64, device=dev)
+        clk.start()
+        ms = _timed(lambda: bub.inject(gcube, cube=cube), args.steps, args.warmup, sync)
+        clocks = clk.stop()
+        n = 301 ** 3
+        _line(args, world, "Bubbles->cube injection Mpts/s @301^3 (20 atoms, lmax 2)",
+              n / ms / 1e3, "Mpts/s", ms, "f64",
+              {"workload": wl, "points_per_axis": 301, "step_bohr": 0.1, "atoms": 20,
+               "lmax": 2, "radial_points": 199, "seed": SEED}, clocks, 1,
+              {"hbm_GBps": 16.0 * n / ms / 1e6})
     elif wl in ("gbfmm_batch_256", "helmholtz_step_301"):
         rng = np.random.default_rng(SEED)
         if wl == "gbfmm_batch_256":
@@ -536,22 +569,7 @@ def run_workload(args, world, rank, local):
         grids, rhos, outs = [], [], []
         inject_ms = None
         if wl == "helmholtz_step_301":
-            # 20 atoms in a 30 bohr box, radial LIP grids of 199 points (33 cells, cell
-            # ends log-spaced on [1e-5, 15]), lmax 2, f_lm = c r^l e^(-zeta r)
-            gcube = dage.Grid3D.cube(-15.0, 50, 0.1)
-            edges = np.concatenate([[0.0], 1e-5 * (15.0 / 1e-5) ** (np.arange(33) / 32)])
-            h = np.diff(edges) / 6
-            rad = dage.Grid1D(0.0, 33, 7, 1, h)
-            r = rad.coordinates()
-            centers = rng.uniform(-15, 15, (20, 3))
-            f = []
-            for _ in range(20):
-                fa = np.zeros((9, len(r)))
-                for l in range(3):
-                    for m in range(-l, l + 1):
-                        fa[l * (l + 1) + m] = rng.uniform(-1, 1) * r ** l * np.exp(-rng.uniform(0.5, 3) * r)
-                f.append(fa)
-            bub = dage.Bubbles(centers, [rad] * 20, f, 2)
+            bub, gcube = _molecule_bubbles(dage, rng)
             base = torch.zeros(301 ** 3, dtype=torch.float64, device=dev)
             inject_ms = _timed(lambda: bub.inject(gcube, cube=base.zero_()), args.steps,
                                args.warmup, sync)
@@ -619,7 +637,7 @@ def main():
                     help="cells per axis (80 -> 481^3, the headline workload)")
     ap.add_argument("--workload", default="coulomb_cube_481",
                     choices=["coulomb_cube_481", "coulomb_cube_121", "gbfmm_241",
-                             "gbfmm_batch_256", "helmholtz_step_301"],
+                             "gbfmm_batch_256", "helmholtz_step_301", "bubbles_inject_301"],
                     help="coulomb_cube_481 is the headline line; the others time the other "
                          "configurations of the path")
     args = ap.parse_args()
