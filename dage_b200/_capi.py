@@ -74,6 +74,7 @@ SIGNATURES = {
                                                ctypes.c_int, _VP, ctypes.c_size_t, _VP]),
     "dage_gbfmm_batch_apply": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint, _D]),
     "dage_gbfmm_batch_set_energies": (ctypes.c_int, [_VP, _D]),
+    "dage_gbfmm_batch_set_bubbles": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int]),
     "dage_gbfmm_batch_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int),

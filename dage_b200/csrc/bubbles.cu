@@ -272,6 +272,31 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
 }
 
 int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, double factor,
+                        double *cube, unsigned flags);
+
+}  // extern "C"
+
+namespace dage {
+// Stream-ordered injection into a device cube whose point coordinates are
+// already on the device (allocates nothing: usable inside a stream capture).
+int bubbles_inject_launch(const dage_bubbles *b, const double *xs, int nx, const double *ys,
+                          int ny, const double *zs, int nz, int lmin, double factor,
+                          double *d_cube, cudaStream_t s) {
+  if (!b || lmin < 0 || lmin > b->lmax) return fail(DAGE_E_INVALID, "bubbles or lmin");
+  const size_t n = (size_t)nx * ny * nz;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
+  inject_kernel<<<blocks, 256, 0, s>>>(b->atoms.as<AtomTab>(), b->natom, b->celld.as<double>(),
+                                       b->hcell.as<double>(), b->coef.as<double>(), b->N, b->lmax,
+                                       lmin, b->nlip, b->first, xs, nx, ys, ny, zs, nz, factor,
+                                       d_cube);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+}  // namespace dage
+
+extern "C" {
+
+int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, double factor,
                         double *cube, unsigned flags) {
   clear_error();
   if (!b || !grid || !cube) return fail(DAGE_E_INVALID, "null argument");

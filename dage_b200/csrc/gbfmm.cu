@@ -1297,6 +1297,10 @@ struct dage_gbfmm_batch {
   };
   std::vector<Kern> kerns;
   std::vector<int> kern_of;  // per density, -1: Coulomb
+  // optional first pipeline stage: rho_i += inject_factor[i] * bubbles
+  const dage_bubbles *bubbles = nullptr;
+  int inject_lmin = 0;
+  std::vector<double> inject_factor;
 };
 
 namespace dage {
@@ -1452,9 +1456,18 @@ int batch_tables(dage_gbfmm_batch *b, const double *const *rho, double *const *V
 
 // The whole pipeline for the current tables, as stream work (captured into
 // the graph or launched directly).
-int batch_launch(dage_gbfmm_batch *b, double *const *V) {
+int batch_launch(dage_gbfmm_batch *b, const double *const *rho, double *const *V) {
   cudaStream_t s = b->stream;
   const GInst *d_inst = b->inst.as<GInst>();
+  if (b->bubbles)
+    for (int i = 0; i < b->n; ++i) {
+      if (b->inject_factor[i] == 0.0) continue;
+      const dage_gbfmm *g = b->plans[b->plan_of[i]];
+      const double *xs = g->d_wbox.as<double>() + (size_t)3 * 64 * g->wstride;
+      DAGE_TRY(bubbles_inject_launch(b->bubbles, xs, g->npts[0], xs + g->wstride, g->npts[1],
+                                     xs + 2 * g->wstride, g->npts[2], b->inject_lmin,
+                                     b->inject_factor[i], const_cast<double *>(rho[i]), s));
+    }
   for (int i = 0; i < b->n; ++i)
     DAGE_CUDA_TRY(cudaMemsetAsync(V[i], 0, sizeof(double) * b->npts[i], s));
   DAGE_TRY(run_multipoles(d_inst, b->n, b->nbox, b->lmax, b->nslab, s));
@@ -1698,7 +1711,7 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
       DAGE_TRY(multipoles_smem(b->N, &threads));
       DAGE_TRY(prepare_fp64_stages());
       DAGE_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      const int rc = batch_launch(b, dv.data());
+      const int rc = batch_launch(b, dr.data(), dv.data());
       cudaGraph_t graph = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(s, &graph);
       if (rc) {
@@ -1715,7 +1728,7 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
   if (use_graph)
     DAGE_CUDA_TRY(cudaGraphLaunch(b->exec, s));
   else
-    DAGE_TRY(batch_launch(b, dv.data()));
+    DAGE_TRY(batch_launch(b, dr.data(), dv.data()));
   if (!(flags & DAGE_DEVICE_PTRS))
     for (int i = 0; i < b->n; ++i)
       DAGE_CUDA_TRY(cudaMemcpyAsync(V[i], dv[i], sizeof(double) * b->npts[i],
@@ -1763,6 +1776,20 @@ int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies) {
     b->kern_of[i] = (int)b->kerns.size() - 1;
   }
   b->graph_key.clear();  // the tables change: capture again on the next apply
+  return 0;
+}
+
+int dage_gbfmm_batch_set_bubbles(dage_gbfmm_batch *b, const dage_bubbles *bubbles,
+                                 const double *factors, int lmin) {
+  clear_error();
+  if (!b) return fail(DAGE_E_INVALID, "null handle");
+  if (bubbles && !factors) return fail(DAGE_E_INVALID, "factors are null");
+  b->bubbles = bubbles;
+  b->inject_lmin = lmin;
+  b->inject_factor.assign(b->n, 0.0);
+  if (bubbles)
+    for (int i = 0; i < b->n; ++i) b->inject_factor[i] = factors[i];
+  b->graph_key.clear();  // the pipeline changes: capture again on the next apply
   return 0;
 }
 

@@ -87,6 +87,11 @@ int build_quadrature(const dage_quad &q, std::vector<double> &tp, std::vector<do
 int build_axis_matrix(const Axis &in, const double *out_points, int n_out, const double *d_tp,
                       int P, double *d_T, cudaStream_t s);
 
+// bubbles -> device cube on a stream (bubbles.cu); coordinates on the device
+int bubbles_inject_launch(const dage_bubbles *b, const double *xs, int nx, const double *ys,
+                          int ny, const double *zs, int nz, int lmin, double factor,
+                          double *d_cube, cudaStream_t s);
+
 // mixed-precision path (op3d_mixed.cu)
 int mixed_setup(dage_op3d *op);
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s);

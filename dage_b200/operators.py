@@ -438,6 +438,20 @@ class GBFMMBatch:
         check(load().dage_gbfmm_batch_set_energies(
             self._h, e.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
 
+    def set_bubbles(self, bubbles, factors, lmin: int = 0) -> None:
+        """First pipeline stage: rho_i += factors[i] * bubbles, in place, before the
+        operator (None removes it).  Keep the Bubbles object alive meanwhile."""
+        if bubbles is None:
+            check(load().dage_gbfmm_batch_set_bubbles(self._h, None, None, 0))
+            self._bubbles = None
+            return
+        f = np.ascontiguousarray(factors, dtype=np.float64)
+        if f.size != len(self.grids):
+            raise ValueError("one factor per density")
+        self._bubbles = (bubbles, f)
+        check(load().dage_gbfmm_batch_set_bubbles(
+            self._h, bubbles._h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), lmin))
+
     def info(self):
         """(plans, near-field chunks, tile widths, nodes of the captured graph)."""
         npl, nch, nodes = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()

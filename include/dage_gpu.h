@@ -201,6 +201,7 @@ int dage_gbfmm_destroy(dage_gbfmm *g);
  * processed in chunks of densities that fit near_budget_bytes (0 = 8 GiB).
  * grids holds 3 axes per density; maxlevel must be 2. */
 typedef struct dage_gbfmm_batch dage_gbfmm_batch;
+typedef struct dage_bubbles dage_bubbles;
 int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int lmax,
                             const dage_quad *quad, size_t near_budget_bytes,
                             dage_gbfmm_batch **out);
@@ -216,6 +217,13 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
  * the Helmholtz kernel e^(-kappa r)/r, kappa = sqrt(-2 energies[i]); 0 the Coulomb
  * kernel (the default).  Densities with equal grids and energies share matrices. */
 int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies);
+/* Optional first stage of the batch pipeline (the SCF step's inject -> near field ->
+ * moments -> M2L -> evaluate, all in the one graph): rho_i += factors[i] * bubbles
+ * (from lmin) on density i's grid, in place, before the operator runs; factors[i] = 0
+ * skips density i; bubbles = NULL removes the stage.  The bubbles object must outlive
+ * the batch's use of it. */
+int dage_gbfmm_batch_set_bubbles(dage_gbfmm_batch *b, const dage_bubbles *bubbles,
+                                 const double *factors, int lmin);
 int dage_gbfmm_batch_info(const dage_gbfmm_batch *b, int *nplans, int *nchunks, int tile_n[3],
                           long long *graph_nodes);
 int dage_gbfmm_batch_set_stream(dage_gbfmm_batch *b, void *stream);
@@ -225,7 +233,6 @@ int dage_gbfmm_batch_destroy(dage_gbfmm_batch *b);
 /* ---------------------------------------------------------------------------
  * Bubbles -> cube injection
  * ------------------------------------------------------------------------ */
-typedef struct dage_bubbles dage_bubbles;
 
 /* Uploads a bubble set: natom centres (3*natom), one radial LIP grid per atom
  * (equidistant-point cells starting at r = 0; any cell steps), lmax <= 12,

@@ -91,3 +91,42 @@ def test_batch_helmholtz_energies(dage, oracle):
         V1, e1 = op.apply(rho, energy=True)
         assert np.abs(V - V1).max() <= 1e-13 * np.abs(V1).max()
         assert abs(e - e1) <= 1e-13 * abs(e1)
+
+
+def test_batch_inject_stage(dage, oracle):
+    """The optional first stage: rho_i += f_i * bubbles in place, then the operator,
+    equal to an explicit injection followed by the single-density apply."""
+    import torch
+
+    ncells = [8, 9, 8]
+    lmax = 4
+    grids, rhos = _densities(dage, oracle, ncells, seed=7)
+    h = oracle.log_radial_grid()
+    rad = dage.Grid1D(0.0, 33, 7, 1, h)
+    r = oracle.Grid1D(0.0, 33, 7, 1, h).points
+    rng = np.random.default_rng(3)
+    centers = rng.uniform(-1.5, 1.5, (3, 3))
+    f = [np.stack([rng.uniform(0.5, 1.5) * r ** (1 if lm else 0) * np.exp(-2 * r)
+                   for lm in range(4)]) for _ in range(3)]
+    bub = dage.Bubbles(centers, [rad] * 3, f, 1)
+    factors = [0.8, 0.0, -1.3]
+    batch = dage.GBFMMBatch(grids, lmax=lmax, quad=dage.GaussQuad(*QUAD))
+    batch.set_bubbles(bub, factors, lmin=0)
+    dr = [torch.from_numpy(x.reshape(-1, order="F").copy()).cuda() for x in rhos]
+    dv = [torch.empty_like(x) for x in dr]
+    E = batch.apply(dr, dv, energy=True)
+    for g, x, fac, r1, V, e in zip(grids, rhos, factors, dr, dv, E):
+        ref = torch.from_numpy(x.reshape(-1, order="F").copy()).cuda()
+        if fac:
+            bub.inject(g, cube=ref, lmin=0, factor=fac)
+        assert torch.equal(r1, ref)  # the stage ran in place on the input cube
+        V1, e1 = _single(dage, g, ref.cpu().numpy().reshape(g.shape, order="F"), lmax)
+        got = V.cpu().numpy().reshape(g.shape, order="F")
+        assert np.abs(got - V1).max() <= 1e-13 * np.abs(V1).max()
+        assert abs(e - e1) <= 1e-13 * abs(e1)
+    # removing the stage: the cubes are left as they are
+    batch.set_bubbles(None, None)
+    before = [x.clone() for x in dr]
+    batch.apply(dr, dv)
+    for a, b in zip(before, dr):
+        assert torch.equal(a, b)
