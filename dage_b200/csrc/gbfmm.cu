@@ -127,16 +127,21 @@ constexpr int kEnergyBlocks = 256;
 // recursion f_l = (2l+3) f_{l+1} + x^2 f_{l+2} (from i_l = (2l+3)/x i_{l+1}
 // + i_{l+2}, src/bubbles/helmholtz3d.F90:879-971; all terms positive).
 // ---------------------------------------------------------------------------
+// Series terms use tabulated reciprocals 1/(k (2n+2k+1)) (k <= kRcK) and
+// 1/(2n+1)!! in place of divisions; uploaded with the harmonic tables.
+constexpr int kRcK = 128;
+__device__ double d_rc[(kRcK + 1) * 16];
+__constant__ double c_dfinv[16];
+
 __device__ __forceinline__ double bessel_ratio_series(double x2h, int n) {
-  double df = 1.0;  // (2n+1)!!
-  for (int i = 3; i <= 2 * n + 1; i += 2) df *= i;
   double term = 1.0, sum = 1.0;
   for (int k = 1; k < 400; ++k) {
-    term *= x2h / (k * (2.0 * n + 2 * k + 1));
+    const double rc = k <= kRcK ? d_rc[k * 16 + n] : 1.0 / (k * (2.0 * n + 2 * k + 1));
+    term *= x2h * rc;
     sum += term;
     if (term < 1e-17 * sum) break;
   }
-  return sum / df;
+  return sum * c_dfinv[n];
 }
 
 __device__ __forceinline__ void bessel_ratios(double x, int L, double *f) {
@@ -147,51 +152,244 @@ __device__ __forceinline__ void bessel_ratios(double x, int L, double *f) {
 }
 
 // ---------------------------------------------------------------------------
-// Multipole moments: block (box, slab, density); each thread accumulates its
-// own column of partial sums in shared memory, then one fixed-order
-// reduction.
+// Recurrence coefficients of solid_harmonics as tables (the same expressions,
+// evaluated once on the host, so the values are bit-identical):
+//   S_lm = A_lm z S_{l-1,m} - B_lm r^2 S_{l-2,m}    (l > |m|)
+//   S_{m,m} = C_m (x S_{m-1,m-1} - y S_{m-1,-(m-1)}) etc. (m >= 2)
 // ---------------------------------------------------------------------------
-__global__ void multipoles_kernel(const GInst *__restrict__ insts, int lmax, int nslab) {
-  extern __shared__ double part[];  // [N][blockDim.x]
-  const GInst I = insts[blockIdx.z];
-  const int N = (lmax + 1) * (lmax + 1);
-  const int T = blockDim.x, tid = threadIdx.x;
+constexpr int kShSize = (kMaxLmax + 1) * (kMaxLmax + 1);
+__constant__ double c_shA[kShSize];
+__constant__ double c_shB[kShSize];
+__constant__ double c_shC[kMaxLmax + 1];
+
+// Uploads the tables to the current device once per process and device
+// (called at plan creation, outside any stream capture).
+int sh_tables_init() {
+  static std::mutex mu;
+  static unsigned long long done = 0;  // one bit per device ordinal
+  int dev = 0;
+  DAGE_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 64 && (done >> dev) & 1ull) return 0;
+  double A[kShSize] = {}, B[kShSize] = {}, C[kMaxLmax + 1] = {};
+  for (int l = 1; l <= kMaxLmax; ++l)
+    for (int m = -(l - 1); m <= l - 1; ++m) {
+      A[lmi(l, m)] = (2.0 * l - 1.0) / sqrt((double)((l + m) * (l - m)));
+      B[lmi(l, m)] = sqrt((double)((l + m - 1) * (l - m - 1)) / (double)((l + m) * (l - m)));
+    }
+  for (int mm = 2; mm <= kMaxLmax; ++mm) C[mm] = sqrt((2.0 * mm - 1.0) / (2.0 * mm));
+  DAGE_CUDA_TRY(cudaMemcpyToSymbol(c_shA, A, sizeof(A)));
+  DAGE_CUDA_TRY(cudaMemcpyToSymbol(c_shB, B, sizeof(B)));
+  DAGE_CUDA_TRY(cudaMemcpyToSymbol(c_shC, C, sizeof(C)));
+  std::vector<double> rc((kRcK + 1) * 16, 0.0);
+  for (int k = 1; k <= kRcK; ++k)
+    for (int n = 0; n < 16; ++n) rc[k * 16 + n] = 1.0 / (k * (2.0 * n + 2 * k + 1));
+  double dfinv[16];
+  for (int n = 0; n < 16; ++n) {
+    double df = 1.0;  // (2n+1)!!
+    for (int i = 3; i <= 2 * n + 1; i += 2) df *= i;
+    dfinv[n] = 1.0 / df;
+  }
+  DAGE_CUDA_TRY(cudaMemcpyToSymbol(d_rc, rc.data(), sizeof(double) * rc.size()));
+  DAGE_CUDA_TRY(cudaMemcpyToSymbol(c_dfinv, dfinv, sizeof(dfinv)));
+  if (dev < 64) done |= 1ull << dev;
+  return 0;
+}
+
+// solid_harmonics with the coefficient tables (every lane of a warp visits
+// the same (l, m) sequence, so the constant-bank reads are uniform).
+template <class F>
+__device__ __forceinline__ void solid_harmonics_tab(int lmax, double x, double y, double z, F &&f) {
+  const double r2 = x * x + y * y + z * z;
+  f(0, 1.0);
+  if (lmax == 0) return;
+  {
+    double p2 = 0.0, p1 = 1.0;
+    for (int l = 1; l <= lmax; ++l) {
+      const double cur = c_shA[lmi(l, 0)] * (z * p1) - c_shB[lmi(l, 0)] * (r2 * p2);
+      f(lmi(l, 0), cur);
+      p2 = p1;
+      p1 = cur;
+    }
+  }
+  double top = x, bot = y;
+  for (int mm = 1; mm <= lmax; ++mm) {
+    if (mm >= 2) {
+      const double c = c_shC[mm];
+      const double nb = c * (y * top + x * bot);
+      const double nt = c * (x * top - y * bot);
+      top = nt;
+      bot = nb;
+    }
+    f(lmi(mm, mm), top);
+    f(lmi(mm, -mm), bot);
+#pragma unroll 1
+    for (int sgn = 0; sgn < 2; ++sgn) {
+      const int m = sgn ? -mm : mm;
+      double p2 = 0.0, p1 = sgn ? bot : top;
+      for (int l = mm + 1; l <= lmax; ++l) {
+        const double cur = c_shA[lmi(l, m)] * (z * p1) - c_shB[lmi(l, m)] * (r2 * p2);
+        f(lmi(l, m), cur);
+        p2 = p1;
+        p1 = cur;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multipole moments q_lm(b) = sum rho w S_lm (Helmholtz: i_l(kappa r) Y_lm).
+//
+// The (lmax+1)^2 harmonics of a point are split into lmax+1 lane tasks of
+// lmax+1 values each: task 0 is the m = 0 chain (l = 0..lmax); the others
+// pair the chain of m = +-mm (l = mm..lmax, lmax+1-mm values) with the
+// chain of m = +-(lmax+1-mm) of the same sign (mm values); for odd lmax the
+// chains m = +h and m = -h, h = (lmax+1)/2, form the last task.  A warp
+// evaluates PP = 32/(lmax+1) points at a time, lane p(lmax+1)+t running task
+// t for point p, each lane keeping its lmax+1 sums in registers.  Warps walk
+// columns of the box (PP neighbouring x, one y, every z); at the end the
+// block sums its lanes in a fixed order into one partial per (box, slab).
+// ---------------------------------------------------------------------------
+constexpr int kMpWarps = 8;
+
+// chains of task t: signed m of the first and second chain (task 0: the
+// m = 0 chain alone, m2 unused) and the first chain's length
+__device__ __forceinline__ void mp_task(int L, int t, int &m1, int &m2, int &len1) {
+  const int h = L / 2;
+  if (t == 0) {
+    m1 = 0;
+    m2 = 0;
+    len1 = L + 1;
+    return;
+  }
+  if (t <= h) {
+    m1 = t;
+    m2 = L + 1 - t;
+  } else if (t <= 2 * h) {
+    m1 = -(t - h);
+    m2 = -(L + 1 - (t - h));
+  } else {
+    m1 = (L + 1) / 2;
+    m2 = -m1;
+  }
+  len1 = L + 1 - abs(m1);
+}
+
+// (l, m) of step k of task t
+__device__ __forceinline__ void mp_step(int L, int t, int k, int &l, int &m) {
+  int m1, m2, len1;
+  mp_task(L, t, m1, m2, len1);
+  if (k < len1) {
+    m = m1;
+    l = abs(m1) + k;
+  } else {
+    m = m2;
+    l = abs(m2) + k - len1;
+  }
+}
+
+template <bool HELM>
+__global__ void __launch_bounds__(kMpWarps * 32, HELM ? 2 : 3)
+    multipoles_kernel(const GInst *__restrict__ insts, int lmax, int nslab) {
+  __shared__ double sA[16 * 16], sB[16 * 16];  // [k][t]
+  __shared__ double red[kMpWarps][32][17];
+  const GInst &I = insts[blockIdx.z];
+  const int L = lmax, L1 = lmax + 1;
+  const int PP = 32 / L1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e = threadIdx.x; e < L1 * L1; e += blockDim.x) {
+    const int t = e / L1, k = e % L1;
+    int l, m;
+    mp_step(L, t, k, l, m);
+    const bool start = l == abs(m);
+    sA[k * 16 + t] = start ? 0.0 : c_shA[lmi(l, m)];
+    sB[k * 16 + t] = start ? 0.0 : c_shB[lmi(l, m)];
+  }
+  __syncthreads();
+  const int p = lane / L1, t = lane % L1;
+  int m1, m2, len1;
+  mp_task(L, t, m1, m2, len1);
+  const int a1 = abs(m1), a2 = abs(m2), amax = t == 0 ? 0 : max(a1, a2);
+  const bool helm = HELM && I.kappa > 0.0;  // a batch may mix kernels
+  double kap_t = 1.0;  // kappa^t
+  for (int l = 0; l < t; ++l) kap_t *= I.kappa;
   const BoxInfo b = I.boxes[blockIdx.x];
-  for (int s = 0; s < N; ++s) part[s * T + tid] = 0.0;
   const int ws = I.wstride;
   const double *wx = I.wbox + (0 * 64 + b.pos[0]) * ws;
   const double *wy = I.wbox + (1 * 64 + b.pos[1]) * ws;
   const double *wz = I.wbox + (2 * 64 + b.pos[2]) * ws;
   const double *xs = I.wbox + (3 * 64) * ws;  // point coordinates per axis
-  const long long plane = (long long)b.np[0] * b.np[1];
-  for (int k = blockIdx.y; k < b.np[2]; k += nslab) {
-    for (long long e = tid; e < plane; e += T) {
-      const int i = (int)(e % b.np[0]), j = (int)(e / b.np[0]);
-      const size_t g = (size_t)(b.p0[0] + i) + (size_t)I.Nx * (b.p0[1] + j) +
-                       (size_t)I.Nx * I.Ny * (b.p0[2] + k);
-      const double v = I.rho[g] * (wx[i] * wy[j] * wz[k]);
-      const double x = xs[b.p0[0] + i] - b.c[0];
-      const double y = xs[ws + b.p0[1] + j] - b.c[1];
-      const double z = xs[2 * ws + b.p0[2] + k] - b.c[2];
-      if (I.kappa > 0.0) {
-        // i_l(kappa r) Y_lm(rhat) = kappa^l f_l(kappa r) S_lm(r)
-        double g[kMaxLmax + 1];
-        bessel_ratios(I.kappa * sqrt(x * x + y * y + z * z), lmax, g);
-        double kp = 1.0;
-        for (int l = 0; l <= lmax; ++l, kp *= I.kappa) g[l] *= v * kp;
-        solid_harmonics(lmax, x, y, z, [&](int lm, double s) {
-          part[lm * T + tid] += g[(int)sqrtf((float)lm + 0.5f)] * s;
-        });
-      } else {
-        solid_harmonics(lmax, x, y, z, [&](int lm, double s) { part[lm * T + tid] += v * s; });
+  const size_t plane = (size_t)I.Nx * I.Ny;
+
+  double acc[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+
+  const int nib = (b.np[0] + PP - 1) / PP;
+  const int nbund = nib * b.np[1];
+  for (int u = blockIdx.y * kMpWarps + warp; u < nbund; u += nslab * kMpWarps) {
+    const int j = u / nib, i = (u % nib) * PP + p;
+    const bool valid = p < PP && i < b.np[0];
+    const int ii = valid ? i : 0;
+    const double x = xs[b.p0[0] + ii] - b.c[0];
+    const double y = xs[ws + b.p0[1] + j] - b.c[1];
+    const double wxy = valid ? wx[ii] * wy[j] : 0.0;
+    // chain starts S_{a1,+-a1}, S_{a2,+-a2} (task 0: S_00 = 1)
+    double s1 = 1.0, s2 = 0.0;
+    {
+      double top = x, bot = y;
+      for (int mm = 1; mm <= amax; ++mm) {
+        if (mm >= 2) {
+          const double c = c_shC[mm];
+          const double nb = c * (y * top + x * bot);
+          const double nt = c * (x * top - y * bot);
+          top = nt;
+          bot = nb;
+        }
+        if (mm == a1) s1 = m1 > 0 ? top : bot;
+        if (mm == a2) s2 = m2 > 0 ? top : bot;
+      }
+    }
+    const double *rcol = I.rho + (size_t)(b.p0[0] + ii) + (size_t)I.Nx * (b.p0[1] + j) +
+                         plane * b.p0[2];
+    for (int kz = 0; kz < b.np[2]; ++kz) {
+      const double v = valid ? rcol[plane * kz] * (wxy * wz[kz]) : 0.0;
+      const double z = xs[2 * ws + b.p0[2] + kz] - b.c[2];
+      const double r2 = x * x + y * y + z * z;
+      // Helmholtz: i_l(kappa r) Y_lm(rhat) = kappa^l f_l(kappa r) S_lm(r); lane
+      // t of a point evaluates f_t for its point and the lanes of the point
+      // exchange them (the lane of step k needs l_k)
+      double gown = 0.0;
+      if (helm) gown = v * kap_t * bessel_ratio_series(0.5 * (I.kappa * I.kappa) * r2, t);
+      double p1 = 0.0, p2 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (k > L) break;
+        const bool st = k == 0 || k == len1;
+        const double rec = sA[k * 16 + t] * (z * p1) - sB[k * 16 + t] * (r2 * p2);
+        const double cur = st ? (k == 0 ? s1 : s2) : rec;
+        p2 = st ? 0.0 : p1;
+        p1 = cur;
+        double f = v;
+        if (helm)
+          f = __shfl_sync(0xffffffffu, gown, (p * L1 + (k < len1 ? a1 + k : a2 + k - len1)) & 31);
+        acc[k] += f * cur;
       }
     }
   }
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+    if (k <= L) red[warp][lane][k] = acc[k];
   __syncthreads();
-  for (int s = tid; s < N; s += T) {
-    double acc = 0.0;
-    for (int t = 0; t < T; ++t) acc += part[s * T + t];
-    I.partial[((size_t)blockIdx.x * nslab + blockIdx.y) * N + s] = acc;
+  const int N = L1 * L1;
+  for (int e = threadIdx.x; e < N; e += blockDim.x) {
+    const int tt = e / L1, k = e % L1;
+    int l, m;
+    mp_step(L, tt, k, l, m);
+    double sum = 0.0;
+    for (int w = 0; w < kMpWarps; ++w)
+      for (int pp = 0; pp < PP; ++pp) sum += red[w][pp * L1 + tt][k];
+    I.partial[((size_t)blockIdx.x * nslab + blockIdx.y) * N + lmi(l, m)] = sum;
   }
 }
 
@@ -304,6 +502,7 @@ __global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__rest
                            int lmax) {
   extern __shared__ double Ls[];
   const GInst &I = insts[blockIdx.z];
+  if (I.kappa > 0.0) return;  // Helmholtz instances: l2p_helm_kernel
   const int N = (lmax + 1) * (lmax + 1);
   const BoxInfo b = I.boxes[blockIdx.y];
   const double *L = Lext ? Lext : I.L;
@@ -320,20 +519,95 @@ __global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__rest
     const int gx = b.p0[0] + i, gy = b.p0[1] + j, gz = b.p0[2] + k;
     double v = 0.0;
     const double x = xs[gx] - b.c[0], y = xs[ws + gy] - b.c[1], z = xs[2 * ws + gz] - b.c[2];
-    if (I.kappa > 0.0) {
-      // 8 kappa sum (2l+1)/(4 pi) i_l(kappa r) Y_lm L_lm
-      // (src/gbfmm/gbfmm_helmholtz3d.F90:1019-1105)
-      double g[kMaxLmax + 1];
-      bessel_ratios(I.kappa * sqrt(x * x + y * y + z * z), lmax, g);
-      double kp = 8.0 * I.kappa / (4.0 * 3.141592653589793238);
-      for (int l = 0; l <= lmax; ++l, kp *= I.kappa) g[l] *= (2 * l + 1) * kp;
-      solid_harmonics(lmax, x, y, z, [&](int lm, double s) {
-        v += g[(int)sqrtf((float)lm + 0.5f)] * Ls[lm] * s;
-      });
-    } else {
-      solid_harmonics(lmax, x, y, z, [&](int lm, double s) { v += Ls[lm] * s; });
-    }
+    solid_harmonics_tab(lmax, x, y, z, [&](int lm, double s) { v += Ls[lm] * s; });
     I.V[(size_t)gx + (size_t)I.Nx * gy + (size_t)I.Nx * I.Ny * gz] += v;
+  }
+}
+
+// Helmholtz L2P, V(r) += 8 kappa sum (2l+1)/(4 pi) i_l(kappa r) Y_lm L_lm
+// (src/gbfmm/gbfmm_helmholtz3d.F90:1019-1105), with the multipole kernel's
+// lane tasks: lane p(lmax+1)+t evaluates task t's harmonics of point p, the
+// Bessel ratio f_t(kappa r) of its point (exchanged between the point's
+// lanes), and the point's lanes sum their terms with a segmented shuffle
+// reduction.  Block (chunk, box, density); Coulomb instances return.
+__global__ void __launch_bounds__(256)
+    l2p_helm_kernel(const GInst *__restrict__ insts, const double *__restrict__ Lext, int lmax) {
+  __shared__ double sA[16 * 16], sB[16 * 16], sLt[16 * 16];  // [k][t]
+  const GInst &I = insts[blockIdx.z];
+  if (!(I.kappa > 0.0)) return;
+  const int L = lmax, L1 = lmax + 1, N = L1 * L1;
+  const int PP = 32 / L1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const BoxInfo b = I.boxes[blockIdx.y];
+  const double *Lb = (Lext ? Lext : I.L) + (size_t)blockIdx.y * N;
+  const double kappa = I.kappa;
+  for (int e = threadIdx.x; e < N; e += blockDim.x) {
+    const int t = e / L1, k = e % L1;
+    int l, m;
+    mp_step(L, t, k, l, m);
+    const bool start = l == abs(m);
+    sA[k * 16 + t] = start ? 0.0 : c_shA[lmi(l, m)];
+    sB[k * 16 + t] = start ? 0.0 : c_shB[lmi(l, m)];
+    double kp = 8.0 * kappa / (4.0 * 3.141592653589793238);  // 8 kappa^(l+1) (2l+1) / (4 pi)
+    for (int i = 0; i < l; ++i) kp *= kappa;
+    sLt[k * 16 + t] = Lb[lmi(l, m)] * ((2 * l + 1) * kp);
+  }
+  __syncthreads();
+  const int p = lane / L1, t = lane % L1;
+  int m1, m2, len1;
+  mp_task(L, t, m1, m2, len1);
+  const int a1 = abs(m1), a2 = abs(m2), amax = t == 0 ? 0 : max(a1, a2);
+  const double *xs = I.wbox + (3 * 64) * I.wstride;
+  const int ws = I.wstride;
+  const long long n = (long long)b.own[0] * b.own[1] * b.own[2];
+  const long long stride = (long long)gridDim.x * (blockDim.x >> 5) * PP;
+  for (long long base = ((long long)blockIdx.x * (blockDim.x >> 5) + warp) * PP; base < n;
+       base += stride) {
+    const long long e = base + p;
+    const bool valid = p < PP && e < n;
+    const long long ee = valid ? e : 0;
+    const int i = (int)(ee % b.own[0]);
+    const long long r = ee / b.own[0];
+    const int j = (int)(r % b.own[1]), k = (int)(r / b.own[1]);
+    const int gx = b.p0[0] + i, gy = b.p0[1] + j, gz = b.p0[2] + k;
+    const double x = xs[gx] - b.c[0], y = xs[ws + gy] - b.c[1], z = xs[2 * ws + gz] - b.c[2];
+    const double r2 = x * x + y * y + z * z;
+    double s1 = 1.0, s2 = 0.0;
+    {
+      double top = x, bot = y;
+      for (int mm = 1; mm <= amax; ++mm) {
+        if (mm >= 2) {
+          const double c = c_shC[mm];
+          const double nb = c * (y * top + x * bot);
+          const double nt = c * (x * top - y * bot);
+          top = nt;
+          bot = nb;
+        }
+        if (mm == a1) s1 = m1 > 0 ? top : bot;
+        if (mm == a2) s2 = m2 > 0 ? top : bot;
+      }
+    }
+    const double fown = bessel_ratio_series(0.5 * (kappa * kappa) * r2, t);
+    double acc = 0.0, p1 = 0.0, p2 = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      if (kk > L) break;
+      const bool st = kk == 0 || kk == len1;
+      const double rec = sA[kk * 16 + t] * (z * p1) - sB[kk * 16 + t] * (r2 * p2);
+      const double cur = st ? (kk == 0 ? s1 : s2) : rec;
+      p2 = st ? 0.0 : p1;
+      p1 = cur;
+      const double f =
+          __shfl_sync(0xffffffffu, fown, (p * L1 + (kk < len1 ? a1 + kk : a2 + kk - len1)) & 31);
+      acc += (sLt[kk * 16 + t] * f) * cur;
+    }
+    // segmented sum over the point's lanes t = 0..L (fixed order)
+#pragma unroll
+    for (int off = 1; off < 16; off <<= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, acc, off);
+      if (t + off < L1) acc += o;
+    }
+    if (valid && t == 0) I.V[(size_t)gx + (size_t)I.Nx * gy + (size_t)I.Nx * I.Ny * gz] += acc;
   }
 }
 
@@ -524,7 +798,7 @@ struct dage_gbfmm {
   std::vector<DevBuf> Tnear[3];
   std::vector<DevBuf> band_near[3];  // K band per (t-point, 128-row tile) of Tnear
   DevBuf d_boxes, d_wbox, d_q, d_L, d_partial, d_Tm2l, d_ffstart, d_ffsrc, d_ffdisp;
-  int wstride = 0, nslab = 8, ndisp = 0;
+  int wstride = 0, nslab = 16, ndisp = 0;
   DevBuf d_U, d_W, d_desc[3];
   size_t U_per_box = 0, W_per_box = 0;
   std::vector<StageDesc> desc[3];
@@ -743,6 +1017,7 @@ void set_weights(dage_gbfmm *g) { weights_for(g, g->energy, g->w); }
 
 int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, int lmax,
                       const dage_quad *quad) {
+  DAGE_TRY(sh_tables_init());
   if (!grid || !quad) return fail(DAGE_E_INVALID, "null argument");
   // one octree level: the local far field of a level-2 box covers every box
   // outside its neighbourhood; deeper levels need M2M/L2L between levels
@@ -1060,31 +1335,13 @@ int max_owned(const dage_gbfmm *g) {
   return m;
 }
 
-// Threads per multipole block and its shared memory; raises the kernel's
-// shared-memory limit only when a larger size is first needed (so a call
-// inside a stream capture changes no attribute once set up).
-int multipoles_smem(int N, int *threads) {
-  static int limit = 0;
-  static std::mutex mu;
-  int t = 128;
-  while ((size_t)sizeof(double) * N * t > 200 * 1024 && t > 32) t -= 32;
-  *threads = t;
-  const int smem = (int)(sizeof(double) * N * t);
-  std::lock_guard<std::mutex> lock(mu);
-  if (smem > limit) {
-    DAGE_CUDA_TRY(
-        cudaFuncSetAttribute(multipoles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    limit = smem;
-  }
-  return 0;
-}
-
-int run_multipoles(const GInst *d_inst, int ninst, int nbox, int lmax, int nslab, cudaStream_t s) {
+int run_multipoles(const GInst *d_inst, int ninst, int nbox, int lmax, int nslab, bool helm,
+                   cudaStream_t s) {
   const int N = (lmax + 1) * (lmax + 1);
-  int threads;
-  DAGE_TRY(multipoles_smem(N, &threads));
-  multipoles_kernel<<<dim3(nbox, nslab, ninst), threads, sizeof(double) * N * threads, s>>>(
-      d_inst, lmax, nslab);
+  if (helm)
+    multipoles_kernel<true><<<dim3(nbox, nslab, ninst), kMpWarps * 32, 0, s>>>(d_inst, lmax, nslab);
+  else
+    multipoles_kernel<false><<<dim3(nbox, nslab, ninst), kMpWarps * 32, 0, s>>>(d_inst, lmax, nslab);
   DAGE_CUDA_TRY(cudaGetLastError());
   reduce_slabs_kernel<<<dim3((nbox * N + 255) / 256, ninst), 256, 0, s>>>(d_inst, nslab, N, nbox);
   DAGE_CUDA_TRY(cudaGetLastError());
@@ -1098,12 +1355,20 @@ int run_m2l(const GInst *d_inst, int ninst, int nbox, int N, cudaStream_t s) {
   return 0;
 }
 
+// Coulomb instances run l2p_kernel, Helmholtz instances (when `helm`)
+// l2p_helm_kernel; each kernel returns at once on the other kind.
 int run_l2p(const GInst *d_inst, int ninst, int nbox, int lmax, int maxown, const double *Lext,
-            cudaStream_t s) {
+            bool helm, cudaStream_t s) {
   const int N = (lmax + 1) * (lmax + 1);
   const int bx = std::min((maxown + 127) / 128, 64);
   l2p_kernel<<<dim3(bx, nbox, ninst), 128, sizeof(double) * N, s>>>(d_inst, Lext, lmax);
   DAGE_CUDA_TRY(cudaGetLastError());
+  if (helm) {
+    const int pts = 8 * (32 / (lmax + 1));  // points per block pass
+    const int hx = std::min((maxown + pts - 1) / pts, 256);
+    l2p_helm_kernel<<<dim3(hx, nbox, ninst), 256, 0, s>>>(d_inst, Lext, lmax);
+    DAGE_CUDA_TRY(cudaGetLastError());
+  }
   return 0;
 }
 
@@ -1370,7 +1635,7 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
   b->N = g0->N;
   b->P = g0->P;
   b->nbox = g0->nbox;
-  b->nslab = g0->nslab;
+  b->nslab = n >= 8 ? 4 : g0->nslab;  // many densities fill the GPU with fewer slabs
   b->w = g0->w;
   for (const auto *g : b->plans) {
     near_bounds(g, b->mt, b->nt);
@@ -1470,14 +1735,16 @@ int batch_launch(dage_gbfmm_batch *b, const double *const *rho, double *const *V
     }
   for (int i = 0; i < b->n; ++i)
     DAGE_CUDA_TRY(cudaMemsetAsync(V[i], 0, sizeof(double) * b->npts[i], s));
-  DAGE_TRY(run_multipoles(d_inst, b->n, b->nbox, b->lmax, b->nslab, s));
+  bool any_helm = false;
+  for (int i = 0; i < b->n; ++i) any_helm |= b->kern_of[i] >= 0;
+  DAGE_TRY(run_multipoles(d_inst, b->n, b->nbox, b->lmax, b->nslab, any_helm, s));
   DAGE_TRY(run_m2l(d_inst, b->n, b->nbox, b->N, s));
   for (auto &c : b->chunks) {
     const StageDesc *dd[3] = {c.desc[0].as<StageDesc>(), c.desc[1].as<StageDesc>(),
                               c.desc[2].as<StageDesc>()};
     DAGE_TRY(run_near(dd, c.njobs, b->mt, b->nt, b->P, b->w, b->tile_n, s));
   }
-  DAGE_TRY(run_l2p(d_inst, b->n, b->nbox, b->lmax, b->maxown, nullptr, s));
+  DAGE_TRY(run_l2p(d_inst, b->n, b->nbox, b->lmax, b->maxown, nullptr, any_helm, s));
   DAGE_TRY(run_energy(d_inst, b->n, b->energy.as<double>(), s));
   return 0;
 }
@@ -1557,14 +1824,14 @@ int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags
   DAGE_TRY(single_setup(g, d_rho, d_V, true));
   const GInst *d_inst = g->d_inst.as<GInst>();
   DAGE_CUDA_TRY(cudaMemsetAsync(d_V, 0, sizeof(double) * n, s));
-  DAGE_TRY(run_multipoles(d_inst, 1, g->nbox, g->lmax, g->nslab, s));
+  DAGE_TRY(run_multipoles(d_inst, 1, g->nbox, g->lmax, g->nslab, g->kappa > 0.0, s));
   DAGE_TRY(run_m2l(d_inst, 1, g->nbox, g->N, s));
   int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
   near_bounds(g, mt, nt);
   const StageDesc *dd[3] = {g->d_desc[0].as<StageDesc>(), g->d_desc[1].as<StageDesc>(),
                             g->d_desc[2].as<StageDesc>()};
   DAGE_TRY(run_near(dd, g->nbox, mt, nt, g->P, g->w, g->tile_n, s));
-  DAGE_TRY(run_l2p(d_inst, 1, g->nbox, g->lmax, max_owned(g), nullptr, s));
+  DAGE_TRY(run_l2p(d_inst, 1, g->nbox, g->lmax, max_owned(g), nullptr, g->kappa > 0.0, s));
   if (flags & DAGE_ENERGY) DAGE_TRY(run_energy(d_inst, 1, g->d_energy.as<double>(), s));
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -1585,7 +1852,8 @@ int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flag
   double *d_V;
   DAGE_TRY(stage_io(g, rho, nullptr, flags & DAGE_DEVICE_PTRS, &d_rho, &d_V));
   DAGE_TRY(single_setup(g, d_rho, nullptr, false));
-  DAGE_TRY(run_multipoles(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, g->nslab, g->stream));
+  DAGE_TRY(run_multipoles(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, g->nslab, g->kappa > 0.0,
+                          g->stream));
   DAGE_CUDA_TRY(cudaMemcpyAsync(moments, g->d_q.ptr, sizeof(double) * g->nbox * g->N,
                                 cudaMemcpyDeviceToHost, g->stream));
   DAGE_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -1617,7 +1885,8 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
     d_V = g->d_V.as<double>();
   }
   DAGE_TRY(single_setup(g, nullptr, d_V, false));
-  DAGE_TRY(run_l2p(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, max_owned(g), dL.as<double>(), s));
+  DAGE_TRY(run_l2p(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, max_owned(g), dL.as<double>(),
+                   g->kappa > 0.0, s));
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1707,8 +1976,6 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
       b->graph = nullptr;
       b->graph_key.clear();
       // kernel attributes are set before capture
-      int threads;
-      DAGE_TRY(multipoles_smem(b->N, &threads));
       DAGE_TRY(prepare_fp64_stages());
       DAGE_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       const int rc = batch_launch(b, dr.data(), dv.data());

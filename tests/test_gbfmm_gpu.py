@@ -93,3 +93,13 @@ def test_gbfmm_close_to_direct_operator(dage, oracle):
     Vd, Ed = dage.Coulomb3D(g, quad=quad).apply(rho, energy=True, coda=False)
     assert np.abs(V - Vd).max() / np.abs(Vd).max() < 5e-3
     assert abs(E - Ed) / abs(Ed) < 1e-3
+
+
+@pytest.mark.parametrize("lmax", [0, 1, 2, 7, 15])  # lane-task splits: 32, 16, 10, 4, 2 points a pass
+def test_multipoles_every_lmax(dage, oracle, lmax):
+    g, go, rho = _setup(dage, oracle, 8, 0.2, seed=lmax)
+    op = dage.GBFMMCoulomb3D(g, lmax=lmax, quad=dage.GaussQuad(4, 4))
+    Qg = op.multipole_moments(rho)
+    plan, Qo = _oracle_moments(oracle, go, rho, lmax)
+    for b in range(plan.nbox):
+        assert np.abs(Qg[:, b] - Qo[:, b]).max() <= 1e-12 * np.abs(Qo[:, b]).max() + 1e-300

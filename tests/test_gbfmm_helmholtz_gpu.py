@@ -73,3 +73,23 @@ def test_helmholtz_close_to_direct_operator_and_back_to_coulomb(dage, oracle):
     Vc = op.apply(rho)
     V0 = dage.GBFMMCoulomb3D(g, lmax=12, quad=quad).apply(rho)
     assert np.abs(Vc - V0).max() <= 1e-14 * np.abs(V0).max()
+
+
+@pytest.mark.parametrize("lmax,energy", [(0, -0.3), (1, -0.5), (8, -2.0), (15, -0.8)])
+def test_helmholtz_l2p_matches_oracle(dage, oracle, lmax, energy):
+    """Far field of given local expansions (the L2P alone) against the oracle."""
+    kappa = np.sqrt(-2 * energy)
+    g, go, rho = _setup(dage, oracle, 8)
+    op = dage.GBFMMHelmholtz3D(g, energy, lmax=lmax, quad=dage.GaussQuad(4, 4))
+    plan = oracle.GBFMMPlan(go, 2)
+    L = np.random.default_rng(lmax).standard_normal(((lmax + 1) ** 2, plan.nbox))
+    V = np.zeros(go.shape, order="F")
+    op.evaluate_local_expansions(L, V)
+    Vo = np.zeros(go.shape, order="F")
+    for b in range(1, plan.nbox + 1):
+        own = plan.owned(b)
+        outs = [go.axes[d].points[own[d][0]:own[d][1]] for d in range(3)]
+        far = np.zeros(tuple(len(o) for o in outs), order="F")
+        oracle.helm_l2p(lmax, kappa, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
+        Vo[tuple(slice(o0, o1) for o0, o1 in own)] = far
+    assert np.abs(V - Vo).max() <= 1e-12 * np.abs(Vo).max()
