@@ -133,6 +133,18 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// accumulate flag known at compile time after unrolling (no predicate setup)
+__device__ __forceinline__ void umma_bf16_c(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, bool accumulate) {
+  if (accumulate)
+    asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, 1;\n" ::"r"(d_tmem),
+                 "l"(adesc), "l"(bdesc), "r"(idesc)
+                 : "memory");
+  else
+    asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, 0;\n" ::"r"(d_tmem),
+                 "l"(adesc), "l"(bdesc), "r"(idesc)
+                 : "memory");
+}
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
@@ -309,6 +321,34 @@ __device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
   return a.nrb ? (mt / a.nrb) * a.d0 + (mt % a.nrb) * BM : mt * BM;
 }
 
+// The MMAs of one K block (one 32-run): the main product (part 0 x part 0)
+// into the fresh partial P, committed to `pfull` as soon as it is issued,
+// and the correction products into the accumulator Cc.  NK K=16 steps;
+// FIRST: the tile's first K block (the correction accumulator starts).
+template <int NSX, int NK, bool FIRST = false>
+__device__ __forceinline__ void mma_kblock(uint32_t P, uint32_t Cc, uint64_t d0, uint32_t idesc,
+                                           bool first, uint32_t pfull_bar) {
+  constexpr int kABytes = BM * BK * 2, kBBytes = BN * BK * 2;  // one part of a tile
+  constexpr int NCORR = NSX == 2 ? 2 : 5;
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    umma_bf16_c(P, d0 + ((k * 32) >> 4), d0 + ((NSX * kABytes + k * 32) >> 4), idesc, k != 0);
+    if (k == NK - 1) umma_commit(pfull_bar);
+#pragma unroll
+    for (int pr = 0; pr < NCORR; ++pr) {
+      int ia, ib;
+      corr_product(NSX, pr, ia, ib);
+      const uint64_t ad = d0 + ((ia * kABytes + k * 32) >> 4);
+      const uint64_t bd = d0 + ((NSX * kABytes + ib * kBBytes + k * 32) >> 4);
+      if (NK == 1) {
+        umma_bf16(Cc, ad, bd, idesc, (!first || pr != 0) ? 1u : 0u);
+      } else {
+        umma_bf16_c(Cc, ad, bd, idesc, !(FIRST && k == 0 && pr == 0));
+      }
+    }
+  }
+}
+
 // NSX parts per operand; NS shared-memory stages; the main product starts a
 // fresh partial every kGroup / 16 MMAs (one 32-run of K).
 // 576 threads x 96 registers (55296 of the SM's 65536): one CTA per SM.
@@ -321,7 +361,6 @@ __global__ void __maxnreg__(96)
                       const __grid_constant__ CUtensorMap mapB1,
                       const __grid_constant__ CUtensorMap mapB2, const StageArgs a) {
   using C = StageCfg<NSX, NS>;
-  constexpr int NCORR = NSX == 2 ? 2 : 5;
   constexpr int GRAN = kGroup / 16;
   // an earlier launch of this apply timed out: do nothing
   if (*reinterpret_cast<volatile int *>(a.err)) return;
@@ -348,10 +387,10 @@ __global__ void __maxnreg__(96)
     }
     for (int i = 0; i < C::kNP; ++i) {
       mbar_init(pfull(i), 1);
-      mbar_init(pempty(i), kEpiThreads);
+      mbar_init(pempty(i), kEpiThreads / 32);  // one arrival per epilogue warp
     }
     mbar_init(cfull, 1);
-    mbar_init(cempty, kEpiThreads);
+    mbar_init(cempty, kEpiThreads / 32);
     mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -412,67 +451,52 @@ __global__ void __maxnreg__(96)
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
+    // The tensor core runs these MMAs back to back only if the issuing
+    // thread spends almost nothing between them (a 128x128x16 MMA is 64
+    // cycles): every K block is straight-line code with compile-time
+    // operand offsets and accumulate flags.
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
-      int g = 0;  // partial counter over all tiles
+      int b = 0;            // partial buffer of the current K block (one 32-run)
+      uint32_t pph = 0;     // phase of the partial buffers' current round
       int t = 0;
       bool ok = true;
-      for (int u = blockIdx.x * a.ng; u < a.ntiles * a.ng && ok && !*abort_flag;
-           u += (u % a.ng == a.ng - 1) ? (gridDim.x - 1) * a.ng + 1 : 1, ++t) {
-        const int tile = u / a.ng, gi = u % a.ng;
+      const uint64_t dbase = sdesc(smem_u32(tiles));
+      int u = blockIdx.x * a.ng;
+      int2 r = u < a.ntiles * a.ng ? kblocks(a, u % a.ng, (u / a.ng) % a.n_ntiles) : make_int2(0, -1);
+      for (; u < a.ntiles * a.ng && ok && !*abort_flag; ++t) {
+        const int tile = u / a.ng;
         const int n0 = (tile % a.n_ntiles) * BN;
         int nt = a.N - n0;
         if (nt > BN) nt = BN;
         nt = (nt + 15) & ~15;
         const uint32_t idesc = idesc_bf16(BM, nt);
-        const int2 r = kblocks(a, gi, tile % a.n_ntiles);
-        const int nsteps = tile_steps(r);
-        int step = 0;  // K=16 step within the tile; K blocks start on a 32-run
-        for (int kb = r.x; kb <= r.y && ok; ++kb) {
-          if (!mbar_wait(full(s), ph, a.wait_limit)) {
+        const int2 rc = r;
+        // next tile's band, loaded while this tile's MMAs run
+        u += (u % a.ng == a.ng - 1) ? (gridDim.x - 1) * a.ng + 1 : 1;
+        if (u < a.ntiles * a.ng) r = kblocks(a, u % a.ng, (u / a.ng) % a.n_ntiles);
+        for (int kb = rc.x; kb <= rc.y; ++kb) {
+          const bool first = kb == rc.x;
+          if (!mbar_wait(full(s), ph, a.wait_limit) ||
+              !mbar_wait(pempty(b), pph ^ 1, a.wait_limit) ||
+              (first && !mbar_wait(cempty, (t & 1) ^ 1, a.wait_limit))) {
             on_timeout();
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t st = smem_u32(tiles + s * C::kStageBytes);
-          const int nk16 = (kb == a.nkb - 1) ? a.last_k16 : BK / 16;
-          for (int k = 0; k < nk16; ++k, ++step) {
-            const int b = g % C::kNP;
-            if (step % GRAN == 0) {
-              if (!mbar_wait(pempty(b), ((g / C::kNP) & 1) ^ 1, a.wait_limit)) {
-                on_timeout();
-                ok = false;
-                break;
-              }
-              tc_fence_after();
-            }
-            umma_bf16(tmem_base + b * BN, sdesc(st + k * 32), sdesc(st + NSX * C::kABytes + k * 32),
-                      idesc, step % GRAN != 0);
-            if (step % GRAN == GRAN - 1 || step == nsteps - 1) {
-              umma_commit(pfull(b));
-              ++g;
-            }
-            if (step == 0) {
-              if (!mbar_wait(cempty, (t & 1) ^ 1, a.wait_limit)) {
-                on_timeout();
-                ok = false;
-                break;
-              }
-              tc_fence_after();
-            }
-#pragma unroll
-            for (int pr = 0; pr < NCORR; ++pr) {
-              int ia, ib;
-              corr_product(NSX, pr, ia, ib);
-              const uint64_t ad = sdesc(st + ia * C::kABytes + k * 32);
-              const uint64_t bd = sdesc(st + NSX * C::kABytes + ib * C::kBBytes + k * 32);
-              umma_bf16(tmem_corr, ad, bd, idesc, (step | pr) != 0);
-            }
-          }
+          const uint64_t d0 = dbase + (uint64_t)((s * C::kStageBytes) >> 4);
+          const uint32_t P = tmem_base + b * BN;
+          if (kb == a.nkb - 1 && a.last_k16 == 1)
+            mma_kblock<NSX, 1>(P, tmem_corr, d0, idesc, first, pfull(b));
+          else if (first)
+            mma_kblock<NSX, 2, true>(P, tmem_corr, d0, idesc, true, pfull(b));
+          else
+            mma_kblock<NSX, 2, false>(P, tmem_corr, d0, idesc, false, pfull(b));
           umma_commit(empty(s));
           if (++s == NS) s = 0, ph ^= 1;
+          if (++b == C::kNP) b = 0, pph ^= 1;
         }
         if (ok) umma_commit(cfull);
       }
@@ -502,8 +526,8 @@ __global__ void __maxnreg__(96)
             (tile_steps(kblocks(a, gi, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
         for (int pi = 0; pi < nparts; ++pi, ++g) {
           const int b = g % C::kNP;
-          const bool got = mbar_wait(pfull(b), (g / C::kNP) & 1, a.wait_limit);
-          __syncwarp();
+          // warp-uniform outcome: the TMEM loads below are warp-collective
+          const bool got = __all_sync(0xffffffffu, mbar_wait(pfull(b), (g / C::kNP) & 1, a.wait_limit));
           if (!got) {
             on_timeout();
             ok = false;
@@ -521,11 +545,11 @@ __global__ void __maxnreg__(96)
                                                        __uint_as_float(r[2 * j + 1])));
           }
           tc_fence_before();
-          mbar_arrive(pempty(b));
+          __syncwarp();
+          if (lane == 0) mbar_arrive(pempty(b));
         }
         if (!ok) break;
-        const bool got = mbar_wait(cfull, t & 1, a.wait_limit);
-        __syncwarp();
+        const bool got = __all_sync(0xffffffffu, mbar_wait(cfull, t & 1, a.wait_limit));
         if (!got) {
           on_timeout();
           ok = false;
@@ -543,7 +567,8 @@ __global__ void __maxnreg__(96)
                                                      __uint_as_float(r[2 * j + 1])));
         }
         tc_fence_before();
-        mbar_arrive(cempty);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(cempty);
         if (FINAL) {
           const int n0 = (tile % a.n_ntiles) * BN + col0;
           const float *sc = a.scale + (size_t)gi * a.N;
