@@ -176,7 +176,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 
 // Shared-memory matrix descriptor of a K-major tile written by TMA with the
 // 64-byte swizzle: rows of 32 bf16 (64 bytes), 8-row swizzle atoms stacked
-// at SBO = 512 bytes.
+// at SBO = 512 bytes.  (K blocks of 64 with 128-byte rows halve the TMA boxes
+// per byte but make the band blocks coarser; measured, the two are within a
+// few percent and 32 is ahead.)
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
@@ -221,6 +223,20 @@ __device__ __forceinline__ void split_lead_f64(double v, double m, __nv_bfloat16
   }
 }
 
+// BF16 pair <-> FP32 pair by bit moves (integer pipe).  The epilogue keeps
+// its FP32 arithmetic packed (FP32x2) and its conversions off the FP32 FMA
+// pipe: dense scalar FP32 work on the MMA issuer's scheduler delays the
+// issue of tcgen05.mma.
+__device__ __forceinline__ float2 bf16x2_to_f32x2(__nv_bfloat162 h) {
+  const uint32_t u = *reinterpret_cast<const uint32_t *>(&h);
+  return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+}
+// exact when both values are representable in BF16 (the low 16 bits are zero)
+__device__ __forceinline__ __nv_bfloat162 f32x2_to_bf16x2_exact(float2 v) {
+  const uint32_t u = __byte_perm(__float_as_uint(v.x), __float_as_uint(v.y), 0x7632);
+  return *reinterpret_cast<const __nv_bfloat162 *>(&u);
+}
+
 // The same split for two values sharing one run maximum m, on packed FP32x2
 // arithmetic; part s of (v.x, v.y) lands in o[s] as a BF16 pair.
 template <int NS>
@@ -229,7 +245,7 @@ __device__ __forceinline__ void split_pair_f32(float2 v, float m, __nv_bfloat162
   float2 l;
   if (NS == 2) {
     o[0] = __floats2bfloat162_rn(v.x, v.y);
-    l = __bfloat1622float2(o[0]);
+    l = bf16x2_to_f32x2(o[0]);
   } else {
     const uint32_t mb = __float_as_uint(m);
     const int E = (int)((mb >> 23) & 0xff) - 127 + ((mb & 0x7fffff) != 0);
@@ -241,13 +257,13 @@ __device__ __forceinline__ void split_pair_f32(float2 v, float m, __nv_bfloat162
       const float2 t = __fmul2_rn(v, make_float2(up, up));
       l = __fmul2_rn(make_float2(rintf(t.x), rintf(t.y)), make_float2(down, down));
     }
-    o[0] = __floats2bfloat162_rn(l.x, l.y);
+    o[0] = f32x2_to_bf16x2_exact(l);  // an 8-bit integer times a power of two
   }
   float2 r = __ffma2_rn(l, neg1, v);  // v - lead, exact
 #pragma unroll
   for (int s = 1; s < NS; ++s) {
     o[s] = __floats2bfloat162_rn(r.x, r.y);
-    r = __ffma2_rn(__bfloat1622float2(o[s]), neg1, r);
+    r = __ffma2_rn(bf16x2_to_f32x2(o[s]), neg1, r);
   }
 }
 
@@ -321,12 +337,13 @@ __device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
   return a.nrb ? (mt / a.nrb) * a.d0 + (mt % a.nrb) * BM : mt * BM;
 }
 
-// The MMAs of one K block (one 32-run): the main product (part 0 x part 0)
-// into the fresh partial P, committed to `pfull` as soon as it is issued,
-// and the correction products into the accumulator Cc.  NK K=16 steps;
-// FIRST: the tile's first K block (the correction accumulator starts).
+// The MMAs of one 32-run of K (d0: the run's first K column in the stage):
+// the main product (part 0 x part 0) into the fresh partial P, committed to
+// `pfull` as soon as it is issued, and the correction products into the
+// accumulator Cc.  NK K=16 steps; FIRST: the tile's first run (the
+// correction accumulator starts).
 template <int NSX, int NK, bool FIRST = false>
-__device__ __forceinline__ void mma_kblock(uint32_t P, uint32_t Cc, uint64_t d0, uint32_t idesc,
+__device__ __forceinline__ void mma_run(uint32_t P, uint32_t Cc, uint64_t d0, uint32_t idesc,
                                            bool first, uint32_t pfull_bar) {
   constexpr int kABytes = BM * BK * 2, kBBytes = BN * BK * 2;  // one part of a tile
   constexpr int NCORR = NSX == 2 ? 2 : 5;
@@ -479,7 +496,6 @@ __global__ void __maxnreg__(96)
         for (int kb = rc.x; kb <= rc.y; ++kb) {
           const bool first = kb == rc.x;
           if (!mbar_wait(full(s), ph, a.wait_limit) ||
-              !mbar_wait(pempty(b), pph ^ 1, a.wait_limit) ||
               (first && !mbar_wait(cempty, (t & 1) ^ 1, a.wait_limit))) {
             on_timeout();
             ok = false;
@@ -487,16 +503,30 @@ __global__ void __maxnreg__(96)
           }
           tc_fence_after();
           const uint64_t d0 = dbase + (uint64_t)((s * C::kStageBytes) >> 4);
-          const uint32_t P = tmem_base + b * BN;
-          if (kb == a.nkb - 1 && a.last_k16 == 1)
-            mma_kblock<NSX, 1>(P, tmem_corr, d0, idesc, first, pfull(b));
-          else if (first)
-            mma_kblock<NSX, 2, true>(P, tmem_corr, d0, idesc, true, pfull(b));
-          else
-            mma_kblock<NSX, 2, false>(P, tmem_corr, d0, idesc, false, pfull(b));
+          const int nk16 = (kb == a.nkb - 1) ? a.last_k16 : BK / 16;
+#pragma unroll
+          for (int rr = 0; rr < BK / kGroup; ++rr) {
+            const int nk = min(nk16 - rr * GRAN, GRAN);  // K=16 steps of this run
+            if (nk <= 0) break;
+            if (!mbar_wait(pempty(b), pph ^ 1, a.wait_limit)) {
+              on_timeout();
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint64_t dr = d0 + (uint64_t)((rr * kGroup * 2) >> 4);
+            const uint32_t P = tmem_base + b * BN;
+            if (nk == 1)
+              mma_run<NSX, 1>(P, tmem_corr, dr, idesc, first && rr == 0, pfull(b));
+            else if (first && rr == 0)
+              mma_run<NSX, 2, true>(P, tmem_corr, dr, idesc, true, pfull(b));
+            else
+              mma_run<NSX, 2, false>(P, tmem_corr, dr, idesc, false, pfull(b));
+            if (++b == C::kNP) b = 0, pph ^= 1;
+          }
+          if (!ok) break;
           umma_commit(empty(s));
           if (++s == NS) s = 0, ph ^= 1;
-          if (++b == C::kNP) b = 0, pph ^= 1;
         }
         if (ok) umma_commit(cfull);
       }
@@ -576,8 +606,9 @@ __global__ void __maxnreg__(96)
 #pragma unroll
           for (int j = 0; j < CW / 2; ++j) {
             const int n = n0 + 2 * j;
-            const float2 f = make_float2(n < a.N ? wg * sc[n] : 0.0f,
-                                         n + 1 < a.N ? wg * sc[n + 1] : 0.0f);
+            const float2 f = __fmul2_rn(make_float2(wg, wg),
+                                        make_float2(n < a.N ? sc[n] : 0.0f,
+                                                    n + 1 < a.N ? sc[n + 1] : 0.0f));
             accg[j] = __ffma2_rn(f, acc[j], accg[j]);
           }
         }
@@ -627,9 +658,9 @@ __global__ void __maxnreg__(96)
             float m = 0.0f;
             if (NSX > 2) {
               const float m0 =
-                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v.x))));
+                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(v.x) & 0x7fffffffu));
               const float m1 =
-                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v.y))));
+                  __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(v.y) & 0x7fffffffu));
               m = odd ? m1 : m0;
             }
             const float recv = __shfl_xor_sync(0xffffffffu, odd ? v.x : v.y, 1);
