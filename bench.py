@@ -174,14 +174,15 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def profiled_traffic(kernel: str, workload: str):
+def profiled_traffic(kernel: str, workload: str, precision: str | None = None):
     """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
     if not os.path.exists(path):
         return None
     for ln in open(path):
         kv = dict(x.split("=", 1) for x in ln.split() if "=" in x)
-        if kv.get("kernel") == kernel and kv.get("workload") == workload:
+        if (kv.get("kernel") == kernel and kv.get("workload") == workload
+                and (precision is None or kv.get("precision", precision) == precision)):
             try:
                 return float(kv["traffic_bytes_per_launch"])
             except (KeyError, ValueError):
@@ -364,7 +365,7 @@ def run_gpu(args, world, rank, local):
     else:
         peak, peak_src = pk["bf16_tflops_sustained"], f"{src} bf16_tflops_sustained"
         kname = "stage_bf16_kernel"
-    traffic = profiled_traffic(kname, f"coulomb_cube_{n}")
+    traffic = profiled_traffic(kname, f"coulomb_cube_{n}", None if prec == "fp64" else prec)
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": traffic, "kernel": kname,
             "peak_source": peak_src,
