@@ -409,6 +409,29 @@ def translate(lmax, q, frm, to) -> np.ndarray:
     return x
 
 
+def translation_dense(lmax, d) -> np.ndarray:
+    """The translation matrix W(d) as a dense lower-triangular matrix with
+    unit diagonal (dtpmv('L', *, 'U') semantics of TranslationMatrix)."""
+    N = (lmax + 1) ** 2
+    Wp = translation_matrix(lmax, d)
+    W = np.eye(N)
+    k = 0
+    for j in range(N):  # packed by columns
+        k += 1  # the (unit) diagonal element
+        for i in range(j + 1, N):
+            W[i, j] = Wp[k]
+            k += 1
+    return W
+
+
+def translate_local(lmax, L, child, parent) -> np.ndarray:
+    """L2L of GBFMMCoulomb3D_translate_potential (gbfmm_coulomb3d.F90:1565-1621):
+    the transposed translation matrix of the displacement child - parent
+    applied to the parent's local expansion."""
+    W = translation_dense(lmax, np.asarray(child, float) - np.asarray(parent, float))
+    return W.T @ _f64(L)
+
+
 _IP = ctypes.POINTER(ctypes.c_int)
 
 
@@ -557,6 +580,33 @@ class GBFMMPlan:
                 c[d] = 0.5 * (a.points[p0] + a.points[p1 - 1])
         return c
 
+    def cells_at(self, ibox, level):
+        """Cells (1-based first, last) per axis of box `ibox` of a coarser
+        `level` (2 <= level <= maxlevel): the union of its descendants at
+        the finest level, so that the levels nest also when the finest split
+        is uneven (for evenly divisible grids this is the reference's split
+        at that level)."""
+        v = box_vector(ibox, level)
+        f = 2 ** (self.level - level)
+        return [(self._axis_cells(d, v[d] * f)[0], self._axis_cells(d, v[d] * f + f - 1)[1])
+                for d in range(3)]
+
+    def center_at(self, ibox, level):
+        """Expansion centre of a box of any level (as `center` at maxlevel)."""
+        if level == self.level:
+            return self.center(ibox)
+        v = box_vector(ibox, level)
+        nbl = 2 ** level
+        c = np.zeros(3)
+        for d, (c0, c1) in enumerate(self.cells_at(ibox, level)):
+            a = self.grid.axes[d]
+            if a.ncell % self.nb == 0:  # gbfmm_parallel_info.F90:1290-1299
+                c[d] = self.ranges[d][0] + (v[d] + 0.5) * ((self.ranges[d][1] - self.ranges[d][0]) / nbl)
+            else:
+                p0, p1 = (c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1)
+                c[d] = 0.5 * (a.points[p0] + a.points[p1])
+        return c
+
     def points(self, ibox):
         """0-based point index range [p0, p1) per axis of the box's sub-grid."""
         return [((c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1) + 1)
@@ -567,6 +617,39 @@ class GBFMMPlan:
         for (c0, c1), a, (p0, p1) in zip(self.cells(ibox), self.grid.axes, self.points(ibox)):
             out.append((p0, p1 if c1 == a.ncell else p1 - 1))
         return out
+
+
+def _far_field_levels(plan, q_fine, lmax):
+    """Local expansions at the finest level of a multi-level GBFMM
+    (gbfmm_coulomb3d.F90:650-905): upward pass q(parent) += W(c_child -
+    c_parent) q(child) (translate_multipoles, :1502-1562) from maxlevel - 1
+    down to level 2; M2L over the local far field at level 2; then for each
+    finer level the parent's local expansion translated down (L2L,
+    translate_potential, :1565-1621) plus that level's own local far field."""
+    N = (lmax + 1) ** 2
+    top = plan.level
+    q = {top: q_fine}
+    for lev in range(top - 1, 1, -1):
+        nb = 8 ** lev
+        ql = np.zeros((N, nb))
+        for p in range(1, nb + 1):
+            cp = plan.center_at(p, lev)
+            for c in range((p - 1) * 8 + 1, p * 8 + 1):
+                ql[:, p - 1] += translate(lmax, q[lev + 1][:, c - 1], plan.center_at(c, lev + 1), cp)
+        q[lev] = ql
+    Lprev = None
+    for lev in range(2, top + 1):
+        nb = 8 ** lev
+        Ll = np.zeros((N, nb))
+        for i in range(1, nb + 1):
+            ci = plan.center_at(i, lev)
+            if Lprev is not None:
+                par = (i - 1) // 8 + 1
+                Ll[:, i - 1] += translate_local(lmax, Lprev[:, par - 1], ci, plan.center_at(par, lev - 1))
+            for j in local_farfield(i, lev):
+                Ll[:, i - 1] += interaction_matrix(lmax, plan.center_at(j, lev) - ci) @ q[lev][:, j - 1]
+        Lprev = Ll
+    return Lprev
 
 
 def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
@@ -592,14 +675,19 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
                 subs[2].points, subs[2].weights(), rho[x0:x1, y0:y1, z0:z1], plan.center(b))
         q[:, b - 1] = (helm_box_multipoles(lmax, kappa, *args) if helm
                        else box_multipoles(lmax, *args))
-    L = np.zeros((N, plan.nbox))
-    for i in range(1, plan.nbox + 1):
-        ci = plan.center(i)
-        for j in local_farfield(i, maxlevel):
-            if helm:
-                L[:, i - 1] += helm_m2l(lmax, kappa, q[:, j - 1], plan.center(j), ci)
-            else:
-                L[:, i - 1] += interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
+    if maxlevel > 2:
+        if helm:
+            raise ValueError("multi-level GBFMM is restated for the Coulomb kernel only")
+        L = _far_field_levels(plan, q, lmax)
+    else:
+        L = np.zeros((N, plan.nbox))
+        for i in range(1, plan.nbox + 1):
+            ci = plan.center(i)
+            for j in local_farfield(i, maxlevel):
+                if helm:
+                    L[:, i - 1] += helm_m2l(lmax, kappa, q[:, j - 1], plan.center(j), ci)
+                else:
+                    L[:, i - 1] += interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
     tp, tw = gauss_quad(*quad)
     w = helmholtz_weights(tp, tw, energy) if helm else coulomb_weights(tw)
     V = np.zeros(grid.shape, order="F")

@@ -99,3 +99,85 @@ def test_gbfmm_matches_direct_operator(oracle):
     E = oracle.integrate_cube(g, rho * V)
     Ed = oracle.integrate_cube(g, rho * Vd)
     assert abs(E - Ed) / abs(Ed) < 1e-3
+
+
+def test_translation_round_trip_and_l2l_adjoint(oracle):
+    """M2M followed by the opposite translation is the identity (exact
+    translation of regular solid harmonics), and L2L is the adjoint of M2M:
+    L . (W q) = (W^T L) . q."""
+    lmax = 6
+    rng = np.random.default_rng(4)
+    q = rng.standard_normal((lmax + 1) ** 2)
+    a, b = np.array([0.3, -0.2, 0.5]), np.array([-0.4, 0.1, 0.2])
+    back = oracle.translate(lmax, oracle.translate(lmax, q, a, b), b, a)
+    assert np.abs(back - q).max() <= 1e-12 * np.abs(q).max()
+    Lv = rng.standard_normal(q.size)
+    lhs = Lv @ oracle.translate(lmax, q, a, b)
+    rhs = oracle.translate_local(lmax, Lv, a, b) @ q
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_multilevel_plan_nests(oracle):
+    """Coarser boxes are the unions of their children (also for uneven
+    finest splits), and evenly divisible grids keep the reference centres."""
+    for ncell in (16, 18):
+        g = oracle.Grid3D.cube(-0.5 * ncell * 6 * 0.2, ncell, 0.2)
+        plan = oracle.GBFMMPlan(g, 3)
+        for p in range(1, 65):
+            cp = plan.cells_at(p, 2)
+            kids = [plan.cells_at(c, 3) for c in range((p - 1) * 8 + 1, p * 8 + 1)]
+            for d in range(3):
+                assert cp[d][0] == min(k[d][0] for k in kids)
+                assert cp[d][1] == max(k[d][1] for k in kids)
+        if ncell == 16:
+            p2 = oracle.GBFMMPlan(g, 2)
+            for p in range(1, 65):
+                assert np.allclose(plan.center_at(p, 2), p2.center(p), rtol=0, atol=1e-14)
+
+
+def test_multilevel_gbfmm_matches_direct_operator(oracle):
+    """Three levels (8^3 finest boxes, M2M/M2L/L2L) against the single-box
+    operator: the same agreement as two levels (the difference is dominated
+    by the direct operator's quadrature, not by the multipoles)."""
+    g = oracle.Grid3D.cube(-9.6, 16, 0.2)
+    rng = np.random.default_rng(2)
+    q = rng.uniform(-1, 2, 6)
+    a = rng.uniform(0.8, 6, 6)
+    c = rng.uniform(-7, 7, (6, 3))
+    rho = oracle.gauss_cube(g, q, a, c)
+    quad = (12, 12, 0.0, 2.0, 1e3)
+    V3 = oracle.gbfmm_apply(g, rho, lmax=8, maxlevel=3, quad=quad)
+    Vd = oracle.coulomb_apply(g, rho, quad=quad, coda=False)
+    assert np.abs(V3 - Vd).max() / np.abs(Vd).max() < 5e-3
+
+
+def test_multilevel_far_field_equals_flat_interaction_list(oracle):
+    """The far field of the finest boxes through M2M -> M2L per level -> L2L
+    equals one flat M2L from every non-neighbouring finest box, up to the
+    multipole truncation (checked on the potential at the owned points)."""
+    g = oracle.Grid3D.cube(-9.6, 16, 0.2)
+    rng = np.random.default_rng(5)
+    rho = oracle.gauss_cube(g, rng.uniform(-1, 2, 5), rng.uniform(0.8, 6, 5),
+                            rng.uniform(-7, 7, (5, 3)))
+    lmax = 10
+    plan = oracle.GBFMMPlan(g, 3)
+    _, q, L, _ = oracle.gbfmm_apply(g, rho, lmax=lmax, maxlevel=3, quad=(4, 4, 0.0, 2.0, 1e3),
+                                    return_parts=True)
+    worst = 0.0
+    for i in rng.choice(np.arange(1, plan.nbox + 1), 12, replace=False):
+        ci = plan.center(int(i))
+        vi = np.array(plan.vec[int(i) - 1])
+        near = {j for j in range(1, plan.nbox + 1)
+                if np.abs(np.array(plan.vec[j - 1]) - vi).max() <= 1}
+        Lf = np.zeros(q.shape[0])
+        for j in range(1, plan.nbox + 1):
+            if j not in near:
+                Lf += oracle.interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
+        own = plan.owned(int(i))
+        outs = [g.axes[d].points[own[d][0]:own[d][1]] for d in range(3)]
+        a = np.zeros(tuple(len(o) for o in outs), order="F")
+        b = np.zeros_like(a)
+        oracle.l2p(lmax, L[:, int(i) - 1], ci, *outs, a)
+        oracle.l2p(lmax, Lf, ci, *outs, b)
+        worst = max(worst, np.abs(a - b).max() / np.abs(b).max())
+    assert worst < 5e-5, worst  # truncation: 2.9e-4, 1.6e-5, 2.7e-7 at lmax 6, 10, 14
