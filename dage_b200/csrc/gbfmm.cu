@@ -115,6 +115,13 @@ struct GInst {
   const int *ffstart, *ffsrc, *ffdisp;  // plan: far-field lists
   const double *wx, *wy, *wz;           // plan: full-grid integration weights
   double kappa;  // 0: Coulomb; > 0: Helmholtz kernel e^(-kappa r)/r
+  // levels: q and L hold every box of levels 2..maxlevel (level 2 first);
+  // the finest level starts at box fine_off.  M2M/L2L: translation matrix
+  // (packed lower triangle) of box g's displacement from its parent,
+  // Wm2m + m2m_disp[g - m2m_base] * Wsize, for boxes of levels >= 3
+  int fine_off, m2m_base;
+  const double *Wm2m;
+  const int *m2m_disp;
 };
 
 constexpr int kEnergyBlocks = 256;
@@ -401,7 +408,7 @@ __global__ void reduce_slabs_kernel(const GInst *__restrict__ insts, int nslab, 
   const int b = idx / N, s = idx % N;
   double acc = 0.0;
   for (int k = 0; k < nslab; ++k) acc += I.partial[((size_t)b * nslab + k) * N + s];
-  I.q[(size_t)b * N + s] = acc;
+  I.q[(size_t)(I.fine_off + b) * N + s] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -495,6 +502,70 @@ __global__ void m2l_apply_kernel(const GInst *__restrict__ insts, int N) {
   if (i < N) I.L[(size_t)b * N + i] = acc;
 }
 
+// Translation matrices W(d) of the distinct child-to-parent displacements
+// (TranslationMatrix_eval, multipole.F90:443-476): packed lower triangle,
+// column by column, W[r] = c1[r] S[lm1[r]] + c2[r] S[lm2[r]] (absent: -1).
+__global__ void translation_matrices_kernel(const double *__restrict__ disp, int lmax,
+                                            const double *__restrict__ c1,
+                                            const double *__restrict__ c2,
+                                            const int *__restrict__ lm1,
+                                            const int *__restrict__ lm2, int M, double *Wall) {
+  extern __shared__ double S[];
+  const double *d = disp + 3 * blockIdx.x;
+  if (threadIdx.x == 0) solid_harmonics(lmax, d[0], d[1], d[2], [&](int lm, double v) { S[lm] = v; });
+  __syncthreads();
+  double *W = Wall + (size_t)blockIdx.x * M;
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double w = 0.0;
+    if (lm1[r] >= 0) w = c1[r] * S[lm1[r]];
+    if (lm2[r] >= 0) w = w + c2[r] * S[lm2[r]];
+    W[r] = w;
+  }
+}
+
+// packed (column-major lower) position of W(i, j), i >= j
+__device__ __forceinline__ size_t wpos(int i, int j, int N) {
+  return (size_t)j * N - (size_t)j * (j - 1) / 2 + (i - j);
+}
+
+// Upward pass, one level: q(parent) = sum over the 8 children c of
+// W(c_c - c_parent) q(c), W applied with a unit diagonal (dtpmv 'L','N','U',
+// gbfmm_coulomb3d.F90:1502-1562).  Block (parent, density); parents of this
+// level start at box `poff`, their children at `coff` (children of parent p
+// are coff + 8 p .. +7).
+__global__ void m2m_kernel(const GInst *__restrict__ insts, int N, int poff, int coff) {
+  const GInst &I = insts[blockIdx.y];
+  const int p = blockIdx.x;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double acc = 0.0;
+    for (int c = 0; c < 8; ++c) {
+      const int gc = coff + 8 * p + c;
+      const double *qc = I.q + (size_t)gc * N;
+      const double *W = I.Wm2m + (size_t)I.m2m_disp[gc - I.m2m_base] * ((size_t)N * (N + 1) / 2);
+      double t = qc[i];
+      for (int j = 0; j < i; ++j) t += W[wpos(i, j, N)] * qc[j];
+      acc += t;
+    }
+    I.q[(size_t)(poff + p) * N + i] = acc;
+  }
+}
+
+// Downward pass, one level: L(child) += W(c_child - c_parent)^T L(parent)
+// with a unit diagonal (translate_potential, gbfmm_coulomb3d.F90:1565-1621).
+// Block (child, density); children of this level start at box `coff`,
+// their parents at `poff`.
+__global__ void l2l_kernel(const GInst *__restrict__ insts, int N, int poff, int coff) {
+  const GInst &I = insts[blockIdx.y];
+  const int c = blockIdx.x, gc = coff + c;
+  const double *Lp = I.L + (size_t)(poff + c / 8) * N;
+  const double *W = I.Wm2m + (size_t)I.m2m_disp[gc - I.m2m_base] * ((size_t)N * (N + 1) / 2);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double t = Lp[i];
+    for (int j = i + 1; j < N; ++j) t += W[wpos(j, i, N)] * Lp[j];
+    I.L[(size_t)gc * N + i] += t;
+  }
+}
+
 // V(r) += sum_lm L_lm S_lm(r - c) over the owned points of every box; block
 // (chunk, box, density).  L = the density's own local expansions unless
 // Lext is given (evaluation of caller-supplied expansions).
@@ -505,7 +576,7 @@ __global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__rest
   if (I.kappa > 0.0) return;  // Helmholtz instances: l2p_helm_kernel
   const int N = (lmax + 1) * (lmax + 1);
   const BoxInfo b = I.boxes[blockIdx.y];
-  const double *L = Lext ? Lext : I.L;
+  const double *L = Lext ? Lext : I.L + (size_t)I.fine_off * N;
   for (int k = threadIdx.x; k < N; k += blockDim.x) Ls[k] = L[(size_t)blockIdx.y * N + k];
   __syncthreads();
   const double *xs = I.wbox + (3 * 64) * I.wstride;
@@ -539,7 +610,7 @@ __global__ void __launch_bounds__(256)
   const int PP = 32 / L1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const BoxInfo b = I.boxes[blockIdx.y];
-  const double *Lb = (Lext ? Lext : I.L) + (size_t)blockIdx.y * N;
+  const double *Lb = (Lext ? Lext : I.L + (size_t)I.fine_off * N) + (size_t)blockIdx.y * N;
   const double kappa = I.kappa;
   for (int e = threadIdx.x; e < N; e += blockDim.x) {
     const int t = e / L1, k = e % L1;
@@ -719,6 +790,57 @@ void m2l_tables(int lmax, M2LTables &t) {
   }
 }
 
+// Host-side translation (M2M/L2L) coefficient tables
+// (TranslationMatrix_compute_coeffs, multipole.F90:372-440): entry r of the
+// packed lower triangle (column s = (j,k), row i = (l,m) >= s) is
+// c1 S_{l-j, m1} + c2 S_{l-j, m2} of the displacement's regular solid
+// harmonics; a term whose order |m1| or |m2| exceeds l - j is absent.
+struct TransTables {
+  std::vector<double> c1, c2;
+  std::vector<int> lm1, lm2;
+};
+
+void translation_tables(int lmax, TransTables &t) {
+  const int N = (lmax + 1) * (lmax + 1);
+  auto lm_of = [](int s, int &l, int &m) {
+    l = 0;
+    while ((l + 1) * (l + 1) <= s) ++l;
+    m = s - l * l - l;
+  };
+  for (int s = 0; s < N; ++s) {
+    int j, k;
+    lm_of(s, j, k);
+    const double hk = k == 0 ? 0.5 : 1.0;  // the reference's ij(delta(0,k))
+    for (int i = s; i < N; ++i) {
+      int l, m;
+      lm_of(i, l, m);
+      const int Lo = l - j;
+      double a = 0.0, b = 0.0;
+      int ma = 0, mb = 0;
+      bool ha = false, hb = false;
+      const int dm = std::abs(m - k), sm = std::abs(m + k);
+      if (m >= 0 && k >= 0) {
+        if (Lo >= 0 && dm <= Lo) ha = true, ma = dm, a = Ccf(Lo, m - k) * hk;
+        if (Lo >= 0 && sm <= Lo) hb = true, mb = sm, b = sg(k) * Ccf(Lo, m + k) * hk;
+      } else if (m >= 0) {  // k < 0
+        if (Lo >= 0 && dm <= Lo) ha = true, ma = -dm, a = Csf(Lo, m - k) * sg(k);
+        if (Lo >= 0 && sm <= Lo) hb = true, mb = -sm, b = -Csf(Lo, m + k);
+      } else if (k >= 0) {  // m < 0
+        if (Lo >= 0 && dm <= Lo) ha = true, ma = -dm, a = -Csf(Lo, m - k) * sg(m) * hk;
+        if (Lo >= 0 && sm <= Lo) hb = true, mb = -sm, b = -Csf(Lo, m + k) * hk * sg(m + k);
+      } else {
+        if (Lo >= 0 && dm <= Lo) ha = true, ma = dm, a = Ccf(Lo, m - k) * sg(m - k);
+        if (Lo >= 0 && sm <= Lo) hb = true, mb = sm, b = -Ccf(Lo, m + k) * sg(m);
+      }
+      const double scale = Df(l, m) * sg(m - k) / Df(j, k);
+      t.c1.push_back(a * scale);
+      t.c2.push_back(b * scale);
+      t.lm1.push_back(ha ? Lo * (Lo + 1) + ma : -1);
+      t.lm2.push_back(hb ? Lo * (Lo + 1) + mb : -1);
+    }
+  }
+}
+
 // octree box index <-> vector (gbfmm_parallel_info.F90:1128-1194)
 void box_vector(int ibox, int level, int v[3]) {
   int vv[3] = {0, 0, 0}, rem;
@@ -798,6 +920,13 @@ struct dage_gbfmm {
   std::vector<DevBuf> Tnear[3];
   std::vector<DevBuf> band_near[3];  // K band per (t-point, 128-row tile) of Tnear
   DevBuf d_boxes, d_wbox, d_q, d_L, d_partial, d_Tm2l, d_ffstart, d_ffsrc, d_ffdisp;
+  // levels 2..level: box offsets (lev_off[l], l = 2..level+1), expansion
+  // centres of every box, M2M/L2L translation matrices per distinct
+  // child-to-parent displacement
+  std::vector<int> lev_off;
+  int nbtot = 0, fine_off = 0, nm2m = 0;
+  std::vector<double> centers;
+  DevBuf d_Wm2m, d_m2m_disp;
   int wstride = 0, nslab = 16, ndisp = 0;
   DevBuf d_U, d_W, d_desc[3];
   size_t U_per_box = 0, W_per_box = 0;
@@ -1019,9 +1148,9 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
                       const dage_quad *quad) {
   DAGE_TRY(sh_tables_init());
   if (!grid || !quad) return fail(DAGE_E_INVALID, "null argument");
-  // one octree level: the local far field of a level-2 box covers every box
-  // outside its neighbourhood; deeper levels need M2M/L2L between levels
-  if (maxlevel != 2) return fail(DAGE_E_UNSUPPORTED, "maxlevel must be 2 (4x4x4 boxes)");
+  // levels 2..maxlevel: M2L at every level (the local far field of a level-2
+  // box is every box outside its neighbourhood), M2M/L2L between levels
+  if (maxlevel < 2 || maxlevel > 5) return fail(DAGE_E_UNSUPPORTED, "maxlevel must be 2..5");
   if (lmax < 0 || lmax > kMaxLmax) return fail(DAGE_E_UNSUPPORTED, "lmax must be 0..%d", kMaxLmax);
   g->level = maxlevel;
   g->lmax = lmax;
@@ -1112,38 +1241,141 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_wbox.ptr, wbox.data(), sizeof(double) * wbox.size(),
                                 cudaMemcpyHostToDevice, s));
 
-  // --- far-field lists grouped by displacement -------------------------------
-  // displacements keyed by integer box-vector differences on a regular box
-  // lattice (all axes divide evenly), else by the exact centre differences
+  // --- levels: box offsets and expansion centres ------------------------------
+  // A box of a coarser level is the union of its descendants at the finest
+  // level (so the levels nest also for uneven splits); centres follow the
+  // reference on evenly divisible axes, else the midpoint of the box's points.
+  g->lev_off.assign(maxlevel + 2, 0);
+  for (int l = 2; l <= maxlevel; ++l) g->lev_off[l + 1] = g->lev_off[l] + (1 << (3 * l));
+  g->nbtot = g->lev_off[maxlevel + 1];
+  g->fine_off = g->lev_off[maxlevel];
+  g->centers.assign(3 * (size_t)g->nbtot, 0.0);
+  for (int l = 2; l <= maxlevel; ++l) {
+    const int nbl = 1 << l, f = 1 << (maxlevel - l);
+    for (int i = 1; i <= (1 << (3 * l)); ++i) {
+      int v[3];
+      box_vector(i, l, v);
+      double *c = &g->centers[3 * (size_t)(g->lev_off[l] + i - 1)];
+      for (int d = 0; d < 3; ++d) {
+        const Axis &a = g->ax[d];
+        if (l == maxlevel) {
+          c[d] = g->boxes[box_index(v, l) - 1].c[d];
+        } else if (a.ncell % nb == 0) {
+          const double qmin = a.points.front(), qmax = a.points.back();
+          c[d] = qmin + (v[d] + 0.5) * ((qmax - qmin) / (nbl + 0.0));
+        } else {
+          const int first = pos_p0[d][v[d] * f];
+          const int last = pos_p0[d][v[d] * f + f - 1] + pos_np[d][v[d] * f + f - 1] - 1;
+          c[d] = 0.5 * (a.points[first] + a.points[last]);
+        }
+      }
+    }
+  }
+
+  // --- far-field lists of every level, grouped by displacement ----------------
+  // displacements keyed by (level, integer box-vector difference) on a regular
+  // box lattice (all axes divide evenly), else by the exact centre differences
   bool regular = true;
   for (int d = 0; d < 3; ++d) regular = regular && (g->ax[d].ncell % nb == 0);
   std::map<std::vector<long long>, int> disp_index;
   std::vector<double> &disp = g->disp;
   std::vector<int> ffstart(1, 0), ffsrc, ffdisp;
-  for (int b = 1; b <= g->nbox; ++b) {
-    for (int j : local_farfield(b, maxlevel)) {
-      double dv[3];
-      std::vector<long long> key(3);
-      for (int d = 0; d < 3; ++d) {
-        dv[d] = g->boxes[j - 1].c[d] - g->boxes[b - 1].c[d];
-        if (regular)
-          key[d] = g->boxes[j - 1].pos[d] - g->boxes[b - 1].pos[d];
-        else
-          std::memcpy(&key[d], &dv[d], 8);
+  for (int l = 2; l <= maxlevel; ++l)
+    for (int b = 1; b <= (1 << (3 * l)); ++b) {
+      int vb[3];
+      box_vector(b, l, vb);
+      const double *cb = &g->centers[3 * (size_t)(g->lev_off[l] + b - 1)];
+      for (int j : local_farfield(b, l)) {
+        int vj[3];
+        box_vector(j, l, vj);
+        const double *cj = &g->centers[3 * (size_t)(g->lev_off[l] + j - 1)];
+        double dv[3];
+        std::vector<long long> key(4);
+        key[3] = regular ? l : 0;
+        for (int d = 0; d < 3; ++d) {
+          dv[d] = cj[d] - cb[d];
+          if (regular)
+            key[d] = vj[d] - vb[d];
+          else
+            std::memcpy(&key[d], &dv[d], 8);
+        }
+        auto it = disp_index.find(key);
+        int di;
+        if (it == disp_index.end()) {
+          di = (int)disp_index.size();
+          disp_index[key] = di;
+          disp.insert(disp.end(), dv, dv + 3);
+        } else {
+          di = it->second;
+        }
+        ffsrc.push_back(g->lev_off[l] + j - 1);
+        ffdisp.push_back(di);
       }
-      auto it = disp_index.find(key);
-      int di;
-      if (it == disp_index.end()) {
-        di = (int)disp_index.size();
-        disp_index[key] = di;
-        disp.insert(disp.end(), dv, dv + 3);
-      } else {
-        di = it->second;
-      }
-      ffsrc.push_back(j - 1);
-      ffdisp.push_back(di);
+      ffstart.push_back((int)ffsrc.size());
     }
-    ffstart.push_back((int)ffsrc.size());
+  if ((double)disp_index.size() * g->N * g->N * 8.0 > 6.0 * (1ull << 30))
+    return fail(DAGE_E_UNSUPPORTED,
+                "%zu distinct far-field displacements (uneven box split at level %d): the M2L "
+                "matrices would exceed 6 GiB; use an evenly divisible grid or fewer levels",
+                disp_index.size(), maxlevel);
+
+  // --- M2M/L2L translation displacements (boxes of levels >= 3) ---------------
+  {
+    std::map<std::vector<long long>, int> tindex;
+    std::vector<double> tdisp;
+    std::vector<int> m2m_disp;
+    for (int l = 3; l <= maxlevel; ++l)
+      for (int i = 1; i <= (1 << (3 * l)); ++i) {
+        const double *cc = &g->centers[3 * (size_t)(g->lev_off[l] + i - 1)];
+        const double *cp = &g->centers[3 * (size_t)(g->lev_off[l - 1] + (i - 1) / 8)];
+        double dv[3];
+        std::vector<long long> key(4);
+        key[3] = regular ? l : 0;
+        for (int d = 0; d < 3; ++d) {
+          dv[d] = cc[d] - cp[d];
+          if (regular)
+            key[d] = (i - 1) % 8;  // the child octant: the displacement of a regular lattice
+          else
+            std::memcpy(&key[d], &dv[d], 8);
+        }
+        if (regular) key[1] = key[2] = 0;
+        auto it = tindex.find(key);
+        int ti;
+        if (it == tindex.end()) {
+          ti = (int)tindex.size();
+          tindex[key] = ti;
+          tdisp.insert(tdisp.end(), dv, dv + 3);
+        } else {
+          ti = it->second;
+        }
+        m2m_disp.push_back(ti);
+      }
+    g->nm2m = (int)tindex.size();
+    if (g->nm2m > 0) {
+      const int M = g->N * (g->N + 1) / 2;
+      TransTables t;
+      translation_tables(lmax, t);
+      DevBuf dd, c1, c2, l1, l2;
+      DAGE_TRY(dd.alloc(sizeof(double) * tdisp.size()));
+      DAGE_TRY(c1.alloc(sizeof(double) * M));
+      DAGE_TRY(c2.alloc(sizeof(double) * M));
+      DAGE_TRY(l1.alloc(sizeof(int) * M));
+      DAGE_TRY(l2.alloc(sizeof(int) * M));
+      DAGE_TRY(g->d_Wm2m.alloc(sizeof(double) * (size_t)g->nm2m * M));
+      DAGE_TRY(g->d_m2m_disp.alloc(sizeof(int) * m2m_disp.size()));
+      DAGE_CUDA_TRY(cudaMemcpyAsync(dd.ptr, tdisp.data(), sizeof(double) * tdisp.size(), cudaMemcpyHostToDevice, s));
+      DAGE_CUDA_TRY(cudaMemcpyAsync(c1.ptr, t.c1.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
+      DAGE_CUDA_TRY(cudaMemcpyAsync(c2.ptr, t.c2.data(), sizeof(double) * M, cudaMemcpyHostToDevice, s));
+      DAGE_CUDA_TRY(cudaMemcpyAsync(l1.ptr, t.lm1.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+      DAGE_CUDA_TRY(cudaMemcpyAsync(l2.ptr, t.lm2.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+      DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_m2m_disp.ptr, m2m_disp.data(), sizeof(int) * m2m_disp.size(),
+                                    cudaMemcpyHostToDevice, s));
+      translation_matrices_kernel<<<g->nm2m, 256, sizeof(double) * g->N, s>>>(
+          dd.as<double>(), lmax, c1.as<double>(), c2.as<double>(), l1.as<int>(), l2.as<int>(), M,
+          g->d_Wm2m.as<double>());
+      DAGE_CUDA_TRY(cudaGetLastError());
+      DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+    }
   }
   g->ndisp = (int)disp_index.size();
   DAGE_TRY(g->d_ffstart.alloc(sizeof(int) * ffstart.size()));
@@ -1158,8 +1390,8 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
                                   cudaMemcpyHostToDevice, s));
   }
   DAGE_TRY(build_m2l(g));
-  DAGE_TRY(g->d_q.alloc(sizeof(double) * g->nbox * g->N));
-  DAGE_TRY(g->d_L.alloc(sizeof(double) * g->nbox * g->N));
+  DAGE_TRY(g->d_q.alloc(sizeof(double) * g->nbtot * g->N));
+  DAGE_TRY(g->d_L.alloc(sizeof(double) * g->nbtot * g->N));
   DAGE_TRY(g->d_partial.alloc(sizeof(double) * (size_t)g->nbox * g->nslab * g->N));
 
   // --- near-field sub-operator matrices per axis position --------------------
@@ -1241,6 +1473,10 @@ GInst plan_inst(const dage_gbfmm *g, const double *rho, double *V, double *q, do
   I.wy = g->wts[1].as<double>();
   I.wz = g->wts[2].as<double>();
   I.kappa = g->kappa;
+  I.fine_off = g->fine_off;
+  I.m2m_base = g->level >= 3 ? g->lev_off[3] : 0;
+  I.Wm2m = g->d_Wm2m.as<double>();
+  I.m2m_disp = g->d_m2m_disp.as<int>();
   return I;
 }
 
@@ -1352,6 +1588,28 @@ int run_m2l(const GInst *d_inst, int ninst, int nbox, int N, cudaStream_t s) {
   const int threads = ((N + 31) / 32) * 32;
   m2l_apply_kernel<<<dim3(nbox, ninst), threads, sizeof(double) * N, s>>>(d_inst, N);
   DAGE_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// Upward pass from the finest level to level 2 (no work for one level).
+int run_m2m(const GInst *d_inst, int ninst, const dage_gbfmm *g, cudaStream_t s) {
+  const int threads = std::min(256, ((g->N + 31) / 32) * 32);
+  for (int l = g->level - 1; l >= 2; --l) {
+    m2m_kernel<<<dim3(1 << (3 * l), ninst), threads, 0, s>>>(d_inst, g->N, g->lev_off[l],
+                                                            g->lev_off[l + 1]);
+    DAGE_CUDA_TRY(cudaGetLastError());
+  }
+  return 0;
+}
+
+// Downward pass from level 3 to the finest level, after the M2L of all levels.
+int run_l2l(const GInst *d_inst, int ninst, const dage_gbfmm *g, cudaStream_t s) {
+  const int threads = std::min(256, ((g->N + 31) / 32) * 32);
+  for (int l = 3; l <= g->level; ++l) {
+    l2l_kernel<<<dim3(1 << (3 * l), ninst), threads, 0, s>>>(d_inst, g->N, g->lev_off[l - 1],
+                                                            g->lev_off[l]);
+    DAGE_CUDA_TRY(cudaGetLastError());
+  }
   return 0;
 }
 
@@ -1641,10 +1899,10 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
     near_bounds(g, b->mt, b->nt);
     b->maxown = std::max(b->maxown, max_owned(g));
   }
-  const size_t per = (size_t)b->nbox * b->N;
+  const size_t per = (size_t)g0->nbtot * b->N;  // every level's boxes
   DAGE_TRY(b->q.alloc(sizeof(double) * per * n));
   DAGE_TRY(b->L.alloc(sizeof(double) * per * n));
-  DAGE_TRY(b->partial.alloc(sizeof(double) * per * b->nslab * n));
+  DAGE_TRY(b->partial.alloc(sizeof(double) * (size_t)b->nbox * b->N * b->nslab * n));
   DAGE_TRY(b->epart.alloc(sizeof(double) * kEnergyBlocks * n));
   DAGE_TRY(b->energy.alloc(sizeof(double) * n));
   DAGE_TRY(b->inst.alloc(sizeof(GInst) * n));
@@ -1685,11 +1943,12 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
 
 // Instance tables and near-field descriptors for a set of device cubes.
 int batch_tables(dage_gbfmm_batch *b, const double *const *rho, double *const *V) {
-  const size_t per = (size_t)b->nbox * b->N;
+  const size_t per = (size_t)b->plans[0]->nbtot * b->N;  // every level's boxes
   std::vector<GInst> ins(b->n);
   for (int i = 0; i < b->n; ++i) {
     ins[i] = plan_inst(b->plans[b->plan_of[i]], rho[i], V[i], b->q.as<double>() + per * i,
-                       b->L.as<double>() + per * i, b->partial.as<double>() + per * b->nslab * i,
+                       b->L.as<double>() + per * i,
+                       b->partial.as<double>() + (size_t)b->nbox * b->N * b->nslab * i,
                        b->epart.as<double>() + (size_t)kEnergyBlocks * i);
     if (b->kern_of[i] >= 0) {
       const auto &k = b->kerns[b->kern_of[i]];
@@ -1738,7 +1997,9 @@ int batch_launch(dage_gbfmm_batch *b, const double *const *rho, double *const *V
   bool any_helm = false;
   for (int i = 0; i < b->n; ++i) any_helm |= b->kern_of[i] >= 0;
   DAGE_TRY(run_multipoles(d_inst, b->n, b->nbox, b->lmax, b->nslab, any_helm, s));
-  DAGE_TRY(run_m2l(d_inst, b->n, b->nbox, b->N, s));
+  DAGE_TRY(run_m2m(d_inst, b->n, b->plans[0], s));
+  DAGE_TRY(run_m2l(d_inst, b->n, b->plans[0]->nbtot, b->N, s));
+  DAGE_TRY(run_l2l(d_inst, b->n, b->plans[0], s));
   for (auto &c : b->chunks) {
     const StageDesc *dd[3] = {c.desc[0].as<StageDesc>(), c.desc[1].as<StageDesc>(),
                               c.desc[2].as<StageDesc>()};
@@ -1789,6 +2050,8 @@ int dage_gbfmm_set_energy(dage_gbfmm *g, double energy) {
   clear_error();
   if (!g) return fail(DAGE_E_INVALID, "null handle");
   if (!(energy <= 0.0)) return fail(DAGE_E_INVALID, "energy must be <= 0 (got %g)", energy);
+  if (energy < 0.0 && g->level > 2)
+    return fail(DAGE_E_UNSUPPORTED, "the Helmholtz GBFMM runs with maxlevel 2 (no Helmholtz M2M/L2L)");
   DAGE_CUDA_TRY(cudaSetDevice(g->device));
   g->energy = energy;
   g->kappa = energy < 0.0 ? std::sqrt(-2.0 * energy) : 0.0;
@@ -1825,7 +2088,9 @@ int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags
   const GInst *d_inst = g->d_inst.as<GInst>();
   DAGE_CUDA_TRY(cudaMemsetAsync(d_V, 0, sizeof(double) * n, s));
   DAGE_TRY(run_multipoles(d_inst, 1, g->nbox, g->lmax, g->nslab, g->kappa > 0.0, s));
-  DAGE_TRY(run_m2l(d_inst, 1, g->nbox, g->N, s));
+  DAGE_TRY(run_m2m(d_inst, 1, g, s));
+  DAGE_TRY(run_m2l(d_inst, 1, g->nbtot, g->N, s));
+  DAGE_TRY(run_l2l(d_inst, 1, g, s));
   int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
   near_bounds(g, mt, nt);
   const StageDesc *dd[3] = {g->d_desc[0].as<StageDesc>(), g->d_desc[1].as<StageDesc>(),
@@ -1854,7 +2119,8 @@ int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flag
   DAGE_TRY(single_setup(g, d_rho, nullptr, false));
   DAGE_TRY(run_multipoles(g->d_inst.as<GInst>(), 1, g->nbox, g->lmax, g->nslab, g->kappa > 0.0,
                           g->stream));
-  DAGE_CUDA_TRY(cudaMemcpyAsync(moments, g->d_q.ptr, sizeof(double) * g->nbox * g->N,
+  DAGE_CUDA_TRY(cudaMemcpyAsync(moments, g->d_q.as<double>() + (size_t)g->fine_off * g->N,
+                                sizeof(double) * g->nbox * g->N,
                                 cudaMemcpyDeviceToHost, g->stream));
   DAGE_CUDA_TRY(cudaStreamSynchronize(g->stream));
   return 0;
@@ -1863,7 +2129,8 @@ int dage_gbfmm_multipole_moments(dage_gbfmm *g, const double *rho, unsigned flag
 int dage_gbfmm_local_expansions(dage_gbfmm *g, double *L) {
   clear_error();
   if (!g || !L) return fail(DAGE_E_INVALID, "null argument");
-  DAGE_CUDA_TRY(cudaMemcpy(L, g->d_L.ptr, sizeof(double) * g->nbox * g->N, cudaMemcpyDeviceToHost));
+  DAGE_CUDA_TRY(cudaMemcpy(L, g->d_L.as<double>() + (size_t)g->fine_off * g->N,
+                           sizeof(double) * g->nbox * g->N, cudaMemcpyDeviceToHost));
   return 0;
 }
 
@@ -2012,8 +2279,11 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
 int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies) {
   clear_error();
   if (!b || !energies) return fail(DAGE_E_INVALID, "null argument");
-  for (int i = 0; i < b->n; ++i)
+  for (int i = 0; i < b->n; ++i) {
     if (!(energies[i] <= 0.0)) return fail(DAGE_E_INVALID, "energy %d must be <= 0", i);
+    if (energies[i] < 0.0 && b->plans[0]->level > 2)
+      return fail(DAGE_E_UNSUPPORTED, "the Helmholtz GBFMM runs with maxlevel 2 (no Helmholtz M2M/L2L)");
+  }
   DAGE_CUDA_TRY(cudaSetDevice(b->device));
   DAGE_CUDA_TRY(cudaStreamSynchronize(b->stream));
   for (auto &k : b->kerns) {

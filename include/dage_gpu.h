@@ -138,11 +138,16 @@ typedef struct dage_gbfmm dage_gbfmm;
 /* Builds the operator for a grid split into 2^maxlevel boxes per axis:
  * near-field sub-operator matrices (quadrature `quad`, the reference's
  * default for the near field is GaussQuad(25, 25)), box geometry, local
- * far-field lists and the M2L matrices of all box displacements, on the GPU.
- * maxlevel must be 2 (the reference default: 4x4x4 boxes, whose local far
- * field needs no M2M/L2L); lmax <= 15; precision must be DAGE_FP64.  Boxes take ncell/2^maxlevel
- * cells per axis; when that does not divide, the first ncell mod 2^maxlevel
- * boxes along the axis take one cell more.
+ * far-field lists of every level and the M2L matrices of all box
+ * displacements, and for maxlevel >= 3 the M2M/L2L translation matrices, on
+ * the GPU.  maxlevel 2..5 (the reference default is 2: 4x4x4 boxes, whose
+ * local far field needs no M2M/L2L; deeper levels run the upward M2M pass,
+ * M2L at every level and the downward L2L pass of gbfmm_coulomb3d.F90:
+ * 650-905, 1502-1621); lmax <= 15; precision must be DAGE_FP64.  Boxes take
+ * ncell/2^maxlevel cells per axis; when that does not divide, the first
+ * ncell mod 2^maxlevel boxes along the axis take one cell more, and a box
+ * of a coarser level is the union of its children.  The Helmholtz kernel
+ * (dage_gbfmm_set_energy with E < 0) runs with maxlevel 2 only.
  * Replaces GBFMMCoulomb3D_init + init_nearfield + init_interaction_matrices
  * and gbfmmcoulomb3d_init_cuda (src/gbfmm/gbfmm_coulomb3d.F90:331-508,
  * 1313-1438; src/gbfmm/gbfmm_coulomb3d.cu:583-600). */

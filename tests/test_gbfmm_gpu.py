@@ -103,3 +103,33 @@ def test_multipoles_every_lmax(dage, oracle, lmax):
     plan, Qo = _oracle_moments(oracle, go, rho, lmax)
     for b in range(plan.nbox):
         assert np.abs(Qg[:, b] - Qo[:, b]).max() <= 1e-12 * np.abs(Qo[:, b]).max() + 1e-300
+
+
+@pytest.mark.parametrize("ncell,lmax", [(16, 8), (18, 6)])  # 18 cells: uneven, nested levels
+def test_multilevel_matches_oracle(dage, oracle, ncell, lmax):
+    """Three levels (8^3 finest boxes): moments, local expansions after
+    M2M -> M2L at levels 2 and 3 -> L2L, and the full potential and energy
+    against the oracle's restatement of the reference's multi-level passes."""
+    g, go, rho = _setup(dage, oracle, ncell, 0.2)
+    quad = (6, 6, 0.0, 2.0, 1e3)
+    op = dage.GBFMMCoulomb3D(g, lmax=lmax, maxlevel=3, quad=dage.GaussQuad(*quad))
+    V, E = op.apply(rho, energy=True)
+    Vo, qo, Lo, _ = oracle.gbfmm_apply(go, rho, lmax=lmax, maxlevel=3, quad=quad,
+                                       return_parts=True)
+    Qg = op.multipole_moments(rho)
+    assert np.abs(Qg - qo).max() <= 1e-12 * np.abs(qo).max()
+    op.apply(rho)
+    Lg = op.local_expansions()
+    assert np.abs(Lg - Lo).max() <= 1e-11 * np.abs(Lo).max()
+    V1 = oracle.gbfmm_apply(go, rho, lmax=lmax, maxlevel=3, quad=quad, libm_1ulp=True)
+    spread = np.abs(V1 - Vo).max() / np.abs(Vo).max()
+    err = np.abs(V - Vo).max() / np.abs(Vo).max()
+    assert err <= max(1e-10, 10 * spread), (err, spread)
+    Eo = oracle.integrate_cube(go, rho * Vo)
+    assert abs(E - Eo) <= 1e-11 * abs(Eo)
+
+
+def test_multilevel_helmholtz_is_refused(dage):
+    g = dage.Grid3D.cube(-9.6, 16, 0.2)
+    with pytest.raises(Exception, match="maxlevel 2"):
+        dage.GBFMMHelmholtz3D(g, -0.5, lmax=4, maxlevel=3, quad=dage.GaussQuad(4, 4))
