@@ -741,3 +741,66 @@ def log_radial_grid(ncell=33, r0=1e-5, r1=15.0, nlip=7):
     log-spaced on [r0, r1] (ncell cells, ncell*(nlip-1)+1 points)."""
     edges = np.concatenate([[0.0], r0 * (r1 / r0) ** (np.arange(ncell) / (ncell - 1))])
     return np.diff(edges) / (nlip - 1)
+
+
+def lip_partial_integrals(nlip):
+    """LIPBasis outward/inward integrals (lip.F90:414-480) of the
+    equidistant basis on local nodes first, first+1, ..., first+nlip-1:
+    out[i, j-1] = int_{x_0}^{x_j} chi_i, inn[i, j] = int_{x_j}^{x_n} chi_i."""
+    first = -((nlip - 1) // 2)
+    x = first + np.arange(nlip, dtype=np.float64)
+    out = np.zeros((nlip, nlip - 1))
+    inn = np.zeros((nlip, nlip - 1))
+    for i in range(nlip):
+        others = np.delete(x, i)
+        P = np.poly1d(others, r=True) / np.prod(x[i] - others)
+        A = np.polyint(P)
+        for j in range(1, nlip):
+            out[i, j - 1] = A(x[j]) - A(x[0])
+        for j in range(nlip - 1):
+            inn[i, j] = A(x[-1]) - A(x[j])
+    return out, inn
+
+
+def bubbles_coulomb_potential(ncell, cell_scales, lmax, f, k=0, nlip=7):
+    """Coulomb3D_evaluate_bubbles_potential (coulomb.F90:222-336) for one atom:
+    V_lm(r) = 4 pi/(2l+1) [ r^-(l+1) int_0^r f_lm s^(l+2+k) ds
+                            + r^l int_r^inf f_lm s^(1-l+k) ds ]
+    with the cumulative LIP integrals of InOutIntegrator1D
+    (evaluators.F90:1263-1318); negative powers are 0 at r = 0
+    (Bubbles_rpow, bubbles.F90:3363-3378).  f: ((lmax+1)^2, npts)."""
+    h = _f64(np.broadcast_to(cell_scales, (ncell,)))
+    n = nlip - 1
+    r = Grid1D(0.0, ncell, nlip, 1, h).points
+    npts = r.size
+    out_i, in_i = lip_partial_integrals(nlip)
+
+    def rpow(p):
+        if p >= 0:
+            return r ** p
+        v = np.zeros_like(r)
+        v[1:] = r[1:] ** p
+        return v
+
+    def outwards(g):
+        res = np.zeros(npts)
+        for c in range(ncell):
+            s = c * n
+            res[s + 1:s + n + 1] = (g[s:s + n + 1] @ out_i) * h[c] + res[s]
+        return res
+
+    def inwards(g):
+        res = np.zeros(npts)
+        for c in range(ncell - 1, -1, -1):
+            s = c * n
+            res[s:s + n] = (g[s:s + n + 1] @ in_i) * h[c] + res[s + n]
+        return res
+
+    f = np.asarray(f, dtype=np.float64).reshape((lmax + 1) ** 2, npts)
+    V = np.zeros_like(f)
+    for l in range(lmax + 1):
+        r1, r2, r3, r4 = rpow(-(l + 1)), rpow(l + 2 + k), rpow(l), rpow(-(l + 1) + 2 + k)
+        for m in range(-l, l + 1):
+            lm = l * (l + 1) + m
+            V[lm] = 4 * np.pi / (2 * l + 1) * (r1 * outwards(f[lm] * r2) + r3 * inwards(f[lm] * r4))
+    return V
