@@ -93,6 +93,8 @@ SIGNATURES = {
                                            ctypes.c_int, _D, ctypes.POINTER(_VP)]),
     "dage_bubbles_inject": (ctypes.c_int, [_VP, ctypes.POINTER(DageGrid1D), ctypes.c_int,
                                            ctypes.c_double, _VP, ctypes.c_uint]),
+    "dage_bubbles_coulomb_potential": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "dage_bubbles_get_f": (ctypes.c_int, [_VP, _D]),
     "dage_bubbles_destroy": (ctypes.c_int, [_VP]),
     "dage_integrate": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, ctypes.c_uint, _D]),
     "dage_op3d_apply_fp64_noalloc": (ctypes.c_int, [ctypes.c_int] * 7 + [_VP, _VP, _VP, _D, _VP,

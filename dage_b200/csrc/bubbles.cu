@@ -186,6 +186,13 @@ struct dage_bubbles {
   double first = -3.0;
   DevBuf atoms, celld, hcell, coef, xs, ys, zs;
   int gshape[3] = {0, 0, 0};
+  // the radial values as given (without r^k), the radial points, per-atom
+  // point counts and offsets; host copies of the centres and radial grids
+  DevBuf fraw, rpts, np, foff;
+  std::vector<double> centers;
+  std::vector<dage_grid1d> radial;
+  std::vector<std::vector<double>> scales;
+  size_t nvals = 0;
 };
 
 extern "C" {
@@ -199,7 +206,9 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
     return fail(DAGE_E_INVALID, "need natom >= 1, 0 <= lmax <= 12, k >= 0");
   auto *b = new dage_bubbles();
   auto cleanup = [&](int rc) {
-    for (DevBuf *x : {&b->atoms, &b->celld, &b->hcell, &b->coef, &b->xs, &b->ys, &b->zs}) x->release();
+    for (DevBuf *x : {&b->atoms, &b->celld, &b->hcell, &b->coef, &b->xs, &b->ys, &b->zs,
+                      &b->fraw, &b->rpts, &b->np, &b->foff})
+      x->release();
     delete b;
     return rc;
   };
@@ -215,7 +224,10 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
   if (rc) return cleanup(rc);
   b->first = L.first;
   std::vector<AtomTab> tab(natom);
-  std::vector<double> celld, hcell, rf;
+  std::vector<double> celld, hcell, rf, rpts;
+  b->centers.assign(centers, centers + 3 * natom);
+  b->radial.assign(radial, radial + natom);
+  b->scales.resize(natom);
   std::vector<int> np(natom), foff(natom), cell0(natom + 1, 0);
   for (int a = 0; a < natom; ++a) {
     if (radial[a].nlip != nlip || radial[a].grid_type != 1)
@@ -234,6 +246,9 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
     cell0[a + 1] = cell0[a] + ax.ncell;
     np[a] = ax.n();
     foff[a] = (int)rf.size();
+    rpts.insert(rpts.end(), ax.points.begin(), ax.points.end());
+    b->scales[a].assign(radial[a].cell_scales, radial[a].cell_scales + ax.ncell);
+    b->radial[a].cell_scales = b->scales[a].data();
     for (int lm = 0; lm < b->N; ++lm)
       for (int j = 0; j < np[a]; ++j) {
         double rp = 1.0;
@@ -259,6 +274,24 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
   cudaMemcpy(d_foff.ptr, foff.data(), sizeof(int) * natom, cudaMemcpyHostToDevice);
   cudaMemcpy(d_cell0.ptr, cell0.data(), sizeof(int) * (natom + 1), cudaMemcpyHostToDevice);
   cudaMemcpy(d_lipc.ptr, L.coeff.data(), sizeof(double) * L.coeff.size(), cudaMemcpyHostToDevice);
+  // raw values and radial points for the radial potential
+  b->nvals = rf.size();
+  if ((rc = b->fraw.alloc(sizeof(double) * rf.size())) || (rc = b->rpts.alloc(sizeof(double) * rpts.size())) ||
+      (rc = b->np.alloc(sizeof(int) * natom)) || (rc = b->foff.alloc(sizeof(int) * natom)))
+    return cleanup(rc);
+  {
+    std::vector<double> raw(rf.size());
+    std::vector<int> poff(natom);
+    for (int a = 0, po = 0; a < natom; ++a) {
+      for (size_t e = 0; e < (size_t)b->N * np[a]; ++e) raw[foff[a] + e] = f[foff[a] + e];
+      poff[a] = po;
+      po += np[a];
+    }
+    cudaMemcpy(b->fraw.ptr, raw.data(), sizeof(double) * raw.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->rpts.ptr, rpts.data(), sizeof(double) * rpts.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->np.ptr, np.data(), sizeof(int) * natom, cudaMemcpyHostToDevice);
+    cudaMemcpy(b->foff.ptr, foff.data(), sizeof(int) * natom, cudaMemcpyHostToDevice);
+  }
   const int total = cell0[natom] * b->N;
   bubble_coeffs_kernel<<<(total + 127) / 128, 128>>>(d_rf.as<double>(), d_np.as<int>(),
                                                      d_foff.as<int>(), d_cell0.as<int>(), natom,
@@ -292,6 +325,78 @@ int bubbles_inject_launch(const dage_bubbles *b, const double *xs, int nx, const
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
+
+namespace {
+// Radial Coulomb potential of every (atom, lm) function
+// (Coulomb3D_evaluate_bubbles_potential, coulomb.F90:222-336):
+//   V_lm(r) = 4 pi/(2l+1) [ r^-(l+1) int_0^r f s^(l+2+k) ds + r^l int_r^inf f s^(1-l+k) ds ]
+// with the cumulative LIP integrals of InOutIntegrator1D (evaluators.F90:
+// 1263-1318): per cell, the values at its points from the cell's LIP
+// partial integrals (outward: from its first point, inward: to its last)
+// times the cell step, plus the running value at the cell boundary.
+// Negative powers are 0 at r = 0 (Bubbles_rpow).  Block = atom, thread = lm;
+// the outward integral is kept in V until the inward pass completes it.
+__global__ void bubbles_potential_kernel(const AtomTab *__restrict__ atoms,
+                                         const double *__restrict__ hcell,
+                                         const double *__restrict__ f,
+                                         const double *__restrict__ rpts,
+                                         const int *__restrict__ np, const int *__restrict__ foff,
+                                         int lmax, int k, int nlip,
+                                         const double *__restrict__ ints_out,
+                                         const double *__restrict__ ints_in, double *V) {
+  const int a = blockIdx.x, N = (lmax + 1) * (lmax + 1);
+  const AtomTab A = atoms[a];
+  int poff = 0;  // offset of this atom's points in rpts
+  for (int b = 0; b < a; ++b) poff += np[b];
+  const double *r = rpts + poff;
+  const int n = nlip - 1, npts = np[a];
+  for (int lm = threadIdx.x; lm < N; lm += blockDim.x) {
+    int l = 0;
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    const double *fl = f + foff[a] + (size_t)lm * npts;
+    double *Vl = V + foff[a] + (size_t)lm * npts;
+    auto rpow = [&](int p, int e) {
+      if (e >= 0) {
+        double v = 1.0;
+        for (int i = 0; i < e; ++i) v *= r[p];
+        return v;
+      }
+      if (p == 0) return 0.0;
+      double v = 1.0;
+      for (int i = 0; i < -e; ++i) v *= r[p];
+      return 1.0 / v;
+    };
+    // outward pass: int_0^{r_p} f s^(l+2+k) ds
+    Vl[0] = 0.0;
+    for (int c = 0; c < A.ncell; ++c) {
+      const int s0 = c * n;
+      const double h = hcell[A.cell0 + c], base = Vl[s0];
+      for (int j = 1; j <= n; ++j) {
+        double acc = 0.0;
+        for (int i = 0; i <= n; ++i) acc += fl[s0 + i] * rpow(s0 + i, l + 2 + k) * ints_out[i * n + j - 1];
+        Vl[s0 + j] = acc * h + base;
+      }
+    }
+    // inward pass: int_{r_p}^inf f s^(1-l+k) ds, combined point by point
+    const double pref = 4.0 * 3.141592653589793238 / (2 * l + 1);
+    double end = 0.0;  // the inward integral at the current cell's last point
+    Vl[npts - 1] = pref * (rpow(npts - 1, -(l + 1)) * Vl[npts - 1]);
+    for (int c = A.ncell - 1; c >= 0; --c) {
+      const int s0 = c * n;
+      const double h = hcell[A.cell0 + c];
+      double vals[8];
+      for (int j = 0; j < n; ++j) {
+        double acc = 0.0;
+        for (int i = 0; i <= n; ++i) acc += fl[s0 + i] * rpow(s0 + i, 1 - l + k) * ints_in[i * n + j];
+        vals[j] = acc * h + end;
+      }
+      for (int j = 0; j < n; ++j)
+        Vl[s0 + j] = pref * (rpow(s0 + j, -(l + 1)) * Vl[s0 + j] + rpow(s0 + j, l) * vals[j]);
+      end = vals[0];
+    }
+  }
+}
+}  // namespace
 }  // namespace dage
 
 extern "C" {
@@ -331,9 +436,58 @@ int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, do
   return 0;
 }
 
+int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out) {
+  clear_error();
+  if (!in || !out) return fail(DAGE_E_INVALID, "null argument");
+  *out = nullptr;
+  DAGE_CUDA_TRY(cudaSetDevice(in->device));
+  // LIP partial integrals on the local nodes (LIPBasis_outward/inward_integrals,
+  // lip.F90:414-480): antiderivative of each basis polynomial by Horner
+  LipBasis L;
+  DAGE_TRY(make_lip_basis(in->nlip, 1, L));
+  const int nl = in->nlip, n = nl - 1;
+  std::vector<double> outi((size_t)nl * n), ini((size_t)nl * n);
+  auto anti = [&](int i, double x) {
+    double v = 0.0;
+    for (int kk = 0; kk < nl; ++kk) v = (v + L.coeff[(size_t)kk * nl + i] / (double)(nl - kk)) * x;
+    return v;
+  };
+  for (int i = 0; i < nl; ++i)
+    for (int j = 0; j < n; ++j) {
+      outi[(size_t)i * n + j] = anti(i, L.first + j + 1) - anti(i, L.first);
+      ini[(size_t)i * n + j] = anti(i, L.last) - anti(i, L.first + j);
+    }
+  DevBuf d_out, d_in, d_V;
+  DAGE_TRY(d_out.alloc(sizeof(double) * outi.size()));
+  DAGE_TRY(d_in.alloc(sizeof(double) * ini.size()));
+  DAGE_TRY(d_V.alloc(sizeof(double) * in->nvals));
+  DAGE_CUDA_TRY(cudaMemcpy(d_out.ptr, outi.data(), sizeof(double) * outi.size(), cudaMemcpyHostToDevice));
+  DAGE_CUDA_TRY(cudaMemcpy(d_in.ptr, ini.data(), sizeof(double) * ini.size(), cudaMemcpyHostToDevice));
+  bubbles_potential_kernel<<<in->natom, std::min(256, ((in->N + 31) / 32) * 32)>>>(
+      in->atoms.as<AtomTab>(), in->hcell.as<double>(), in->fraw.as<double>(),
+      in->rpts.as<double>(), in->np.as<int>(), in->foff.as<int>(), in->lmax, in->k, in->nlip,
+      d_out.as<double>(), d_in.as<double>(), d_V.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  std::vector<double> V(in->nvals);
+  DAGE_CUDA_TRY(cudaMemcpy(V.data(), d_V.ptr, sizeof(double) * V.size(), cudaMemcpyDeviceToHost));
+  // the potential is a bubble set of its own (k = 0) on the same centres and grids
+  return dage_bubbles_create(in->natom, in->centers.data(), in->radial.data(), in->lmax, 0,
+                             V.data(), out);
+}
+
+int dage_bubbles_get_f(const dage_bubbles *b, double *f) {
+  clear_error();
+  if (!b || !f) return fail(DAGE_E_INVALID, "null argument");
+  DAGE_CUDA_TRY(cudaSetDevice(b->device));
+  DAGE_CUDA_TRY(cudaMemcpy(f, b->fraw.ptr, sizeof(double) * b->nvals, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
 int dage_bubbles_destroy(dage_bubbles *b) {
   if (!b) return 0;
-  for (DevBuf *x : {&b->atoms, &b->celld, &b->hcell, &b->coef, &b->xs, &b->ys, &b->zs}) x->release();
+  for (DevBuf *x : {&b->atoms, &b->celld, &b->hcell, &b->coef, &b->xs, &b->ys, &b->zs, &b->fraw,
+                    &b->rpts, &b->np, &b->foff})
+    x->release();
   delete b;
   return 0;
 }

@@ -518,6 +518,35 @@ class Bubbles:
                 pass
             self._h = None
 
+    @classmethod
+    def _wrap(cls, handle, like: "Bubbles") -> "Bubbles":
+        obj = cls.__new__(cls)
+        obj.natom = like.natom
+        obj.lmax = like.lmax
+        obj._grids = like._grids
+        obj._h = handle
+        return obj
+
+    def coulomb_potential(self) -> "Bubbles":
+        """The radial Coulomb potential of these bubbles as a bubble set of
+        its own (Coulomb3D_evaluate_bubbles_potential, coulomb.F90:222-336),
+        computed on the GPU."""
+        h = ctypes.c_void_p()
+        check(load().dage_bubbles_coulomb_potential(self._h, ctypes.byref(h)))
+        return Bubbles._wrap(h, self)
+
+    def radial_values(self):
+        """Per atom, the ((lmax+1)^2, npoints) radial values (as given)."""
+        sizes = [int(gr.ncell * (gr.nlip - 1) + 1) for gr in self._grids]
+        N = (self.lmax + 1) ** 2
+        flat = np.zeros(N * sum(sizes))
+        check(load().dage_bubbles_get_f(self._h, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        out, o = [], 0
+        for npts in sizes:
+            out.append(flat[o:o + N * npts].reshape(N, npts))
+            o += N * npts
+        return out
+
     def inject(self, grid: Grid3D, cube=None, lmin: int = 0, factor: float = 1.0):
         """cube += factor * bubbles at the grid points; returns the cube."""
         n = int(np.prod(grid.shape))

@@ -255,6 +255,19 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
  * (src/bubbles/bubbles_cuda.cu:3090-3350, 3774-3776). */
 int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, double factor,
                         double *cube, unsigned flags);
+/* Radial Coulomb potential of a bubble set (Coulomb3D_evaluate_bubbles_potential,
+ * src/bubbles/coulomb.F90:222-336): a new bubble set (k = 0, same centres,
+ * radial grids and lmax) holding, per atom and (l, m),
+ *   V_lm(r) = 4 pi/(2l+1) [ r^-(l+1) int_0^r f s^(l+2+k) ds + r^l int_r^inf f s^(1-l+k) ds ]
+ * by the cumulative LIP integrals of InOutIntegrator1D
+ * (src/bubbles/evaluators.F90:1263-1318), computed on the GPU.  The result
+ * can be injected into a cube like any bubble set. */
+int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out);
+
+/* Copies the radial values of a bubble set (as given at creation: per atom,
+ * (lmax+1)^2 functions of the atom's radial points) to host memory. */
+int dage_bubbles_get_f(const dage_bubbles *b, double *f);
+
 int dage_bubbles_destroy(dage_bubbles *b);
 
 /* ---------------------------------------------------------------------------

@@ -51,3 +51,36 @@ def test_inject_device_cube_and_analytic(dage, oracle):
     exact = np.exp(-np.sqrt((X - 0.13) ** 2 + (Y + 0.21) ** 2 + (Z - 0.07) ** 2))
     got = cube.cpu().numpy().reshape(-1).reshape(go.shape, order="F")
     assert np.abs(got - exact).max() < 1e-6  # LIP interpolation error on the log grid
+
+
+@pytest.mark.parametrize("natom,lmax,k", [(1, 0, 0), (3, 2, 0), (2, 4, 1)])
+def test_coulomb_potential_matches_oracle(dage, oracle, natom, lmax, k):
+    """Radial Coulomb potential of every (atom, lm) function on the GPU against
+    the oracle's restatement of Coulomb3D_evaluate_bubbles_potential."""
+    centers, ncells, hs, f = _bubbles(oracle, natom, lmax)
+    rad = [dage.Grid1D(0.0, n, 7, 1, h) for n, h in zip(ncells, hs)]
+    b = dage.Bubbles(centers, rad, f, lmax, k=k)
+    pot = b.coulomb_potential()
+    got = pot.radial_values()
+    for a in range(natom):
+        ref = oracle.bubbles_coulomb_potential(ncells[a], hs[a], lmax, f[a], k=k)
+        assert np.abs(got[a] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_coulomb_potential_of_gaussian_injects_erf(dage, oracle):
+    """A Gaussian monopole bubble -> potential bubble -> injected into a cube:
+    pi^{3/2} erf(r)/r within the LIP interpolation error."""
+    from scipy.special import erf
+
+    h = oracle.log_radial_grid(60, 1e-4, 12.0)
+    r = oracle.Grid1D(0.0, 60, 7, 1, h).points
+    b = dage.Bubbles([[0.1, -0.2, 0.05]], [dage.Grid1D(0.0, 60, 7, 1, h)], [np.exp(-r ** 2)[None, :]], 0)
+    pot = b.coulomb_potential()
+    g = dage.Grid3D.cube(-4.0, 10, 0.2)
+    go = oracle.Grid3D.cube(-4.0, 10, 0.2)
+    cube = pot.inject(g)
+    X, Y, Z = np.meshgrid(*(a.points for a in go.axes), indexing="ij")
+    d = np.sqrt((X - 0.1) ** 2 + (Y + 0.2) ** 2 + (Z - 0.05) ** 2)
+    exact = np.pi ** 1.5 * erf(d) / d
+    inside = d < 11.5  # the radial grid (and so the bubble) ends at r = 12
+    assert np.abs(cube - exact)[inside].max() <= 1e-6 * np.abs(exact).max()
