@@ -18,7 +18,8 @@ from .operators import (  # noqa: F401
     Operator3D,
     dot,
     integrate,
+    multiply,
 )
 
 __all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GBFMMHelmholtz3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
-           "DageError", "dot", "integrate", "load"]
+           "DageError", "dot", "integrate", "load", "multiply"]

@@ -12,6 +12,7 @@ DAGE_ENERGY = 2
 DAGE_NO_CODA = 4
 DAGE_ACCUMULATE = 8
 DAGE_NO_GRAPH = 16
+DAGE_PRODUCT_COMPLETE = 32
 
 DAGE_FP64 = 0
 DAGE_MIXED_BF16X3 = 1
@@ -95,6 +96,13 @@ SIGNATURES = {
                                            ctypes.c_double, _VP, ctypes.c_uint]),
     "dage_bubbles_coulomb_potential": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "dage_bubbles_get_f": (ctypes.c_int, [_VP, _D]),
+    "dage_bubbles_multiply": (ctypes.c_int, [_VP, _VP, ctypes.c_uint, ctypes.POINTER(_VP)]),
+    "dage_product_table": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), _D,
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "dage_function3d_multiply": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, _VP, _VP,
+                                                _VP, _VP, ctypes.c_uint]),
     "dage_bubbles_destroy": (ctypes.c_int, [_VP]),
     "dage_integrate": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, ctypes.c_uint, _D]),
     "dage_op3d_apply_fp64_noalloc": (ctypes.c_int, [ctypes.c_int] * 7 + [_VP, _VP, _VP, _D, _VP,

@@ -33,7 +33,7 @@ constexpr int kMaxAtomsSmem = 256;
 // Racah-normalised real spherical harmonics of a unit vector: the regular
 // solid-harmonic recursion with r^2 = 1, visiting each (l, m) once.
 template <class F>
-__device__ __forceinline__ void unit_harmonics(int lmax, double x, double y, double z, F &&f) {
+__host__ __device__ __forceinline__ void unit_harmonics(int lmax, double x, double y, double z, F &&f) {
   f(0, 1.0);
   if (lmax == 0) return;
   {
@@ -173,6 +173,120 @@ __global__ void __launch_bounds__(256)
       });
     }
     cube[i] += factor * acc;
+  }
+}
+
+// Radial cell of distance d (1-based, Grid1D_get_icell), 0 when d is outside.
+__device__ __forceinline__ int radial_cell(const double *cd, int ncell, double d) {
+  if (cd[ncell - 1] <= d) return ncell;
+  int icell = ncell / 2, maxi = ncell - 1, mini = 1;
+  for (int it = 0; it < 64; ++it) {
+    if (d >= cd[icell]) {
+      if (d < cd[icell + 1]) return icell + 1;
+      mini = icell + 2;
+    } else {
+      if (d >= cd[icell - 1]) return icell;
+      maxi = icell - 1;
+    }
+    icell = (mini + maxi) / 2;
+  }
+  return 0;
+}
+
+// The cube part of a function product in one pass (Function3D_multiply,
+// function3d.F90:1097-1409; the reference GPU path injects each bubble set
+// in its own launches per atom, multiplies the cubes, then de-injects,
+// bubbles_cuda.cu:3533-3690):
+//   out = (c1 + B1)(c2 + B2) - Br
+// The three bubble sets share atoms and radial grids, so every atom's
+// distance, radial cell, cell coordinate and harmonics are computed once per
+// point for all three; Ni = 0 marks an absent set.
+__global__ void __launch_bounds__(256)
+    function_product_kernel(const AtomTab *__restrict__ atoms, int natom,
+                            const double *__restrict__ celld, const double *__restrict__ hcell,
+                            const double *__restrict__ coef1, int N1,
+                            const double *__restrict__ coef2, int N2,
+                            const double *__restrict__ coefr, int Nr, int lmax, int nlip,
+                            double first, const double *__restrict__ xs, int nx,
+                            const double *__restrict__ ys, int ny, const double *__restrict__ zs,
+                            int nz, const double *c1, const double *c2, double *out) {
+  __shared__ AtomTab sa[kMaxAtomsSmem];
+  for (int a = threadIdx.x; a < natom && a < kMaxAtomsSmem; a += blockDim.x) sa[a] = atoms[a];
+  __syncthreads();
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % nx);
+    const long long r = i / nx;
+    const int iy = (int)(r % ny), iz = (int)(r / ny);
+    const double px = xs[ix], py = ys[iy], pz = zs[iz];
+    double v1 = 0.0, v2 = 0.0, vr = 0.0;
+    for (int a = 0; a < natom; ++a) {
+      const AtomTab A = a < kMaxAtomsSmem ? sa[a] : atoms[a];
+      const double dx = px - A.cx, dy = py - A.cy, dz = pz - A.cz;
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      if (d > A.rmax) continue;
+      const double *cd = celld + A.cell0;
+      const int ic = radial_cell(cd, A.ncell, d);
+      if (!ic) continue;
+      const double t = (d - cd[ic - 1]) / hcell[A.cell0 + ic - 1] + first;
+      const size_t cell = (size_t)(A.cell0 + ic - 1);
+      double ux = 0.0, uy = 0.0, uz = 0.0;
+      const bool at_centre = !(d > 0.0);
+      if (!at_centre) {
+        const double inv = 1.0 / d;
+        ux = dx * inv;
+        uy = dy * inv;
+        uz = dz * inv;
+      }
+      auto horner = [&](const double *c) {
+        double v = c[0];
+        for (int kk = 1; kk < nlip; ++kk) v = v * t + c[kk];
+        return v;
+      };
+      unit_harmonics(lmax, ux, uy, uz, [&](int lm, double Y) {
+        if (at_centre && lm > 0) return;
+        if (lm < N1) v1 += horner(coef1 + (cell * N1 + lm) * 8) * Y;
+        if (lm < N2) v2 += horner(coef2 + (cell * N2 + lm) * 8) * Y;
+        if (lm < Nr) vr += horner(coefr + (cell * Nr + lm) * 8) * Y;
+      });
+    }
+    out[i] = (c1[i] + v1) * (c2[i] + v2) - vr;
+  }
+}
+
+struct ProdTerm {
+  int a, b, lm, pad;
+  double c;
+};
+
+// Radial product of two bubble sets on the same atoms and radial points
+// (Bubble_product_kernel, bubbles_multiplier.cu:65-106): one thread per
+// (atom, radial point); for every term of the product table
+//   out_LM += C * (f1_a f2_b + f1_b f2_a [a != b]),   a <= b.
+// The values are the raw radial functions (without r^k).
+__global__ void bubbles_product_kernel(const double *__restrict__ f1, int N1,
+                                       const double *__restrict__ f2, int N2,
+                                       const int *__restrict__ np, const int *__restrict__ poff,
+                                       int natom, const ProdTerm *__restrict__ terms, int nterms,
+                                       int Nr, double *out) {
+  const int total = poff[natom];
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  int a = 0;
+  while (poff[a + 1] <= idx) ++a;
+  const int j = idx - poff[a], npts = np[a];
+  // (lm, point) rows of this atom in each set: atoms are stored one after
+  // the other, N rows of npts points each
+  const double *g1 = f1 + (size_t)N1 * poff[a] + j;
+  const double *g2 = f2 + (size_t)N2 * poff[a] + j;
+  double *o = out + (size_t)Nr * poff[a] + j;
+  for (int t = 0; t < nterms; ++t) {
+    const ProdTerm T = terms[t];
+    double s = 0.0;
+    if (T.a < N1 && T.b < N2) s += g1[(size_t)T.a * npts] * g2[(size_t)T.b * npts];
+    if (T.a != T.b && T.b < N1 && T.a < N2) s += g1[(size_t)T.b * npts] * g2[(size_t)T.a * npts];
+    o[(size_t)T.lm * npts] += T.c * s;
   }
 }
 
@@ -396,6 +510,103 @@ __global__ void bubbles_potential_kernel(const AtomTab *__restrict__ atoms,
     }
   }
 }
+// Gauss-Legendre nodes and weights on [-1, 1]: Newton's method on P_n from
+// the three-term recurrence, started at cos(pi (i - 1/4) / (n + 1/2)).
+void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// Expansion of products of real harmonics, Y_a Y_b = sum C_ab^LM Y_LM
+// (the table of YProduct_init, harmonic.F90:884-951), for a <= b < (lmax+1)^2
+// and L <= result_lmax.  Each coefficient is the projection
+//   C = (2L+1)/(4 pi) * int Y_a Y_b Y_LM dOmega
+// (the Racah-normalised Y_LM have norm 4 pi/(2L+1)), by a Gauss-Legendre x
+// trapezoid product rule exact for the polynomial degrees involved.  Only
+// the (L, M) that the parity and m selection rules allow are projected.
+// Unless `complete`, the reference's term set is kept: its enumeration
+// (harmonic.F90:914-926) leaves out every term with L < |m1 - m2|, whose
+// content then stays in the cube part of a product.
+std::vector<ProdTerm> product_table(int lmax, int result_lmax, bool complete) {
+  const int deg = 2 * lmax + result_lmax;
+  const int nz = deg / 2 + 2, nphi = deg + 2;
+  std::vector<double> zx, zw;
+  gauss_legendre(nz, zx, zw);
+  const int L = std::max(lmax, result_lmax), NY = (L + 1) * (L + 1);
+  std::vector<double> Y((size_t)nz * nphi * NY), W((size_t)nz * nphi);
+  for (int i = 0; i < nz; ++i)
+    for (int j = 0; j < nphi; ++j) {
+      const double st = std::sqrt(1.0 - zx[i] * zx[i]), ph = 2.0 * M_PI * j / nphi;
+      double *y = &Y[((size_t)i * nphi + j) * NY];
+      unit_harmonics(L, st * std::cos(ph), st * std::sin(ph), zx[i],
+                     [&](int lm, double v) { y[lm] = v; });
+      W[(size_t)i * nphi + j] = zw[i] * 2.0 * M_PI / nphi;
+    }
+  const size_t nodes = (size_t)nz * nphi;
+  std::vector<double> P(nodes);
+  std::vector<ProdTerm> out;
+  const int N = (lmax + 1) * (lmax + 1);
+  for (int a = 0; a < N; ++a) {
+    const int l1 = (int)std::sqrt((double)a), m1 = a - l1 * (l1 + 1);
+    for (int b = a; b < N; ++b) {
+      const int l2 = (int)std::sqrt((double)b), m2 = b - l2 * (l2 + 1);
+      for (size_t q = 0; q < nodes; ++q) P[q] = Y[q * NY + a] * Y[q * NY + b] * W[q];
+      const int ms[4] = {std::abs(m1 - m2), -std::abs(m1 - m2), std::abs(m1 + m2),
+                         -std::abs(m1 + m2)};
+      for (int l = std::abs(l1 - l2); l <= std::min(l1 + l2, result_lmax); l += 2) {
+        if (!complete && l < std::abs(m1 - m2)) continue;
+        for (int e = 0; e < 4; ++e) {
+          const int m = ms[e];
+          bool dup = std::abs(m) > l;
+          for (int f = 0; f < e; ++f) dup = dup || ms[f] == m;
+          if (dup) continue;
+          double c = 0.0;
+          for (size_t q = 0; q < nodes; ++q) c += P[q] * Y[q * NY + l * (l + 1) + m];
+          c *= (2.0 * l + 1.0) / (4.0 * M_PI);
+          if (std::fabs(c) > 1e-13) out.push_back({a, b, l * (l + 1) + m, 0, c});
+        }
+      }
+    }
+  }
+  return out;
+}
+
+// Same atoms (centres) and the same radial grids: the product routines share
+// every atom's radial cell between the sets.
+bool same_layout(const dage_bubbles *x, const dage_bubbles *y) {
+  if (x->natom != y->natom || x->nlip != y->nlip || x->centers != y->centers) return false;
+  for (int a = 0; a < x->natom; ++a)
+    if (x->radial[a].ncell != y->radial[a].ncell || x->scales[a] != y->scales[a]) return false;
+  return true;
+}
+
 }  // namespace
 }  // namespace dage
 
@@ -473,6 +684,117 @@ int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out) {
   // the potential is a bubble set of its own (k = 0) on the same centres and grids
   return dage_bubbles_create(in->natom, in->centers.data(), in->radial.data(), in->lmax, 0,
                              V.data(), out);
+}
+
+int dage_bubbles_multiply(const dage_bubbles *x, const dage_bubbles *y, unsigned flags,
+                          dage_bubbles **out) {
+  clear_error();
+  if (!x || !y || !out) return fail(DAGE_E_INVALID, "null argument");
+  *out = nullptr;
+  if (!same_layout(x, y))
+    return fail(DAGE_E_UNSUPPORTED, "bubble product: the sets need the same atoms and radial grids");
+  const int lr = x->lmax + y->lmax;
+  if (lr > 12) return fail(DAGE_E_INVALID, "bubble product: lmax1 + lmax2 > 12");
+  DAGE_CUDA_TRY(cudaSetDevice(x->device));
+  const std::vector<ProdTerm> terms =
+      product_table(std::max(x->lmax, y->lmax), lr, (flags & DAGE_PRODUCT_COMPLETE) != 0);
+  const int Nr = (lr + 1) * (lr + 1);
+  std::vector<int> poff(x->natom + 1, 0), np(x->natom);
+  for (int a = 0; a < x->natom; ++a) {
+    np[a] = x->radial[a].ncell * (x->nlip - 1) + 1;
+    poff[a + 1] = poff[a] + np[a];
+  }
+  const size_t nout = (size_t)Nr * poff[x->natom];
+  DevBuf d_terms, d_np, d_poff, d_out;
+  DAGE_TRY(d_terms.alloc(sizeof(ProdTerm) * std::max<size_t>(terms.size(), 1)));
+  DAGE_TRY(d_np.alloc(sizeof(int) * np.size()));
+  DAGE_TRY(d_poff.alloc(sizeof(int) * poff.size()));
+  DAGE_TRY(d_out.alloc(sizeof(double) * nout));
+  DAGE_CUDA_TRY(cudaMemcpy(d_terms.ptr, terms.data(), sizeof(ProdTerm) * terms.size(),
+                           cudaMemcpyHostToDevice));
+  DAGE_CUDA_TRY(cudaMemcpy(d_np.ptr, np.data(), sizeof(int) * np.size(), cudaMemcpyHostToDevice));
+  DAGE_CUDA_TRY(cudaMemcpy(d_poff.ptr, poff.data(), sizeof(int) * poff.size(), cudaMemcpyHostToDevice));
+  DAGE_CUDA_TRY(cudaMemset(d_out.ptr, 0, sizeof(double) * nout));
+  const int total = poff[x->natom];
+  bubbles_product_kernel<<<(total + 127) / 128, 128>>>(
+      x->fraw.as<double>(), x->N, y->fraw.as<double>(), y->N, d_np.as<int>(), d_poff.as<int>(),
+      x->natom, d_terms.as<ProdTerm>(), (int)terms.size(), Nr, d_out.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  std::vector<double> prod(nout);
+  DAGE_CUDA_TRY(cudaMemcpy(prod.data(), d_out.ptr, sizeof(double) * nout, cudaMemcpyDeviceToHost));
+  return dage_bubbles_create(x->natom, x->centers.data(), x->radial.data(), lr, x->k + y->k,
+                             prod.data(), out);
+}
+
+int dage_product_table(int lmax, int result_lmax, unsigned flags, int cap, int *a, int *b, int *lm,
+                       double *c, int *nterms) {
+  clear_error();
+  if (!nterms || lmax < 0 || lmax > 12 || result_lmax < 0 || result_lmax > 24)
+    return fail(DAGE_E_INVALID, "need 0 <= lmax <= 12, 0 <= result_lmax <= 24");
+  const std::vector<ProdTerm> t = product_table(lmax, result_lmax, (flags & DAGE_PRODUCT_COMPLETE) != 0);
+  *nterms = (int)t.size();
+  if (cap < (int)t.size() || !a || !b || !lm || !c) return 0;
+  for (size_t i = 0; i < t.size(); ++i) {
+    a[i] = t[i].a;
+    b[i] = t[i].b;
+    lm[i] = t[i].lm;
+    c[i] = t[i].c;
+  }
+  return 0;
+}
+
+int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, const dage_bubbles *b1,
+                             const double *cube2, const dage_bubbles *b2, const dage_bubbles *br,
+                             double *out, unsigned flags) {
+  clear_error();
+  if (!grid || !cube1 || !cube2 || !out) return fail(DAGE_E_INVALID, "null argument");
+  const dage_bubbles *sets[3] = {b1, b2, br};
+  const dage_bubbles *ref = nullptr;
+  for (const dage_bubbles *s : sets)
+    if (s) {
+      if (ref && !same_layout(ref, s))
+        return fail(DAGE_E_UNSUPPORTED,
+                    "function product: the bubble sets need the same atoms and radial grids");
+      if (!ref) ref = s;
+    }
+  Axis ax[3];
+  for (int d = 0; d < 3; ++d) DAGE_TRY(make_axis(grid[d], ax[d]));
+  const size_t n = (size_t)ax[0].n() * ax[1].n() * ax[2].n();
+  DevBuf pts[3], s1, s2, so;
+  for (int d = 0; d < 3; ++d) {
+    DAGE_TRY(pts[d].alloc(sizeof(double) * ax[d].n()));
+    DAGE_CUDA_TRY(cudaMemcpy(pts[d].ptr, ax[d].points.data(), sizeof(double) * ax[d].n(),
+                             cudaMemcpyHostToDevice));
+  }
+  const double *d1 = cube1, *d2 = cube2;
+  double *dout = out;
+  if (!(flags & DAGE_DEVICE_PTRS)) {
+    DAGE_TRY(s1.alloc(sizeof(double) * n));
+    DAGE_TRY(s2.alloc(sizeof(double) * n));
+    DAGE_TRY(so.alloc(sizeof(double) * n));
+    DAGE_CUDA_TRY(cudaMemcpy(s1.ptr, cube1, sizeof(double) * n, cudaMemcpyHostToDevice));
+    DAGE_CUDA_TRY(cudaMemcpy(s2.ptr, cube2, sizeof(double) * n, cudaMemcpyHostToDevice));
+    d1 = s1.as<double>();
+    d2 = s2.as<double>();
+    dout = so.as<double>();
+  }
+  int lmax = 0;
+  for (const dage_bubbles *s : sets)
+    if (s) lmax = std::max(lmax, s->lmax);
+  auto coef = [&](const dage_bubbles *s) { return s ? s->coef.as<double>() : nullptr; };
+  auto rows = [&](const dage_bubbles *s) { return s ? s->N : 0; };
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
+  function_product_kernel<<<blocks, 256>>>(
+      ref ? ref->atoms.as<AtomTab>() : nullptr, ref ? ref->natom : 0,
+      ref ? ref->celld.as<double>() : nullptr, ref ? ref->hcell.as<double>() : nullptr, coef(b1),
+      rows(b1), coef(b2), rows(b2), coef(br), rows(br), lmax, ref ? ref->nlip : 7,
+      ref ? ref->first : 0.0, pts[0].as<double>(), ax[0].n(), pts[1].as<double>(), ax[1].n(),
+      pts[2].as<double>(), ax[2].n(), d1, d2, dout);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  if (!(flags & DAGE_DEVICE_PTRS))
+    DAGE_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  DAGE_CUDA_TRY(cudaDeviceSynchronize());
+  return 0;
 }
 
 int dage_bubbles_get_f(const dage_bubbles *b, double *f) {

@@ -547,6 +547,21 @@ class Bubbles:
             o += N * npts
         return out
 
+    def multiply(self, other: "Bubbles", complete: bool = False) -> "Bubbles":
+        """Radial product with another bubble set on the same atoms and radial
+        grids (BubblesMultiplier_multiply, bubbles.F90:3567-3690): lmax and k
+        add.  ``complete`` also keeps the terms with L < |m1 - m2| that the
+        reference's product table (harmonic.F90:914-926) leaves out."""
+        h = ctypes.c_void_p()
+        check(load().dage_bubbles_multiply(self._h, other._h,
+                                           _capi.DAGE_PRODUCT_COMPLETE if complete else 0,
+                                           ctypes.byref(h)))
+        res = Bubbles._wrap(h, self)
+        res.lmax = self.lmax + other.lmax
+        return res
+
+    __mul__ = multiply
+
     def inject(self, grid: Grid3D, cube=None, lmin: int = 0, factor: float = 1.0):
         """cube += factor * bubbles at the grid points; returns the cube."""
         n = int(np.prod(grid.shape))
@@ -557,3 +572,24 @@ class Bubbles:
         check(load().dage_bubbles_inject(self._h, g, lmin, float(factor), p,
                                          _capi.DAGE_DEVICE_PTRS if dev else 0))
         return cube
+
+
+def multiply(grid: Grid3D, cube1, cube2, bubbles1: Bubbles | None = None,
+             bubbles2: Bubbles | None = None, result_bubbles: Bubbles | None = None, out=None):
+    """Cube part of the product of two functions (cube + bubbles each), as
+    Function3D_multiply (function3d.F90:1097-1409) forms it:
+    out = (cube1 + bubbles1)(cube2 + bubbles2) - result_bubbles, in one GPU
+    pass.  ``result_bubbles`` is normally ``bubbles1 * bubbles2``."""
+    n = int(np.prod(grid.shape))
+    if out is None:
+        out = cube1.new_empty(cube1.shape) if hasattr(cube1, "is_cuda") else np.zeros(grid.shape, order="F")
+    p1, dev1 = _ptr(cube1, n)
+    p2, dev2 = _ptr(cube2, n)
+    po, devo = _ptr(out, n)
+    if not (dev1 == dev2 == devo):
+        raise ValueError("cubes must all be host arrays or all CUDA tensors")
+    h = lambda b: b._h if b is not None else None
+    check(load().dage_function3d_multiply(grid.c(), p1, h(bubbles1), p2, h(bubbles2),
+                                          h(result_bubbles), po,
+                                          _capi.DAGE_DEVICE_PTRS if dev1 else 0))
+    return out

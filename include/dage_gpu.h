@@ -42,6 +42,7 @@ extern "C" {
 #define DAGE_NO_CODA 4u       /* skip the coda term for this call */
 #define DAGE_ACCUMULATE 8u    /* V += result instead of V = result */
 #define DAGE_NO_GRAPH 16u     /* batch apply: launch the pipeline directly, no CUDA graph */
+#define DAGE_PRODUCT_COMPLETE 32u /* bubble product: also the terms the reference table omits */
 
 /* operator precisions */
 #define DAGE_FP64 0            /* FP64 everywhere: the drop-in */
@@ -267,6 +268,35 @@ int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out);
 /* Copies the radial values of a bubble set (as given at creation: per atom,
  * (lmax+1)^2 functions of the atom's radial points) to host memory. */
 int dage_bubbles_get_f(const dage_bubbles *b, double *f);
+
+/* Product of two bubble sets on the same atoms and radial grids
+ * (BubblesMultiplier_multiply, option (2), src/bubbles/bubbles.F90:3567-3690;
+ * Bubble_product_kernel, src/bubbles/bubbles_multiplier.cu:65-106): a new set
+ * with lmax = lmax_x + lmax_y (<= 12) and k = k_x + k_y whose radial functions
+ * are sum_{a<=b} C_ab^LM (x_a y_b + x_b y_a [a != b]), C the real-harmonic
+ * product coefficients of YProduct (src/bubbles/harmonic.F90:884-1089).  By
+ * default the reference's term set is kept (it leaves out terms with
+ * L < |m1 - m2|); DAGE_PRODUCT_COMPLETE includes them. */
+int dage_bubbles_multiply(const dage_bubbles *x, const dage_bubbles *y, unsigned flags,
+                          dage_bubbles **out);
+
+/* The real-harmonic product table the bubble product uses (host only, no
+ * GPU call): Y_a Y_b = sum c Y_lm for a <= b < (lmax+1)^2, l <= result_lmax
+ * (YProduct_init, src/bubbles/harmonic.F90:884-951).  Sets *nterms; fills
+ * a, b, lm, c when cap >= *nterms. */
+int dage_product_table(int lmax, int result_lmax, unsigned flags, int cap, int *a, int *b, int *lm,
+                       double *c, int *nterms);
+
+/* Cube part of a function product (Function3D_multiply,
+ * src/bubbles/function3d.F90:1097-1409; Function3DMultiplier::multiply,
+ * src/bubbles/bubbles_cuda.cu:3533-3690) in one kernel:
+ *   out = (cube1 + b1)(cube2 + b2) - br        at every point of `grid`
+ * Any of b1, b2, br may be NULL; those given must share atoms and radial
+ * grids.  `out` may alias cube1 or cube2.  DAGE_DEVICE_PTRS: the cubes are
+ * device pointers. */
+int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, const dage_bubbles *b1,
+                             const double *cube2, const dage_bubbles *b2, const dage_bubbles *br,
+                             double *out, unsigned flags);
 
 int dage_bubbles_destroy(dage_bubbles *b);
 

@@ -804,3 +804,116 @@ def bubbles_coulomb_potential(ncell, cell_scales, lmax, f, k=0, nlip=7):
             lm = l * (l + 1) + m
             V[lm] = 4 * np.pi / (2 * l + 1) * (r1 * outwards(f[lm] * r2) + r3 * inwards(f[lm] * r4))
     return V
+
+
+# ---------------------------------------------------------------------------
+# Products of functions (the density producer)
+# ---------------------------------------------------------------------------
+def _clebsch_gordan(l1, m1, l2, m2, l, m):
+    """<l1 m1 l2 m2 | l m> by Racah's closed formula (harmonic.F90:991-1031)."""
+    from math import factorial as F, sqrt
+    if l < abs(l1 - l2) or l > l1 + l2 or abs(m1) > l1 or abs(m2) > l2 or abs(m) > l \
+            or m != m1 + m2:
+        return 0.0
+    pre = sqrt((2 * l + 1.0) / F(l1 + l2 + l + 1) * F(l1 + l2 - l) * F(l2 + l - l1)
+               * F(l + l1 - l2) * F(l1 + m1) * F(l1 - m1) * F(l2 + m2) * F(l2 - m2)
+               * F(l + m) * F(l - m))
+    s = 0.0
+    for kk in range(max(l1 + m2 - l, l2 - m1 - l, 0), min(l1 + l2 - l, l1 - m1, l2 + m2) + 1):
+        t = (F(l1 + l2 - l - kk) * F(l - l1 - m2 + kk) * F(l - l2 + m1 + kk)
+             * F(l1 - m1 - kk) * F(l2 + m2 - kk) * F(kk))
+        s += (-1.0 if kk % 2 else 1.0) / t
+    return pre * s
+
+
+def _real_product_coeff(l1, m1, l2, m2, l, m):
+    """Coefficient of Y_lm in Y_l1m1 * Y_l2m2 for the Racah-normalised real
+    harmonics (prod_coeff, harmonic.F90:1034-1089): a product of two
+    Clebsch-Gordan coefficients with the real-harmonic phase rule."""
+    sgn = lambda v: 1 if v >= 0 else -1  # Fortran sign(1, v)
+    cp = lambda v: 0.5 if v < 0 else float(v)
+    cm = lambda v: v - 0.5 if v < 0 else 0.0
+    if (l - l1 - l2) % 2 or sgn(m1) * sgn(m2) * sgn(m) < 0:
+        return 0.0
+    if m == m1 + m2:
+        f, a, b = cp(m1) + cp(m2) - cp(m), m1, m2
+    elif m == m1 - m2:
+        f, a, b = cp(m1) + cm(m2) - cp(m), m1, -m2
+    elif m == -m1 + m2:
+        f, a, b = cm(m1) + cp(m2) - cp(m), -m1, m2
+    elif m == -m1 - m2:
+        f, a, b = cm(m1) + cm(m2) - cp(m), -m1, -m2
+    else:
+        return 0.0
+    # Fortran nint of a REAL32 half-integer rounds away from zero
+    e = int(np.floor(abs(f) + 0.5)) * (1 if f >= 0 else -1)
+    res = _clebsch_gordan(l1, 0, l2, 0, l, 0) * _clebsch_gordan(l1, a, l2, b, l, m) * (-1.0) ** e
+    if m1 * m2 * m != 0:
+        res /= np.sqrt(2.0)
+    return res
+
+
+def yproduct(lmax, result_lmax=None):
+    """YProduct_init (harmonic.F90:884-951): for every unordered pair of
+    harmonic indices a <= b (lm = l(l+1)+m, 0-based) the list of
+    (result index, coefficient) with Y_a Y_b = sum C Y_LM."""
+    if result_lmax is None:
+        result_lmax = 2 * lmax
+    table = {}
+    for l1 in range(lmax + 1):
+        for m1 in range(-l1, l1 + 1):
+            for l2 in range(l1, lmax + 1):
+                for m2 in range(m1 if l1 == l2 else -l2, l2 + 1):
+                    sgn = (1 if m1 >= 0 else -1) * (1 if m2 >= 0 else -1)
+                    terms = []
+                    for l in range(abs(l1 - l2), min(result_lmax, l1 + l2) + 1, 2):
+                        m = sgn * abs(m1 - m2)
+                        if abs(m) > l:
+                            continue
+                        terms.append((l * (l + 1) + m, _real_product_coeff(l1, m1, l2, m2, l, m)))
+                        if m1 * m2 != 0 and (sgn == 1 or m1 + m2 != 0):
+                            m = sgn * abs(m1 + m2)
+                            if abs(m) > l:
+                                continue
+                            terms.append((l * (l + 1) + m,
+                                          _real_product_coeff(l1, m1, l2, m2, l, m)))
+                    table[(l1 * (l1 + 1) + m1, l2 * (l2 + 1) + m2)] = terms
+    return table
+
+
+def bubbles_multiply(f1, lmax1, f2, lmax2):
+    """Radial product of two bubbles on one atom (Bubble_product_kernel,
+    bubbles_multiplier.cu:65-106, option (2) of BubblesMultiplier_multiply,
+    bubbles.F90:3567-3690): result ((lmax1+lmax2+1)^2, npts) with
+    r_LM = sum_{a<=b} C_ab^LM (f1_a f2_b + f1_b f2_a [a != b]); k adds."""
+    f1 = np.asarray(f1, dtype=np.float64)
+    f2 = np.asarray(f2, dtype=np.float64)
+    N1, N2 = (lmax1 + 1) ** 2, (lmax2 + 1) ** 2
+    lr = lmax1 + lmax2
+    out = np.zeros(((lr + 1) ** 2, f1.shape[1]))
+    for (a, b), terms in yproduct(max(lmax1, lmax2), lr).items():
+        s = np.zeros(f1.shape[1])
+        if a < N1 and b < N2:
+            s = s + f1[a] * f2[b]
+        if a != b and b < N1 and a < N2:
+            s = s + f1[b] * f2[a]
+        for LM, C in terms:
+            out[LM] += C * s
+    return out
+
+
+def function3d_multiply(grid: Grid3D, cube1, cube2, bubbles1=None, bubbles2=None,
+                        result_bubbles=None):
+    """Cube part of Function3D_multiply (function3d.F90:1097-1409, the
+    non-CUDA branch at :1372-1390): (cube1 + bubbles1)(cube2 + bubbles2)
+    - result_bubbles on the grid.  Each bubbles argument is a dict of
+    bubbles_inject keyword arguments (centers, ncells, cell_scales, lmax, f, k)."""
+    def with_bubbles(cube, b, factor=1.0):
+        c = np.array(cube, dtype=np.float64, order="F", copy=True)
+        if b is not None:
+            bubbles_inject(grid=grid, cube=c, factor=factor, **b)
+        return c
+    out = with_bubbles(cube1, bubbles1) * with_bubbles(cube2, bubbles2)
+    if result_bubbles is not None:
+        bubbles_inject(grid=grid, cube=out, factor=-1.0, **result_bubbles)
+    return out

@@ -33,3 +33,16 @@ def dage():
 
     dage_b200.load()
     return dage_b200
+
+
+@pytest.fixture(scope="session")
+def dage_host():
+    """The package with its library loaded, for host-only entry points
+    (no GPU call)."""
+    from dage_b200 import build
+
+    build.build()
+    import dage_b200
+
+    dage_b200.load()
+    return dage_b200
