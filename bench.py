@@ -494,24 +494,29 @@ def _gauss_cube(dev, n_cell, step, q, a, c):
     return density_torch(axis_points(n_cell, step), q, a, c, dev)
 
 
-def _molecule_bubbles(dage, rng):
+def _molecule_bubbles(dage, rng, nsets=1):
     """20 atoms uniform in a 30 bohr box, each a radial LIP grid of 199 points
     (33 cells, cell ends log-spaced on [1e-5, 15] bohr) with lmax 2 radial
     functions c r^l e^(-zeta r), c ~ U[-1, 1], zeta ~ U[0.5, 3]; and the
-    301^3 cube (step 0.1) they are injected into."""
+    301^3 cube (step 0.1) they are injected into.  nsets > 1: that many
+    bubble sets (orbitals) on the same atoms, returned as a list."""
     gcube = dage.Grid3D.cube(-15.0, 50, 0.1)
     edges = np.concatenate([[0.0], 1e-5 * (15.0 / 1e-5) ** (np.arange(33) / 32)])
     rad = dage.Grid1D(0.0, 33, 7, 1, np.diff(edges) / 6)
     r = rad.coordinates()
     centers = rng.uniform(-15, 15, (20, 3))
-    f = []
-    for _ in range(20):
-        fa = np.zeros((9, len(r)))
-        for l in range(3):
-            for m in range(-l, l + 1):
-                fa[l * (l + 1) + m] = rng.uniform(-1, 1) * r ** l * np.exp(-rng.uniform(0.5, 3) * r)
-        f.append(fa)
-    return dage.Bubbles(centers, [rad] * 20, f, 2), gcube
+    sets = []
+    for _ in range(nsets):
+        f = []
+        for _ in range(20):
+            fa = np.zeros((9, len(r)))
+            for l in range(3):
+                for m in range(-l, l + 1):
+                    fa[l * (l + 1) + m] = (rng.uniform(-1, 1) * r ** l
+                                           * np.exp(-rng.uniform(0.5, 3) * r))
+            f.append(fa)
+        sets.append(dage.Bubbles(centers, [rad] * 20, f, 2))
+    return (sets[0] if nsets == 1 else sets), gcube
 
 
 def run_workload(args, world, rank, local):
@@ -588,6 +593,41 @@ def run_workload(args, world, rank, local):
               {"workload": wl, "points_per_axis": 301, "step_bohr": 0.1, "atoms": 20,
                "lmax": 2, "radial_points": 199, "seed": SEED}, clocks, 1,
               {"hbm_GBps": 16.0 * n / ms / 1e6})
+    elif wl == "density_product_301":
+        # Function3D_multiply of two orbitals (cube + lmax 2 bubbles each, 20
+        # atoms) at 301^3: out = (c1 + B1)(c2 + B2) - B1*B2, B1*B2 lmax 4
+        rng = np.random.default_rng(SEED)
+        (b1, b2), gcube = _molecule_bubbles(dage, rng, nsets=2)
+        br = b1 * b2
+        n = 301 ** 3
+        gen = torch.Generator(device=dev).manual_seed(SEED)
+        c1 = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
+        c2 = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
+        out = torch.empty_like(c1)
+        clk.start()
+        ms = _timed(lambda: dage.multiply(gcube, c1, c2, b1, b2, br, out=out), args.steps,
+                    args.warmup, sync)
+        clocks = clk.stop()
+        # the same product as separate passes (the reference GPU path's
+        # structure: inject B1, inject B2, multiply, de-inject B1*B2)
+        t1, t2 = torch.empty_like(c1), torch.empty_like(c2)
+
+        def unfused():
+            t1.copy_(c1)
+            t2.copy_(c2)
+            b1.inject(gcube, cube=t1)
+            b2.inject(gcube, cube=t2)
+            torch.mul(t1, t2, out=t1)
+            br.inject(gcube, cube=t1, factor=-1.0)
+
+        ms_unfused = _timed(unfused, max(1, args.steps // 2), 1, sync)
+        err = float((t1 - out).abs().max() / out.abs().max())
+        _line(args, world, "Function3D product Mpts/s @301^3 (20 atoms, bubbles lmax 2 x 2 -> 4)",
+              n / ms / 1e3, "Mpts/s", ms, "f64",
+              {"workload": wl, "points_per_axis": 301, "step_bohr": 0.1, "atoms": 20,
+               "lmax": [2, 2, 4], "radial_points": 199, "seed": SEED}, clocks, 1,
+              {"hbm_GBps": 24.0 * n / ms / 1e6,
+               "separate_passes": {"ms": ms_unfused, "launches": 4, "max_rel_diff": err}})
     elif wl in ("gbfmm_batch_256", "helmholtz_step_301"):
         rng = np.random.default_rng(SEED)
         if wl == "gbfmm_batch_256":
@@ -671,7 +711,8 @@ def main():
                     help="cells per axis (80 -> 481^3, the headline workload)")
     ap.add_argument("--workload", default="coulomb_cube_481",
                     choices=["coulomb_cube_481", "coulomb_cube_121", "gbfmm_241",
-                             "gbfmm_batch_256", "helmholtz_step_301", "bubbles_inject_301"],
+                             "gbfmm_batch_256", "helmholtz_step_301", "bubbles_inject_301",
+                             "density_product_301"],
                     help="coulomb_cube_481 is the headline line; the others time the other "
                          "configurations of the path")
     args = ap.parse_args()

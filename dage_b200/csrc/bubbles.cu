@@ -74,6 +74,66 @@ __host__ __device__ __forceinline__ void unit_harmonics(int lmax, double x, doub
   }
 }
 
+// The same recursion for a compile-time lmax, fully unrolled, so that every
+// callback sees a constant lm.
+template <int LS, class F>
+__device__ __forceinline__ void unit_harmonics_fixed(double x, double y, double z, F &&f) {
+  f(0, 1.0);
+  if constexpr (LS > 0) {
+    double p2 = 1.0, p1 = z;
+    f(2, z);
+#pragma unroll
+    for (int l = 2; l <= LS; ++l) {
+      double cur = (2.0 * l - 1.0) * (z * p1) - sqrt((double)((l - 1) * (l - 1))) * p2;
+      cur = cur * (1.0 / sqrt((double)(l * l)));
+      f(l * (l + 1), cur);
+      p2 = p1;
+      p1 = cur;
+    }
+    double top = x, bot = y;
+#pragma unroll
+    for (int mm = 1; mm <= LS; ++mm) {
+      if (mm >= 2) {
+        const double c = sqrt(1.0 - 0.5 / mm);
+        const double nb = c * (top * y + bot * x);
+        const double nt = c * (top * x - bot * y);
+        top = nt;
+        bot = nb;
+      }
+      f(mm * (mm + 1) + mm, top);
+      f(mm * (mm + 1) - mm, bot);
+#pragma unroll
+      for (int sg = 0; sg < 2; ++sg) {
+        const int m = sg ? -mm : mm;
+        double q2 = 0.0, q1 = sg ? bot : top;
+#pragma unroll
+        for (int l = mm + 1; l <= LS; ++l) {
+          double cur = (2.0 * l - 1.0) * (q1 * z);
+          if (l - mm > 1) cur = cur - sqrt((l + m - 1.0) * (l - m - 1.0)) * q2;
+          cur = (1.0 / sqrt(1.0 * (l - m) * (l + m))) * cur;
+          f(l * (l + 1) + m, cur);
+          q2 = q1;
+          q1 = cur;
+        }
+      }
+    }
+  }
+}
+
+// A 7-point cell's polynomial (coefficients highest power first, padded to
+// 8) at t, the coefficients read as four 16-byte loads.
+__device__ __forceinline__ double horner7(const double *c, double t) {
+  const double2 *q = reinterpret_cast<const double2 *>(c);
+  const double2 a = __ldg(q), b = __ldg(q + 1), e = __ldg(q + 2), g = __ldg(q + 3);
+  double v = a.x;
+  v = v * t + a.y;
+  v = v * t + b.x;
+  v = v * t + b.y;
+  v = v * t + e.x;
+  v = v * t + e.y;
+  return v * t + g.x;
+}
+
 // LIP values of one cell -> monomial coefficients in the cell coordinate
 // (highest power first), padded to 8 per (cell, lm).
 __global__ void bubble_coeffs_kernel(const double *__restrict__ rf, const int *__restrict__ atom_np,
@@ -98,11 +158,36 @@ __global__ void bubble_coeffs_kernel(const double *__restrict__ rf, const int *_
   }
 }
 
+// Cube points in 8 x 8 x 4 bricks, one brick per 256-thread block and step:
+// a warp holds 8 x 4 neighbouring (x, y) points, so its lanes mostly share
+// each atom's radial cell (one coefficient block, little divergence in the
+// cell search), and a block's points are 0.8 x 0.8 x 0.4 cells apart at most
+// instead of a 256-point line.  Requires blockDim.x == 256.
+struct BrickGrid {
+  int nx, ny, nz, nbx, nby;
+  long long count;
+  __device__ BrickGrid(int nx_, int ny_, int nz_)
+      : nx(nx_), ny(ny_), nz(nz_), nbx((nx_ + 7) / 8), nby((ny_ + 7) / 8),
+        count((long long)((nx_ + 7) / 8) * ((ny_ + 7) / 8) * ((nz_ + 3) / 4)) {}
+  __device__ bool point(long long bk, int &ix, int &iy, int &iz) const {
+    const int bx = (int)(bk % nbx);
+    const long long r = bk / nbx;
+    const int by = (int)(r % nby), bz = (int)(r / nby);
+    ix = bx * 8 + (threadIdx.x & 7);
+    iy = by * 8 + ((threadIdx.x >> 3) & 7);
+    iz = bz * 4 + (threadIdx.x >> 6);
+    return ix < nx && iy < ny && iz < nz;
+  }
+};
+
 struct AtomTab {
   double cx, cy, cz, rmax;
   int cell0, ncell;
 };
 
+// LS >= 0: lmax <= LS and 7-point cells (harmonics unrolled, 16-byte
+// coefficient loads); LS = -1: any lmax and cell size.
+template <int LS>
 __global__ void __launch_bounds__(256)
     inject_kernel(const AtomTab *__restrict__ atoms, int natom, const double *__restrict__ celld,
                   const double *__restrict__ hcell, const double *__restrict__ coef, int N,
@@ -112,13 +197,12 @@ __global__ void __launch_bounds__(256)
   __shared__ AtomTab sa[kMaxAtomsSmem];
   for (int a = threadIdx.x; a < natom && a < kMaxAtomsSmem; a += blockDim.x) sa[a] = atoms[a];
   __syncthreads();
-  const long long n = (long long)nx * ny * nz;
   const int lm0 = lmin * lmin;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % nx);
-    const long long r = i / nx;
-    const int iy = (int)(r % ny), iz = (int)(r / ny);
+  const BrickGrid B(nx, ny, nz);
+  for (long long bk = blockIdx.x; bk < B.count; bk += gridDim.x) {
+    int ix, iy, iz;
+    if (!B.point(bk, ix, iy, iz)) continue;
+    const long long i = ix + (long long)nx * (iy + (long long)ny * iz);
     const double px = xs[ix], py = ys[iy], pz = zs[iz];
     double acc = 0.0;
     for (int a = 0; a < natom; ++a) {
@@ -163,14 +247,22 @@ __global__ void __launch_bounds__(256)
         uy = dy * inv;
         uz = dz * inv;
       }
-      unit_harmonics(lmax, ux, uy, uz, [&](int lm, double Y) {
-        if (lm < lm0) return;
-        if (at_centre && lm > 0) return;
-        const double *c = cf + (size_t)lm * 8;
-        double v = c[0];
-        for (int kk = 1; kk < nlip; ++kk) v = v * t + c[kk];
-        acc += v * Y;
-      });
+      if constexpr (LS >= 0) {
+        unit_harmonics_fixed<LS>(ux, uy, uz, [&](int lm, double Y) {
+          if (lm < lm0 || lm >= N) return;
+          if (at_centre && lm > 0) return;
+          acc += horner7(cf + (size_t)lm * 8, t) * Y;
+        });
+      } else {
+        unit_harmonics(lmax, ux, uy, uz, [&](int lm, double Y) {
+          if (lm < lm0) return;
+          if (at_centre && lm > 0) return;
+          const double *c = cf + (size_t)lm * 8;
+          double v = c[0];
+          for (int kk = 1; kk < nlip; ++kk) v = v * t + c[kk];
+          acc += v * Y;
+        });
+      }
     }
     cube[i] += factor * acc;
   }
@@ -201,6 +293,9 @@ __device__ __forceinline__ int radial_cell(const double *cd, int ncell, double d
 // The three bubble sets share atoms and radial grids, so every atom's
 // distance, radial cell, cell coordinate and harmonics are computed once per
 // point for all three; Ni = 0 marks an absent set.
+// LS >= 0: every set has lmax <= LS and 7-point cells (harmonics unrolled,
+// 16-byte coefficient loads); LS = -1: any lmax and cell size.
+template <int LS>
 __global__ void __launch_bounds__(256)
     function_product_kernel(const AtomTab *__restrict__ atoms, int natom,
                             const double *__restrict__ celld, const double *__restrict__ hcell,
@@ -213,12 +308,11 @@ __global__ void __launch_bounds__(256)
   __shared__ AtomTab sa[kMaxAtomsSmem];
   for (int a = threadIdx.x; a < natom && a < kMaxAtomsSmem; a += blockDim.x) sa[a] = atoms[a];
   __syncthreads();
-  const long long n = (long long)nx * ny * nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % nx);
-    const long long r = i / nx;
-    const int iy = (int)(r % ny), iz = (int)(r / ny);
+  const BrickGrid B(nx, ny, nz);
+  for (long long bk = blockIdx.x; bk < B.count; bk += gridDim.x) {
+    int ix, iy, iz;
+    if (!B.point(bk, ix, iy, iz)) continue;
+    const long long i = ix + (long long)nx * (iy + (long long)ny * iz);
     const double px = xs[ix], py = ys[iy], pz = zs[iz];
     double v1 = 0.0, v2 = 0.0, vr = 0.0;
     for (int a = 0; a < natom; ++a) {
@@ -239,17 +333,26 @@ __global__ void __launch_bounds__(256)
         uy = dy * inv;
         uz = dz * inv;
       }
-      auto horner = [&](const double *c) {
-        double v = c[0];
-        for (int kk = 1; kk < nlip; ++kk) v = v * t + c[kk];
-        return v;
-      };
-      unit_harmonics(lmax, ux, uy, uz, [&](int lm, double Y) {
-        if (at_centre && lm > 0) return;
-        if (lm < N1) v1 += horner(coef1 + (cell * N1 + lm) * 8) * Y;
-        if (lm < N2) v2 += horner(coef2 + (cell * N2 + lm) * 8) * Y;
-        if (lm < Nr) vr += horner(coefr + (cell * Nr + lm) * 8) * Y;
-      });
+      if constexpr (LS >= 0) {
+        unit_harmonics_fixed<LS>(ux, uy, uz, [&](int lm, double Y) {
+          if (at_centre && lm > 0) return;
+          if (lm < N1) v1 += horner7(coef1 + (cell * N1 + lm) * 8, t) * Y;
+          if (lm < N2) v2 += horner7(coef2 + (cell * N2 + lm) * 8, t) * Y;
+          if (lm < Nr) vr += horner7(coefr + (cell * Nr + lm) * 8, t) * Y;
+        });
+      } else {
+        auto horner = [&](const double *c) {
+          double v = c[0];
+          for (int kk = 1; kk < nlip; ++kk) v = v * t + c[kk];
+          return v;
+        };
+        unit_harmonics(lmax, ux, uy, uz, [&](int lm, double Y) {
+          if (at_centre && lm > 0) return;
+          if (lm < N1) v1 += horner(coef1 + (cell * N1 + lm) * 8) * Y;
+          if (lm < N2) v2 += horner(coef2 + (cell * N2 + lm) * 8) * Y;
+          if (lm < Nr) vr += horner(coefr + (cell * Nr + lm) * 8) * Y;
+        });
+      }
     }
     out[i] = (c1[i] + v1) * (c2[i] + v2) - vr;
   }
@@ -308,6 +411,24 @@ struct dage_bubbles {
   std::vector<std::vector<double>> scales;
   size_t nvals = 0;
 };
+
+namespace dage {
+namespace {
+void inject_dispatch(const dage_bubbles *b, int blocks, cudaStream_t s, int lmin, const double *xs,
+                     int nx, const double *ys, int ny, const double *zs, int nz, double factor,
+                     double *d_cube) {
+  auto go = [&](auto kernel) {
+    kernel<<<blocks, 256, 0, s>>>(b->atoms.as<AtomTab>(), b->natom, b->celld.as<double>(),
+                                  b->hcell.as<double>(), b->coef.as<double>(), b->N, b->lmax, lmin,
+                                  b->nlip, b->first, xs, nx, ys, ny, zs, nz, factor, d_cube);
+  };
+  if (b->nlip != 7 || b->lmax > 6) go(inject_kernel<-1>);
+  else if (b->lmax <= 2) go(inject_kernel<2>);
+  else if (b->lmax <= 4) go(inject_kernel<4>);
+  else go(inject_kernel<6>);
+}
+}  // namespace
+}  // namespace dage
 
 extern "C" {
 
@@ -432,10 +553,7 @@ int bubbles_inject_launch(const dage_bubbles *b, const double *xs, int nx, const
   if (!b || lmin < 0 || lmin > b->lmax) return fail(DAGE_E_INVALID, "bubbles or lmin");
   const size_t n = (size_t)nx * ny * nz;
   const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
-  inject_kernel<<<blocks, 256, 0, s>>>(b->atoms.as<AtomTab>(), b->natom, b->celld.as<double>(),
-                                       b->hcell.as<double>(), b->coef.as<double>(), b->N, b->lmax,
-                                       lmin, b->nlip, b->first, xs, nx, ys, ny, zs, nz, factor,
-                                       d_cube);
+  inject_dispatch(b, blocks, s, lmin, xs, nx, ys, ny, zs, nz, factor, d_cube);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -635,11 +753,8 @@ int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, do
     d_cube = staging.as<double>();
   }
   const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
-  inject_kernel<<<blocks, 256>>>(b->atoms.as<AtomTab>(), b->natom, b->celld.as<double>(),
-                                 b->hcell.as<double>(), b->coef.as<double>(), b->N, b->lmax, lmin,
-                                 b->nlip, b->first, b->xs.as<double>(), ax[0].n(),
-                                 b->ys.as<double>(), ax[1].n(), b->zs.as<double>(), ax[2].n(),
-                                 factor, d_cube);
+  inject_dispatch(b, blocks, 0, lmin, b->xs.as<double>(), ax[0].n(), b->ys.as<double>(),
+                  ax[1].n(), b->zs.as<double>(), ax[2].n(), factor, d_cube);
   DAGE_CUDA_TRY(cudaGetLastError());
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpy(cube, d_cube, sizeof(double) * n, cudaMemcpyDeviceToHost));
@@ -784,12 +899,19 @@ int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, con
   auto coef = [&](const dage_bubbles *s) { return s ? s->coef.as<double>() : nullptr; };
   auto rows = [&](const dage_bubbles *s) { return s ? s->N : 0; };
   const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
-  function_product_kernel<<<blocks, 256>>>(
-      ref ? ref->atoms.as<AtomTab>() : nullptr, ref ? ref->natom : 0,
-      ref ? ref->celld.as<double>() : nullptr, ref ? ref->hcell.as<double>() : nullptr, coef(b1),
-      rows(b1), coef(b2), rows(b2), coef(br), rows(br), lmax, ref ? ref->nlip : 7,
-      ref ? ref->first : 0.0, pts[0].as<double>(), ax[0].n(), pts[1].as<double>(), ax[1].n(),
-      pts[2].as<double>(), ax[2].n(), d1, d2, dout);
+  const int nlip = ref ? ref->nlip : 7;
+  auto go = [&](auto kernel) {
+    kernel<<<blocks, 256>>>(
+        ref ? ref->atoms.as<AtomTab>() : nullptr, ref ? ref->natom : 0,
+        ref ? ref->celld.as<double>() : nullptr, ref ? ref->hcell.as<double>() : nullptr,
+        coef(b1), rows(b1), coef(b2), rows(b2), coef(br), rows(br), lmax, nlip,
+        ref ? ref->first : 0.0, pts[0].as<double>(), ax[0].n(), pts[1].as<double>(), ax[1].n(),
+        pts[2].as<double>(), ax[2].n(), d1, d2, dout);
+  };
+  if (nlip != 7 || lmax > 6) go(function_product_kernel<-1>);
+  else if (lmax <= 2) go(function_product_kernel<2>);
+  else if (lmax <= 4) go(function_product_kernel<4>);
+  else go(function_product_kernel<6>);
   DAGE_CUDA_TRY(cudaGetLastError());
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
