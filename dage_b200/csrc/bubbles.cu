@@ -6,8 +6,9 @@
 // r = 0).  At creation each cell's LIP values are turned into monomial
 // coefficients in the cell coordinate (the reference's calc_cf,
 // src/bubbles/bubbles_cuda.cu:197-300), on the GPU, once per bubble set.  The
-// injection is ONE kernel over all atoms: every thread owns cube points,
-// loops over the atoms (centres, radial cell starts and steps staged in
+// injection is ONE kernel over all atoms: every thread owns cube points
+// (8 x 8 x 4 bricks per block, so a warp's lanes share radial cells), loops
+// over the atoms (centres, radial cell starts and steps staged in
 // shared memory), finds the radial cell by the same binary search as
 // Grid1D_get_icell (src/bubbles/grid.F90:1212-1245, valid for any radial
 // grid, not only the reference GPU path's closed-form cell index), evaluates
