@@ -569,6 +569,7 @@ namespace {
 // times the cell step, plus the running value at the cell boundary.
 // Negative powers are 0 at r = 0 (Bubbles_rpow).  Block = atom, thread = lm;
 // the outward integral is kept in V until the inward pass completes it.
+template <bool HELM>
 __global__ void bubbles_potential_kernel(const AtomTab *__restrict__ atoms,
                                          const double *__restrict__ hcell,
                                          const double *__restrict__ f,
@@ -576,7 +577,10 @@ __global__ void bubbles_potential_kernel(const AtomTab *__restrict__ atoms,
                                          const int *__restrict__ np, const int *__restrict__ foff,
                                          int lmax, int k, int nlip,
                                          const double *__restrict__ ints_out,
-                                         const double *__restrict__ ints_in, double *V) {
+                                         const double *__restrict__ ints_in,
+                                         const double *__restrict__ besi,
+                                         const double *__restrict__ besk, int total,
+                                         double kappa, double *V) {
   const int a = blockIdx.x, N = (lmax + 1) * (lmax + 1);
   const AtomTab A = atoms[a];
   int poff = 0;  // offset of this atom's points in rpts
@@ -588,6 +592,7 @@ __global__ void bubbles_potential_kernel(const AtomTab *__restrict__ atoms,
     while ((l + 1) * (l + 1) <= lm) ++l;
     const double *fl = f + foff[a] + (size_t)lm * npts;
     double *Vl = V + foff[a] + (size_t)lm * npts;
+    const double *Il = besi + (size_t)l * total + poff, *Kl = besk + (size_t)l * total + poff;
     auto rpow = [&](int p, int e) {
       if (e >= 0) {
         double v = 1.0;
@@ -599,36 +604,111 @@ __global__ void bubbles_potential_kernel(const AtomTab *__restrict__ atoms,
       for (int i = 0; i < -e; ++i) v *= r[p];
       return 1.0 / v;
     };
-    // outward pass: int_0^{r_p} f s^(l+2+k) ds
+    // integrands of the outward and inward integrals at point p
+    auto g_out = [&](int p) {
+      return HELM ? rpow(p, 2 + k) * Il[p] * fl[p] : fl[p] * rpow(p, l + 2 + k);
+    };
+    auto g_in_raw = [&](int p) {
+      return HELM ? rpow(p, 2 + k) * Kl[p] * fl[p] : fl[p] * rpow(p, 1 - l + k);
+    };
+    auto g_in = [&](int p) {
+      if (HELM && p == 0)  // extrapolate_first_nlip7: order 3 for l = 0, else 0
+        return l == 0 ? 3.0 * g_in_raw(1) - 3.0 * g_in_raw(2) + g_in_raw(3) : 0.0;
+      return g_in_raw(p);
+    };
+    // outward pass: int_0^{r_p} g_out
     Vl[0] = 0.0;
     for (int c = 0; c < A.ncell; ++c) {
       const int s0 = c * n;
       const double h = hcell[A.cell0 + c], base = Vl[s0];
       for (int j = 1; j <= n; ++j) {
         double acc = 0.0;
-        for (int i = 0; i <= n; ++i) acc += fl[s0 + i] * rpow(s0 + i, l + 2 + k) * ints_out[i * n + j - 1];
+        for (int i = 0; i <= n; ++i) acc += g_out(s0 + i) * ints_out[i * n + j - 1];
         Vl[s0 + j] = acc * h + base;
       }
     }
-    // inward pass: int_{r_p}^inf f s^(1-l+k) ds, combined point by point
-    const double pref = 4.0 * 3.141592653589793238 / (2 * l + 1);
+    // inward pass: int_{r_p}^inf g_in, combined point by point
+    const double pref = HELM ? 8.0 * kappa : 4.0 * 3.141592653589793238 / (2 * l + 1);
+    auto combine = [&](int p, double outv, double inv) {
+      return HELM ? pref * (Kl[p] * outv + Il[p] * inv)
+                  : pref * (rpow(p, -(l + 1)) * outv + rpow(p, l) * inv);
+    };
     double end = 0.0;  // the inward integral at the current cell's last point
-    Vl[npts - 1] = pref * (rpow(npts - 1, -(l + 1)) * Vl[npts - 1]);
+    Vl[npts - 1] = combine(npts - 1, Vl[npts - 1], 0.0);
     for (int c = A.ncell - 1; c >= 0; --c) {
       const int s0 = c * n;
       const double h = hcell[A.cell0 + c];
       double vals[8];
       for (int j = 0; j < n; ++j) {
         double acc = 0.0;
-        for (int i = 0; i <= n; ++i) acc += fl[s0 + i] * rpow(s0 + i, 1 - l + k) * ints_in[i * n + j];
+        for (int i = 0; i <= n; ++i) acc += g_in(s0 + i) * ints_in[i * n + j];
         vals[j] = acc * h + end;
       }
-      for (int j = 0; j < n; ++j)
-        Vl[s0 + j] = pref * (rpow(s0 + j, -(l + 1)) * Vl[s0 + j] + rpow(s0 + j, l) * vals[j]);
+      for (int j = 0; j < n; ++j) Vl[s0 + j] = combine(s0 + j, Vl[s0 + j], vals[j]);
       end = vals[0];
     }
   }
 }
+
+// i_l(kappa r), k_l(kappa r) for l <= lmax at every radial point (thread =
+// point): i_l by its power series for l = lmax, lmax - 1 and downward
+// recursion, k_l from k_0 = pi/2 e^-x/x, k_1 = pi/2 e^-x (x+1)/x^2 and upward
+// recursion (FirstModSphBesselCollection / SecondModSphBesselCollection,
+// helmholtz3d.F90:851-1060, there in 128-bit arithmetic); both 0 except
+// i_0 = 1 at x = 0.  Output rows [l][point].
+__device__ double besseli_series(double x, int n) {
+  double pref = 1.0;
+  for (int j = 1; j <= n; ++j) pref *= x / (2 * j + 1);
+  const double a = 0.5 * x * x;
+  double term = 1.0, sum = 1.0;
+  for (int i = 1; i < 300; ++i) {
+    term *= a / (i * (2.0 * n + 2 * i + 1));
+    sum += term;
+    if (term <= 1e-17 * sum) break;
+  }
+  return pref * sum;
+}
+
+__global__ void bessel_tables_kernel(const double *__restrict__ rpts, int total, int lmax,
+                                     double kappa, double *besi, double *besk) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= total) return;
+  const double x = kappa * rpts[p];
+  if (!(x > 2.220446049250313e-16)) {
+    for (int l = 0; l <= lmax; ++l) {
+      besi[(size_t)l * total + p] = l == 0 ? 1.0 : 0.0;
+      besk[(size_t)l * total + p] = 0.0;
+    }
+    return;
+  }
+  if (lmax == 0) {
+    besi[p] = besseli_series(x, 0);
+  } else {
+    double up = besseli_series(x, lmax), cur = besseli_series(x, lmax - 1);
+    besi[(size_t)lmax * total + p] = up;
+    besi[(size_t)(lmax - 1) * total + p] = cur;
+    for (int l = lmax - 2; l >= 0; --l) {
+      const double v = (2 * l + 3) * cur / x + up;
+      besi[(size_t)l * total + p] = v;
+      up = cur;
+      cur = v;
+    }
+  }
+  const double hp = 1.5707963267948966;
+  double k0 = hp * exp(-x) / x;
+  besk[p] = k0;
+  if (lmax >= 1) {
+    double k1 = hp * exp(-x) * (x + 1.0) / (x * x);
+    besk[(size_t)total + p] = k1;
+    for (int l = 2; l <= lmax; ++l) {
+      const double v = (2 * l - 1) * k1 / x + k0;
+      besk[(size_t)l * total + p] = v;
+      k0 = k1;
+      k1 = v;
+    }
+  }
+}
+
 // Gauss-Legendre nodes and weights on [-1, 1]: Newton's method on P_n from
 // the three-term recurrence, started at cos(pi (i - 1/4) / (n + 1/2)).
 void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w) {
@@ -763,10 +843,13 @@ int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, do
   return 0;
 }
 
-int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out) {
-  clear_error();
-  if (!in || !out) return fail(DAGE_E_INVALID, "null argument");
-  *out = nullptr;
+}  // extern "C"
+
+namespace dage {
+namespace {
+// Radial Coulomb (helm = false) or Helmholtz (kernel e^-kappa r / r) potential
+// of every (atom, lm) function, as a new bubble set with k = 0.
+int bubbles_radial_potential(const dage_bubbles *in, bool helm, double kappa, dage_bubbles **out) {
   DAGE_CUDA_TRY(cudaSetDevice(in->device));
   // LIP partial integrals on the local nodes (LIPBasis_outward/inward_integrals,
   // lip.F90:414-480): antiderivative of each basis polynomial by Horner
@@ -790,16 +873,48 @@ int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out) {
   DAGE_TRY(d_V.alloc(sizeof(double) * in->nvals));
   DAGE_CUDA_TRY(cudaMemcpy(d_out.ptr, outi.data(), sizeof(double) * outi.size(), cudaMemcpyHostToDevice));
   DAGE_CUDA_TRY(cudaMemcpy(d_in.ptr, ini.data(), sizeof(double) * ini.size(), cudaMemcpyHostToDevice));
-  bubbles_potential_kernel<<<in->natom, std::min(256, ((in->N + 31) / 32) * 32)>>>(
-      in->atoms.as<AtomTab>(), in->hcell.as<double>(), in->fraw.as<double>(),
-      in->rpts.as<double>(), in->np.as<int>(), in->foff.as<int>(), in->lmax, in->k, in->nlip,
-      d_out.as<double>(), d_in.as<double>(), d_V.as<double>());
+  const int total = (int)(in->nvals / in->N);
+  DevBuf d_I, d_K;
+  if (helm) {
+    DAGE_TRY(d_I.alloc(sizeof(double) * (size_t)(in->lmax + 1) * total));
+    DAGE_TRY(d_K.alloc(sizeof(double) * (size_t)(in->lmax + 1) * total));
+    bessel_tables_kernel<<<(total + 127) / 128, 128>>>(in->rpts.as<double>(), total, in->lmax, kappa,
+                                                       d_I.as<double>(), d_K.as<double>());
+  }
+  auto go = [&](auto kernel) {
+    kernel<<<in->natom, std::min(256, ((in->N + 31) / 32) * 32)>>>(
+        in->atoms.as<AtomTab>(), in->hcell.as<double>(), in->fraw.as<double>(),
+        in->rpts.as<double>(), in->np.as<int>(), in->foff.as<int>(), in->lmax, in->k, in->nlip,
+        d_out.as<double>(), d_in.as<double>(), d_I.as<double>(), d_K.as<double>(), total, kappa,
+        d_V.as<double>());
+  };
+  if (helm) go(bubbles_potential_kernel<true>);
+  else go(bubbles_potential_kernel<false>);
   DAGE_CUDA_TRY(cudaGetLastError());
   std::vector<double> V(in->nvals);
   DAGE_CUDA_TRY(cudaMemcpy(V.data(), d_V.ptr, sizeof(double) * V.size(), cudaMemcpyDeviceToHost));
   // the potential is a bubble set of its own (k = 0) on the same centres and grids
   return dage_bubbles_create(in->natom, in->centers.data(), in->radial.data(), in->lmax, 0,
                              V.data(), out);
+}
+}  // namespace
+}  // namespace dage
+
+extern "C" {
+
+int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out) {
+  clear_error();
+  if (!in || !out) return fail(DAGE_E_INVALID, "null argument");
+  *out = nullptr;
+  return bubbles_radial_potential(in, false, 0.0, out);
+}
+
+int dage_bubbles_helmholtz_potential(const dage_bubbles *in, double energy, dage_bubbles **out) {
+  clear_error();
+  if (!in || !out) return fail(DAGE_E_INVALID, "null argument");
+  *out = nullptr;
+  if (!(energy < 0.0)) return fail(DAGE_E_INVALID, "Helmholtz bubbles: need energy < 0");
+  return bubbles_radial_potential(in, true, std::sqrt(-2.0 * energy), out);
 }
 
 int dage_bubbles_multiply(const dage_bubbles *x, const dage_bubbles *y, unsigned flags,

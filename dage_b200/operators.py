@@ -535,6 +535,14 @@ class Bubbles:
         check(load().dage_bubbles_coulomb_potential(self._h, ctypes.byref(h)))
         return Bubbles._wrap(h, self)
 
+    def helmholtz_potential(self, energy: float) -> "Bubbles":
+        """The radial potential of these bubbles for the kernel
+        e^(-kappa r)/r, kappa = sqrt(-2 energy) (Helmholtz3D_bubbles,
+        helmholtz3d.F90:506-650), computed on the GPU."""
+        h = ctypes.c_void_p()
+        check(load().dage_bubbles_helmholtz_potential(self._h, float(energy), ctypes.byref(h)))
+        return Bubbles._wrap(h, self)
+
     def radial_values(self):
         """Per atom, the ((lmax+1)^2, npoints) radial values (as given)."""
         sizes = [int(gr.ncell * (gr.nlip - 1) + 1) for gr in self._grids]

@@ -265,6 +265,15 @@ int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, do
  * can be injected into a cube like any bubble set. */
 int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out);
 
+/* Radial Helmholtz potential of a bubble set for the kernel e^(-kappa r)/r,
+ * kappa = sqrt(-2 energy), energy < 0 (Helmholtz3D_transform_bubbles_sub,
+ * src/bubbles/helmholtz3d.F90:519-650): a new bubble set (k = 0) holding
+ *   V_lm(r) = 8 kappa [ k_l(kappa r) int_0^r i_l(kappa s) f s^(2+k) ds
+ *                       + i_l(kappa r) int_r^inf k_l(kappa s) f s^(2+k) ds ]
+ * with the modified spherical Bessel functions i_0 = sinh x/x,
+ * k_0 = pi/2 e^-x/x (helmholtz3d.F90:851-1060), computed on the GPU. */
+int dage_bubbles_helmholtz_potential(const dage_bubbles *in, double energy, dage_bubbles **out);
+
 /* Copies the radial values of a bubble set (as given at creation: per atom,
  * (lmax+1)^2 functions of the atom's radial points) to host memory. */
 int dage_bubbles_get_f(const dage_bubbles *b, double *f);

@@ -917,3 +917,56 @@ def function3d_multiply(grid: Grid3D, cube1, cube2, bubbles1=None, bubbles2=None
     if result_bubbles is not None:
         bubbles_inject(grid=grid, cube=out, factor=-1.0, **result_bubbles)
     return out
+
+
+def bubbles_helmholtz_potential(ncell, cell_scales, lmax, f, kappa, k=0, nlip=7):
+    """Helmholtz3D_transform_bubbles_sub (helmholtz3d.F90:519-650) for one
+    atom: with i_l, k_l the modified spherical Bessel functions
+    (i_0 = sinh x / x, k_0 = pi/2 e^-x / x; both 0 except i_0 = 1 at x = 0,
+    helmholtz3d.F90:851-1060),
+      V_lm(r) = 8 kappa [ k_l(kr) int_0^r i_l(ks) f s^(2+k) ds
+                          + i_l(kr) int_r^inf k_l(ks) f s^(2+k) ds ],
+    the inward integrand's value at r = 0 replaced by the 3-point
+    extrapolation 3 g1 - 3 g2 + g3 for l = 0 and by 0 otherwise
+    (extrapolate_first_nlip7, evaluators.F90:1588-1600).  The cumulative
+    integrals are those of bubbles_coulomb_potential."""
+    from scipy.special import spherical_in, spherical_kn
+    h = _f64(np.broadcast_to(cell_scales, (ncell,)))
+    n = nlip - 1
+    r = Grid1D(0.0, ncell, nlip, 1, h).points
+    npts = r.size
+    out_i, in_i = lip_partial_integrals(nlip)
+    x = kappa * r
+    I = np.zeros((lmax + 1, npts))
+    K = np.zeros((lmax + 1, npts))
+    nz = x > np.finfo(np.float64).eps
+    for l in range(lmax + 1):
+        I[l, nz] = spherical_in(l, x[nz])
+        K[l, nz] = spherical_kn(l, x[nz])
+    I[0, ~nz] = 1.0
+    rp = r ** (2 + k)
+
+    def outwards(g):
+        res = np.zeros(npts)
+        for c in range(ncell):
+            s = c * n
+            res[s + 1:s + n + 1] = (g[s:s + n + 1] @ out_i) * h[c] + res[s]
+        return res
+
+    def inwards(g):
+        res = np.zeros(npts)
+        for c in range(ncell - 1, -1, -1):
+            s = c * n
+            res[s:s + n] = (g[s:s + n + 1] @ in_i) * h[c] + res[s + n]
+        return res
+
+    f = np.asarray(f, dtype=np.float64).reshape((lmax + 1) ** 2, npts)
+    V = np.zeros_like(f)
+    for l in range(lmax + 1):
+        for m in range(-l, l + 1):
+            lm = l * (l + 1) + m
+            t1 = rp * I[l] * f[lm]
+            t2 = rp * K[l] * f[lm]
+            t2[0] = 3 * t2[1] - 3 * t2[2] + t2[3] if l == 0 else 0.0
+            V[lm] = 8 * kappa * (K[l] * outwards(t1) + I[l] * inwards(t2))
+    return V

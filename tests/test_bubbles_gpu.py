@@ -84,3 +84,41 @@ def test_coulomb_potential_of_gaussian_injects_erf(dage, oracle):
     exact = np.pi ** 1.5 * erf(d) / d
     inside = d < 11.5  # the radial grid (and so the bubble) ends at r = 12
     assert np.abs(cube - exact)[inside].max() <= 1e-6 * np.abs(exact).max()
+
+
+@pytest.mark.parametrize("natom,lmax,k,energy", [(1, 0, 0, -0.125), (3, 2, 0, -0.5), (2, 4, 1, -2.0),
+                                                 (1, 8, 0, -0.8)])
+def test_helmholtz_potential_matches_oracle(dage, oracle, natom, lmax, k, energy):
+    """Radial Helmholtz potential of every (atom, lm) function on the GPU
+    against the oracle's restatement of Helmholtz3D_transform_bubbles_sub."""
+    centers, ncells, hs, f = _bubbles(oracle, natom, lmax)
+    rad = [dage.Grid1D(0.0, n, 7, 1, h) for n, h in zip(ncells, hs)]
+    V = dage.Bubbles(centers, rad, f, lmax, k=k).helmholtz_potential(energy).radial_values()
+    kappa = np.sqrt(-2 * energy)
+    for a in range(natom):
+        ref = oracle.bubbles_helmholtz_potential(ncells[a], hs[a], lmax, f[a], kappa, k=k)
+        assert np.abs(V[a] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_helmholtz_potential_of_gaussian(dage, oracle):
+    """rho = e^-r^2 -> pi^1.5/(2r) e^(k^2/4) [e^-kr erfc(k/2 - r) - e^kr erfc(k/2 + r)]."""
+    from scipy.special import erfc
+
+    h = oracle.log_radial_grid(60, 1e-4, 12.0)
+    r = oracle.Grid1D(0.0, 60, 7, 1, h).points
+    kappa = 1.3
+    b = dage.Bubbles([[0.0, 0.0, 0.0]], [dage.Grid1D(0.0, 60, 7, 1, h)], [np.exp(-r ** 2)[None, :]], 0)
+    V = b.helmholtz_potential(-0.5 * kappa ** 2).radial_values()[0][0]
+    rr = r[1:]
+    exact = (np.pi ** 1.5 / (2 * rr) * np.exp(kappa ** 2 / 4)
+             * (np.exp(-kappa * rr) * erfc(kappa / 2 - rr) - np.exp(kappa * rr) * erfc(kappa / 2 + rr)))
+    sel = rr < 8.0
+    assert np.abs(V[1:][sel] - exact[sel]).max() < 2e-8 * np.abs(exact).max()
+
+
+def test_helmholtz_potential_needs_negative_energy(dage, oracle):
+    h = oracle.log_radial_grid()
+    r = oracle.Grid1D(0.0, 33, 7, 1, h).points
+    b = dage.Bubbles([[0.0, 0.0, 0.0]], [dage.Grid1D(0.0, 33, 7, 1, h)], [np.exp(-r)[None, :]], 0)
+    with pytest.raises(dage.DageError):
+        b.helmholtz_potential(0.0)
