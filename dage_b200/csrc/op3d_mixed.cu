@@ -68,11 +68,6 @@ constexpr int BM = 128;           // tile rows (TMEM lanes)
 constexpr int BN = 128;           // tile columns
 constexpr int BK = 32;            // K extent of one shared-memory stage (64-byte rows)
 constexpr int kGroup = 32;        // K extent sharing one quantum in a leading part
-// 32-runs of K per main-product partial: 1 for bf16x6 (fixed-point leads: a
-// 32-run's partial is exact in FP32); bf16x3's floating leads make no run
-// exact, so its partials span 2 runs (half the epilogue drains).
-template <int NSX>
-constexpr int runs_per_partial() { return NSX == 2 ? 2 : 1; }
 constexpr int kThreads = 576;     // 18 warps
 constexpr int kEpiThreads = 512;  // warps 2-17
 constexpr int kMaxGroup = 8;      // t-points summed per pass of the last stage
@@ -343,21 +338,19 @@ __device__ __forceinline__ int tile_row0(const StageArgs &a, int mt) {
 }
 
 // The MMAs of one 32-run of K (d0: the run's first K column in the stage):
-// the main product (part 0 x part 0) into the partial P, committed to
-// `pfull` as soon as it is issued when the run closes the partial, and the
-// correction products into the accumulator Cc.  NK K=16 steps; FIRST: the
-// tile's first run (the correction accumulator starts); OPEN: the run starts
-// the partial; CLOSE: it ends it.
-template <int NSX, int NK, bool FIRST = false, bool OPEN = true, bool CLOSE = true>
+// the main product (part 0 x part 0) into the fresh partial P, committed to
+// `pfull` as soon as it is issued, and the correction products into the
+// accumulator Cc.  NK K=16 steps; FIRST: the tile's first run (the
+// correction accumulator starts).
+template <int NSX, int NK, bool FIRST = false>
 __device__ __forceinline__ void mma_run(uint32_t P, uint32_t Cc, uint64_t d0, uint32_t idesc,
                                            bool first, uint32_t pfull_bar) {
   constexpr int kABytes = BM * BK * 2, kBBytes = BN * BK * 2;  // one part of a tile
   constexpr int NCORR = NSX == 2 ? 2 : 5;
 #pragma unroll
   for (int k = 0; k < NK; ++k) {
-    umma_bf16_c(P, d0 + ((k * 32) >> 4), d0 + ((NSX * kABytes + k * 32) >> 4), idesc,
-                k != 0 || !OPEN);
-    if (CLOSE && k == NK - 1) umma_commit(pfull_bar);
+    umma_bf16_c(P, d0 + ((k * 32) >> 4), d0 + ((NSX * kABytes + k * 32) >> 4), idesc, k != 0);
+    if (k == NK - 1) umma_commit(pfull_bar);
 #pragma unroll
     for (int pr = 0; pr < NCORR; ++pr) {
       int ia, ib;
@@ -386,7 +379,6 @@ __global__ void __maxnreg__(96)
                       const __grid_constant__ CUtensorMap mapB2, const StageArgs a) {
   using C = StageCfg<NSX, NS>;
   constexpr int GRAN = kGroup / 16;
-  constexpr int RUNS = runs_per_partial<NSX>();
   // an earlier launch of this apply timed out: do nothing
   if (*reinterpret_cast<volatile int *>(a.err)) return;
   extern __shared__ uint8_t smem_raw[];
@@ -501,7 +493,6 @@ __global__ void __maxnreg__(96)
         // next tile's band, loaded while this tile's MMAs run
         u += (u % a.ng == a.ng - 1) ? (gridDim.x - 1) * a.ng + 1 : 1;
         if (u < a.ntiles * a.ng) r = kblocks(a, u % a.ng, (u / a.ng) % a.n_ntiles);
-        int j = 0;  // 32-runs already in the current partial
         for (int kb = rc.x; kb <= rc.y; ++kb) {
           const bool first = kb == rc.x;
           if (!mbar_wait(full(s), ph, a.wait_limit) ||
@@ -517,10 +508,7 @@ __global__ void __maxnreg__(96)
           for (int rr = 0; rr < BK / kGroup; ++rr) {
             const int nk = min(nk16 - rr * GRAN, GRAN);  // K=16 steps of this run
             if (nk <= 0) break;
-            const bool open = j == 0;
-            const bool close = j == RUNS - 1 ||
-                               (kb == rc.y && (rr + 1 == BK / kGroup || nk16 <= (rr + 1) * GRAN));
-            if (open && !mbar_wait(pempty(b), pph ^ 1, a.wait_limit)) {
+            if (!mbar_wait(pempty(b), pph ^ 1, a.wait_limit)) {
               on_timeout();
               ok = false;
               break;
@@ -528,36 +516,13 @@ __global__ void __maxnreg__(96)
             tc_fence_after();
             const uint64_t dr = d0 + (uint64_t)((rr * kGroup * 2) >> 4);
             const uint32_t P = tmem_base + b * BN;
-            const bool f0 = first && rr == 0;
-            if constexpr (RUNS == 1) {
-              if (nk == 1)
-                mma_run<NSX, 1>(P, tmem_corr, dr, idesc, f0, pfull(b));
-              else if (f0)
-                mma_run<NSX, 2, true>(P, tmem_corr, dr, idesc, true, pfull(b));
-              else
-                mma_run<NSX, 2, false>(P, tmem_corr, dr, idesc, false, pfull(b));
-            } else {
-              // (nk, first, open, close) -> straight-line MMA block
-              const int sel = (nk == 1 ? 8 : 0) | (f0 ? 4 : 0) | (open ? 2 : 0) | (close ? 1 : 0);
-              switch (sel) {
-                case 0: mma_run<NSX, 2, false, false, false>(P, tmem_corr, dr, idesc, false, pfull(b)); break;
-                case 1: mma_run<NSX, 2, false, false, true>(P, tmem_corr, dr, idesc, false, pfull(b)); break;
-                case 2: mma_run<NSX, 2, false, true, false>(P, tmem_corr, dr, idesc, false, pfull(b)); break;
-                case 3: mma_run<NSX, 2, false, true, true>(P, tmem_corr, dr, idesc, false, pfull(b)); break;
-                case 6: mma_run<NSX, 2, true, true, false>(P, tmem_corr, dr, idesc, true, pfull(b)); break;
-                case 7: mma_run<NSX, 2, true, true, true>(P, tmem_corr, dr, idesc, true, pfull(b)); break;
-                case 8: case 12: mma_run<NSX, 1, false, false, false>(P, tmem_corr, dr, idesc, f0, pfull(b)); break;
-                case 9: case 13: mma_run<NSX, 1, false, false, true>(P, tmem_corr, dr, idesc, f0, pfull(b)); break;
-                case 10: case 14: mma_run<NSX, 1, false, true, false>(P, tmem_corr, dr, idesc, f0, pfull(b)); break;
-                default: mma_run<NSX, 1, false, true, true>(P, tmem_corr, dr, idesc, f0, pfull(b)); break;
-              }
-            }
-            if (close) {
-              if (++b == C::kNP) b = 0, pph ^= 1;
-              j = 0;
-            } else {
-              ++j;
-            }
+            if (nk == 1)
+              mma_run<NSX, 1>(P, tmem_corr, dr, idesc, first && rr == 0, pfull(b));
+            else if (first && rr == 0)
+              mma_run<NSX, 2, true>(P, tmem_corr, dr, idesc, true, pfull(b));
+            else
+              mma_run<NSX, 2, false>(P, tmem_corr, dr, idesc, false, pfull(b));
+            if (++b == C::kNP) b = 0, pph ^= 1;
           }
           if (!ok) break;
           umma_commit(empty(s));
@@ -587,8 +552,8 @@ __global__ void __maxnreg__(96)
       for (int gi = 0; gi < a.ng && ok; ++gi, ++t) {
 #pragma unroll
         for (int j = 0; j < CW / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
-        const int nruns = (tile_steps(kblocks(a, gi, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
-        const int nparts = (nruns + RUNS - 1) / RUNS;
+        const int nparts =
+            (tile_steps(kblocks(a, gi, tile % a.n_ntiles)) + GRAN - 1) / GRAN;
         for (int pi = 0; pi < nparts; ++pi, ++g) {
           const int b = g % C::kNP;
           // warp-uniform outcome: the TMEM loads below are warp-collective
