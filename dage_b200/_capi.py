@@ -67,6 +67,9 @@ SIGNATURES = {
     "dage_gbfmm_create": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(DageQuad), ctypes.c_int,
                                          ctypes.POINTER(_VP)]),
+    "dage_gbfmm_create_adaptive": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(DageQuad), ctypes.c_int,
+                                         ctypes.POINTER(_VP)]),
     "dage_gbfmm_apply": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint, _D]),
     "dage_gbfmm_multipole_moments": (ctypes.c_int, [_VP, _VP, ctypes.c_uint, _D]),
     "dage_gbfmm_local_expansions": (ctypes.c_int, [_VP, _D]),

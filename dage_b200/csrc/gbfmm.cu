@@ -900,6 +900,34 @@ std::vector<int> local_farfield(int ibox, int level) {
   return out;
 }
 
+// Adaptive mode (GBFMMParallelInfo_get_local_farfield_indices evaluation
+// types 1 and 2, gbfmm_parallel_info.F90:827-983, as gbfmm_coulomb3d.F90:
+// 1386-1433 uses them): of the neighbours of ibox's parent, those with a
+// child among ibox's nearest neighbours contribute their other children
+// (`partial`, boxes of `level`); the others contribute as whole boxes of
+// level - 1 (`whole`).
+void local_farfield_adaptive(int ibox, int level, std::vector<int> &partial,
+                             std::vector<int> &whole) {
+  partial.clear();
+  whole.clear();
+  if (level < 2) return;
+  const auto pnn = neighbours((ibox - 1) / 8 + 1, level - 1);
+  const auto nn = neighbours(ibox, level);
+  for (int p : pnn) {
+    bool has_nn = false;
+    for (int c = 1; c <= 8 && !has_nn; ++c)
+      has_nn = std::find(nn.begin(), nn.end(), (p - 1) * 8 + c) != nn.end();
+    if (!has_nn) {
+      whole.push_back(p);
+      continue;
+    }
+    for (int c = 1; c <= 8; ++c) {
+      const int child = (p - 1) * 8 + c;
+      if (std::find(nn.begin(), nn.end(), child) == nn.end()) partial.push_back(child);
+    }
+  }
+}
+
 }  // namespace
 }  // namespace dage
 
@@ -910,6 +938,7 @@ struct dage_gbfmm {
   double energy = 0.0, kappa = 0.0;  // kernel: Coulomb (energy 0) or e^(-kappa r)/r
   std::vector<double> disp;          // distinct far-field displacements (x, y, z)
   int level = 2, lmax = 12, nbox = 0, N = 0, P = 0, precision = DAGE_FP64;
+  int lev0 = 2;  // coarsest level with multipoles: 1 in the adaptive mode
   Axis ax[3];
   int npts[3];
   dage_quad quad{};
@@ -1246,11 +1275,11 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   // level (so the levels nest also for uneven splits); centres follow the
   // reference on evenly divisible axes, else the midpoint of the box's points.
   g->lev_off.assign(maxlevel + 2, 0);
-  for (int l = 2; l <= maxlevel; ++l) g->lev_off[l + 1] = g->lev_off[l] + (1 << (3 * l));
+  for (int l = g->lev0; l <= maxlevel; ++l) g->lev_off[l + 1] = g->lev_off[l] + (1 << (3 * l));
   g->nbtot = g->lev_off[maxlevel + 1];
   g->fine_off = g->lev_off[maxlevel];
   g->centers.assign(3 * (size_t)g->nbtot, 0.0);
-  for (int l = 2; l <= maxlevel; ++l) {
+  for (int l = g->lev0; l <= maxlevel; ++l) {
     const int nbl = 1 << l, f = 1 << (maxlevel - l);
     for (int i = 1; i <= (1 << (3 * l)); ++i) {
       int v[3];
@@ -1280,22 +1309,35 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   std::map<std::vector<long long>, int> disp_index;
   std::vector<double> &disp = g->disp;
   std::vector<int> ffstart(1, 0), ffsrc, ffdisp;
-  for (int l = 2; l <= maxlevel; ++l)
+  std::vector<int> partial, whole;
+  for (int l = g->lev0; l <= maxlevel; ++l)
     for (int b = 1; b <= (1 << (3 * l)); ++b) {
       int vb[3];
       box_vector(b, l, vb);
       const double *cb = &g->centers[3 * (size_t)(g->lev_off[l] + b - 1)];
-      for (int j : local_farfield(b, l)) {
+      // sources: (box, level) pairs
+      std::vector<std::pair<int, int>> srcs;
+      if (g->lev0 == 1) {
+        local_farfield_adaptive(b, l, partial, whole);
+        for (int j : partial) srcs.emplace_back(j, l);
+        for (int j : whole) srcs.emplace_back(j, l - 1);
+      } else {
+        for (int j : local_farfield(b, l)) srcs.emplace_back(j, l);
+      }
+      for (const auto &src : srcs) {
+        const int j = src.first, lj = src.second;
         int vj[3];
-        box_vector(j, l, vj);
-        const double *cj = &g->centers[3 * (size_t)(g->lev_off[l] + j - 1)];
+        box_vector(j, lj, vj);
+        const double *cj = &g->centers[3 * (size_t)(g->lev_off[lj] + j - 1)];
         double dv[3];
         std::vector<long long> key(4);
-        key[3] = regular ? l : 0;
+        // same level: the box-vector difference; a level - 1 source: the
+        // centre difference in half boxes of level l (4 vj - 2 vb + 1)
+        key[3] = regular ? (lj == l ? l : -l) : 0;
         for (int d = 0; d < 3; ++d) {
           dv[d] = cj[d] - cb[d];
           if (regular)
-            key[d] = vj[d] - vb[d];
+            key[d] = lj == l ? vj[d] - vb[d] : 4LL * vj[d] - 2LL * vb[d] + 1;
           else
             std::memcpy(&key[d], &dv[d], 8);
         }
@@ -1308,7 +1350,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
         } else {
           di = it->second;
         }
-        ffsrc.push_back(g->lev_off[l] + j - 1);
+        ffsrc.push_back(g->lev_off[lj] + j - 1);
         ffdisp.push_back(di);
       }
       ffstart.push_back((int)ffsrc.size());
@@ -1324,7 +1366,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
     std::map<std::vector<long long>, int> tindex;
     std::vector<double> tdisp;
     std::vector<int> m2m_disp;
-    for (int l = 3; l <= maxlevel; ++l)
+    for (int l = g->lev0 + 1; l <= maxlevel; ++l)
       for (int i = 1; i <= (1 << (3 * l)); ++i) {
         const double *cc = &g->centers[3 * (size_t)(g->lev_off[l] + i - 1)];
         const double *cp = &g->centers[3 * (size_t)(g->lev_off[l - 1] + (i - 1) / 8)];
@@ -1474,7 +1516,7 @@ GInst plan_inst(const dage_gbfmm *g, const double *rho, double *V, double *q, do
   I.wz = g->wts[2].as<double>();
   I.kappa = g->kappa;
   I.fine_off = g->fine_off;
-  I.m2m_base = g->level >= 3 ? g->lev_off[3] : 0;
+  I.m2m_base = g->level > g->lev0 ? g->lev_off[g->lev0 + 1] : 0;
   I.Wm2m = g->d_Wm2m.as<double>();
   I.m2m_disp = g->d_m2m_disp.as<int>();
   return I;
@@ -1591,10 +1633,10 @@ int run_m2l(const GInst *d_inst, int ninst, int nbox, int N, cudaStream_t s) {
   return 0;
 }
 
-// Upward pass from the finest level to level 2 (no work for one level).
+// Upward pass from the finest level to level 2 (1 in the adaptive mode).
 int run_m2m(const GInst *d_inst, int ninst, const dage_gbfmm *g, cudaStream_t s) {
   const int threads = std::min(256, ((g->N + 31) / 32) * 32);
-  for (int l = g->level - 1; l >= 2; --l) {
+  for (int l = g->level - 1; l >= g->lev0; --l) {
     m2m_kernel<<<dim3(1 << (3 * l), ninst), threads, 0, s>>>(d_inst, g->N, g->lev_off[l],
                                                             g->lev_off[l + 1]);
     DAGE_CUDA_TRY(cudaGetLastError());
@@ -2034,6 +2076,26 @@ int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const d
   return 0;
 }
 
+int dage_gbfmm_create_adaptive(const dage_grid1d grid[3], int maxlevel, int lmax,
+                               const dage_quad *quad, int precision, dage_gbfmm **out) {
+  clear_error();
+  if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
+  *out = nullptr;
+  if (precision != DAGE_FP64)
+    return fail(DAGE_E_UNSUPPORTED, "the GBFMM operator runs in FP64 (DAGE_FP64)");
+  auto *g = new dage_gbfmm();
+  g->precision = precision;
+  g->lev0 = 1;
+  int rc = gbfmm_create_impl(g, grid, maxlevel, lmax, quad);
+  if (!rc) rc = gbfmm_autotune(g);
+  if (rc) {
+    gbfmm_destroy_impl(g);
+    return rc;
+  }
+  *out = g;
+  return 0;
+}
+
 int dage_gbfmm_destroy(dage_gbfmm *g) {
   clear_error();
   gbfmm_destroy_impl(g);
@@ -2050,8 +2112,9 @@ int dage_gbfmm_set_energy(dage_gbfmm *g, double energy) {
   clear_error();
   if (!g) return fail(DAGE_E_INVALID, "null handle");
   if (!(energy <= 0.0)) return fail(DAGE_E_INVALID, "energy must be <= 0 (got %g)", energy);
-  if (energy < 0.0 && g->level > 2)
-    return fail(DAGE_E_UNSUPPORTED, "the Helmholtz GBFMM runs with maxlevel 2 (no Helmholtz M2M/L2L)");
+  if (energy < 0.0 && (g->level > 2 || g->lev0 < 2))
+    return fail(DAGE_E_UNSUPPORTED,
+                "the Helmholtz GBFMM runs with maxlevel 2, not adaptive (no Helmholtz M2M/L2L)");
   DAGE_CUDA_TRY(cudaSetDevice(g->device));
   g->energy = energy;
   g->kappa = energy < 0.0 ? std::sqrt(-2.0 * energy) : 0.0;

@@ -297,19 +297,24 @@ class GBFMMCoulomb3D:
     """GBFMMCoulomb3D (src/gbfmm/gbfmm_coulomb3d.F90:331-819), FP64: near
     field by per-box sub-operators, far field by multipoles (lmax) and M2L,
     2^maxlevel boxes per axis.  The near-field quadrature defaults to the
-    reference's GaussQuad(25, 25)."""
+    reference's GaussQuad(25, 25).  ``adaptive_mode``: the reference's
+    adaptive mode (gbfmm_coulomb3d.F90:374-384, 1386-1433): multipoles up to
+    level 1, and neighbours of a box's parent that hold none of the box's
+    nearest neighbours interact as whole parent-level boxes (Coulomb only)."""
 
     def __init__(self, grid: Grid3D, lmax: int = 12, maxlevel: int = 2,
-                 quad: GaussQuad | None = None):
+                 quad: GaussQuad | None = None, adaptive_mode: bool = False):
         lib = load()
         self.grid = grid
         self.lmax = lmax
         self.maxlevel = maxlevel
+        self.adaptive_mode = adaptive_mode
         self.quad = quad if quad is not None else GaussQuad(25, 25)
         self._keep = (grid.c(), self.quad.c())
         h = ctypes.c_void_p()
-        check(lib.dage_gbfmm_create(self._keep[0], maxlevel, lmax, ctypes.byref(self._keep[1]),
-                                    _capi.DAGE_FP64, ctypes.byref(h)))
+        create = lib.dage_gbfmm_create_adaptive if adaptive_mode else lib.dage_gbfmm_create
+        check(create(self._keep[0], maxlevel, lmax, ctypes.byref(self._keep[1]),
+                     _capi.DAGE_FP64, ctypes.byref(h)))
         self._h = h
         nb, nlm = ctypes.c_int(), ctypes.c_int()
         check(lib.dage_gbfmm_box_count(h, ctypes.byref(nb), ctypes.byref(nlm)))

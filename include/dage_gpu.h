@@ -155,6 +155,17 @@ typedef struct dage_gbfmm dage_gbfmm;
 int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const dage_quad *quad,
                       int precision, dage_gbfmm **g);
 
+/* As dage_gbfmm_create, in the reference's adaptive mode (GBFMMCoulomb3D_init
+ * with adaptive_mode, src/gbfmm/gbfmm_coulomb3d.F90:374-384; far-field lists
+ * of gbfmm_coulomb3d.F90:1386-1433 with GBFMMParallelInfo evaluation types 1
+ * and 2, src/gbfmm/gbfmm_parallel_info.F90:827-983): multipoles are
+ * translated up to level 1; a box of level l >= 2 takes M2L from the children
+ * of its parent's neighbours that contain one of its nearest neighbours
+ * (minus those neighbours) and, as whole boxes of level l - 1, from its
+ * parent's other neighbours.  Coulomb kernel only. */
+int dage_gbfmm_create_adaptive(const dage_grid1d grid[3], int maxlevel, int lmax,
+                               const dage_quad *quad, int precision, dage_gbfmm **g);
+
 /* V = near field + far field (multipoles -> M2L -> L2P), every point taking
  * the contributions of the box that owns it; optional LIP-weighted energy.
  * Replaces GBFMMCoulomb3D_calculate_potential's CUDA path

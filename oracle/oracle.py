@@ -458,6 +458,26 @@ def local_farfield(ibox, level):
     return list(out[:n])
 
 
+def local_farfield_adaptive(ibox, level):
+    """The adaptive mode's far field of box `ibox` of `level`
+    (GBFMMParallelInfo_get_local_farfield_indices evaluation types 1 and 2,
+    gbfmm_parallel_info.F90:827-983, used at gbfmm_coulomb3d.F90:1386-1433):
+    (boxes of `level`: the children of the parent's neighbours that contain
+    one of ibox's nearest neighbours, minus those neighbours; boxes of
+    level - 1: the parent's other neighbours)."""
+    if level < 2:
+        return [], []
+    nn = set(nearest_neighbors(ibox, level))
+    partial, whole = [], []
+    for p in nearest_neighbors((ibox - 1) // 8 + 1, level - 1):
+        kids = range((p - 1) * 8 + 1, p * 8 + 1)
+        if any(c in nn for c in kids):
+            partial += [c for c in kids if c not in nn]
+        else:
+            whole.append(p)
+    return partial, whole
+
+
 def box_multipoles(lmax, px, wx, py, wy, pz, wz, cube_sub, center):
     q = np.zeros((lmax + 1) ** 2)
     c = np.asfortranarray(cube_sub, dtype=np.float64)
@@ -619,17 +639,19 @@ class GBFMMPlan:
         return out
 
 
-def _far_field_levels(plan, q_fine, lmax):
+def _far_field_levels(plan, q_fine, lmax, adaptive=False):
     """Local expansions at the finest level of a multi-level GBFMM
     (gbfmm_coulomb3d.F90:650-905): upward pass q(parent) += W(c_child -
     c_parent) q(child) (translate_multipoles, :1502-1562) from maxlevel - 1
-    down to level 2; M2L over the local far field at level 2; then for each
-    finer level the parent's local expansion translated down (L2L,
-    translate_potential, :1565-1621) plus that level's own local far field."""
+    down to level 2 (1 in the adaptive mode); M2L over the local far field
+    at level 2; then for each finer level the parent's local expansion
+    translated down (L2L, translate_potential, :1565-1621) plus that level's
+    own local far field (adaptive: local_farfield_adaptive, the level - 1
+    boxes about their own centres)."""
     N = (lmax + 1) ** 2
     top = plan.level
     q = {top: q_fine}
-    for lev in range(top - 1, 1, -1):
+    for lev in range(top - 1, 0 if adaptive else 1, -1):
         nb = 8 ** lev
         ql = np.zeros((N, nb))
         for p in range(1, nb + 1):
@@ -646,14 +668,19 @@ def _far_field_levels(plan, q_fine, lmax):
             if Lprev is not None:
                 par = (i - 1) // 8 + 1
                 Ll[:, i - 1] += translate_local(lmax, Lprev[:, par - 1], ci, plan.center_at(par, lev - 1))
-            for j in local_farfield(i, lev):
-                Ll[:, i - 1] += interaction_matrix(lmax, plan.center_at(j, lev) - ci) @ q[lev][:, j - 1]
+            if adaptive:
+                partial, whole = local_farfield_adaptive(i, lev)
+                srcs = [(j, lev) for j in partial] + [(j, lev - 1) for j in whole]
+            else:
+                srcs = [(j, lev) for j in local_farfield(i, lev)]
+            for j, lj in srcs:
+                Ll[:, i - 1] += interaction_matrix(lmax, plan.center_at(j, lj) - ci) @ q[lj][:, j - 1]
         Lprev = Ll
     return Lprev
 
 
 def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
-                return_parts=False, libm_1ulp=False, energy=0.0):
+                return_parts=False, libm_1ulp=False, energy=0.0, adaptive=False):
     """GBFMMCoulomb3D_calculate_potential along the reference's CUDA path
     (gbfmm_coulomb3d.F90:650-819, gbfmm_coulomb3d.cu:478-573): multipoles per
     box, M2L over the local far field, near field by the sub-operator of
@@ -661,7 +688,8 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
     and far contributions of the box that owns it.  energy < 0: the
     GBFMMHelmholtz3D kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)
     (gbfmm_helmholtz3d.F90:478-1105): Helmholtz near-field weights, Bessel
-    multipoles, the Helmholtz multipole-to-local converter and L2P."""
+    multipoles, the Helmholtz multipole-to-local converter and L2P.
+    adaptive: the reference's adaptive mode (Coulomb only, _far_field_levels)."""
     plan = GBFMMPlan(grid, maxlevel)
     rho = np.asfortranarray(rho)
     N = (lmax + 1) ** 2
@@ -675,10 +703,10 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
                 subs[2].points, subs[2].weights(), rho[x0:x1, y0:y1, z0:z1], plan.center(b))
         q[:, b - 1] = (helm_box_multipoles(lmax, kappa, *args) if helm
                        else box_multipoles(lmax, *args))
-    if maxlevel > 2:
+    if maxlevel > 2 or adaptive:
         if helm:
             raise ValueError("multi-level GBFMM is restated for the Coulomb kernel only")
-        L = _far_field_levels(plan, q, lmax)
+        L = _far_field_levels(plan, q, lmax, adaptive)
     else:
         L = np.zeros((N, plan.nbox))
         for i in range(1, plan.nbox + 1):

@@ -133,3 +133,36 @@ def test_multilevel_helmholtz_is_refused(dage):
     g = dage.Grid3D.cube(-9.6, 16, 0.2)
     with pytest.raises(Exception, match="maxlevel 2"):
         dage.GBFMMHelmholtz3D(g, -0.5, lmax=4, maxlevel=3, quad=dage.GaussQuad(4, 4))
+
+
+@pytest.mark.parametrize("ncell,lmax,maxlevel", [(16, 8, 2), (16, 8, 3), (18, 6, 3)])
+def test_adaptive_matches_oracle(dage, oracle, ncell, lmax, maxlevel):
+    """The adaptive mode (multipoles up to level 1, whole parent-level boxes
+    in the far field) against the oracle's restatement: moments, local
+    expansions, potential and energy."""
+    g, go, rho = _setup(dage, oracle, ncell, 0.2)
+    quad = (6, 6, 0.0, 2.0, 1e3)
+    op = dage.GBFMMCoulomb3D(g, lmax=lmax, maxlevel=maxlevel, quad=dage.GaussQuad(*quad),
+                             adaptive_mode=True)
+    V, E = op.apply(rho, energy=True)
+    Vo, qo, Lo, _ = oracle.gbfmm_apply(go, rho, lmax=lmax, maxlevel=maxlevel, quad=quad,
+                                       return_parts=True, adaptive=True)
+    Qg = op.multipole_moments(rho)
+    assert np.abs(Qg - qo).max() <= 1e-12 * np.abs(qo).max()
+    op.apply(rho)
+    Lg = op.local_expansions()
+    assert np.abs(Lg - Lo).max() <= 1e-11 * np.abs(Lo).max()
+    V1 = oracle.gbfmm_apply(go, rho, lmax=lmax, maxlevel=maxlevel, quad=quad, libm_1ulp=True,
+                            adaptive=True)
+    spread = np.abs(V1 - Vo).max() / np.abs(Vo).max()
+    err = np.abs(V - Vo).max() / np.abs(Vo).max()
+    assert err <= max(1e-10, 10 * spread), (err, spread)
+    Eo = oracle.integrate_cube(go, rho * Vo)
+    assert abs(E - Eo) <= 1e-11 * abs(Eo)
+
+
+def test_adaptive_helmholtz_is_refused(dage):
+    g = dage.Grid3D.cube(-9.6, 16, 0.2)
+    op = dage.GBFMMCoulomb3D(g, lmax=4, maxlevel=2, quad=dage.GaussQuad(4, 4), adaptive_mode=True)
+    with pytest.raises(dage.DageError, match="not adaptive"):
+        dage._capi.check(dage.load().dage_gbfmm_set_energy(op._h, -0.5))

@@ -88,3 +88,26 @@ def test_mixed_device_pointers(dage, oracle):
     Vh = op.apply(rho)
     Vd = op.apply(torch.from_numpy(rho.reshape(-1, order="F").copy()).cuda())
     np.testing.assert_array_equal(Vd.cpu().numpy().reshape(-1), Vh.reshape(-1, order="F"))
+
+
+def test_headline_workload_meets_the_bounds(dage):
+    """The 481^3 workload that bench.py times (32 Gaussians, 64 t-points):
+    both split-precision modes within 1e-6 max-norm relative potential and
+    1e-7 relative energy of the FP64 GPU operator."""
+    import torch
+
+    import bench
+
+    g = dage.Grid3D.cube(-0.5 * bench.N_CELL * 6 * bench.STEP, bench.N_CELL, bench.STEP)
+    quad = dage.GaussQuad(bench.NLIN, bench.NLOG, 0.0, bench.TLIN, bench.TLOG)
+    q, a, c = bench.gaussians()
+    rho = bench.density_torch(bench.axis_points(), q, a, c, torch.device("cuda"))
+    V64 = torch.empty_like(rho)
+    _, E64 = dage.Coulomb3D(g, quad=quad).apply(rho, out=V64, energy=True)
+    scale = V64.abs().max().item()
+    for prec in ("bf16x3", "bf16x6"):
+        V = torch.empty_like(rho)
+        _, E = dage.Coulomb3D(g, quad=quad, precision=prec).apply(rho, out=V, energy=True)
+        err = (V - V64).abs().max().item() / scale
+        assert err <= 1e-6, (prec, err)
+        assert abs(E - E64) <= 1e-7 * abs(E64), (prec, abs(E - E64) / abs(E64))
