@@ -302,6 +302,40 @@ def band_fraction(T, bk=64, bn=128):
     return issued / (no * ni * P)
 
 
+def analytic_errors(V, V64, ncell, q, a, c, dev):
+    """Max and RMS error, relative to max |Va| and RMS Va, of the operator's
+    potentials against the analytic sum q erf(sqrt(a) r)/r of the Gaussians,
+    at the grid points (z slabs of 32 planes)."""
+    import torch
+
+    x = torch.tensor(axis_points(ncell), dtype=torch.float64, device=dev)
+    n = len(x)
+    out = {}
+    vmax = 0.0
+    ssq = 0.0
+    err = {"mixed": [0.0, 0.0], "fp64": [0.0, 0.0]}
+    for z0 in range(0, n, 32):
+        zs = x[z0:z0 + 32]
+        Z, Y, X = torch.meshgrid(zs, x, x, indexing="ij")
+        Va = torch.zeros_like(X)
+        for qi, ai, ci in zip(q, a, c):
+            r = torch.sqrt((X - ci[0]) ** 2 + (Y - ci[1]) ** 2 + (Z - ci[2]) ** 2)
+            small = r < 1e-12
+            val = qi * torch.erf(np.sqrt(ai) * r) / torch.where(small, torch.ones_like(r), r)
+            Va += torch.where(small, torch.full_like(r, qi * 2 * np.sqrt(ai / np.pi)), val)
+        sl = slice(z0 * n * n, (z0 + len(zs)) * n * n)
+        vmax = max(vmax, float(Va.abs().max()))
+        ssq += float((Va * Va).sum())
+        for key, W in (("mixed", V), ("fp64", V64)):
+            dv = W[sl].reshape(Va.shape) - Va
+            err[key][0] = max(err[key][0], float(dv.abs().max()))
+            err[key][1] += float((dv * dv).sum())
+    for key in err:
+        out[key] = {"max_rel": err[key][0] / vmax, "rms_rel": float(np.sqrt(err[key][1] / ssq))}
+    out["vs"] = "analytic sum q erf(sqrt(a) r)/r at the grid points"
+    return out
+
+
 def run_gpu(args, world, rank, local):
     import torch
 
@@ -408,6 +442,7 @@ def run_gpu(args, world, rank, local):
             "fp64_ms_per_step": fp64_ms,
             "fp64_mpts": fp64_mpts,
             "speedup_vs_fp64": fp64_ms / ms,
+            "vs_analytic": analytic_errors(V, V64, ncell, q, a, c, dev),
         }
         del op64
         if not args.skip_alt:
