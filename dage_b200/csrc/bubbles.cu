@@ -914,6 +914,10 @@ int dage_bubbles_helmholtz_potential(const dage_bubbles *in, double energy, dage
   if (!in || !out) return fail(DAGE_E_INVALID, "null argument");
   *out = nullptr;
   if (!(energy < 0.0)) return fail(DAGE_E_INVALID, "Helmholtz bubbles: need energy < 0");
+  // the r = 0 extrapolation reads the first four radial points of every atom
+  for (int a = 0; a < in->natom; ++a)
+    if (in->radial[a].ncell * (in->nlip - 1) + 1 < 4)
+      return fail(DAGE_E_UNSUPPORTED, "Helmholtz bubbles: every radial grid needs >= 4 points");
   return bubbles_radial_potential(in, true, std::sqrt(-2.0 * energy), out);
 }
 
