@@ -16,10 +16,11 @@ from .operators import (  # noqa: F401
     Grid3D,
     Helmholtz3D,
     Operator3D,
+    apply_batched,
     dot,
     integrate,
     multiply,
 )
 
 __all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GBFMMHelmholtz3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
-           "DageError", "dot", "integrate", "load", "multiply"]
+           "DageError", "apply_batched", "dot", "integrate", "load", "multiply"]

@@ -54,6 +54,8 @@ SIGNATURES = {
                                         ctypes.POINTER(DageQuad), ctypes.c_int,
                                         ctypes.POINTER(_VP)]),
     "dage_op3d_apply": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint, _D]),
+    "dage_op3d_apply_batched": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_VP), ctypes.POINTER(_VP),
+                                               ctypes.POINTER(_VP), ctypes.c_uint, _D]),
     "dage_op3d_set_weights": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "dage_op3d_set_energy": (ctypes.c_int, [_VP, ctypes.c_double]),
     "dage_op3d_set_coda": (ctypes.c_int, [_VP, ctypes.c_double]),

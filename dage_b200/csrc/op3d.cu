@@ -797,9 +797,9 @@ int dage_op3d_last_time_ms(const dage_op3d *op, float *ms) {
   return 0;
 }
 
-int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
-                    double *energy) {
-  clear_error();
+namespace {
+// Everything of one apply up to (not including) the wait for its stream.
+int op3d_enqueue(dage_op3d *op, const double *rho, double *V, unsigned flags, double *energy) {
   if (!op || !rho || !V) return fail(DAGE_E_INVALID, "null argument");
   if ((flags & DAGE_ENERGY) && !energy) return fail(DAGE_E_INVALID, "energy pointer is null");
   DAGE_CUDA_TRY(cudaSetDevice(op->device));
@@ -841,9 +841,39 @@ int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
     DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
   if (d_res) DAGE_CUDA_TRY(cudaMemcpyAsync(energy, d_res, sizeof(double), cudaMemcpyDeviceToHost, s));
   DAGE_CUDA_TRY(cudaEventRecord(op->ev1, s));
-  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int op3d_finish(dage_op3d *op) {
+  DAGE_CUDA_TRY(cudaSetDevice(op->device));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
   DAGE_CUDA_TRY(cudaEventElapsedTime(&op->last_ms, op->ev0, op->ev1));
   DAGE_TRY(op->tcollect());
+  return 0;
+}
+}  // namespace
+
+int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
+                    double *energy) {
+  clear_error();
+  DAGE_TRY(op3d_enqueue(op, rho, V, flags, energy));
+  return op3d_finish(op);
+}
+
+int dage_op3d_apply_batched(int n, dage_op3d *const *ops, const double *const *rho,
+                            double *const *V, unsigned flags, double *energies) {
+  clear_error();
+  if (n < 0 || (n > 0 && (!ops || !rho || !V))) return fail(DAGE_E_INVALID, "null argument");
+  if ((flags & DAGE_ENERGY) && n > 0 && !energies)
+    return fail(DAGE_E_INVALID, "energies pointer is null");
+  for (int i = 0; i < n; ++i)
+    DAGE_TRY(op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr));
+  // one wait per distinct operator, after everything is queued
+  for (int i = 0; i < n; ++i) {
+    bool seen = false;
+    for (int j = 0; j < i && !seen; ++j) seen = ops[j] == ops[i];
+    if (!seen) DAGE_TRY(op3d_finish(ops[i]));
+  }
   return 0;
 }
 

@@ -247,6 +247,33 @@ class Operator3D:
     __call__ = apply
 
 
+def apply_batched(ops, rhos, outs, energy: bool = False, coda: bool = True):
+    """Applies ops[i] to rhos[i] into outs[i] for every i, all queued before
+    one wait per distinct operator (applies on distinct operators overlap on
+    their streams).  Cubes: all host or all device.  Returns the energies
+    (numpy array) when ``energy`` is set."""
+    n = len(ops)
+    if not (len(rhos) == len(outs) == n):
+        raise ValueError("ops, rhos and outs need the same length")
+    rp, vp, devs = [], [], set()
+    for op, r, v in zip(ops, rhos, outs):
+        p1, d1 = _ptr(r, int(np.prod(op.gridin.shape)))
+        p2, d2 = _ptr(v, int(np.prod(op.gridout.shape)))
+        rp.append(p1.value)
+        vp.append(p2.value)
+        devs.update((d1, d2))
+    if len(devs) > 1:
+        raise ValueError("cubes must all be host arrays or all CUDA tensors")
+    dev = devs.pop() if devs else False
+    flags = (_capi.DAGE_DEVICE_PTRS if dev else 0) | (_capi.DAGE_ENERGY if energy else 0)
+    flags |= 0 if coda else _capi.DAGE_NO_CODA
+    arr = lambda xs: (ctypes.c_void_p * n)(*xs)
+    e = np.zeros(max(n, 1))
+    check(load().dage_op3d_apply_batched(n, arr([op._h.value for op in ops]), arr(rp), arr(vp),
+                                         flags, e.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return e[:n] if energy else None
+
+
 class Coulomb3D(Operator3D):
     """Coulomb3D (src/bubbles/coulomb.F90:109-195), cube part:
     w_p = 2/sqrt(pi) tw_p, coda = pi/tlog^2."""

@@ -95,6 +95,15 @@ int dage_op3d_create(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3]
 int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
                     double *energy);
 
+/* n applies queued back to back (each as dage_op3d_apply with the same
+ * flags) on their operators' streams, with one wait per distinct operator at
+ * the end: applies on distinct operators overlap.  energies[i] receives apply
+ * i's energy with DAGE_ENERGY.  An operator's last_time_ms covers its last
+ * apply of the batch.  Replaces the per-orbital loop of operate calls with
+ * Operator3D_transform_cuda_cube (src/bubbles/function3d.F90:4354-4480). */
+int dage_op3d_apply_batched(int n, dage_op3d *const *ops, const double *const *rho,
+                            double *const *V, unsigned flags, double *energies);
+
 /* Replaces the quadrature weights (length P = nlin+nlog).
  * Operator3D%set_transformation_weights, used by Helmholtz3D_set_energy
  * (src/bubbles/helmholtz3d.F90:411-444). */

@@ -236,3 +236,29 @@ def test_invalid_arguments_raise(dage):
         op.set_transformation_weights(np.ones(3))
     with pytest.raises(ValueError):
         op.apply(np.zeros((3, 3, 3), order="F"))
+
+
+def test_apply_batched_matches_single_applies(dage, oracle):
+    """Several densities through two operators (FP64 and split precision) in
+    one batched call, device and host cubes, equal to one apply each."""
+    import torch
+
+    g = dage.Grid3D.cube(-3.0, 5, 0.2)
+    go = oracle.Grid3D.cube(-3.0, 5, 0.2)
+    quad = dage.GaussQuad(6, 6)
+    op64 = dage.Coulomb3D(g, quad=quad)
+    opmx = dage.Coulomb3D(g, quad=quad, precision="bf16x6")
+    rng = np.random.default_rng(11)
+    rhos = [oracle.gauss_cube(go, rng.uniform(0.5, 2, 2), rng.uniform(0.5, 4, 2),
+                              rng.uniform(-1, 1, (2, 3))) for _ in range(4)]
+    ops = [op64, opmx, op64, opmx]
+    want = [op.apply(r, energy=True) for op, r in zip(ops, rhos)]
+    outs = [np.zeros(go.shape, order="F") for _ in rhos]
+    E = dage.apply_batched(ops, rhos, outs, energy=True)
+    for (Vw, Ew), V, e in zip(want, outs, E):
+        assert np.array_equal(V, Vw) and e == Ew
+    drho = [torch.from_numpy(r.reshape(-1, order="F").copy()).cuda() for r in rhos]
+    dout = [torch.empty_like(r) for r in drho]
+    E2 = dage.apply_batched(ops, drho, dout, energy=True)
+    for (Vw, Ew), V, e in zip(want, dout, E2):
+        assert np.array_equal(V.cpu().numpy(), Vw.reshape(-1, order="F")) and e == Ew
