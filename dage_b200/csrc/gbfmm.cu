@@ -484,22 +484,39 @@ __global__ void helm_m2l_matrices_kernel(const double *__restrict__ R, int rblk,
 }
 
 // L(b) = sum over the far field of b of T(disp) q(src); block (box, density).
+// kM2LGroups thread groups of Npad threads share a target box: group h takes
+// the sources e = start + h, start + h + kM2LGroups, ... and the groups'
+// sums are added in group order (deterministic).
+constexpr int kM2LGroups = 4;
+
 __global__ void m2l_apply_kernel(const GInst *__restrict__ insts, int N) {
-  extern __shared__ double qs[];
+  extern __shared__ double qs[];  // [kM2LGroups][N] sources, then [kM2LGroups][N] sums
   const GInst &I = insts[blockIdx.y];
   const int b = blockIdx.x;
+  const int npad = blockDim.x / kM2LGroups;
+  const int h = threadIdx.x / npad, i = threadIdx.x % npad;
+  double *q = qs + (size_t)h * N;
   double acc = 0.0;
-  const int i = threadIdx.x;
-  for (int e = I.ffstart[b]; e < I.ffstart[b + 1]; ++e) {
+  const int e0 = I.ffstart[b], e1 = I.ffstart[b + 1];
+  for (int base = e0; base < e1; base += kM2LGroups) {
+    const int e = base + h;
     __syncthreads();
-    for (int k = threadIdx.x; k < N; k += blockDim.x) qs[k] = I.q[(size_t)I.ffsrc[e] * N + k];
+    if (e < e1)
+      for (int k = i; k < N; k += npad) q[k] = I.q[(size_t)I.ffsrc[e] * N + k];
     __syncthreads();
-    if (i < N) {
+    if (e < e1 && i < N) {
       const double *T = I.Tm2l + (size_t)I.ffdisp[e] * N * N;
-      for (int k = 0; k < N; ++k) acc += T[(size_t)k * N + i] * qs[k];
+      for (int k = 0; k < N; ++k) acc += T[(size_t)k * N + i] * q[k];
     }
   }
-  if (i < N) I.L[(size_t)b * N + i] = acc;
+  double *sums = qs + (size_t)kM2LGroups * N;
+  if (i < N) sums[(size_t)h * N + i] = acc;
+  __syncthreads();
+  if (h == 0 && i < N) {
+    double t = sums[i];
+    for (int g = 1; g < kM2LGroups; ++g) t += sums[(size_t)g * N + i];
+    I.L[(size_t)b * N + i] = t;
+  }
 }
 
 // Translation matrices W(d) of the distinct child-to-parent displacements
@@ -1627,8 +1644,9 @@ int run_multipoles(const GInst *d_inst, int ninst, int nbox, int lmax, int nslab
 }
 
 int run_m2l(const GInst *d_inst, int ninst, int nbox, int N, cudaStream_t s) {
-  const int threads = ((N + 31) / 32) * 32;
-  m2l_apply_kernel<<<dim3(nbox, ninst), threads, sizeof(double) * N, s>>>(d_inst, N);
+  const int threads = ((N + 31) / 32) * 32 * kM2LGroups;  // N <= 256: at most 1024
+  m2l_apply_kernel<<<dim3(nbox, ninst), threads, sizeof(double) * N * 2 * kM2LGroups, s>>>(d_inst,
+                                                                                        N);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
