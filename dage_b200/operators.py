@@ -246,6 +246,14 @@ class Operator3D:
 
     __call__ = apply
 
+    def operate_on(self, cube, bubbles: "Bubbles | None" = None, out=None):
+        """Operator3D_operate_on_Function3D (function3d.F90:3727-3882) for a
+        function held as a cube plus bubbles: (V cube, V bubbles) with the
+        cube operator applied to the cube and the radial Coulomb potential
+        of the bubbles (coulomb.F90:222-336; None without bubbles)."""
+        V = self.apply(cube, out)
+        return V, (bubbles.coulomb_potential() if bubbles is not None else None)
+
 
 def apply_batched(ops, rhos, outs, energy: bool = False, coda: bool = True):
     """Applies ops[i] to rhos[i] into outs[i] for every i, all queued before
@@ -300,6 +308,14 @@ class Helmholtz3D:
             check(load().dage_op3d_set_energy(self.coulomb_operator._h, 0.0))
 
     __call__ = apply
+
+    def operate_on(self, cube, bubbles: "Bubbles | None" = None, out=None):
+        """Helmholtz3D_operate (helmholtz3d.F90:445-481): the cube operator at
+        this energy applied to the cube, and the radial Helmholtz potential
+        of the bubbles (Helmholtz3D_transform_bubbles_sub, :519-650; None
+        without bubbles)."""
+        V = self.apply(cube, out)
+        return V, (bubbles.helmholtz_potential(self.energy) if bubbles is not None else None)
 
 
 def integrate(grid: Grid3D, f1, f2=None) -> float:

@@ -122,3 +122,24 @@ def test_helmholtz_potential_needs_negative_energy(dage, oracle):
     b = dage.Bubbles([[0.0, 0.0, 0.0]], [dage.Grid1D(0.0, 33, 7, 1, h)], [np.exp(-r)[None, :]], 0)
     with pytest.raises(dage.DageError):
         b.helmholtz_potential(0.0)
+
+
+def test_operate_on_cube_and_bubbles(dage, oracle):
+    """operate_on: the cube operator on the cube part and the radial
+    potential of the bubbles (Coulomb and Helmholtz)."""
+    centers, ncells, hs, f = _bubbles(oracle, 2, 2)
+    rad = [dage.Grid1D(0.0, n, 7, 1, h) for n, h in zip(ncells, hs)]
+    b = dage.Bubbles(centers, rad, f, 2)
+    g = dage.Grid3D.cube(-2.4, 4, 0.2)
+    cube = np.asfortranarray(np.random.default_rng(2).standard_normal(tuple(a.n for a in g.axes)))
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(4, 4))
+    V, Vb = op.operate_on(cube, b)
+    assert np.array_equal(V, op.apply(cube))
+    for a in range(2):
+        ref = oracle.bubbles_coulomb_potential(ncells[a], hs[a], 2, f[a])
+        assert np.abs(Vb.radial_values()[a] - ref).max() <= 1e-12 * np.abs(ref).max()
+    hop = dage.Helmholtz3D(op, -0.5)
+    V2, Vb2 = hop.operate_on(cube, b)
+    assert np.array_equal(V2, hop.apply(cube))
+    ref = oracle.bubbles_helmholtz_potential(ncells[0], hs[0], 2, f[0], 1.0)
+    assert np.abs(Vb2.radial_values()[0] - ref).max() <= 1e-12 * np.abs(ref).max()
