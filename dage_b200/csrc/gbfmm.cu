@@ -484,16 +484,15 @@ __global__ void helm_m2l_matrices_kernel(const double *__restrict__ R, int rblk,
 }
 
 // L(b) = sum over the far field of b of T(disp) q(src); block (box, density).
-// kM2LGroups thread groups of Npad threads share a target box: group h takes
-// the sources e = start + h, start + h + kM2LGroups, ... and the groups'
-// sums are added in group order (deterministic).
-constexpr int kM2LGroups = 4;
-
-__global__ void m2l_apply_kernel(const GInst *__restrict__ insts, int N) {
-  extern __shared__ double qs[];  // [kM2LGroups][N] sources, then [kM2LGroups][N] sums
+// G = blockDim.x / npad thread groups of npad (N rounded up to warps)
+// threads share a target box: group h takes the sources e = start + h,
+// start + h + G, ... and the groups' sums are added in group order
+// (deterministic).
+__global__ void m2l_apply_kernel(const GInst *__restrict__ insts, int N, int npad) {
+  extern __shared__ double qs[];  // [G][N] sources, then [G][N] sums
   const GInst &I = insts[blockIdx.y];
   const int b = blockIdx.x;
-  const int npad = blockDim.x / kM2LGroups;
+  const int kM2LGroups = blockDim.x / npad;
   const int h = threadIdx.x / npad, i = threadIdx.x % npad;
   double *q = qs + (size_t)h * N;
   double acc = 0.0;
@@ -1644,9 +1643,10 @@ int run_multipoles(const GInst *d_inst, int ninst, int nbox, int lmax, int nslab
 }
 
 int run_m2l(const GInst *d_inst, int ninst, int nbox, int N, cudaStream_t s) {
-  const int threads = ((N + 31) / 32) * 32 * kM2LGroups;  // N <= 256: at most 1024
-  m2l_apply_kernel<<<dim3(nbox, ninst), threads, sizeof(double) * N * 2 * kM2LGroups, s>>>(d_inst,
-                                                                                        N);
+  const int npad = ((N + 31) / 32) * 32;           // N <= 256
+  const int groups = std::max(1, std::min(8, 1024 / npad));
+  m2l_apply_kernel<<<dim3(nbox, ninst), npad * groups, sizeof(double) * N * 2 * groups, s>>>(
+      d_inst, N, npad);
   DAGE_CUDA_TRY(cudaGetLastError());
   return 0;
 }
