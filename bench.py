@@ -596,33 +596,41 @@ def run_workload(args, world, rank, local):
               {"workload": wl, "points_per_axis": 121, "step_bohr": 0.2, "t_points": 40,
                "gaussians": 2, "seed": SEED}, clocks, 3 * 40 + 2,
               {"accuracy": {"vs": "analytic sum q erf(sqrt(a) r)/r", "max_rel": err}})
-    elif wl in ("gbfmm_241", "gbfmm_241_adaptive"):
+    elif wl in ("gbfmm_241", "gbfmm_241_adaptive", "helmholtz_gbfmm_241", "helmholtz_gbfmm_241"):
         # FP64 GBFMM, 241^3 (40 cells, step 0.2), 4^3 boxes, lmax 12, 16 Gaussians
-        # (the adaptive variant: the reference's adaptive mode, level-1 moments)
+        # (the adaptive variant: the reference's adaptive mode, level-1 moments;
+        # the Helmholtz variant: kernel e^(-kappa r)/r at E = -0.5, kappa = 1)
         adaptive = wl.endswith("adaptive")
+        helm = wl.startswith("helmholtz")
         rng = np.random.default_rng(SEED)
         q, a = rng.uniform(-1, 2, 16), rng.uniform(0.3, 6, 16)
         c = rng.uniform(-24, 24, (16, 3))
         g = dage.Grid3D.cube(-24.0, 40, 0.2)
         rho = _gauss_cube(dev, 40, 0.2, q, a, c)
         quad = dage.GaussQuad(20, 20, 0.0, TLIN, TLOG)
-        op = dage.GBFMMCoulomb3D(g, lmax=12, quad=quad, adaptive_mode=adaptive)
+        op = (dage.GBFMMHelmholtz3D(g, -0.5, lmax=12, quad=quad) if helm
+              else dage.GBFMMCoulomb3D(g, lmax=12, quad=quad, adaptive_mode=adaptive))
         V = torch.empty_like(rho)
         clk.start()
         ms = _timed(lambda: op.apply(rho, out=V, energy=True), args.steps, args.warmup, sync)
         clocks = clk.stop()
         _, E = op.apply(rho, out=V, energy=True)
         Vd = torch.empty_like(rho)
-        _, Ed = dage.Coulomb3D(g, quad=quad).apply(rho, out=Vd, energy=True, coda=False)
+        direct = dage.Coulomb3D(g, quad=quad)
+        if helm:
+            direct = dage.Helmholtz3D(direct, -0.5)
+        _, Ed = direct.apply(rho, out=Vd, energy=True, coda=False)
         err = float((V - Vd).abs().max() / Vd.abs().max())
         n = 241 ** 3
-        _line(args, world, "GBFMM Coulomb Mpts/s @241^3 FP64 (lmax 12, 4^3 boxes%s)"
-              % (", adaptive mode" if adaptive else ""), n / ms / 1e3,
+        _line(args, world, "GBFMM %s Mpts/s @241^3 FP64 (lmax 12, 4^3 boxes%s)"
+              % ("Helmholtz (kappa 1)" if helm else "Coulomb",
+                 ", adaptive mode" if adaptive else ""), n / ms / 1e3,
               "Mpts/s", ms, "f64",
               {"workload": wl, "points_per_axis": 241, "step_bohr": 0.2, "t_points": 40,
                "lmax": 12, "boxes": 64, "gaussians": 16, "seed": SEED,
                "near_field_tiles": list(op.tiles)}, clocks, 3 * 40 + 9,
-              {"accuracy": {"vs": "single-box FP64 operator (no coda)", "max_rel": err,
+              {"accuracy": {"vs": "single-box FP64 operator of the same kernel (no coda)",
+                            "max_rel": err,
                             "energy_rel": abs(E - Ed) / abs(Ed)}})
     elif wl == "bubbles_inject_301":
         rng = np.random.default_rng(SEED)
@@ -754,7 +762,7 @@ def main():
     ap.add_argument("--n-cell", type=int, default=N_CELL,
                     help="cells per axis (80 -> 481^3, the headline workload)")
     ap.add_argument("--workload", default="coulomb_cube_481",
-                    choices=["coulomb_cube_481", "coulomb_cube_121", "gbfmm_241", "gbfmm_241_adaptive",
+                    choices=["coulomb_cube_481", "coulomb_cube_121", "gbfmm_241", "gbfmm_241_adaptive", "helmholtz_gbfmm_241",
                              "gbfmm_batch_256", "helmholtz_step_301", "bubbles_inject_301",
                              "density_product_301"],
                     help="coulomb_cube_481 is the headline line; the others time the other "
