@@ -613,13 +613,18 @@ __global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__rest
 
 // Helmholtz L2P, V(r) += 8 kappa sum (2l+1)/(4 pi) i_l(kappa r) Y_lm L_lm
 // (src/gbfmm/gbfmm_helmholtz3d.F90:1019-1105), with the multipole kernel's
-// lane tasks: lane p(lmax+1)+t evaluates task t's harmonics of point p, the
-// Bessel ratio f_t(kappa r) of its point (exchanged between the point's
-// lanes), and the point's lanes sum their terms with a segmented shuffle
-// reduction.  Block (chunk, box, density); Coulomb instances return.
+// lane tasks: lane p(lmax+1)+t evaluates task t's harmonics of point p and
+// the point's lanes sum their terms with a segmented shuffle reduction.  The
+// Bessel ratios f_l(kappa r), l = 0..lmax, come first for 32 points per
+// warp, one lane per point (series for lmax and lmax - 1, then the downward
+// recursion f_l = (2l+3) f_{l+1} + (kappa r)^2 f_{l+2}), into shared memory.
+// Block (chunk, box, density); Coulomb instances return.
+constexpr int kL2pHelmWarps = 8;
+
 __global__ void __launch_bounds__(256)
     l2p_helm_kernel(const GInst *__restrict__ insts, const double *__restrict__ Lext, int lmax) {
   __shared__ double sA[16 * 16], sB[16 * 16], sLt[16 * 16];  // [k][t]
+  __shared__ double sF[kL2pHelmWarps][32][17];              // [warp][point][l]
   const GInst &I = insts[blockIdx.z];
   if (!(I.kappa > 0.0)) return;
   const int L = lmax, L1 = lmax + 1, N = L1 * L1;
@@ -647,11 +652,27 @@ __global__ void __launch_bounds__(256)
   const double *xs = I.wbox + (3 * 64) * I.wstride;
   const int ws = I.wstride;
   const long long n = (long long)b.own[0] * b.own[1] * b.own[2];
-  const long long stride = (long long)gridDim.x * (blockDim.x >> 5) * PP;
-  for (long long base = ((long long)blockIdx.x * (blockDim.x >> 5) + warp) * PP; base < n;
-       base += stride) {
-    const long long e = base + p;
-    const bool valid = p < PP && e < n;
+  double(*F)[17] = sF[warp];
+  const long long stride32 = (long long)gridDim.x * (blockDim.x >> 5) * 32;
+  for (long long base32 = ((long long)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base32 < n;
+       base32 += stride32) {
+  {  // Bessel ratios of the 32 points, lane = point
+    const long long e = min(base32 + lane, n - 1);
+    const int i = (int)(e % b.own[0]);
+    const long long r = e / b.own[0];
+    const int j = (int)(r % b.own[1]), k = (int)(r / b.own[1]);
+    const double x = xs[b.p0[0] + i] - b.c[0], y = xs[ws + b.p0[1] + j] - b.c[1],
+                 z = xs[2 * ws + b.p0[2] + k] - b.c[2];
+    const double x2 = (kappa * kappa) * (x * x + y * y + z * z);
+    double *f = F[lane];
+    f[L] = bessel_ratio_series(0.5 * x2, L);
+    if (L >= 1) f[L - 1] = bessel_ratio_series(0.5 * x2, L - 1);
+    for (int l = L - 2; l >= 0; --l) f[l] = (2 * l + 3) * f[l + 1] + x2 * f[l + 2];
+  }
+  __syncwarp();
+  for (int sub = 0; sub < 32; sub += PP) {
+    const long long e = base32 + sub + p;
+    const bool valid = p < PP && sub + p < 32 && e < n;
     const long long ee = valid ? e : 0;
     const int i = (int)(ee % b.own[0]);
     const long long r = ee / b.own[0];
@@ -674,7 +695,7 @@ __global__ void __launch_bounds__(256)
         if (mm == a2) s2 = m2 > 0 ? top : bot;
       }
     }
-    const double fown = bessel_ratio_series(0.5 * (kappa * kappa) * r2, t);
+    const double *fp = F[valid ? sub + p : 0];
     double acc = 0.0, p1 = 0.0, p2 = 0.0;
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
@@ -684,8 +705,7 @@ __global__ void __launch_bounds__(256)
       const double cur = st ? (kk == 0 ? s1 : s2) : rec;
       p2 = st ? 0.0 : p1;
       p1 = cur;
-      const double f =
-          __shfl_sync(0xffffffffu, fown, (p * L1 + (kk < len1 ? a1 + kk : a2 + kk - len1)) & 31);
+      const double f = fp[kk < len1 ? a1 + kk : a2 + kk - len1];
       acc += (sLt[kk * 16 + t] * f) * cur;
     }
     // segmented sum over the point's lanes t = 0..L (fixed order)
@@ -695,6 +715,8 @@ __global__ void __launch_bounds__(256)
       if (t + off < L1) acc += o;
     }
     if (valid && t == 0) I.V[(size_t)gx + (size_t)I.Nx * gy + (size_t)I.Nx * I.Ny * gz] += acc;
+  }
+  __syncwarp();
   }
 }
 
@@ -1682,7 +1704,7 @@ int run_l2p(const GInst *d_inst, int ninst, int nbox, int lmax, int maxown, cons
   l2p_kernel<<<dim3(bx, nbox, ninst), 128, sizeof(double) * N, s>>>(d_inst, Lext, lmax);
   DAGE_CUDA_TRY(cudaGetLastError());
   if (helm) {
-    const int pts = 8 * (32 / (lmax + 1));  // points per block pass
+    const int pts = kL2pHelmWarps * 32;  // points per block pass
     const int hx = std::min((maxown + pts - 1) / pts, 256);
     l2p_helm_kernel<<<dim3(hx, nbox, ninst), 256, 0, s>>>(d_inst, Lext, lmax);
     DAGE_CUDA_TRY(cudaGetLastError());
