@@ -318,8 +318,6 @@ __global__ void __launch_bounds__(kMpWarps * 32, HELM ? 2 : 3)
   mp_task(L, t, m1, m2, len1);
   const int a1 = abs(m1), a2 = abs(m2), amax = t == 0 ? 0 : max(a1, a2);
   const bool helm = HELM && I.kappa > 0.0;  // a batch may mix kernels
-  double kap_t = 1.0;  // kappa^t
-  for (int l = 0; l < t; ++l) kap_t *= I.kappa;
   const BoxInfo b = I.boxes[blockIdx.x];
   const int ws = I.wstride;
   const double *wx = I.wbox + (0 * 64 + b.pos[0]) * ws;
@@ -359,29 +357,69 @@ __global__ void __launch_bounds__(kMpWarps * 32, HELM ? 2 : 3)
     }
     const double *rcol = I.rho + (size_t)(b.p0[0] + ii) + (size_t)I.Nx * (b.p0[1] + j) +
                          plane * b.p0[2];
-    for (int kz = 0; kz < b.np[2]; ++kz) {
-      const double v = valid ? rcol[plane * kz] * (wxy * wz[kz]) : 0.0;
-      const double z = xs[2 * ws + b.p0[2] + kz] - b.c[2];
-      const double r2 = x * x + y * y + z * z;
-      // Helmholtz: i_l(kappa r) Y_lm(rhat) = kappa^l f_l(kappa r) S_lm(r); lane
-      // t of a point evaluates f_t for its point and the lanes of the point
-      // exchange them (the lane of step k needs l_k)
-      double gown = 0.0;
-      if (helm) gown = v * kap_t * bessel_ratio_series(0.5 * (I.kappa * I.kappa) * r2, t);
-      double p1 = 0.0, p2 = 0.0;
+    // Helmholtz: i_l(kappa r) Y_lm(rhat) = kappa^l f_l(kappa r) S_lm(r).  The
+    // factors g_l = kappa^l f_l of the bundle's next CZ z values of each of
+    // its PP columns come first, one lane per point (series for L and L - 1,
+    // downward recursion), into this warp's rows of `red` (free until the
+    // final reduction).
+    if constexpr (!HELM) {
+      for (int kz = 0; kz < b.np[2]; ++kz) {
+        const double v = valid ? rcol[plane * kz] * (wxy * wz[kz]) : 0.0;
+        const double z = xs[2 * ws + b.p0[2] + kz] - b.c[2];
+        const double r2 = x * x + y * y + z * z;
+        double p1 = 0.0, p2 = 0.0;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        if (k > L) break;
-        const bool st = k == 0 || k == len1;
-        const double rec = sA[k * 16 + t] * (z * p1) - sB[k * 16 + t] * (r2 * p2);
-        const double cur = st ? (k == 0 ? s1 : s2) : rec;
-        p2 = st ? 0.0 : p1;
-        p1 = cur;
-        double f = v;
-        if (helm)
-          f = __shfl_sync(0xffffffffu, gown, (p * L1 + (k < len1 ? a1 + k : a2 + k - len1)) & 31);
-        acc[k] += f * cur;
+        for (int k = 0; k < 16; ++k) {
+          if (k > L) break;
+          const bool st = k == 0 || k == len1;
+          const double rec = sA[k * 16 + t] * (z * p1) - sB[k * 16 + t] * (r2 * p2);
+          const double cur = st ? (k == 0 ? s1 : s2) : rec;
+          p2 = st ? 0.0 : p1;
+          p1 = cur;
+          acc[k] += v * cur;
+        }
       }
+      continue;
+    }
+    const int CZ = 32 / PP;
+    const int pi = p < PP ? p : 0;
+    for (int kz0 = 0; kz0 < b.np[2]; kz0 += CZ) {
+      if (helm) {
+        const int ic = min((u % nib) * PP + lane / CZ, b.np[0] - 1);
+        const int kc = min(kz0 + lane % CZ, b.np[2] - 1);
+        const double xc = xs[b.p0[0] + ic] - b.c[0], zc = xs[2 * ws + b.p0[2] + kc] - b.c[2];
+        const double x2 = (I.kappa * I.kappa) * (xc * xc + y * y + zc * zc);
+        double *g = red[warp][lane];
+        g[L] = bessel_ratio_series(0.5 * x2, L);
+        if (L >= 1) g[L - 1] = bessel_ratio_series(0.5 * x2, L - 1);
+        for (int l = L - 2; l >= 0; --l) g[l] = (2 * l + 3) * g[l + 1] + x2 * g[l + 2];
+        double kp = 1.0;
+        for (int l = 0; l <= L; ++l) {
+          g[l] *= kp;
+          kp *= I.kappa;
+        }
+        __syncwarp();
+      }
+      const int kzend = min(kz0 + CZ, b.np[2]);
+      for (int kz = kz0; kz < kzend; ++kz) {
+        const double v = valid ? rcol[plane * kz] * (wxy * wz[kz]) : 0.0;
+        const double z = xs[2 * ws + b.p0[2] + kz] - b.c[2];
+        const double r2 = x * x + y * y + z * z;
+        const double *gp = red[warp][pi * CZ + (kz - kz0)];
+        double p1 = 0.0, p2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          if (k > L) break;
+          const bool st = k == 0 || k == len1;
+          const double rec = sA[k * 16 + t] * (z * p1) - sB[k * 16 + t] * (r2 * p2);
+          const double cur = st ? (k == 0 ? s1 : s2) : rec;
+          p2 = st ? 0.0 : p1;
+          p1 = cur;
+          const double f = helm ? v * gp[k < len1 ? a1 + k : a2 + k - len1] : v;
+          acc[k] += f * cur;
+        }
+      }
+      if (helm) __syncwarp();
     }
   }
 #pragma unroll
