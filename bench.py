@@ -190,14 +190,22 @@ def profiled_traffic(kernel: str, workload: str, precision: str | None = None):
     return None
 
 
+def headline_config(n: int, world: int) -> dict:
+    """The `config` of the headline line, shared by the GPU and CPU arms."""
+    return {"workload": f"coulomb_cube_{n}", "points_per_axis": n, "step_bohr": STEP,
+            "t_points": NLIN + NLOG, "gaussians": N_GAUSS, "seed": SEED,
+            "l2": f"inputs larger than L2 (rho {8 * n ** 3 / 1e9:.2f} GB)",
+            "parallelism": f"replicas x{world}"}
+
+
 # ---------------------------------------------------------------------------
 # CPU arms
 # ---------------------------------------------------------------------------
 _CPU_SETUP = {}
 
 
-def _cpu_setup(n_cell, step, n_t):
-    key = (n_cell, step, n_t)
+def _cpu_setup(n_cell, step):
+    key = (n_cell, step)
     if key not in _CPU_SETUP:
         from oracle import oracle as O
 
@@ -206,48 +214,53 @@ def _cpu_setup(n_cell, step, n_t):
         q, a, c = gaussians()
         rho = O.gauss_cube(g, q, a, c)
         tp, tw = O.gauss_quad(NLIN, NLOG, 0.0, TLIN, TLOG)
-        idx = np.linspace(0, len(tp) - 1, n_t).round().astype(int)
-        T = O.coulomb_matrix(g.axes[0], g.axes[0].points, tp[idx])
-        w = O.coulomb_weights(tw)[idx]
+        T = O.coulomb_matrix(g.axes[0], g.axes[0].points, tp)
+        w = O.coulomb_weights(tw)
         _CPU_SETUP.clear()
         _CPU_SETUP[key] = (g, rho, tp, T, w)
     return _CPU_SETUP[key]
 
 
-def cpu_sample(n_cell=N_CELL, step=STEP, n_t=1, threads=None):
+def cpu_sample(n_cell=N_CELL, step=STEP, ip=0):
     """Times the CPU restatement (oracle, numpy/OpenBLAS DGEMM per mode
-    product) on a bounded sample: n_t of the 64 t-points of the 481^3
-    operator.  Returns (Mpts/s scaled to all 64 t-points, seconds, sample
-    description, threads)."""
+    product, all host threads) on one t-point (index ip) of the 481^3
+    operator: 1/64 of an apply.  Returns (seconds, points, t-points)."""
     from oracle import oracle as O
 
-    g, rho, tp, T, w = _cpu_setup(n_cell, step, n_t)
+    g, rho, tp, T, w = _cpu_setup(n_cell, step)
+    ip = ip % len(tp)
     t0 = time.perf_counter()
-    O.transform_cube_blas(T, T, T, w, rho, 0.0)
-    dt = time.perf_counter() - t0
-    npts = float(g.shape[0]) ** 3
-    per_apply = dt * len(tp) / n_t
-    ncores = threads or os.cpu_count()
-    return npts / per_apply / 1e6, dt, f"{n_t} of {len(tp)} t-points of the {g.shape[0]}^3 apply, scaled x{len(tp) / n_t:.0f}", ncores
+    O.transform_cube_blas(T, T, T, w, rho, 0.0, p_subset=[ip])
+    return time.perf_counter() - t0, float(g.shape[0]) ** 3, len(tp)
 
 
 def run_reference(args, world, rank):
+    """The reference algorithm's CPU path on the host cores.  One step = one
+    t-point of the 481^3 apply (1/64 of the work of one apply; the dense
+    DGEMMs cost the same for every t-point), cycling through the t-points;
+    the line's rate is points x t-points processed / time, i.e. the apply
+    rate, and the per-apply time it implies is reported as extrapolated."""
     if rank != 0:
         return
-    steps = []
+    times = []
+    npts = n_t = None
     for i in range(args.warmup + args.steps):
-        v, dt, sample, cores = cpu_sample(n_t=1)
+        dt, npts, n_t = cpu_sample(ip=i * 13)
         if i >= args.warmup:
-            steps.append(v)
-    value = float(np.median(steps))
+            times.append(dt)
+    sample_s = float(np.mean(times))
+    value = npts / (sample_s * n_t) / 1e6
     n = N_CELL * 6 + 1
+    cores = os.cpu_count()
+    sample = (f"{args.steps} timed steps of one t-point each (of {n_t}) of the {n}^3 apply, "
+              f"OpenBLAS DGEMM on {cores} host threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpts/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": float(n ** 3 / value / 1e6 * 1e3), "higher_is_better": True,
+        "ms_per_step": sample_s * 1e3, "step": f"one t-point of {n_t} (1/{n_t} of an apply)",
+        "extrapolated_ms_per_apply": sample_s * n_t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "coulomb_cube_481", "points_per_axis": n, "t_points": NLIN + NLOG,
-                   "gaussians": N_GAUSS, "seed": SEED},
+        "config": headline_config(n, world),
         "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -426,11 +439,14 @@ def run_gpu(args, world, rank, local):
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         nrep = max(1, args.fp64_steps)
+        clk64 = ClockSampler(local)
+        clk64.start()
         f0.record()
         for _ in range(nrep):
             op64.apply(rho, out=V64, energy=True)
         f1.record()
         torch.cuda.synchronize()
+        clocks64 = clk64.stop()
         fp64_ms = f0.elapsed_time(f1) / nrep
         fp64_mpts = npts / (fp64_ms / 1e3) / 1e6
         d = (V - V64).abs()
@@ -442,8 +458,12 @@ def run_gpu(args, world, rank, local):
             "fp64_ms_per_step": fp64_ms,
             "fp64_mpts": fp64_mpts,
             "speedup_vs_fp64": fp64_ms / ms,
+            "fp64_steps": nrep, "fp64_clocks": clocks64,
             "vs_analytic": analytic_errors(V, V64, ncell, q, a, c, dev),
         }
+        if clocks.get("sm_mhz") and clocks64.get("sm_mhz"):
+            # the same ratio in cycles (time x median SM clock of each arm)
+            accuracy["speedup_vs_fp64_cycles"] = (fp64_ms * clocks64["sm_mhz"]) / (ms * clocks["sm_mhz"])
         del op64
         if not args.skip_alt:
             # the other split-precision mode on the same input, same checks
@@ -479,9 +499,14 @@ def run_gpu(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        v, dt, sample, cores = cpu_sample(n_cell=ncell, n_t=1)
-        cpu = {"value": v, "unit": "Mpts/s", "cores": cores, "kind": "port", "sample": sample,
-               "seconds": dt}
+        dts = [cpu_sample(n_cell=ncell, ip=13 * i)[0] for i in range(4)]
+        dt = float(np.mean(dts[1:]))
+        cores = os.cpu_count()
+        cpu = {"value": npts / (dt * (NLIN + NLOG)) / 1e6, "unit": "Mpts/s", "cores": cores,
+               "kind": "port",
+               "sample": f"3 of the {NLIN + NLOG} t-points of the {n}^3 apply after one warm-up "
+                         f"(OpenBLAS DGEMM, {cores} host threads); rate = points x t-points / time",
+               "seconds_per_t_point": dt}
 
     if rank == 0:
         line = {
@@ -490,10 +515,7 @@ def run_gpu(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16" if prec != "fp64" else "f64", "precision": prec,
             "data": "synthetic",
-            "config": {"workload": f"coulomb_cube_{n}", "points_per_axis": n, "step_bohr": STEP,
-                       "t_points": NLIN + NLOG, "gaussians": N_GAUSS, "seed": SEED,
-                       "l2": "inputs larger than L2 (rho 0.89 GB)",
-                       "parallelism": f"replicas x{world}"},
+            "config": headline_config(n, world),
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": int(launches), "accuracy": accuracy, "energy": energy,
             "alternative": alternative,
@@ -754,7 +776,7 @@ def main():
     ap.add_argument("--impl", default="dage", choices=["dage", "reference"])
     ap.add_argument("--precision", default=os.environ.get("DAGE_BENCH_PRECISION", "bf16x3"),
                     choices=["fp64", "bf16x3", "bf16x6"])
-    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=5)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")

@@ -199,6 +199,12 @@ int sh_tables_init() {
   }
   DAGE_CUDA_TRY(cudaMemcpyToSymbol(d_rc, rc.data(), sizeof(double) * rc.size()));
   DAGE_CUDA_TRY(cudaMemcpyToSymbol(c_dfinv, dfinv, sizeof(dfinv)));
+  // These copies come from pageable memory on the legacy stream: they may
+  // return before the DMA lands, and the kernels that read the tables run on
+  // non-blocking streams, which are not ordered after the legacy stream.
+  // Without this wait a kernel could read zeros (a Bessel series cut to its
+  // leading term, harmonics of zero).
+  DAGE_CUDA_TRY(cudaDeviceSynchronize());
   if (dev < 64) done |= 1ull << dev;
   return 0;
 }
@@ -419,9 +425,14 @@ __global__ void __launch_bounds__(kMpWarps * 32, HELM ? 2 : 3)
           acc[k] += f * cur;
         }
       }
+      // Required before the next chunk's factors overwrite `red` and before
+      // the final store below overwrites it with this lane's sums: every
+      // lane of the warp must be done reading the factor rows.
       if (helm) __syncwarp();
     }
   }
+  // (Helmholtz: ordered after the last reads of the factor rows by the
+  // __syncwarp at the end of the chunk loop above.)
 #pragma unroll
   for (int k = 0; k < 16; ++k)
     if (k <= L) red[warp][lane][k] = acc[k];
@@ -658,8 +669,9 @@ __global__ void l2p_kernel(const GInst *__restrict__ insts, const double *__rest
 // recursion f_l = (2l+3) f_{l+1} + (kappa r)^2 f_{l+2}), into shared memory.
 // Block (chunk, box, density); Coulomb instances return.
 constexpr int kL2pHelmWarps = 8;
+constexpr int kL2pHelmThreads = kL2pHelmWarps * 32;  // sF has one row block per warp
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kL2pHelmThreads)
     l2p_helm_kernel(const GInst *__restrict__ insts, const double *__restrict__ Lext, int lmax) {
   __shared__ double sA[16 * 16], sB[16 * 16], sLt[16 * 16];  // [k][t]
   __shared__ double sF[kL2pHelmWarps][32][17];              // [warp][point][l]
@@ -1742,9 +1754,9 @@ int run_l2p(const GInst *d_inst, int ninst, int nbox, int lmax, int maxown, cons
   l2p_kernel<<<dim3(bx, nbox, ninst), 128, sizeof(double) * N, s>>>(d_inst, Lext, lmax);
   DAGE_CUDA_TRY(cudaGetLastError());
   if (helm) {
-    const int pts = kL2pHelmWarps * 32;  // points per block pass
+    const int pts = kL2pHelmThreads;  // points per block pass (one per thread)
     const int hx = std::min((maxown + pts - 1) / pts, 256);
-    l2p_helm_kernel<<<dim3(hx, nbox, ninst), 256, 0, s>>>(d_inst, Lext, lmax);
+    l2p_helm_kernel<<<dim3(hx, nbox, ninst), kL2pHelmThreads, 0, s>>>(d_inst, Lext, lmax);
     DAGE_CUDA_TRY(cudaGetLastError());
   }
   return 0;

@@ -141,6 +141,10 @@ void orc_bessel_i(double x, int lmax, double *out);
 void orc_bessel_k(double x, int lmax, double *out);
 void orc_aligned_ml(const double *bessel, int lmax, int lin, double *out);
 void orc_rotation(const double *dhat, int lmax, double *out);
+void orc_ref_real_rotation(double alpha, double beta, double gamma, int lmax, int repaired,
+                           double *out);
+int orc_helm_m2l_lsq(int lmax, int lin, double kappa, const double *M, const double *src,
+                     const double *dst, double *L);
 int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double *src,
                  const double *dst, double *L);
 int orc_helm_box_multipoles(int lmax, double kappa, int nx, const double *px, const double *wx,

@@ -4,13 +4,13 @@
 // translation, rotation back) and local-expansion evaluation.
 //
 // TEST INFRASTRUCTURE ONLY (see dage_oracle.h).  Each routine restates the
-// reference routine cited beside it.  The one deliberate difference: the
-// rotation of real spherical-harmonic expansions is computed from its
-// defining property (the rotated expansion represents the same function in
-// a frame whose z axis is the translation direction) by least squares on the
-// solid harmonics, where the reference uses the recursions of Blanco, Florez
-// & Bermejo (J. Mol. Struct. Theochem 419 (1997) 19) in
-// helmholtz_multipole_tools.F90:919-1200; both are the exact rotation.
+// reference routine cited beside it.  The rotation of real
+// spherical-harmonic expansions follows the reference's recursions of
+// Blanco, Florez & Bermejo (J. Mol. Struct. Theochem 419 (1997) 19),
+// helmholtz_multipole_tools.F90:911-1200, with the reference's Euler angles
+// (:695-701) and its forward/backward rotation (:240-256).  orc_rotation, a
+// rotation computed instead from its defining property by least squares on
+// the solid harmonics, is kept as an independent check of that restatement.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -40,6 +40,223 @@ ext bessel_i_series(ext z, int n) {
     reslt += addition;
   }
   return prefactor * reslt;
+}
+
+// helmholtz_multipole_tools.F90:1003-1200 get_rotation_coefficient_matrices:
+// the small-d matrices d^l_{m' m}(beta) by the recursions of Blanco, Florez &
+// Bermejo, stored as the reference's array reslt(-lmax:lmax, 0:lmax, 0:lmax)
+// indexed (m', m, l), m >= 0.
+struct DMat {
+  int L;
+  std::vector<double> v;
+  explicit DMat(int lmax) : L(lmax), v((size_t)(2 * lmax + 1) * (lmax + 1) * (lmax + 1), 0.0) {}
+  double &operator()(int mp, int m, int l) {
+    return v[((size_t)l * (L + 1) + m) * (2 * L + 1) + (mp + L)];
+  }
+};
+
+double fact_int(int x) {  // the reference's factorial: integer(16) product
+  unsigned __int128 r = 1;
+  for (int i = 1; i <= x; ++i) r *= (unsigned __int128)i;
+  return (double)r;
+}
+
+double ipow(double b, int e) {  // Fortran x**n for integer n
+  double r = 1.0;
+  for (int i = 0; i < e; ++i) r *= b;
+  return r;
+}
+
+// Explicit Wigner sum for one small-d entry in the reference's convention
+// R(m', m, l), in extended precision (used by the repaired recursion only).
+double wigner_d(int l, int m, int mp, double beta) {
+  // R(m', m, l) = d^l_{m m'}(beta) with d^j_{a b} = sum_s (-1)^(a - b + s)
+  //   sqrt((j+a)!(j-a)!(j+b)!(j-b)!) / ((j+b-s)! s! (a-b+s)! (j-a-s)!)
+  //   cos(beta/2)^(2j+b-a-2s) sin(beta/2)^(a-b+2s)
+  const int a = m, b = mp;
+  const long double c = cosl(0.5L * beta), s = sinl(0.5L * beta);
+  auto f = [](int n) {
+    long double r = 1.0L;
+    for (int i = 2; i <= n; ++i) r *= i;
+    return r;
+  };
+  long double sum = 0.0L;
+  for (int k = 0; k <= 2 * l; ++k) {
+    if (l + b - k < 0 || a - b + k < 0 || l - a - k < 0) continue;
+    const long double den = f(l + b - k) * f(k) * f(a - b + k) * f(l - a - k);
+    const long double term = powl(c, 2 * l + b - a - 2 * k) * powl(s, a - b + 2 * k) / den;
+    sum += ((a - b + k) % 2 ? -1.0L : 1.0L) * term;
+  }
+  return (double)(sqrtl(f(l + a) * f(l - a) * f(l + b) * f(l - b)) * sum);
+}
+
+// repaired = false: the reference as written.  repaired = true: its two
+// defects corrected -- the single-precision literal sqrt(2.0) (:1018; every
+// rotation then carries ~3e-8 relative error) becomes a double, and the rows
+// m = l - 1 of eq. 68 (:1119-1131), whose step divides by l cos(beta) - m'
+// and hits 0/0 where l cos(beta) is an integer (e.g. the lattice direction
+// (2, 1, 2) at l = 3, 6, 9, ...; the reference's epsilon guard then zeroes the
+// rest of the row), are taken from the explicit Wigner sum (wigner_d).
+void ref_rotation_dmatrices(double beta, int lmax, DMat &R, bool repaired) {
+  const double pi = 3.14159265358979323846;
+  // sqrt(2.0): a default-real (single-precision) literal in the reference
+  const double sqrt_2 = repaired ? std::sqrt(2.0) : (double)std::sqrt(2.0f);
+  const double cos_beta = std::cos(beta), sin_beta = std::sin(beta);
+  const double cos_beta_p2 = std::cos(0.5 * beta), sin_beta_p2 = std::sin(0.5 * beta);
+  const double tan_beta_p2 = std::tan(0.5 * beta);
+  R(0, 0, 0) = 1.0;
+  if (lmax < 1) return;
+  R(0, 0, 1) = cos_beta;
+  R(-1, 1, 1) = std::pow(sin_beta_p2, 2.0);
+  R(0, 1, 1) = -1.0 / sqrt_2 * sin_beta;
+  R(-1, 0, 1) = R(0, 1, 1);
+  R(1, 0, 1) = -1.0 * R(0, 1, 1);
+  R(1, 1, 1) = cos_beta_p2 * cos_beta_p2;
+  auto general = [&](int l) {
+    for (int m = 0; m <= l - 2; ++m) {
+      for (int mp = -m; mp <= 0; ++mp) {
+        R(mp, m, l) = l * (2 * l - 1) / std::sqrt((double)((l * l - m * m) * (l * l - mp * mp))) *
+                      ((R(0, 0, 1) - m * mp / (double)(l * (l - 1))) * R(mp, m, l - 1) -
+                       std::sqrt((double)(((l - 1) * (l - 1) - m * m) * ((l - 1) * (l - 1) - mp * mp))) *
+                           R(mp, m, l - 2) / ((l - 1) * (2 * l - 1)));
+        R(-m, -mp, l) = R(mp, m, l);
+      }
+      R(m, 0, l) = ipow(-1.0, m) * R(0, m, l);
+      for (int mp = 1; mp <= m; ++mp) {
+        R(mp, m, l) = l * (2 * l - 1) / std::sqrt((double)((l * l - m * m) * (l * l - mp * mp))) *
+                      ((R(0, 0, 1) - m * mp / (double)(l * (l - 1))) * R(mp, m, l - 1) -
+                       std::sqrt((double)(((l - 1) * (l - 1) - m * m) * ((l - 1) * (l - 1) - mp * mp))) *
+                           R(mp, m, l - 2) / ((l - 1) * (2 * l - 1)));
+        R(m, mp, l) = ipow(-1.0, mp + m) * R(mp, m, l);
+      }
+    }
+    R(l, l, l) = R(1, 1, 1) * R(l - 1, l - 1, l - 1);
+    R(l - 1, l - 1, l) = (l * R(0, 0, 1) - l + 1) * R(l - 1, l - 1, l - 1);
+  };
+  auto eq67 = [&](int l) {
+    for (int mp = -1; mp >= -l + 1; --mp) {
+      R(mp, l - 1, l) = (l * cos_beta - mp) *
+                        std::sqrt(fact_int(2 * l - 1) / (fact_int(l + mp) * fact_int(l - mp))) *
+                        ipow(cos_beta_p2, l + mp - 1) * ipow(-sin_beta_p2, l - mp - 1);
+      R(-(l - 1), -mp, l) = R(mp, l - 1, l);
+    }
+  };
+  if ((pi - std::fabs(beta)) > 1e-5) {
+    for (int l = 2; l <= lmax; ++l) {
+      general(l);
+      for (int mp = l; mp >= 1; --mp) {
+        R(mp - 1, l, l) = -1.0 * std::sqrt((double)(l + mp) / (double)(l - mp + 1)) * tan_beta_p2 *
+                          R(mp, l, l);
+        R(l, mp - 1, l) = ipow(-1.0, l + mp - 1) * R(mp - 1, l, l);
+      }
+      R(-l, 0, l) = R(0, l, l);
+      R(l, 0, l) = ipow(-1.0, l) * R(0, l, l);
+      for (int mp = 0; mp >= -l + 1; --mp) {
+        R(mp - 1, l, l) = -1.0 * std::sqrt((double)(l + mp) / (double)(l - mp + 1)) * tan_beta_p2 *
+                          R(mp, l, l);
+        R(-l, -(mp - 1), l) = R(mp - 1, l, l);
+      }
+      R(-l + 1, l, l) = std::sqrt(fact_int(2 * l) / (fact_int(1) * fact_int(2 * l - 1))) *
+                        ipow(cos_beta_p2, 1) * ipow(-sin_beta_p2, 2 * l - 1);
+      for (int mp = l - 1; mp >= 1 && repaired; --mp) {
+        R(mp - 1, l - 1, l) = wigner_d(l, l - 1, mp - 1, beta);
+        R(l - 1, mp - 1, l) = ipow(-1.0, l - 1 + mp - 1) * R(mp - 1, l - 1, l);
+      }
+      for (int mp = l - 1; mp >= 1 && !repaired; --mp) {
+        if (std::fabs(R(mp, l - 1, l)) > 2.220446049250313e-16)
+          R(mp - 1, l - 1, l) = -1.0 * (l * cos_beta - mp + 1) / (l * cos_beta - mp) *
+                                std::sqrt((double)(l + mp) / (double)(l - mp + 1)) * tan_beta_p2 *
+                                R(mp, l - 1, l);
+        else
+          R(mp - 1, l - 1, l) = 0.0;
+        R(l - 1, mp - 1, l) = ipow(-1.0, l - 1 + mp - 1) * R(mp - 1, l - 1, l);
+      }
+      R(-(l - 1), 0, l) = R(0, l - 1, l);
+      R((l - 1), 0, l) = ipow(-1.0, l - 1) * R(0, l - 1, l);
+      eq67(l);
+    }
+  } else {
+    for (int l = 2; l <= lmax; ++l) {
+      general(l);
+      for (int mp = -lmax; mp <= lmax; ++mp) R(mp, l, l) = 0.0;
+      for (int m = 0; m <= lmax; ++m) R(-l, m, l) = 0.0;
+      for (int mp = -lmax; mp <= lmax; ++mp) R(mp, l - 1, l) = 0.0;
+      for (int m = 0; m <= lmax; ++m) R(-(l - 1), m, l) = 0.0;
+      R(-l, l, l) = 1.0;
+      R(1 - l, l - 1, l) = -1.0;
+      R(-(l - 1), -(1 - l), l) = -1.0;
+      eq67(l);
+    }
+  }
+}
+
+// helmholtz_multipole_tools.F90:911-1001 get_real_spherical_harmonic_
+// rotation_coefficients: out[l][(m'+l)(2l+1) + (m+l)] = reslt(m', m, l) for
+// Euler angles (alpha, beta, gamma), m the original order, m' the new.
+void ref_real_rotation(double alpha, double beta, double gamma, int lmax,
+                       std::vector<std::vector<double>> &out, bool repaired) {
+  const double sqrt_2 = std::sqrt(2.0);
+  std::vector<double> cma(lmax + 1), sma(lmax + 1), cmg(lmax + 1), smg(lmax + 1);
+  for (int m = 0; m <= lmax; ++m) {
+    cma[m] = std::cos(m * alpha);
+    sma[m] = std::sin(m * alpha);
+    cmg[m] = std::cos(m * gamma);
+    smg[m] = std::sin(m * gamma);
+  }
+  DMat D(lmax);
+  ref_rotation_dmatrices(beta, lmax, D, repaired);
+  out.assign(lmax + 1, {});
+  for (int l = 0; l <= lmax; ++l) {
+    const int w = 2 * l + 1;
+    std::vector<double> &r = out[l];
+    r.assign((size_t)w * w, 0.0);
+    auto at = [&](int mp, int m) -> double & { return r[(size_t)(mp + l) * w + (m + l)]; };
+    for (int m = -l; m <= -1; ++m) {
+      const double sg = ipow(-1.0, -m);
+      for (int mp = -l; mp <= -1; ++mp)
+        at(mp, m) = -2.0 * sma[-m] * smg[-mp] * (D(-m, -mp, l) + sg * D(mp, -m, l)) / 2.0 +
+                    2.0 * cma[-m] * cmg[-mp] * (D(-m, -mp, l) - sg * D(mp, -m, l)) / 2.0;
+      at(0, m) = sqrt_2 * sma[-m] * (D(-m, 0, l) + sg * D(0, -m, l)) / 2.0 +
+                 sqrt_2 * cma[-m] * (D(-m, 0, l) - sg * D(0, -m, l)) / 2.0;
+      for (int mp = 1; mp <= l; ++mp)
+        at(mp, m) = +2.0 * sma[-m] * cmg[mp] * (D(-m, mp, l) + sg * D(-mp, -m, l)) / 2.0 +
+                    2.0 * cma[-m] * smg[mp] * (D(-m, mp, l) - sg * D(-mp, -m, l)) / 2.0;
+    }
+    for (int mp = -l; mp <= -1; ++mp)
+      at(mp, 0) = -sqrt_2 * smg[-mp] * (D(0, -mp, l) + D(mp, 0, l)) / 2.0 -
+                  sqrt_2 * cmg[-mp] * (D(0, -mp, l) - D(mp, 0, l)) / 2.0;
+    at(0, 0) = 1.0 * (D(0, 0, l) + D(0, 0, l)) / 2.0;
+    for (int mp = 1; mp <= l; ++mp)
+      at(mp, 0) = sqrt_2 * cmg[mp] * (D(0, mp, l) + D(-mp, 0, l)) / 2.0 -
+                  sqrt_2 * smg[mp] * (D(0, mp, l) - D(-mp, 0, l)) / 2.0;
+    for (int m = 1; m <= l; ++m) {
+      const double sg = ipow(-1.0, m);
+      for (int mp = -l; mp <= -1; ++mp)
+        at(mp, m) = -2.0 * cma[m] * smg[-mp] * (D(m, -mp, l) + sg * D(mp, m, l)) / 2.0 -
+                    2.0 * sma[m] * cmg[-mp] * (D(m, -mp, l) - sg * D(mp, m, l)) / 2.0;
+      at(0, m) = sqrt_2 * cma[m] * (D(m, 0, l) + sg * D(0, m, l)) / 2.0 -
+                 sqrt_2 * sma[m] * (D(m, 0, l) - sg * D(0, m, l)) / 2.0;
+      for (int mp = 1; mp <= l; ++mp)
+        at(mp, m) = 2.0 * cma[m] * cmg[mp] * (D(m, mp, l) + sg * D(-mp, m, l)) / 2.0 -
+                    2.0 * sma[m] * smg[mp] * (D(m, mp, l) - sg * D(-mp, m, l)) / 2.0;
+    }
+  }
+}
+
+// helmholtz_multipole_tools.F90:737-758 rotate_real_spherical_harmonic_
+// expansion: reslt(l, m) = sum_m2 coefficients(m, m2, l) values(l, m2).
+void ref_rotate_real(const double *in, int lmax, double alpha, double beta, double gamma,
+                     double *out, bool repaired) {
+  std::vector<std::vector<double>> C;
+  ref_real_rotation(alpha, beta, gamma, lmax, C, repaired);
+  for (int l = 0; l <= lmax; ++l) {
+    const int w = 2 * l + 1;
+    for (int m = -l; m <= l; ++m) {
+      double s = 0.0;
+      for (int m2 = -l; m2 <= l; ++m2) s += C[l][(size_t)(m + l) * w + (m2 + l)] * in[lm_map(l, m2)];
+      out[lm_map(l, m)] = s;
+    }
+  }
 }
 
 }  // namespace
@@ -193,45 +410,61 @@ void orc_rotation(const double *dhat, int lmax, double *out) {
   }
 }
 
-// helmholtz_multipole_tools.F90:172-278 HelmholtzExpansionTranslator_
-// translate_real with the HelmholtzMultipoleConverter (:385-426): Racah ->
-// orthonormal scaling, rotation to the axis destination - source, coaxial
-// translation (real basis: C(l, n, |m|) acting on (n, m) for both signs of m,
-// :280-331 with :760-800), rotation back, orthonormal -> Racah scaling.
-int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double *src,
-                 const double *dst, double *L) {
+// Exposed for the oracle's own tests: the reference's real rotation
+// coefficients, blocks l = 0..lmax of (2l+1)^2 values, [m'][m].
+void orc_ref_real_rotation(double alpha, double beta, double gamma, int lmax, int repaired,
+                           double *out) {
+  std::vector<std::vector<double>> C;
+  ref_real_rotation(alpha, beta, gamma, lmax, C, repaired != 0);
+  size_t off = 0;
+  for (int l = 0; l <= lmax; ++l) {
+    std::memcpy(out + off, C[l].data(), sizeof(double) * C[l].size());
+    off += C[l].size();
+  }
+}
+
+// Multipole-to-local conversion: Racah -> orthonormal scaling, rotation to
+// the axis destination - source, coaxial translation (real basis:
+// C(l, n, |m|) acting on (n, m) for both signs of m, :280-331 with
+// :760-800), rotation back, orthonormal -> Racah scaling.
+static int helm_m2l_impl(int lmax, int lin, double kappa, const double *M, const double *src,
+                         const double *dst, double *L, bool lsq) {
   const double pi = 3.14159265358979323846;
   const double d[3] = {dst[0] - src[0], dst[1] - src[1], dst[2] - src[2]};
   const double dist = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
   if (dist == 0.0) return -1;
-  const int Lr = lmax > lin ? lmax : lin;
   const int Nin = (lin + 1) * (lin + 1), Nout = (lmax + 1) * (lmax + 1);
-  std::vector<double> R(0);
-  {
-    size_t tot = 0;
-    for (int l = 0; l <= Lr; ++l) tot += (size_t)(2 * l + 1) * (2 * l + 1);
-    R.resize(tot);
-  }
-  orc_rotation(d, Lr, R.data());
+  // Racah -> orthonormal scaling of the input (:209-214)
+  std::vector<double> a(Nin, 0.0), t(Nin, 0.0);
+  for (int l = 0; l <= lin; ++l)
+    for (int m = -l; m <= l; ++m) t[lm_map(l, m)] = std::sqrt((2 * l + 1) / (4 * pi)) * M[lm_map(l, m)];
+  // rotation to the frame whose z axis is (destination - source) / distance
+  const double zv[3] = {d[0] / dist, d[1] / dist, d[2] / dist};
+  const double beta = std::acos(zv[2]), alpha = std::atan2(zv[1], zv[0]), gamma = 0.0;  // :695-701
+  const int Lr = lmax > lin ? lmax : lin;
+  std::vector<double> R;
   std::vector<size_t> roff(Lr + 2, 0);
-  for (int l = 0; l <= Lr; ++l) roff[l + 1] = roff[l] + (size_t)(2 * l + 1) * (2 * l + 1);
-  // scale and rotate the input
-  std::vector<double> a(Nin, 0.0);
-  for (int l = 0; l <= lin; ++l) {
-    const int w = 2 * l + 1;
-    const double sc = std::sqrt((2 * l + 1) / (4 * pi));
-    for (int mp = -l; mp <= l; ++mp) {
-      double s = 0.0;
-      for (int m = -l; m <= l; ++m) s += R[roff[l] + (size_t)(mp + l) * w + (m + l)] * M[lm_map(l, m)];
-      a[lm_map(l, mp)] = sc * s;
+  if (lsq) {
+    for (int l = 0; l <= Lr; ++l) roff[l + 1] = roff[l] + (size_t)(2 * l + 1) * (2 * l + 1);
+    R.resize(roff[Lr + 1]);
+    orc_rotation(d, Lr, R.data());
+    for (int l = 0; l <= lin; ++l) {
+      const int w = 2 * l + 1;
+      for (int mp = -l; mp <= l; ++mp) {
+        double s = 0.0;
+        for (int m = -l; m <= l; ++m) s += R[roff[l] + (size_t)(mp + l) * w + (m + l)] * t[lm_map(l, m)];
+        a[lm_map(l, mp)] = s;
+      }
     }
+  } else {
+    ref_rotate_real(t.data(), lin, alpha, beta, gamma, a.data(), true);  // :240-241
   }
-  // coaxial translation
+  // coaxial translation (:245-246)
   std::vector<double> bess(lin + 2);
   orc_bessel_k(kappa * dist, lin + 1, bess.data());
   std::vector<double> C((size_t)(lmax + 1) * (lin + 1) * (lmax + 1));
   orc_aligned_ml(bess.data(), lmax, lin, C.data());
-  std::vector<double> b(Nout, 0.0);
+  std::vector<double> b(Nout, 0.0), c(Nout, 0.0);
   for (int l = 0; l <= lmax; ++l)
     for (int m = -l; m <= l; ++m) {
       const int am = std::abs(m);
@@ -240,17 +473,37 @@ int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double 
         s += C[((size_t)l * (lin + 1) + n) * (lmax + 1) + am] * a[lm_map(n, m)];
       b[lm_map(l, m)] = s;
     }
-  // rotate back (R is orthogonal) and rescale
-  for (int l = 0; l <= lmax; ++l) {
-    const int w = 2 * l + 1;
-    const double sc = std::sqrt(4 * pi / (2 * l + 1));
-    for (int m = -l; m <= l; ++m) {
-      double s = 0.0;
-      for (int mp = -l; mp <= l; ++mp) s += R[roff[l] + (size_t)(mp + l) * w + (m + l)] * b[lm_map(l, mp)];
-      L[lm_map(l, m)] = sc * s;
+  // rotation back (:252-253) and orthonormal -> Racah scaling (:256-261)
+  if (lsq) {
+    for (int l = 0; l <= lmax; ++l) {
+      const int w = 2 * l + 1;
+      for (int m = -l; m <= l; ++m) {
+        double s = 0.0;
+        for (int mp = -l; mp <= l; ++mp) s += R[roff[l] + (size_t)(mp + l) * w + (m + l)] * b[lm_map(l, mp)];
+        c[lm_map(l, m)] = s;
+      }
     }
+  } else {
+    ref_rotate_real(b.data(), lmax, -gamma, -beta, -alpha, c.data(), true);
   }
+  for (int l = 0; l <= lmax; ++l)
+    for (int m = -l; m <= l; ++m) L[lm_map(l, m)] = std::sqrt(4 * pi / (2 * l + 1)) * c[lm_map(l, m)];
   return 0;
+}
+
+// helmholtz_multipole_tools.F90:172-278 HelmholtzExpansionTranslator_
+// translate_real with the HelmholtzMultipoleConverter (:385-426), the
+// rotations by the reference's recursions (ref_rotate_real).
+int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double *src,
+                 const double *dst, double *L) {
+  return helm_m2l_impl(lmax, lin, kappa, M, src, dst, L, false);
+}
+
+// The same conversion with the least-squares rotation (orc_rotation): an
+// independent check of the recursion restatement.
+int orc_helm_m2l_lsq(int lmax, int lin, double kappa, const double *M, const double *src,
+                     const double *dst, double *L) {
+  return helm_m2l_impl(lmax, lin, kappa, M, src, dst, L, true);
 }
 
 // gbfmm_helmholtz3d.F90:1491-1577: q_lm(box) = sum rho w i_l(kappa r) Y_lm(rhat)

@@ -49,6 +49,8 @@ def lib(libm_1ulp: bool = False):
             "orc_aligned_ml": (None, [_D, _I, _I, _D]),
             "orc_rotation": (None, [_D, _I, _D]),
             "orc_helm_m2l": (_I, [_I, _I, _F, _D, _D, _D, _D]),
+            "orc_helm_m2l_lsq": (_I, [_I, _I, _F, _D, _D, _D, _D]),
+            "orc_ref_real_rotation": (None, [_F, _F, _F, _I, _I, _D]),
             "orc_helm_box_multipoles": (_I, [_I, _F, _I, _D, _D, _I, _D, _D, _I, _D, _D, _D, _D,
                                              _D]),
             "orc_helm_l2p": (_I, [_I, _F, _D, _D, _I, _D, _I, _D, _I, _D, _D]),
@@ -520,16 +522,35 @@ def helm_box_multipoles(lmax, kappa, px, wx, py, wy, pz, wz, cube_sub, center):
     return q
 
 
-def helm_m2l(lmax, kappa, M, src, dst, lin=None):
+def helm_m2l(lmax, kappa, M, src, dst, lin=None, least_squares=False):
     """Local expansion at dst of the Helmholtz multipoles M at src
-    (HelmholtzMultipoleConverter, helmholtz_multipole_tools.F90:172-511)."""
+    (HelmholtzMultipoleConverter, helmholtz_multipole_tools.F90:172-511),
+    rotating with the reference's recursions (:911-1200); least_squares:
+    with the independent least-squares rotation instead."""
     lin = lmax if lin is None else lin
     L = np.zeros((lmax + 1) ** 2)
-    rc = lib().orc_helm_m2l(lmax, lin, float(kappa), _p(_f64(M)), _p(_f64(src)), _p(_f64(dst)),
-                            _p(L))
+    fn = lib().orc_helm_m2l_lsq if least_squares else lib().orc_helm_m2l
+    rc = fn(lmax, lin, float(kappa), _p(_f64(M)), _p(_f64(src)), _p(_f64(dst)), _p(L))
     if rc:
         raise ValueError("zero translation distance")
     return L
+
+
+def ref_real_rotation(alpha, beta, gamma, lmax, repaired=True):
+    """The reference's real spherical-harmonic rotation coefficients
+    (get_real_spherical_harmonic_rotation_coefficients,
+    helmholtz_multipole_tools.F90:911-1001): a list over l of (2l+1, 2l+1)
+    arrays [m' + l, m + l].  repaired=False: exactly as the reference computes
+    them, with its single-precision sqrt(2.0) and the 0/0 of its eq. 68 step."""
+    out = np.zeros(sum((2 * l + 1) ** 2 for l in range(lmax + 1)))
+    lib().orc_ref_real_rotation(float(alpha), float(beta), float(gamma), lmax, int(repaired),
+                                _p(out))
+    blocks, off = [], 0
+    for l in range(lmax + 1):
+        w = 2 * l + 1
+        blocks.append(out[off:off + w * w].reshape(w, w))
+        off += w * w
+    return blocks
 
 
 def helm_l2p(lmax, kappa, L, center, px, py, pz, out):
@@ -679,8 +700,32 @@ def _far_field_levels(plan, q_fine, lmax, adaptive=False):
     return Lprev
 
 
+def gbfmm_near_field(grid: Grid3D, rho, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
+                     libm_1ulp=False, energy=0.0, blas=False) -> np.ndarray:
+    """Near-field part of the GBFMM potential (gbfmm_coulomb3d.F90:933-1098):
+    each box's sub-operator (coulomb.F90:517-635) applied to the density on
+    the box's near-field cells, written to the points the box owns (no coda).
+    energy < 0: Helmholtz weights.  blas: the contractions as DGEMMs."""
+    plan = GBFMMPlan(grid, maxlevel)
+    rho = np.asfortranarray(rho)
+    tp, tw = gauss_quad(*quad)
+    w = helmholtz_weights(tp, tw, energy) if energy < 0.0 else coulomb_weights(tw)
+    Vnear = np.zeros(grid.shape, order="F")
+    for b in range(1, plan.nbox + 1):
+        ncl = plan.near_cells(b)
+        gin = [subgrid(a, c0, c1) for a, (c0, c1) in zip(grid.axes, ncl)]
+        own = plan.owned(b)
+        outs = [grid.axes[d].points[own[d][0]:own[d][1]] for d in range(3)]
+        Ts = [coulomb_matrix(gin[d], outs[d], tp, libm_1ulp=libm_1ulp) for d in range(3)]
+        pin = [((c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1) + 1) for a, (c0, c1) in zip(grid.axes, ncl)]
+        sub = np.asfortranarray(rho[pin[0][0]:pin[0][1], pin[1][0]:pin[1][1], pin[2][0]:pin[2][1]])
+        vn = (transform_cube_blas if blas else transform_cube)(*Ts, w, sub, 0.0)
+        Vnear[tuple(slice(o0, o1) for o0, o1 in own)] = vn
+    return Vnear
+
+
 def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 1.0e3),
-                return_parts=False, libm_1ulp=False, energy=0.0, adaptive=False):
+                return_parts=False, libm_1ulp=False, energy=0.0, adaptive=False, blas=False):
     """GBFMMCoulomb3D_calculate_potential along the reference's CUDA path
     (gbfmm_coulomb3d.F90:650-819, gbfmm_coulomb3d.cu:478-573): multipoles per
     box, M2L over the local far field, near field by the sub-operator of
@@ -689,7 +734,9 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
     GBFMMHelmholtz3D kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)
     (gbfmm_helmholtz3d.F90:478-1105): Helmholtz near-field weights, Bessel
     multipoles, the Helmholtz multipole-to-local converter and L2P.
-    adaptive: the reference's adaptive mode (Coulomb only, _far_field_levels)."""
+    adaptive: the reference's adaptive mode (Coulomb only, _far_field_levels).
+    blas: each box's near-field contraction as DGEMMs (transform_cube_blas,
+    the same sums in BLAS order; for grids of 181^3 and more)."""
     plan = GBFMMPlan(grid, maxlevel)
     rho = np.asfortranarray(rho)
     N = (lmax + 1) ** 2
@@ -716,27 +763,17 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
                     L[:, i - 1] += helm_m2l(lmax, kappa, q[:, j - 1], plan.center(j), ci)
                 else:
                     L[:, i - 1] += interaction_matrix(lmax, plan.center(j) - ci) @ q[:, j - 1]
-    tp, tw = gauss_quad(*quad)
-    w = helmholtz_weights(tp, tw, energy) if helm else coulomb_weights(tw)
-    V = np.zeros(grid.shape, order="F")
-    Vnear = np.zeros(grid.shape, order="F")
+    Vnear = gbfmm_near_field(grid, rho, maxlevel, quad, libm_1ulp, energy, blas)
+    V = Vnear.copy(order="F")
     for b in range(1, plan.nbox + 1):
-        ncl = plan.near_cells(b)
-        gin = [subgrid(a, c0, c1) for a, (c0, c1) in zip(grid.axes, ncl)]
         own = plan.owned(b)
         outs = [grid.axes[d].points[own[d][0]:own[d][1]] for d in range(3)]
-        Ts = [coulomb_matrix(gin[d], outs[d], tp, libm_1ulp=libm_1ulp) for d in range(3)]
-        pin = [((c0 - 1) * (a.nlip - 1), c1 * (a.nlip - 1) + 1) for a, (c0, c1) in zip(grid.axes, ncl)]
-        sub = np.asfortranarray(rho[pin[0][0]:pin[0][1], pin[1][0]:pin[1][1], pin[2][0]:pin[2][1]])
-        vn = transform_cube(*Ts, w, sub, 0.0)
-        far = np.zeros(vn.shape, order="F")
+        far = np.zeros(tuple(len(o) for o in outs), order="F")
         if helm:
             helm_l2p(lmax, kappa, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
         else:
             l2p(lmax, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
-        sl = tuple(slice(o0, o1) for o0, o1 in own)
-        V[sl] = vn + far
-        Vnear[sl] = vn
+        V[tuple(slice(o0, o1) for o0, o1 in own)] += far
     if return_parts:
         return V, q, L, Vnear
     return V

@@ -48,3 +48,14 @@ def test_abi_version_and_error_string_without_gpu():
     assert lib.dage_op3d_create(None, None, None, 0, None) == -1
     assert b"null" in lib.dage_last_error()
     assert lib.dage_set_wait_limit(0) == -1
+
+
+def test_fortran_interface_block_binds_every_entry_point():
+    """The Fortran module in INTEGRATION.md binds each C symbol the header
+    declares (bind(C, name="...")), and nothing else."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = doc[doc.index("```fortran\nmodule dage_gpu_m"):]
+    block = block[:block.index("end module")]
+    bound = set(re.findall(r'bind\(C, name="(dage_[a-z0-9_]+)"\)', block))
+    assert bound == declared_functions(), (sorted(declared_functions() - bound),
+                                           sorted(bound - declared_functions()))

@@ -19,9 +19,12 @@ def _setup(dage, oracle, ncell, step=0.2, ng=6, seed=3):
     return g, go, oracle.gauss_cube(go, q, a, c)
 
 
-@pytest.mark.parametrize("ncell,energy", [(16, -0.5), (15, -1.2)])  # 15 cells: uneven split
-def test_helmholtz_moments_and_local_expansions(dage, oracle, ncell, energy):
-    lmax = 8
+# 15 cells: uneven split (box point counts not a multiple of the moment
+# kernel's chunk of z values, 32 / (32 // (lmax + 1))); lmax 0 has no
+# lmax - 1 series, lmax 1 no downward recursion
+@pytest.mark.parametrize("ncell,energy,lmax", [(16, -0.5, 8), (15, -1.2, 8), (15, -0.7, 0),
+                                               (15, -0.9, 1), (15, -1.5, 15)])
+def test_helmholtz_moments_and_local_expansions(dage, oracle, ncell, energy, lmax):
     kappa = np.sqrt(-2 * energy)
     g, go, rho = _setup(dage, oracle, ncell)
     op = dage.GBFMMHelmholtz3D(g, energy, lmax=lmax, quad=dage.GaussQuad(6, 6))
@@ -93,3 +96,33 @@ def test_helmholtz_l2p_matches_oracle(dage, oracle, lmax, energy):
         oracle.helm_l2p(lmax, kappa, L[:, b - 1], plan.center(b), outs[0], outs[1], outs[2], far)
         Vo[tuple(slice(o0, o1) for o0, o1 in own)] = far
     assert np.abs(V - Vo).max() <= 1e-12 * np.abs(Vo).max()
+
+
+@pytest.mark.parametrize("lmax,energy", [(8, -0.18), (12, -0.5), (15, -1.2)])
+def test_helmholtz_l2p_plane_wave_identity(dage, oracle, lmax, energy):
+    """The plane-wave expansion sum_l (2l+1) i_l(kappa r) P_l(cos theta) =
+    e^(kappa z) (the identity behind tests/multipole_translation_test.F90
+    first_bessel_test): with L_l0 = 4 pi / (8 kappa) and every other
+    coefficient zero, the GPU's L2P is e^(kappa (z - c_z)) at every point of
+    every box, up to the truncation at lmax (bounded with the oracle's i_l)."""
+    kappa = np.sqrt(-2 * energy)
+    g, go, rho = _setup(dage, oracle, 8)
+    op = dage.GBFMMHelmholtz3D(g, energy, lmax=lmax, quad=dage.GaussQuad(4, 4))
+    plan = oracle.GBFMMPlan(go, 2)
+    L = np.zeros(((lmax + 1) ** 2, plan.nbox))
+    for l in range(lmax + 1):
+        L[l * (l + 1), :] = 4 * np.pi / (8 * kappa)
+    V = np.zeros(go.shape, order="F")
+    op.evaluate_local_expansions(L, V)
+    Vx = np.zeros(go.shape, order="F")
+    rmax = 0.0
+    for b in range(1, plan.nbox + 1):
+        own = plan.owned(b)
+        c = plan.center(b)
+        pts = [go.axes[d].points[own[d][0]:own[d][1]] - c[d] for d in range(3)]
+        Vx[tuple(slice(o0, o1) for o0, o1 in own)] = np.exp(kappa * pts[2])[None, None, :]
+        rmax = max(rmax, np.sqrt(sum(np.abs(p).max() ** 2 for p in pts)))
+    lt = np.arange(lmax + 1, lmax + 30)
+    tail = ((2 * lt + 1) * oracle.bessel_i(kappa * rmax, lmax + 29)[lmax + 1:]).sum()
+    err = np.abs(V - Vx).max()
+    assert err <= 2 * tail + 1e-13 * np.abs(Vx).max(), (err, tail)

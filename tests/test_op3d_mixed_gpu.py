@@ -47,6 +47,8 @@ def test_mixed_vs_fp64(dage, oracle, prec, axes, quad):
 
 @pytest.mark.parametrize("prec", ["bf16x6", "bf16x3"])
 def test_mixed_config1_121(dage, oracle, prec):
+    """The single-box configuration (121^3, 2 Gaussians, 40 t-points) at
+    the target bars, 1e-6 potential and 1e-7 energy, for both modes."""
     rng = np.random.default_rng(1)
     q = rng.uniform(0.5, 2, 2)
     a = rng.uniform(0.5, 4, 2)
@@ -58,7 +60,8 @@ def test_mixed_config1_121(dage, oracle, prec):
     V64, E64 = dage.Coulomb3D(g, quad=quad).apply(rho, energy=True)
     V, E = dage.Coulomb3D(g, quad=quad, precision=prec).apply(rho, energy=True)
     ev, ee = _errs(V, V64, E, E64)
-    assert ev <= BARS[prec][0] and ee <= BARS[prec][1], (ev, ee)
+    print(f"  {prec} at 121^3: potential {ev:.2e}, energy {ee:.2e}")
+    assert ev <= 1e-6 and ee <= 1e-7, (ev, ee)
 
 
 def test_mixed_repeatable_and_linear(dage, oracle):
@@ -76,8 +79,11 @@ def test_mixed_helmholtz(dage, oracle):
     g, go, rho, q = _case(dage, oracle, ((-3.0, 5, 0.2),) * 3, (8, 8, 0.0, 2.0, 1e3))
     E = -0.5 * 1.2 ** 2
     V64 = dage.Helmholtz3D(dage.Coulomb3D(g, quad=q), E).apply(rho)
-    V = dage.Helmholtz3D(dage.Coulomb3D(g, quad=q, precision="bf16x6"), E).apply(rho)
-    assert np.abs(V - V64).max() <= 2e-6 * np.abs(V64).max()
+    for prec in ("bf16x6", "bf16x3"):
+        V = dage.Helmholtz3D(dage.Coulomb3D(g, quad=q, precision=prec), E).apply(rho)
+        err = np.abs(V - V64).max() / np.abs(V64).max()
+        print(f"  {prec} Helmholtz: potential {err:.2e}")
+        assert err <= 1e-6, (prec, err)
 
 
 def test_mixed_device_pointers(dage, oracle):

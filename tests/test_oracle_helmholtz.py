@@ -53,3 +53,75 @@ def test_m2l_is_linear_and_zero_free(oracle):
     L2 = oracle.helm_m2l(6, 1.3, M2, a, b)
     L12 = oracle.helm_m2l(6, 1.3, 2 * M1 - M2, a, b)
     assert np.allclose(L12, 2 * L1 - L2, rtol=1e-12, atol=1e-14 * np.abs(L1).max())
+
+
+def test_reference_bessel_identities(oracle):
+    """The identities tests/multipole_translation_test.F90 evaluates
+    (first_bessel_test :567-603, potential_test :519-565; the reference
+    prints them): sum (2l+1) i_l(z) = e^z, sum (-1)^l (2l+1) i_l(z) = e^-z on
+    its radial points r_i = 0.005 * 1.5^i (kappa = 1, arguments up to 8, where
+    lmax 40 truncates below 1e-15), and the Yukawa addition theorem
+    (2 kappa / pi) sum (2l+1) i_l(kappa r_i) k_l(kappa r_j) = e^(-kappa (r_j - r_i)) / (r_j - r_i)
+    for collinear points with r_i <= r_j / 2 (lmax 50)."""
+    r = 0.005 * 1.5 ** np.arange(25)
+    for z in r[r <= 8.0]:
+        i = oracle.bessel_i(z, 40)
+        l = np.arange(41)
+        assert abs(((2 * l + 1) * i).sum() - np.exp(z)) <= 2e-15 * np.exp(z)
+        assert abs(((-1.0) ** l * (2 * l + 1) * i).sum() - np.exp(-z)) <= 1e-15 * np.exp(z)
+    kappa = 1.0
+    pts = np.linspace(0.0, 1.0, 21)[1:]
+    l = np.arange(51)
+    for ri in pts:
+        for rj in pts[pts >= 2 * ri]:
+            s = ((2 * l + 1) * oracle.bessel_i(kappa * ri, 50) * oracle.bessel_k(kappa * rj, 50)).sum()
+            exact = np.exp(-kappa * (rj - ri)) / (rj - ri)
+            assert abs(2 * kappa / np.pi * s - exact) <= 1e-13 * exact, (ri, rj)
+
+
+def _lattice_dirs():
+    import itertools
+
+    return [v for v in itertools.product(range(-3, 4), repeat=3) if max(abs(x) for x in v) >= 2]
+
+
+def _orth_err(oracle, d, lmax, repaired):
+    d = np.asarray(d, float) / np.linalg.norm(d)
+    B = oracle.ref_real_rotation(np.arctan2(d[1], d[0]), np.arccos(d[2]), 0.0, lmax, repaired)
+    return max(np.abs(b @ b.T - np.eye(len(b))).max() for b in B)
+
+
+def test_reference_rotation_recursion_defects(oracle):
+    """Two defects of the reference's rotation of real expansions
+    (helmholtz_multipole_tools.F90:911-1200), restated as written: its
+    sqrt(2.0) is a single-precision literal, so every rotation is orthogonal
+    only to ~3e-8; and its eq. 68 step divides by l cos(beta) - m', which is
+    0/0 where l cos(beta) is an integer -- e.g. the level-2 box displacement
+    (2, 1, 2), cos(beta) = 2/3 -- where the result is no rotation at all."""
+    rng = np.random.default_rng(0)
+    generic = max(_orth_err(oracle, rng.standard_normal(3), 12, False) for _ in range(10))
+    assert 1e-9 < generic < 1e-7
+    assert _orth_err(oracle, (2, 1, 2), 12, False) > 0.1
+    bad = [v for v in _lattice_dirs() if _orth_err(oracle, v, 12, False) > 1e-6]
+    assert len(bad) == 16  # of the 316 level-2 far-field displacement directions
+
+
+@pytest.mark.parametrize("lmax", [0, 1, 3, 8, 12, 15])
+def test_repaired_rotation_matches_least_squares(oracle, lmax):
+    """The oracle's M2L rotates with the reference's recursion, the two
+    defects repaired (double sqrt 2; the eq. 68 rows from the explicit Wigner
+    sum).  That rotation is orthogonal on every lattice direction, and the
+    conversion equals the one built with an independent least-squares
+    rotation (the method the library uses) to rounding."""
+    rng = np.random.default_rng(lmax)
+    assert max(_orth_err(oracle, v, lmax, True) for v in _lattice_dirs()) < 1e-13
+    N = (lmax + 1) ** 2
+    worst = 0.0
+    cases = [(rng.uniform(-1, 1, 3), rng.uniform(-6, 6, 3)) for _ in range(4)]
+    cases += [(np.zeros(3), 2.4 * np.asarray(v, float)) for v in _lattice_dirs()[::7]]
+    for src, d in cases:
+        M = rng.standard_normal(N)
+        a = oracle.helm_m2l(lmax, 1.1, M, src, src + d)
+        b = oracle.helm_m2l(lmax, 1.1, M, src, src + d, least_squares=True)
+        worst = max(worst, np.abs(a - b).max() / np.abs(b).max())
+    assert worst < 1e-13, worst

@@ -52,6 +52,39 @@ def test_noalloc_matches_regular_apply(dage, oracle, axes):
         assert (V - ref).abs().max().item() <= 1e-12 * ref.abs().max().item()
 
 
+def test_noalloc_on_a_caller_stream(dage, oracle):
+    """All stage launches go to the stream the caller passes: the result is
+    complete once that stream (and nothing else) has been synchronised."""
+    import torch
+
+    lib = dage.load()
+    axes = ((-3.0, 5, 0.2),) * 3
+    g = dage.Grid3D(tuple(dage.Grid1D.equidistant(*a) for a in axes))
+    go = oracle.Grid3D(tuple(oracle.Grid1D.equidistant(*a) for a in axes))
+    rho = oracle.gauss_cube(go, [1.3], [2.2], [[0.2, -0.1, 0.3]])
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(6, 6))
+    nx, ny, nz = g.shape
+    rd = torch.from_numpy(rho.reshape(-1, order="F").copy()).cuda()
+    Vref = op.apply(rd, coda=False).reshape(-1)
+    T = [_device_matrices(op, d) for d in range(3)]
+    _, w = op.quadrature()
+    w = np.ascontiguousarray(w)
+    dp = ctypes.POINTER(ctypes.c_double)
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    V = torch.full((nx * ny * nz,), float("nan"), dtype=torch.float64, device="cuda")
+    rc = lib.dage_op3d_apply_fp64_noalloc(
+        nx, ny, nz, nx, ny, nz, len(w), ctypes.c_void_p(T[0].data_ptr()),
+        ctypes.c_void_p(T[1].data_ptr()), ctypes.c_void_p(T[2].data_ptr()),
+        w.ctypes.data_as(dp), ctypes.c_void_p(rd.data_ptr()), ctypes.c_void_p(V.data_ptr()),
+        ctypes.c_void_p(s.cuda_stream))
+    assert rc == 0, lib.dage_last_error()
+    s.synchronize()
+    with torch.cuda.stream(s):
+        err = (V - Vref).abs().max().item()
+    assert err <= 1e-12 * Vref.abs().max().item()
+
+
 def test_noalloc_rejects_cubes_beyond_its_scratch(dage):
     import torch
 
