@@ -17,6 +17,7 @@ DAGE_PRODUCT_COMPLETE = 32
 DAGE_FP64 = 0
 DAGE_MIXED_BF16X3 = 1
 DAGE_MIXED_BF16X6 = 2
+DAGE_MIXED_FP16X3 = 3
 
 
 class DageGrid1D(ctypes.Structure):

@@ -594,7 +594,7 @@ static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[
   if (quad->nlog > 0 && !(quad->tlog > quad->tlin && quad->tlin > 0.0))
     return fail(DAGE_E_INVALID, "logarithmic tail needs 0 < tlin < tlog");
   if (precision != DAGE_FP64 && precision != DAGE_MIXED_BF16X3 &&
-      precision != DAGE_MIXED_BF16X6)
+      precision != DAGE_MIXED_BF16X6 && precision != DAGE_MIXED_FP16X3)
     return fail(DAGE_E_INVALID, "unknown precision %d", precision);
   op->precision = precision;
   op->quad = *quad;

@@ -38,6 +38,19 @@
 // reductions; the sum over t-points is FP64.  K blocks outside the band of
 // the matrix tile (entries below 2^-64 of their row's scale) are skipped.
 //
+// "fp16x3" keeps the bf16x3 structure (two parts, three products, per-run
+// main-product partials) with FP16 parts: 11-bit significands give the two
+// parts ~22 bits, so the representation error drops from ~2^-18 to ~2^-23
+// per element.  FP16's narrow exponent range is handled by power-of-two
+// scales: matrix rows as above times 2^14, stage inputs by one scale per
+// stage and t-point from an a-priori bound of the stage's values (max |rho|
+// times the largest row L1 norm of each earlier stage's matrix), so every
+// stored value is below 2^15 and values below 2^-39 of the bound flush.  The
+// tensor core's toward-zero rounding of the FP32 partials (~0.5 ulp per
+// rounding, all of one sign for positive sums) is then the largest error
+// left; the epilogue adds half an ulp to each partial on average (+1 ulp to
+// the odd ones) before summing, which removes that bias.
+//
 // Kernel structure (one persistent CTA per SM, 18 warps):
 //   warp 0      TMA producer: X and T tiles -> shared-memory ring (SW64)
 //   warp 1      TMEM allocator + single-thread MMA issuer
@@ -51,6 +64,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstring>
@@ -189,9 +203,11 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   return d;
 }
 
-// kind::f16 instruction descriptor: BF16 A and B, FP32 D, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+// kind::f16 instruction descriptor: BF16 (F16 = false) or FP16 A and B,
+// FP32 D, both K-major.
+template <bool F16>
+__host__ __device__ constexpr uint32_t idesc_f16kind(int M, int N) {
+  return (1u << 4) | (F16 ? 0u : (1u << 7) | (1u << 10)) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
 
@@ -223,6 +239,13 @@ __device__ __forceinline__ void split_lead_f64(double v, double m, __nv_bfloat16
   }
 }
 
+// FP16: floating lead fp16(v) and the fp16 rounding of the rest (the value
+// is already scaled into FP16 range).
+__device__ __forceinline__ void split_f16_f64(double v, __half (&o)[2]) {
+  o[0] = __double2half(v);
+  o[1] = __double2half(v - (double)__half2float(o[0]));
+}
+
 // BF16 pair <-> FP32 pair by bit moves (integer pipe).  The epilogue keeps
 // its FP32 arithmetic packed (FP32x2) and its conversions off the FP32 FMA
 // pipe: dense scalar FP32 work on the MMA issuer's scheduler delays the
@@ -235,6 +258,23 @@ __device__ __forceinline__ float2 bf16x2_to_f32x2(__nv_bfloat162 h) {
 __device__ __forceinline__ __nv_bfloat162 f32x2_to_bf16x2_exact(float2 v) {
   const uint32_t u = __byte_perm(__float_as_uint(v.x), __float_as_uint(v.y), 0x7632);
   return *reinterpret_cast<const __nv_bfloat162 *>(&u);
+}
+
+// Two FP16 parts of a scaled FP32 pair (floating lead), as two half2.
+__device__ __forceinline__ void split_pair_f16(float2 v, __half2 (&o)[2]) {
+  o[0] = __floats2half2_rn(v.x, v.y);
+  const float2 l = __half22float2(o[0]);
+  o[1] = __floats2half2_rn(v.x - l.x, v.y - l.y);
+}
+
+// One ulp toward larger magnitude: the tensor core rounds its FP32 sums
+// toward zero, and a main-product partial (two K=16 MMAs) comes out low in
+// magnitude by about one ulp on B200 (measured with FP16 parts: relative
+// energy bias -2.2e-7 at 121^3 and -2.8e-7 at 481^3 without this step, i.e.
+// 0.8 and 1.1 ulp per partial).  Adding 1 to the bit pattern moves the value
+// one ulp away from zero (a zero becomes the smallest subnormal).
+__device__ __forceinline__ float unbias_rz(float p) {
+  return __uint_as_float(__float_as_uint(p) + 1u);
 }
 
 // The same split for two values sharing one run maximum m, on packed FP32x2
@@ -286,9 +326,12 @@ struct StageArgs {
   int ng, gM;
   const float *scale;    // s_n, row scales of the t-points
   const float *wcoef;    // w_p of the t-points (device)
+  // FP16 intermediate stages: the stage's power-of-two output factor (device
+  // scalar, from the bound-based input scales); null for the BF16 modes
+  const float *gscale;
   // intermediate output: part s of element (R, n) at
   //   out[s][(R / d0 + d1 * n) * ldn + R % d0]
-  __nv_bfloat16 *out0, *out1, *out2;
+  __nv_bfloat16 *out0, *out1, *out2;  // FP16 mode: the same bytes as __half
   int d0, d1;
   long long ldn;
   // final output V[R + M * n] (FP64)
@@ -369,7 +412,7 @@ __device__ __forceinline__ void mma_run(uint32_t P, uint32_t Cc, uint64_t d0, ui
 // NSX parts per operand; NS shared-memory stages; the main product starts a
 // fresh partial every kGroup / 16 MMAs (one 32-run of K).
 // 576 threads x 96 registers (55296 of the SM's 65536): one CTA per SM.
-template <int NSX, int NS, bool FINAL>
+template <int NSX, int NS, bool FINAL, bool F16 = false>
 __global__ void __maxnreg__(96)
     stage_bf16_kernel(const __grid_constant__ CUtensorMap mapA0,
                       const __grid_constant__ CUtensorMap mapA1,
@@ -488,7 +531,7 @@ __global__ void __maxnreg__(96)
         int nt = a.N - n0;
         if (nt > BN) nt = BN;
         nt = (nt + 15) & ~15;
-        const uint32_t idesc = idesc_bf16(BM, nt);
+        const uint32_t idesc = idesc_f16kind<F16>(BM, nt);
         const int2 rc = r;
         // next tile's band, loaded while this tile's MMAs run
         u += (u % a.ng == a.ng - 1) ? (gridDim.x - 1) * a.ng + 1 : 1;
@@ -539,6 +582,12 @@ __global__ void __maxnreg__(96)
     // 16 warps, four per scheduler: warp w reads TMEM lanes 32 (w % 4) ..
     // +31 (the hardware's lane quarter) and the 32 columns (w - 2) / 4.
     constexpr int CW = BN / 4;
+    // Per-column matrix scales matter only for bf16x6 (fixed-point matrix
+    // leads on a per-row quantum); bf16x3 splits the unscaled matrix and
+    // fp16x3 scales each t-point's matrix by one power of two, folded into
+    // the stage factor gfac.
+    constexpr bool kColScale = NSX > 2;
+    const float gfac = (F16 && !FINAL) ? *a.gscale : 1.0f;
     const int q = warp & 3;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
     const uint32_t col0 = ((warp - 2) >> 2) * CW;
@@ -549,7 +598,13 @@ __global__ void __maxnreg__(96)
 #pragma unroll
       for (int j = 0; j < CW / 2; ++j) accg[j] = make_float2(0.0f, 0.0f);
       bool ok = true;
+      const int ncol = (tile % a.n_ntiles) * BN + col0 + lane;  // this lane's column
+      // intermediate stages: the scale of column ncol, loaded before the
+      // partial drains so its latency overlaps them
+      const float scl = (!FINAL && kColScale && ncol < a.N) ? a.scale[ncol] : 0.0f;
       for (int gi = 0; gi < a.ng && ok; ++gi, ++t) {
+        // last stage: w_p s_n of column ncol for sub-problem gi
+        const float fcol = (FINAL && ncol < a.N) ? a.wcoef[gi] * a.scale[(size_t)gi * a.N + ncol] : 0.0f;
 #pragma unroll
         for (int j = 0; j < CW / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
         const int nparts =
@@ -569,10 +624,11 @@ __global__ void __maxnreg__(96)
             uint32_t r[16];
             tmem_ld16(tmem_base + lane_off + b * BN + col0 + hh * 16, r);
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-              acc[hh * 8 + j] = __fadd2_rn(acc[hh * 8 + j],
-                                           make_float2(__uint_as_float(r[2 * j]),
-                                                       __uint_as_float(r[2 * j + 1])));
+            for (int j = 0; j < 8; ++j) {
+              float2 pv = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
+              if (F16) pv = make_float2(unbias_rz(pv.x), unbias_rz(pv.y));
+              acc[hh * 8 + j] = __fadd2_rn(acc[hh * 8 + j], pv);
+            }
           }
           tc_fence_before();
           __syncwarp();
@@ -600,15 +656,10 @@ __global__ void __maxnreg__(96)
         __syncwarp();
         if (lane == 0) mbar_arrive(cempty);
         if (FINAL) {
-          const int n0 = (tile % a.n_ntiles) * BN + col0;
-          const float *sc = a.scale + (size_t)gi * a.N;
-          const float wg = a.wcoef[gi];
 #pragma unroll
           for (int j = 0; j < CW / 2; ++j) {
-            const int n = n0 + 2 * j;
-            const float2 f = __fmul2_rn(make_float2(wg, wg),
-                                        make_float2(n < a.N ? sc[n] : 0.0f,
-                                                    n + 1 < a.N ? sc[n + 1] : 0.0f));
+            const float2 f = make_float2(__shfl_sync(0xffffffffu, fcol, 2 * j),
+                                         __shfl_sync(0xffffffffu, fcol, 2 * j + 1));
             accg[j] = __ffma2_rn(f, acc[j], accg[j]);
           }
         }
@@ -648,13 +699,20 @@ __global__ void __maxnreg__(96)
         const bool valid = r0 < a.d0;
         const bool odd = lane & 1;
         const int rpair = r0 & ~1;
+        // The warp's 32 column scales are one per lane (scl, loaded at the
+        // tile's start): loads placed between the loop's global stores could
+        // not be moved ahead of them (the compiler cannot rule out aliasing),
+        // and each would expose its full latency.
 #pragma unroll
         for (int j = 0; j < CW; j += 2) {
           const int n = n0 + j;
           if (n < a.N) {  // uniform across the warp
             const bool has1 = n + 1 < a.N;
-            const float2 sc = make_float2(a.scale[n], has1 ? a.scale[n + 1] : 0.0f);
-            const float2 v = valid ? __fmul2_rn(acc[j >> 1], sc) : make_float2(0.0f, 0.0f);
+            const float2 sc = kColScale ? make_float2(__shfl_sync(0xffffffffu, scl, j),
+                                                      __shfl_sync(0xffffffffu, scl, j + 1))
+                                        : make_float2(gfac, gfac);
+            const float2 v = !valid ? make_float2(0.0f, 0.0f)
+                             : (kColScale || F16) ? __fmul2_rn(acc[j >> 1], sc) : acc[j >> 1];
             float m = 0.0f;
             if (NSX > 2) {
               const float m0 =
@@ -665,14 +723,25 @@ __global__ void __maxnreg__(96)
             }
             const float recv = __shfl_xor_sync(0xffffffffu, odd ? v.x : v.y, 1);
             const float mine = odd ? v.y : v.x;
-            __nv_bfloat162 pp[NSX];
-            split_pair_f32<NSX>(odd ? make_float2(recv, mine) : make_float2(mine, recv), m, pp);
-            if (rpair < a.d0 && (!odd || has1)) {
-              const size_t off =
-                  (size_t)(r1 + (long long)a.d1 * (n + (odd ? 1 : 0))) * a.ldn + rpair;
-              *reinterpret_cast<__nv_bfloat162 *>(a.out0 + off) = pp[0];
-              *reinterpret_cast<__nv_bfloat162 *>(a.out1 + off) = pp[1];
-              if (NSX > 2) *reinterpret_cast<__nv_bfloat162 *>(a.out2 + off) = pp[NSX > 2 ? 2 : 0];
+            const float2 vv = odd ? make_float2(recv, mine) : make_float2(mine, recv);
+            const size_t off =
+                (size_t)(r1 + (long long)a.d1 * (n + (odd ? 1 : 0))) * a.ldn + rpair;
+            const bool store = rpair < a.d0 && (!odd || has1);
+            if (F16) {
+              __half2 hh2[2];
+              split_pair_f16(vv, hh2);
+              if (store) {
+                *reinterpret_cast<__half2 *>(a.out0 + off) = hh2[0];
+                *reinterpret_cast<__half2 *>(a.out1 + off) = hh2[1];
+              }
+            } else {
+              __nv_bfloat162 pp[NSX];
+              split_pair_f32<NSX>(vv, m, pp);
+              if (store) {
+                *reinterpret_cast<__nv_bfloat162 *>(a.out0 + off) = pp[0];
+                *reinterpret_cast<__nv_bfloat162 *>(a.out1 + off) = pp[1];
+                if (NSX > 2) *reinterpret_cast<__nv_bfloat162 *>(a.out2 + off) = pp[NSX > 2 ? 2 : 0];
+              }
             }
           }
         }
@@ -721,12 +790,100 @@ __global__ void split_input_kernel(const double *__restrict__ rho, int K, long l
   }
 }
 
-// One block per matrix row (p, n): s = 2^ceil(log2 max_K |T|), parts of
-// T / s with the leading part on the quantum 2^-7.
-template <int NSX>
+// FP16 mode: rho * 2^-e0 (device scalar *gin, from max |rho|) -> two FP16
+// parts, rows of ld elements, zeros from K to ld.
+__global__ void split_input_f16_kernel(const double *__restrict__ rho, int K, long long rows,
+                                       long long ld, const float *__restrict__ gin, __half *o0,
+                                       __half *o1) {
+  const double g = (double)*gin;
+  const long long n = rows * ld;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / ld;
+    const int k = (int)(e % ld);
+    __half p[2];
+    split_f16_f64(k < K ? rho[r * K + k] * g : 0.0, p);
+    o0[e] = p[0];
+    o1[e] = p[1];
+  }
+}
+
+// max |rho| as the bits of a non-negative float (ordered like the values);
+// *out must start at 0.
+__global__ void absmax_kernel(const double *__restrict__ x, long long n, unsigned *out) {
+  float m = 0.0f;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, (float)fabs(x[e]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// Power-of-two scales of the FP16 mode for one apply.  With M = max |rho|
+// (rounded up to a float) and L_a(p) the largest row L1 norm of axis a's
+// matrix at t-point p, stage s of t-point p stores its input times 2^-e_s(p),
+//   e_0 = floor(log2 M) - 14,  e_1(p) = floor(log2(M L_x)) - 14,
+//   e_2(p) = floor(log2(M L_x L_y)) - 14,
+// so every stored value is below 2^15.  Axis a's matrix parts at t-point p
+// carry 2^14 / S_a(p), S_a(p) the power of two at or above the matrix's
+// largest |entry|; the stage epilogues multiply by g_s(p) = S(p) 2^(e_s - 14 -
+// e_(s+1)) and the last stage by w_p S_z(p) 2^(e_2 - 14).  gin = 2^-e_0.
+__global__ void f16_scales_kernel(const unsigned *maxbits, const double *l1x, const double *l1y,
+                                  const double *sx, const double *sy, const double *sz,
+                                  const double *w, int P, float *gin, float *g01, float *wcoef) {
+  const double M = (double)__uint_as_float(*maxbits);
+  auto ex = [](double b) { return b > 0.0 ? (int)floor(log2(b)) - 14 : 0; };
+  const int e0 = ex(M);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *gin = (float)ldexp(1.0, -e0);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int e1 = ex(M * l1x[p]), e2 = ex(M * l1x[p] * l1y[p]);
+    g01[p] = (float)(sx[p] * ldexp(1.0, e0 - 14 - e1));
+    g01[P + p] = (float)(sy[p] * ldexp(1.0, e1 - 14 - e2));
+    wcoef[p] = (float)(w[p] * sz[p] * ldexp(1.0, e2 - 14));
+  }
+}
+
+// Per t-point: the largest row L1 norm of the matrix (out) and the power of
+// two at or above its largest |entry| (pscale); one block per t-point over
+// its n rows of K values.
+__global__ void row_l1max_kernel(const double *__restrict__ T, int N, int K, double *out,
+                                 double *pscale) {
+  const double *Tp = T + (size_t)blockIdx.x * N * K;
+  double m = 0.0, mx = 0.0;
+  for (int n = threadIdx.x >> 5; n < N; n += blockDim.x >> 5) {
+    double sum = 0.0;
+    for (int k = threadIdx.x & 31; k < K; k += 32) {
+      const double v = fabs(Tp[(size_t)n * K + k]);
+      sum += v;
+      mx = fmax(mx, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    m = fmax(m, sum);
+  }
+  __shared__ double red[32], redx[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m, redx[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0, rx = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r = fmax(r, red[i]), rx = fmax(rx, redx[i]);
+    out[blockIdx.x] = r;
+    pscale[blockIdx.x] = rx > 0.0 ? exp2(ceil(log2(rx))) : 1.0;
+  }
+}
+
+// One block per matrix row (p, n).  bf16x6: s = 2^ceil(log2 max_K |T|),
+// parts of T / s with the leading part on the quantum 2^-7.  bf16x3: the
+// floating BF16 parts of T itself (s = 1).  fp16x3: floating FP16 parts of
+// 2^14 T / S(p), S(p) the t-point's power-of-two scale (pscale, rows of N),
+// and s = 1 (S(p) goes into the stage factors).
+template <int NSX, bool F16 = false>
 __global__ void split_matrix_kernel(const double *__restrict__ T, int K, long long ld,
                                     float *scale, double *scale64, __nv_bfloat16 *o0,
-                                    __nv_bfloat16 *o1, __nv_bfloat16 *o2) {
+                                    __nv_bfloat16 *o1, __nv_bfloat16 *o2,
+                                    const double *__restrict__ pscale = nullptr, int N = 1) {
   const long long row = blockIdx.x;
   const double *src = T + row * K;
   __shared__ double red[32];
@@ -742,15 +899,23 @@ __global__ void split_matrix_kernel(const double *__restrict__ T, int K, long lo
   }
   __syncthreads();
   // power-of-two scale: the division is exact
-  const double s = red[0] > 0.0 ? exp2(ceil(log2(red[0]))) : 1.0;
+  const double s = (NSX == 2 || F16) ? 1.0 : red[0] > 0.0 ? exp2(ceil(log2(red[0]))) : 1.0;
+  const double tsc = F16 ? ldexp(1.0, 14) / pscale[row / N] : 1.0;
   if (threadIdx.x == 0) {
     scale[row] = (float)s;
     scale64[row] = s;
   }
   for (int k = threadIdx.x; k < (int)ld; k += blockDim.x) {
+    const size_t off = (size_t)row * ld + k;
+    if (F16) {
+      __half h[2];
+      split_f16_f64(k < K ? src[k] * tsc : 0.0, h);
+      reinterpret_cast<__half *>(o0)[off] = h[0];
+      reinterpret_cast<__half *>(o1)[off] = h[1];
+      continue;
+    }
     __nv_bfloat16 p[NSX];
     split_lead_f64<NSX>(k < K ? src[k] / s : 0.0, 1.0, p);
-    const size_t off = (size_t)row * ld + k;
     o0[off] = p[0];
     o1[off] = p[1];
     if (NSX > 2) o2[off] = p[NSX > 2 ? 2 : 0];
@@ -795,6 +960,7 @@ int make_map(CUtensorMap *m, const void *base, long long inner, long long rows, 
 }
 
 struct MixedState {
+  bool f16 = false; // FP16 parts (fp16x3) instead of BF16
   int nparts = 2;   // BF16 parts per operand
   int G = 1;        // t-points per pass of the last stage (slots of X[2])
   DevBuf wdev;      // w_p as FP32 on the device
@@ -806,6 +972,9 @@ struct MixedState {
   int towner[3];
   CUtensorMap mapA[3][3], mapB[3][3];
   DevBuf err;
+  // FP16 mode: per-t-point largest row L1 norm of each owner axis's matrix,
+  // the weights in FP64, and the per-apply scales (f16_scales_kernel)
+  DevBuf l1[3], psc[3], w64, maxbits, gin, g01, wcoef;
 };
 
 long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
@@ -816,11 +985,11 @@ __nv_bfloat16 *plane(DevBuf &b, int part, long long plane_elems) {
 
 // One stage launch.  nrb > 0 selects the two-dimensional M tiling of the
 // intermediate stages (see StageArgs).
-template <int NSX, int NS, bool FINAL>
+template <int NSX, int NS, bool FINAL, bool F16>
 int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, int nrb, int ng,
                  const StageArgs &base, cudaStream_t s) {
   using C = StageCfg<NSX, NS>;
-  auto kern = stage_bf16_kernel<NSX, NS, FINAL>;
+  auto kern = stage_bf16_kernel<NSX, NS, FINAL, F16>;
   static bool attr_set = false;
   if (!attr_set) {
     DAGE_CUDA_TRY(
@@ -849,19 +1018,37 @@ int launch_stage(MixedState &st, int stage, int M, int N, int K, int p, int nrb,
   return 0;
 }
 
-template <int NSX, int NS>
+template <int NSX, int NS, bool F16>
 int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, cudaStream_t s) {
   const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
   const int nox = op->nout[0], noy = op->nout[1], noz = op->nout[2];
   const long long pe[3] = {st.rows[0] * st.ld[0], st.rows[1] * st.ld[1], st.rows[2] * st.ld[2]};
-  // input split
+  // input split (FP16: after the bound-based scales of this input)
   {
     const int t = op->tmark_begin(1);
-    const long long nwarps = st.rows[0] * ((st.ld[0] + kGroup - 1) / kGroup);
-    const int blocks = (int)std::min<long long>((nwarps + 7) / 8, sm_count() * 16LL);
-    split_input_kernel<NSX><<<blocks, 256, 0, s>>>(
-        d_rho, nix, st.rows[0], st.ld[0], plane(st.X[0], 0, pe[0]), plane(st.X[0], 1, pe[0]),
-        plane(st.X[0], NSX > 2 ? 2 : 1, pe[0]));
+    if (F16) {
+      const long long n = (long long)nix * st.rows[0];
+      const int blocks = (int)std::min<long long>((n + 255) / 256, sm_count() * 8LL);
+      DAGE_CUDA_TRY(cudaMemsetAsync(st.maxbits.ptr, 0, sizeof(unsigned), s));
+      absmax_kernel<<<blocks, 256, 0, s>>>(d_rho, n, st.maxbits.as<unsigned>());
+      f16_scales_kernel<<<1, 128, 0, s>>>(
+          st.maxbits.as<unsigned>(), st.l1[st.towner[0]].as<double>(),
+          st.l1[st.towner[1]].as<double>(), st.psc[st.towner[0]].as<double>(),
+          st.psc[st.towner[1]].as<double>(), st.psc[st.towner[2]].as<double>(),
+          st.w64.as<double>(), op->P, st.gin.as<float>(), st.g01.as<float>(),
+          st.wcoef.as<float>());
+      const long long ne = st.rows[0] * st.ld[0];
+      split_input_f16_kernel<<<(int)std::min<long long>((ne + 255) / 256, sm_count() * 16LL), 256, 0,
+                               s>>>(d_rho, nix, st.rows[0], st.ld[0], st.gin.as<float>(),
+                                    reinterpret_cast<__half *>(plane(st.X[0], 0, pe[0])),
+                                    reinterpret_cast<__half *>(plane(st.X[0], 1, pe[0])));
+    } else {
+      const long long nwarps = st.rows[0] * ((st.ld[0] + kGroup - 1) / kGroup);
+      const int blocks = (int)std::min<long long>((nwarps + 7) / 8, sm_count() * 16LL);
+      split_input_kernel<NSX><<<blocks, 256, 0, s>>>(
+          d_rho, nix, st.rows[0], st.ld[0], plane(st.X[0], 0, pe[0]), plane(st.X[0], 1, pe[0]),
+          plane(st.X[0], NSX > 2 ? 2 : 1, pe[0]));
+    }
     DAGE_CUDA_TRY(cudaGetLastError());
     op->tmark_end(t);
   }
@@ -893,20 +1080,21 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
       a.d0 = d0[stage];
       a.d1 = d1[stage];
       a.ldn = st.ld[stage + 1];
+      if (F16) a.gscale = st.g01.as<float>() + (size_t)stage * op->P + p;
       const int t = op->tmark_begin(0);
-      DAGE_TRY((launch_stage<NSX, NS, false>(st, stage, (int)M[stage], no[stage], ni[stage], p,
-                                             ceil_div(d0[stage], BM), 1, a, s)));
+      DAGE_TRY((launch_stage<NSX, NS, false, F16>(st, stage, (int)M[stage], no[stage], ni[stage], p,
+                                                  ceil_div(d0[stage], BM), 1, a, s)));
       op->tmark_end(t);
     }
     if (p - p0 + 1 == st.G || p == op->P - 1) {
       StageArgs a = base;
       common(a, 2, p0);
       const int ng = p - p0 + 1;
-      a.wcoef = st.wdev.as<float>() + p0;
+      a.wcoef = (F16 ? st.wcoef.as<float>() : st.wdev.as<float>()) + p0;
       a.V = d_V;
       a.accumulate = p0 > 0;
       const int t = op->tmark_begin(0);
-      DAGE_TRY((launch_stage<NSX, NS, true>(st, 2, (int)M[2], no[2], ni[2], p0, 0, ng, a, s)));
+      DAGE_TRY((launch_stage<NSX, NS, true, F16>(st, 2, (int)M[2], no[2], ni[2], p0, 0, ng, a, s)));
       op->tmark_end(t);
       p0 = p + 1;
     }
@@ -919,7 +1107,8 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
 int mixed_setup(dage_op3d *op) {
   auto *st = new MixedState();
   op->mixed = st;
-  st->nparts = op->precision == DAGE_MIXED_BF16X3 ? 2 : 3;
+  st->f16 = op->precision == DAGE_MIXED_FP16X3;
+  st->nparts = op->precision == DAGE_MIXED_BF16X6 ? 3 : 2;
   const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
   const int nox = op->nout[0], noy = op->nout[1];
   const int ni[3] = {nix, niy, niz};
@@ -951,7 +1140,15 @@ int mixed_setup(dage_op3d *op) {
     DAGE_TRY(st->sc64[ax].alloc(sizeof(double) * nrows));
     __nv_bfloat16 *o0 = plane(st->Tp[ax], 0, pe), *o1 = plane(st->Tp[ax], 1, pe),
                   *o2 = plane(st->Tp[ax], st->nparts > 2 ? 2 : 1, pe);
-    if (st->nparts == 2)
+    if (st->f16) {
+      DAGE_TRY(st->l1[ax].alloc(sizeof(double) * op->P));
+      DAGE_TRY(st->psc[ax].alloc(sizeof(double) * op->P));
+      row_l1max_kernel<<<op->P, 256, 0, op->stream>>>(op->T(ax), N, K, st->l1[ax].as<double>(),
+                                                      st->psc[ax].as<double>());
+      split_matrix_kernel<2, true><<<(unsigned)nrows, 256, 0, op->stream>>>(
+          op->T(ax), K, ld, st->sc[ax].as<float>(), st->sc64[ax].as<double>(), o0, o1, o2,
+          st->psc[ax].as<double>(), N);
+    } else if (st->nparts == 2)
       split_matrix_kernel<2><<<(unsigned)nrows, 256, 0, op->stream>>>(
           op->T(ax), K, ld, st->sc[ax].as<float>(), st->sc64[ax].as<double>(), o0, o1, o2);
     else
@@ -960,6 +1157,12 @@ int mixed_setup(dage_op3d *op) {
     DAGE_CUDA_TRY(cudaGetLastError());
     for (int i = 0; i < st->nparts; ++i)
       DAGE_TRY(make_map(&st->mapB[ax][i], plane(st->Tp[ax], i, pe), K, nrows, ld, BK, BN));
+  }
+  if (st->f16) {
+    DAGE_TRY(st->maxbits.alloc(sizeof(unsigned)));
+    DAGE_TRY(st->gin.alloc(sizeof(float)));
+    DAGE_TRY(st->g01.alloc(sizeof(float) * 2 * op->P));
+    DAGE_TRY(st->wcoef.alloc(sizeof(float) * op->P));
   }
   return mixed_set_weights(op);
 }
@@ -971,14 +1174,20 @@ int mixed_set_weights(dage_op3d *op) {
   DAGE_TRY(st->wdev.alloc(sizeof(float) * w.size()));
   DAGE_CUDA_TRY(cudaMemcpyAsync(st->wdev.ptr, w.data(), sizeof(float) * w.size(),
                                 cudaMemcpyHostToDevice, op->stream));
+  if (st->f16) {
+    DAGE_TRY(st->w64.alloc(sizeof(double) * op->w.size()));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(st->w64.ptr, op->w.data(), sizeof(double) * op->w.size(),
+                                  cudaMemcpyHostToDevice, op->stream));
+  }
   return cudaStreamSynchronize(op->stream) == cudaSuccess ? 0 : fail(DAGE_E_CUDA, "weights upload");
 }
 
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
   auto *st = static_cast<MixedState *>(op->mixed);
   if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
-  const int rc = st->nparts == 2 ? run_stages<2, 6>(op, *st, d_rho, d_V, s)
-                                 : run_stages<3, 4>(op, *st, d_rho, d_V, s);
+  const int rc = st->f16 ? run_stages<2, 6, true>(op, *st, d_rho, d_V, s)
+                 : st->nparts == 2 ? run_stages<2, 6, false>(op, *st, d_rho, d_V, s)
+                                   : run_stages<3, 4, false>(op, *st, d_rho, d_V, s);
   if (rc) return rc;
   int herr = 0;
   DAGE_CUDA_TRY(cudaMemcpyAsync(&herr, st->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -998,7 +1207,14 @@ void mixed_destroy(dage_op3d *op) {
     st->Tp[i].release();
     st->sc[i].release();
     st->sc64[i].release();
+    st->l1[i].release();
+    st->psc[i].release();
   }
+  st->w64.release();
+  st->maxbits.release();
+  st->gin.release();
+  st->g01.release();
+  st->wcoef.release();
   st->err.release();
   st->wdev.release();
   delete st;

@@ -27,6 +27,7 @@ PRECISIONS = {
     "fp64": _capi.DAGE_FP64,
     "bf16x3": _capi.DAGE_MIXED_BF16X3,
     "bf16x6": _capi.DAGE_MIXED_BF16X6,
+    "fp16x3": _capi.DAGE_MIXED_FP16X3,
 }
 
 

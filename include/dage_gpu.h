@@ -48,6 +48,9 @@ extern "C" {
 #define DAGE_FP64 0            /* FP64 everywhere: the drop-in */
 #define DAGE_MIXED_BF16X3 1    /* 2-way BF16 splits, 3 products, FP32 accum */
 #define DAGE_MIXED_BF16X6 2    /* 3-way BF16 splits, 6 products, FP32 accum */
+#define DAGE_MIXED_FP16X3 3    /* 2-way FP16 splits with power-of-two stage scales,
+                                  3 products, FP32 accum with the toward-zero
+                                  rounding bias removed */
 
 /* One axis of a Grid3D: ncell LIP cells of nlip points each; the axis holds
  * ncell*(nlip-1)+1 points (src/bubbles/grid.F90:446-534, Grid1D_init_step).

@@ -292,6 +292,60 @@ def integrate_cube(grid: Grid3D, f) -> float:
 # ---------------------------------------------------------------------------
 # Test densities
 # ---------------------------------------------------------------------------
+def slater_dens(zeta, l, r):
+    """Radial Slater density 2 zeta^(l+3) (1+2l) / (pi (l+2)!) r^l e^(-2 zeta r)
+    (slater_generator.F90:453-464, slater_dens)."""
+    norm = 2.0 * zeta ** (l + 3) * (1.0 + 2 * l) / np.pi / float(np.prod(np.arange(2, l + 3)))
+    return norm * np.asarray(r, dtype=np.float64) ** l * np.exp(-2.0 * zeta * np.asarray(r))
+
+
+def slater_analytical_energy(coeffs, expos, centers) -> float:
+    """Self-interaction of Slater s-densities (slater_analytical_energy,
+    analytical.F90:70-188, without periodic images): sum_i U_i + 2 sum_{i<j}
+    U_ij, U_i = q^2 5 zeta / 8, U_ij the closed form for equal or unequal
+    exponents (:155-187)."""
+    q = [float(x) for x in coeffs]
+    z = [float(x) for x in expos]
+    C = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
+
+    def uij(zi, zj, qi, qj, r):
+        if r <= 1e-14:
+            return qi * qj * zi * zj * (zi ** 2 + 3.0 * zi * zj + zj ** 2) / (zi + zj) ** 3
+        if zi == zj:
+            ei = np.exp(-2.0 * zi * r)
+            f = zi * r
+            return qi * qj * (1.0 - ei * (1.0 + 11.0 / 8.0 * f + 3.0 / 4.0 * f ** 2
+                                          + 1.0 / 6.0 * f ** 3)) / r
+        f = 1.0 / (zi * zi - zj * zj)
+        ei = np.exp(-2.0 * zi * r)
+        ej = np.exp(-2.0 * zj * r)
+        return (qi * qj / r) * (1.0 - zi ** 4 * zj ** 4 * f ** 2 * (ei * (1.0 + zi * r) / zi ** 4
+                                                                     - ej * (1.0 + zj * r) / zj ** 4)
+                                - 2.0 * zi ** 4 * zj ** 4 * f ** 3 * (ei / zi ** 2 - ej / zj ** 2))
+
+    E = 0.0
+    for i in range(len(q)):
+        E += q[i] ** 2 * 5.0 / 8.0 * z[i]
+        for j in range(i + 1, len(q)):
+            E += 2.0 * uij(z[i], z[j], q[i], q[j], float(np.sqrt(((C[i] - C[j]) ** 2).sum())))
+    return float(E)
+
+
+def radial_grid_charge(z, n0=100, nlip=7, r_max=20.0) -> Grid1D:
+    """Grid1D_init_radial (grid.F90:568-599): int(n0 z^(1/4)) cells whose ends
+    follow x_i = c / ((r_max + c) / (i dx) - 1), c = 8 z^(-3/2), dx = r_max /
+    ncell; equidistant points inside each cell."""
+    ncell = int(n0 * z ** 0.25)
+    const = 8.0 * z ** (-1.5)
+    dx = r_max / ncell
+    x0, scales = 0.0, []
+    for i in range(1, ncell + 1):
+        x1 = const / ((r_max + const) / (i * dx) - 1.0)
+        scales.append((x1 - x0) / (nlip - 1))
+        x0 = x1
+    return Grid1D(0.0, ncell, nlip, 1, np.array(scales))
+
+
 def gauss_extent(q, alpha, thres=1e-12):
     q = _f64(q)
     a = _f64(alpha)

@@ -12,6 +12,15 @@ multipole_test_kat.json holds the golden errors of the reference's
 multipole test (tests/multipole_test.F90, displaced_monopoles_test), which
 pin the M2L interaction matrix and the M2M translation matrix.
 
+slater_test_kat.json holds the values of the reference's Slater test
+(tests/slater_test.F90, TESTs 1-2): the Slater s-densities (explicit and
+parsed input), the analytic self-interaction energies that its
+SlaterGenerator%selfint returns (slater_analytical_energy, analytical.F90),
+and the numerical <rho|V rho> it asserts.  The numerical values came from a
+version of SlaterGenerator whose bubbles constructor is commented out in
+the reference snapshot (slater_generator.F90:264-284), with Taylor-series
+cusp treatment in the product; they are recorded with that provenance.
+
 oracle_small.json freezes oracle outputs for a small operator (matrices and
 potential samples) so the GPU tests have committed fixtures to compare with.
 Regenerate with:  python tests/golden/make_golden.py
@@ -65,6 +74,25 @@ MULTIPOLE_KAT = {
 }
 
 
+SLATER_KAT = {
+    "source": "DAGE tests/slater_test.F90 (TEST 1 :70-101, TEST 2 :106-143)",
+    "tolerance": 1e-14,
+    "cases": [
+        {"name": "TEST1", "step": 0.2,
+         # centers of the shells, charge q, exponent zeta (l = m = 0)
+         "shells": [[[-0.8660254037844387, -0.5, 0.1], 1.0, 1.0],
+                    [[0.8660254037844387, 0.5, 0.1], 1.0, 1.0]],
+         "selfint_numerical": 2.1019438083447435, "selfint_analytic": 2.1019485856493985},
+        {"name": "TEST2", "step": 0.4,
+         "shells": [[[1.0, 0.5, 1.5], 1.0, 1.0], [[1.0, 0.5, 1.5], 1.0, 2.0],
+                    [[-1.5, 3.0, 0.5], 1.0, 1.0],
+                    [[-0.5, -1.5, -1.0], 1.0, 2.0], [[-0.5, -1.5, -1.0], 1.0, 1.0],
+                    [[-0.5, -1.5, -1.0], 2.0, 3.0]],
+         "selfint_numerical": 31.8808479535843396, "selfint_analytic": 31.8912297114622483},
+    ],
+}
+
+
 def small_fixture():
     g = O.Grid3D.cube(-2.4, 4, 0.2)  # 25 points per axis
     tp, tw = O.gauss_quad(6, 6, 0.0, 2.0, 1.0e3)
@@ -91,6 +119,8 @@ if __name__ == "__main__":
         json.dump(KAT, f, indent=1)
     with open(os.path.join(HERE, "multipole_test_kat.json"), "w") as f:
         json.dump(MULTIPOLE_KAT, f, indent=1)
+    with open(os.path.join(HERE, "slater_test_kat.json"), "w") as f:
+        json.dump(SLATER_KAT, f, indent=1)
     with open(os.path.join(HERE, "oracle_small.json"), "w") as f:
         json.dump(small_fixture(), f, indent=1)
     print("wrote", HERE)

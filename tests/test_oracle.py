@@ -110,3 +110,21 @@ def test_potential_close_to_analytic(oracle):
     V = oracle.coulomb_apply(g, rho, quad=(20, 20, 0.0, 2.0, 1.0e3))
     Va = oracle.gauss_pot_cube(g, q, a, c)
     assert np.abs(V - Va).max() / np.abs(Va).max() < 2e-4
+
+
+def test_slater_analytic_energies_match_reference_goldens(oracle):
+    """tests/slater_test.F90 TESTs 1-2: the analytic self-interaction of the
+    Slater densities (SlaterGenerator%selfint -> slater_analytical_energy,
+    analytical.F90:70-188) reproduces the reference's golden values to its
+    tolerance 1e-14, and the restated densities carry unit charge per q."""
+    kat = json.load(open(os.path.join(GOLD, "slater_test_kat.json")))
+    for case in kat["cases"]:
+        c = [s[0] for s in case["shells"]]
+        q = [s[1] for s in case["shells"]]
+        z = [s[2] for s in case["shells"]]
+        E = oracle.slater_analytical_energy(q, z, c)
+        assert abs(E - case["selfint_analytic"]) <= kat["tolerance"] * abs(case["selfint_analytic"])
+    r = np.linspace(0.0, 40.0, 400001)
+    for zeta in (1.0, 2.0, 3.0):
+        rho = oracle.slater_dens(zeta, 0, r)
+        assert abs(np.trapezoid(4 * np.pi * r * r * rho, r) - 1.0) < 1e-9
