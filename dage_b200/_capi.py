@@ -78,7 +78,7 @@ SIGNATURES = {
     "dage_gbfmm_local_expansions": (ctypes.c_int, [_VP, _D]),
     "dage_gbfmm_evaluate_le": (ctypes.c_int, [_VP, _D, _VP, ctypes.c_uint]),
     "dage_gbfmm_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(DageGrid1D), ctypes.c_int,
-                                               ctypes.c_int, _VP, ctypes.c_size_t, _VP]),
+                                               ctypes.c_int, _VP, ctypes.c_int, ctypes.c_size_t, _VP]),
     "dage_gbfmm_batch_apply": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint, _D]),
     "dage_gbfmm_batch_set_energies": (ctypes.c_int, [_VP, _D]),
     "dage_gbfmm_batch_set_bubbles": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int]),

@@ -24,6 +24,7 @@
 // no box).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <array>
 #include <limits>
@@ -32,6 +33,7 @@
 #include <vector>
 
 #include "fp64_stage.cuh"
+#include "near_mixed.cuh"
 #include "op3d.cuh"
 
 struct dage_gbfmm;
@@ -1049,6 +1051,11 @@ struct dage_gbfmm {
   size_t U_per_box = 0, W_per_box = 0;
   std::vector<StageDesc> desc[3];
   int tile_n[3] = {64, 64, 64};  // near-field stage tile widths (autotuned)
+  // fp16x3 near field on the tensor cores (near_mixed.cu): FP16 matrix
+  // parts of the plan, the single-density set, the weights on the device
+  NearF16Plan *near16 = nullptr;
+  NearF16Set *near16set = nullptr;
+  DevBuf d_wn;
   DevBuf wts[3], d_epart, d_energy, d_inst, d_rho, d_V;
   cudaStream_t own_stream = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1561,8 +1568,10 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   }
   g->U_per_box = maxU;
   g->W_per_box = maxW;
-  DAGE_TRY(g->d_U.alloc(sizeof(double) * maxU * g->nbox));
-  DAGE_TRY(g->d_W.alloc(sizeof(double) * maxW * g->nbox));
+  if (g->precision == DAGE_FP64) {  // the FP64 near field's intermediates
+    DAGE_TRY(g->d_U.alloc(sizeof(double) * maxU * g->nbox));
+    DAGE_TRY(g->d_W.alloc(sizeof(double) * maxW * g->nbox));
+  }
   for (int d = 0; d < 3; ++d) {
     DAGE_TRY(g->wts[d].alloc(sizeof(double) * g->npts[d]));
     DAGE_CUDA_TRY(cudaMemcpyAsync(g->wts[d].ptr, g->ax[d].weights.data(),
@@ -1853,6 +1862,124 @@ int gbfmm_autotune(dage_gbfmm *g) {
   return 0;
 }
 
+// --- fp16x3 near field (near_mixed.cu) ---------------------------------------
+NearGeom near_geom(const dage_gbfmm *g) {
+  NearGeom G;
+  G.P = g->P;
+  const int nb = 1 << g->level;
+  for (int d = 0; d < 3; ++d) {
+    G.npts[d] = g->npts[d];
+    G.q0[d].assign(nb, 0);
+    G.nq[d].assign(nb, 0);
+    G.own[d].assign(nb, 0);
+    G.p0[d].assign(nb, 0);
+    for (const auto &B : g->boxes) {
+      const int v = B.pos[d];
+      G.q0[d][v] = B.q0[d];
+      G.nq[d][v] = B.nq[d];
+      G.own[d][v] = B.own[d];
+      G.p0[d][v] = B.p0[d];
+    }
+    for (int v = 0; v < nb; ++v) {
+      G.T[d].push_back(g->Tnear[d][v].as<double>());
+      G.band[d].push_back(g->band_near[d][v].as<int2>());
+    }
+  }
+  return G;
+}
+
+std::vector<NearBox> near_boxes(const dage_gbfmm *g) {
+  std::vector<NearBox> v;
+  for (const auto &B : g->boxes) v.push_back(NearBox{{B.pos[0], B.pos[1], B.pos[2]}});
+  return v;
+}
+
+// the near-field weights w_p on the device
+int upload_near_w(dage_gbfmm *g) {
+  DAGE_TRY(g->d_wn.alloc(sizeof(double) * g->P));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(g->d_wn.ptr, g->w.data(), sizeof(double) * g->P,
+                                cudaMemcpyHostToDevice, g->stream));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return 0;
+}
+
+// Tile width of the fp16x3 near field (64 or 128 output columns), chosen by
+// timing one near-field pass of each on scratch cubes; cached per (points
+// per axis, t-points, boxes) for the process.
+std::map<std::array<int, 5>, int> g_tune16_cache;
+
+int near16_tune(dage_gbfmm *g, int *tile) {
+  // DAGE_NEAR16_TILE=64|128 fixes the width (tests of both code paths)
+  if (const char *e = std::getenv("DAGE_NEAR16_TILE")) {
+    *tile = std::atoi(e) == 128 ? 128 : 64;
+    return 0;
+  }
+  const std::array<int, 5> key = {g->npts[0], g->npts[1], g->npts[2], g->P, g->nbox};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune16_cache.find(key);
+    if (it != g_tune16_cache.end()) {
+      *tile = it->second;
+      return 0;
+    }
+  }
+  cudaStream_t s = g->stream;
+  const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
+  DevBuf rho, V;
+  DAGE_TRY(rho.alloc(sizeof(double) * n));
+  DAGE_TRY(V.alloc(sizeof(double) * n));
+  DAGE_CUDA_TRY(cudaMemsetAsync(rho.ptr, 0, sizeof(double) * n, s));
+  cudaEvent_t e0, e1;
+  DAGE_CUDA_TRY(cudaEventCreate(&e0));
+  DAGE_CUDA_TRY(cudaEventCreate(&e1));
+  const auto boxes = near_boxes(g);
+  float best = std::numeric_limits<float>::max();
+  int rc = 0;
+  for (int tn : {64, 128}) {
+    NearF16Set *set = nullptr;
+    rc = near_f16_set_create(&set, g->near16, boxes, 1, tn, s);
+    const double *rr[1] = {rho.as<double>()};
+    double *vv[1] = {V.as<double>()};
+    const double *ww[1] = {g->d_wn.as<double>()};
+    if (!rc) rc = near_f16_set_bind(set, rr, vv, ww, s);
+    for (int r = 0; r < 3 && !rc; ++r) {
+      if (r == 1) cudaEventRecord(e0, s);
+      rc = near_f16_set_run(set, s);
+    }
+    if (!rc) {
+      cudaEventRecord(e1, s);
+      rc = near_f16_set_check(set, s);
+    }
+    float ms = 0.f;
+    if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    near_f16_set_destroy(set);
+    if (rc) break;
+    if (ms < best) {
+      best = ms;
+      *tile = tn;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune16_cache[key] = *tile;
+  return 0;
+}
+
+// FP16 matrix parts, weights and tile width; with `single`, the set of the
+// single-density apply.
+int near16_init(dage_gbfmm *g, bool single) {
+  DAGE_TRY(near_f16_prepare());
+  DAGE_TRY(near_f16_plan_create(&g->near16, near_geom(g), g->stream));
+  DAGE_TRY(upload_near_w(g));
+  int tile = 64;
+  DAGE_TRY(near16_tune(g, &tile));
+  for (int d = 0; d < 3; ++d) g->tile_n[d] = tile;
+  if (single) DAGE_TRY(near_f16_set_create(&g->near16set, g->near16, near_boxes(g), 1, tile, g->stream));
+  return 0;
+}
+
 // Uploads the single-density instance table and, for a full apply, the
 // near-field descriptors.
 int single_setup(dage_gbfmm *g, const double *rho, double *V, bool near) {
@@ -1874,6 +2001,9 @@ int single_setup(dage_gbfmm *g, const double *rho, double *V, bool near) {
 void gbfmm_destroy_impl(dage_gbfmm *g) {
   if (!g) return;
   if (g->stream) cudaStreamSynchronize(g->stream);
+  near_f16_set_destroy(g->near16set);
+  near_f16_plan_destroy(g->near16);
+  g->d_wn.release();
   for (int d = 0; d < 3; ++d) {
     for (auto &b : g->Tnear[d]) b.release();
     for (auto &b : g->band_near[d]) b.release();
@@ -1931,6 +2061,14 @@ struct dage_gbfmm_batch {
   };
   std::vector<Chunk> chunks;
   DevBuf U, W;
+  // fp16x3 near field: sets of densities of one plan each, within the budget
+  int precision = DAGE_FP64;
+  struct MSet {
+    int plan = 0;
+    std::vector<int> dens;
+    NearF16Set *set = nullptr;
+  };
+  std::vector<MSet> msets;
   int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0}, maxown = 0;
   int tile_n[3] = {64, 64, 64};
   bool tuned = false;
@@ -1975,6 +2113,7 @@ void batch_destroy_impl(dage_gbfmm_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto &m : b->msets) near_f16_set_destroy(m.set);
   for (auto *g : b->plans) gbfmm_destroy_impl(g);
   for (auto &c : b->chunks)
     for (auto &d : c.desc) d.release();
@@ -1992,7 +2131,7 @@ void batch_destroy_impl(dage_gbfmm_batch *b) {
 }
 
 int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int maxlevel, int lmax,
-                      const dage_quad *quad, size_t budget) {
+                      const dage_quad *quad, int precision, size_t budget) {
   DAGE_CUDA_TRY(cudaGetDevice(&b->device));
   DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking));
   b->stream = b->own_stream;
@@ -2008,7 +2147,9 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
       if (same_grid(b->plans[k], gi)) found = (int)k;
     if (found < 0) {
       auto *g = new dage_gbfmm();
-      const int rc = gbfmm_create_impl(g, gi, maxlevel, lmax, quad);
+      g->precision = precision;
+      int rc = gbfmm_create_impl(g, gi, maxlevel, lmax, quad);
+      if (!rc && precision != DAGE_FP64) rc = near16_init(g, false);
       if (rc) {
         gbfmm_destroy_impl(g);
         return rc;
@@ -2038,6 +2179,34 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
   DAGE_TRY(b->epart.alloc(sizeof(double) * kEnergyBlocks * n));
   DAGE_TRY(b->energy.alloc(sizeof(double) * n));
   DAGE_TRY(b->inst.alloc(sizeof(GInst) * n));
+  b->precision = precision;
+  if (precision != DAGE_FP64) {
+    // per plan: consecutive densities of the plan while the set fits the budget
+    for (size_t k = 0; k < b->plans.size(); ++k) {
+      const auto boxes = near_boxes(b->plans[k]);
+      dage_gbfmm_batch::MSet cur;
+      cur.plan = (int)k;
+      for (int i = 0; i < n; ++i) {
+        if (b->plan_of[i] != (int)k) continue;
+        if (!cur.dens.empty() &&
+            near_f16_set_bytes(b->plans[k]->near16, boxes, (int)cur.dens.size() + 1) > budget) {
+          b->msets.push_back(cur);
+          cur.dens.clear();
+        }
+        cur.dens.push_back(i);
+      }
+      if (!cur.dens.empty()) b->msets.push_back(cur);
+    }
+    for (auto &m : b->msets) {
+      const dage_gbfmm *g = b->plans[m.plan];
+      DAGE_TRY(near_f16_set_create(&m.set, g->near16, near_boxes(g), (int)m.dens.size(),
+                                   g->tile_n[0], b->stream));
+    }
+    for (int d = 0; d < 3; ++d) b->tile_n[d] = b->plans[0]->tile_n[d];
+    b->tuned = true;
+    for (auto *g : b->plans) g->stream = b->stream;
+    return 0;
+  }
   // near-field chunks: consecutive densities while their intermediates fit
   size_t umax = 0, wmax = 0, ucur = 0, wcur = 0;
   dage_gbfmm_batch::Chunk cur;
@@ -2090,6 +2259,17 @@ int batch_tables(dage_gbfmm_batch *b, const double *const *rho, double *const *V
   }
   DAGE_CUDA_TRY(cudaMemcpyAsync(b->inst.ptr, ins.data(), sizeof(GInst) * b->n,
                                 cudaMemcpyHostToDevice, b->stream));
+  for (auto &m : b->msets) {
+    std::vector<const double *> rr, ww;
+    std::vector<double *> vv;
+    for (int i : m.dens) {
+      rr.push_back(rho[i]);
+      vv.push_back(V[i]);
+      ww.push_back(b->kern_of[i] >= 0 ? b->kerns[b->kern_of[i]].w.as<double>()
+                                      : b->plans[m.plan]->d_wn.as<double>());
+    }
+    DAGE_TRY(near_f16_set_bind(m.set, rr.data(), vv.data(), ww.data(), b->stream));
+  }
   std::vector<std::vector<StageDesc>> keep;
   for (auto &c : b->chunks) {
     std::vector<StageDesc> ds[3];
@@ -2137,6 +2317,7 @@ int batch_launch(dage_gbfmm_batch *b, const double *const *rho, double *const *V
                               c.desc[2].as<StageDesc>()};
     DAGE_TRY(run_near(dd, c.njobs, b->mt, b->nt, b->P, b->w, b->tile_n, s));
   }
+  for (auto &m : b->msets) DAGE_TRY(near_f16_set_run(m.set, s));
   DAGE_TRY(run_l2p(d_inst, b->n, b->nbox, b->lmax, b->maxown, nullptr, any_helm, s));
   DAGE_TRY(run_energy(d_inst, b->n, b->energy.as<double>(), s));
   return 0;
@@ -2152,12 +2333,13 @@ int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const d
   clear_error();
   if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
   *out = nullptr;
-  if (precision != DAGE_FP64)
-    return fail(DAGE_E_UNSUPPORTED, "the GBFMM operator runs in FP64 (DAGE_FP64)");
+  if (precision != DAGE_FP64 && precision != DAGE_MIXED_FP16X3)
+    return fail(DAGE_E_UNSUPPORTED,
+                "the GBFMM operator runs in DAGE_FP64 or DAGE_MIXED_FP16X3 (near field)");
   auto *g = new dage_gbfmm();
   g->precision = precision;
   int rc = gbfmm_create_impl(g, grid, maxlevel, lmax, quad);
-  if (!rc) rc = gbfmm_autotune(g);
+  if (!rc) rc = precision == DAGE_FP64 ? gbfmm_autotune(g) : near16_init(g, true);
   if (rc) {
     gbfmm_destroy_impl(g);
     return rc;
@@ -2171,13 +2353,14 @@ int dage_gbfmm_create_adaptive(const dage_grid1d grid[3], int maxlevel, int lmax
   clear_error();
   if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
   *out = nullptr;
-  if (precision != DAGE_FP64)
-    return fail(DAGE_E_UNSUPPORTED, "the GBFMM operator runs in FP64 (DAGE_FP64)");
+  if (precision != DAGE_FP64 && precision != DAGE_MIXED_FP16X3)
+    return fail(DAGE_E_UNSUPPORTED,
+                "the GBFMM operator runs in DAGE_FP64 or DAGE_MIXED_FP16X3 (near field)");
   auto *g = new dage_gbfmm();
   g->precision = precision;
   g->lev0 = 1;
   int rc = gbfmm_create_impl(g, grid, maxlevel, lmax, quad);
-  if (!rc) rc = gbfmm_autotune(g);
+  if (!rc) rc = precision == DAGE_FP64 ? gbfmm_autotune(g) : near16_init(g, true);
   if (rc) {
     gbfmm_destroy_impl(g);
     return rc;
@@ -2209,6 +2392,7 @@ int dage_gbfmm_set_energy(dage_gbfmm *g, double energy) {
   g->energy = energy;
   g->kappa = energy < 0.0 ? std::sqrt(-2.0 * energy) : 0.0;
   set_weights(g);
+  if (g->near16) DAGE_TRY(upload_near_w(g));
   return build_m2l(g);
 }
 
@@ -2237,18 +2421,28 @@ int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags
   const double *d_rho;
   double *d_V;
   DAGE_TRY(stage_io(g, rho, V, flags, &d_rho, &d_V));
-  DAGE_TRY(single_setup(g, d_rho, d_V, true));
+  if (g->near16set) {
+    const double *rr[1] = {d_rho};
+    double *vv[1] = {d_V};
+    const double *ww[1] = {g->d_wn.as<double>()};
+    DAGE_TRY(near_f16_set_bind(g->near16set, rr, vv, ww, s));
+  }
+  DAGE_TRY(single_setup(g, d_rho, d_V, g->near16set == nullptr));
   const GInst *d_inst = g->d_inst.as<GInst>();
   DAGE_CUDA_TRY(cudaMemsetAsync(d_V, 0, sizeof(double) * n, s));
   DAGE_TRY(run_multipoles(d_inst, 1, g->nbox, g->lmax, g->nslab, g->kappa > 0.0, s));
   DAGE_TRY(run_m2m(d_inst, 1, g, s));
   DAGE_TRY(run_m2l(d_inst, 1, g->nbtot, g->N, s));
   DAGE_TRY(run_l2l(d_inst, 1, g, s));
-  int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
-  near_bounds(g, mt, nt);
-  const StageDesc *dd[3] = {g->d_desc[0].as<StageDesc>(), g->d_desc[1].as<StageDesc>(),
-                            g->d_desc[2].as<StageDesc>()};
-  DAGE_TRY(run_near(dd, g->nbox, mt, nt, g->P, g->w, g->tile_n, s));
+  if (g->near16set) {
+    DAGE_TRY(near_f16_set_run(g->near16set, s));
+  } else {
+    int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
+    near_bounds(g, mt, nt);
+    const StageDesc *dd[3] = {g->d_desc[0].as<StageDesc>(), g->d_desc[1].as<StageDesc>(),
+                              g->d_desc[2].as<StageDesc>()};
+    DAGE_TRY(run_near(dd, g->nbox, mt, nt, g->P, g->w, g->tile_n, s));
+  }
   DAGE_TRY(run_l2p(d_inst, 1, g->nbox, g->lmax, max_owned(g), nullptr, g->kappa > 0.0, s));
   if (flags & DAGE_ENERGY) DAGE_TRY(run_energy(d_inst, 1, g->d_energy.as<double>(), s));
   if (!(flags & DAGE_DEVICE_PTRS))
@@ -2258,6 +2452,7 @@ int dage_gbfmm_apply(dage_gbfmm *g, const double *rho, double *V, unsigned flags
   DAGE_CUDA_TRY(cudaEventRecord(g->ev1, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   DAGE_CUDA_TRY(cudaEventElapsedTime(&g->last_ms, g->ev0, g->ev1));
+  if (g->near16set) DAGE_TRY(near_f16_set_check(g->near16set, s));
   return 0;
 }
 
@@ -2321,16 +2516,19 @@ int dage_gbfmm_last_time_ms(const dage_gbfmm *g, float *ms) {
 
 // ----------------------------------------------------------------- batch
 int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int lmax,
-                            const dage_quad *quad, size_t near_budget_bytes,
+                            const dage_quad *quad, int precision, size_t near_budget_bytes,
                             dage_gbfmm_batch **out) {
   clear_error();
   if (!out) return fail(DAGE_E_INVALID, "null output handle pointer");
   *out = nullptr;
   if (n < 1 || n > 65535 || !grids || !quad)
     return fail(DAGE_E_INVALID, "need 1..65535 densities, grids and a quadrature");
+  if (precision != DAGE_FP64 && precision != DAGE_MIXED_FP16X3)
+    return fail(DAGE_E_UNSUPPORTED,
+                "the GBFMM batch runs in DAGE_FP64 or DAGE_MIXED_FP16X3 (near field)");
   auto *b = new dage_gbfmm_batch();
   const size_t budget = near_budget_bytes ? near_budget_bytes : ((size_t)8 << 30);
-  const int rc = batch_create_impl(b, n, grids, maxlevel, lmax, quad, budget);
+  const int rc = batch_create_impl(b, n, grids, maxlevel, lmax, quad, precision, budget);
   if (rc) {
     batch_destroy_impl(b);
     return rc;
@@ -2397,6 +2595,7 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
       b->graph_key.clear();
       // kernel attributes are set before capture
       DAGE_TRY(prepare_fp64_stages());
+      DAGE_TRY(near_f16_prepare());
       DAGE_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       const int rc = batch_launch(b, dr.data(), dv.data());
       cudaGraph_t graph = nullptr;
@@ -2426,6 +2625,7 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
   DAGE_CUDA_TRY(cudaEventRecord(b->ev1, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));
   DAGE_CUDA_TRY(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  for (auto &m : b->msets) DAGE_TRY(near_f16_set_check(m.set, s));
   return 0;
 }
 
@@ -2487,7 +2687,7 @@ int dage_gbfmm_batch_info(const dage_gbfmm_batch *b, int *nplans, int *nchunks, 
                           long long *graph_nodes) {
   if (!b) return fail(DAGE_E_INVALID, "null handle");
   if (nplans) *nplans = (int)b->plans.size();
-  if (nchunks) *nchunks = (int)b->chunks.size();
+  if (nchunks) *nchunks = (int)(b->precision == DAGE_FP64 ? b->chunks.size() : b->msets.size());
   if (tile_n)
     for (int d = 0; d < 3; ++d) tile_n[d] = b->tile_n[d];
   if (graph_nodes) *graph_nodes = (long long)b->graph_nodes;

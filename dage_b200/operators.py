@@ -344,21 +344,27 @@ class GBFMMCoulomb3D:
     reference's GaussQuad(25, 25).  ``adaptive_mode``: the reference's
     adaptive mode (gbfmm_coulomb3d.F90:374-384, 1386-1433): multipoles up to
     level 1, and neighbours of a box's parent that hold none of the box's
-    nearest neighbours interact as whole parent-level boxes (Coulomb only)."""
+    nearest neighbours interact as whole parent-level boxes (Coulomb only).
+    ``precision``: "fp64" (the drop-in) or "fp16x3" (the near field on the
+    tensor cores in the split precision; multipoles, M2L and L2P stay FP64)."""
 
     def __init__(self, grid: Grid3D, lmax: int = 12, maxlevel: int = 2,
-                 quad: GaussQuad | None = None, adaptive_mode: bool = False):
+                 quad: GaussQuad | None = None, adaptive_mode: bool = False,
+                 precision: str = "fp64"):
         lib = load()
         self.grid = grid
         self.lmax = lmax
         self.maxlevel = maxlevel
         self.adaptive_mode = adaptive_mode
+        if precision not in ("fp64", "fp16x3"):
+            raise ValueError("GBFMM precision must be 'fp64' or 'fp16x3'")
+        self.precision = precision
         self.quad = quad if quad is not None else GaussQuad(25, 25)
         self._keep = (grid.c(), self.quad.c())
         h = ctypes.c_void_p()
         create = lib.dage_gbfmm_create_adaptive if adaptive_mode else lib.dage_gbfmm_create
         check(create(self._keep[0], maxlevel, lmax, ctypes.byref(self._keep[1]),
-                     _capi.DAGE_FP64, ctypes.byref(h)))
+                     PRECISIONS[precision], ctypes.byref(h)))
         self._h = h
         nb, nlm = ctypes.c_int(), ctypes.c_int()
         check(lib.dage_gbfmm_box_count(h, ctypes.byref(nb), ctypes.byref(nlm)))
@@ -439,8 +445,8 @@ class GBFMMHelmholtz3D(GBFMMCoulomb3D):
     operator with the kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)."""
 
     def __init__(self, grid: Grid3D, energy: float, lmax: int = 12, maxlevel: int = 2,
-                 quad: GaussQuad | None = None):
-        super().__init__(grid, lmax=lmax, maxlevel=maxlevel, quad=quad)
+                 quad: GaussQuad | None = None, precision: str = "fp64"):
+        super().__init__(grid, lmax=lmax, maxlevel=maxlevel, quad=quad, precision=precision)
         self.set_energy(energy)
 
     def set_energy(self, energy: float) -> None:
@@ -452,11 +458,16 @@ class GBFMMBatch:
     (config: hundreds of orbitals of uneven grid sizes in one SCF step).
     Densities on equal grids share one plan; each pipeline stage is one
     launch over all densities, and the pipeline runs as a CUDA graph
-    captured for the set of device cubes it is given."""
+    captured for the set of device cubes it is given.  ``precision``:
+    "fp64" or "fp16x3" (near field on the tensor cores)."""
 
     def __init__(self, grids, lmax: int = 12, maxlevel: int = 2,
-                 quad: GaussQuad | None = None, near_budget_bytes: int = 0):
+                 quad: GaussQuad | None = None, near_budget_bytes: int = 0,
+                 precision: str = "fp64"):
         lib = load()
+        if precision not in ("fp64", "fp16x3"):
+            raise ValueError("GBFMM precision must be 'fp64' or 'fp16x3'")
+        self.precision = precision
         self.grids = list(grids)
         self.lmax = lmax
         self.quad = quad if quad is not None else GaussQuad(25, 25)
@@ -465,8 +476,8 @@ class GBFMMBatch:
         self._keep = (arr, self.grids, self.quad.c())
         h = ctypes.c_void_p()
         check(lib.dage_gbfmm_batch_create(len(self.grids), arr, maxlevel, lmax,
-                                          ctypes.byref(self._keep[2]), near_budget_bytes,
-                                          ctypes.byref(h)))
+                                          ctypes.byref(self._keep[2]), PRECISIONS[precision],
+                                          near_budget_bytes, ctypes.byref(h)))
         self._h = h
 
     def __del__(self):

@@ -232,7 +232,7 @@ int dage_gbfmm_destroy(dage_gbfmm *g);
 typedef struct dage_gbfmm_batch dage_gbfmm_batch;
 typedef struct dage_bubbles dage_bubbles;
 int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int lmax,
-                            const dage_quad *quad, size_t near_budget_bytes,
+                            const dage_quad *quad, int precision, size_t near_budget_bytes,
                             dage_gbfmm_batch **out);
 /* rho[i], V[i]: cube i (host arrays, or device pointers with DAGE_DEVICE_PTRS);
  * energies[n] receives each int rho V with DAGE_ENERGY.  The pipeline is
