@@ -625,41 +625,65 @@ def run_workload(args, world, rank, local):
                "gaussians": 2, "seed": SEED}, clocks, 3 * 40 + 2,
               {"accuracy": {"vs": "analytic sum q erf(sqrt(a) r)/r", "max_rel": err}})
     elif wl in ("gbfmm_241", "gbfmm_241_adaptive", "helmholtz_gbfmm_241", "helmholtz_gbfmm_241"):
-        # FP64 GBFMM, 241^3 (40 cells, step 0.2), 4^3 boxes, lmax 12, 16 Gaussians
+        # GBFMM, 241^3 (40 cells, step 0.2), 4^3 boxes, lmax 12, 16 Gaussians
         # (the adaptive variant: the reference's adaptive mode, level-1 moments;
-        # the Helmholtz variant: kernel e^(-kappa r)/r at E = -0.5, kappa = 1)
+        # the Helmholtz variant: kernel e^(-kappa r)/r at E = -0.5, kappa = 1).
+        # --precision fp64 times the FP64 operator; any split mode times the
+        # fp16x3 near field (the GBFMM's mixed form) beside the FP64 operator.
         adaptive = wl.endswith("adaptive")
         helm = wl.startswith("helmholtz")
+        prec = "fp64" if args.precision == "fp64" else "fp16x3"
         rng = np.random.default_rng(SEED)
         q, a = rng.uniform(-1, 2, 16), rng.uniform(0.3, 6, 16)
         c = rng.uniform(-24, 24, (16, 3))
         g = dage.Grid3D.cube(-24.0, 40, 0.2)
         rho = _gauss_cube(dev, 40, 0.2, q, a, c)
         quad = dage.GaussQuad(20, 20, 0.0, TLIN, TLOG)
-        op = (dage.GBFMMHelmholtz3D(g, -0.5, lmax=12, quad=quad) if helm
-              else dage.GBFMMCoulomb3D(g, lmax=12, quad=quad, adaptive_mode=adaptive))
+
+        def make(pr):
+            return (dage.GBFMMHelmholtz3D(g, -0.5, lmax=12, quad=quad, precision=pr) if helm
+                    else dage.GBFMMCoulomb3D(g, lmax=12, quad=quad, adaptive_mode=adaptive,
+                                             precision=pr))
+        op = make(prec)
         V = torch.empty_like(rho)
         clk.start()
         ms = _timed(lambda: op.apply(rho, out=V, energy=True), args.steps, args.warmup, sync)
         clocks = clk.stop()
         _, E = op.apply(rho, out=V, energy=True)
+        extra = {}
+        V64, E64 = V, E
+        if prec != "fp64":
+            op64 = make("fp64")
+            V64 = torch.empty_like(rho)
+            ms64 = _timed(lambda: op64.apply(rho, out=V64, energy=True), max(2, args.steps // 3),
+                          1, sync)
+            _, E64 = op64.apply(rho, out=V64, energy=True)
+            d = (V - V64).abs()
+            s64 = V64.abs().max()
+            extra["mixed_vs_fp64"] = {"max_rel": float(d.max() / s64),
+                                      "rms_rel": float(d.pow(2).mean().sqrt() / s64),
+                                      "energy_rel": abs(E - E64) / abs(E64),
+                                      "fp64_ms_per_step": ms64,
+                                      "speedup_vs_fp64": ms64 / ms}
+            del op64
         Vd = torch.empty_like(rho)
         direct = dage.Coulomb3D(g, quad=quad)
         if helm:
             direct = dage.Helmholtz3D(direct, -0.5)
         _, Ed = direct.apply(rho, out=Vd, energy=True, coda=False)
-        err = float((V - Vd).abs().max() / Vd.abs().max())
+        err = float((V64 - Vd).abs().max() / Vd.abs().max())
         n = 241 ** 3
-        _line(args, world, "GBFMM %s Mpts/s @241^3 FP64 (lmax 12, 4^3 boxes%s)"
+        extra["accuracy"] = {"vs": "single-box FP64 operator of the same kernel (no coda)",
+                             "fp64_gbfmm_max_rel": err,
+                             "fp64_gbfmm_energy_rel": abs(E64 - Ed) / abs(Ed)}
+        _line(args, world, "GBFMM %s Mpts/s @241^3 %s (lmax 12, 4^3 boxes%s)"
               % ("Helmholtz (kappa 1)" if helm else "Coulomb",
+                 "FP64" if prec == "fp64" else "fp16x3 near field",
                  ", adaptive mode" if adaptive else ""), n / ms / 1e3,
-              "Mpts/s", ms, "f64",
+              "Mpts/s", ms, "f64" if prec == "fp64" else "f16",
               {"workload": wl, "points_per_axis": 241, "step_bohr": 0.2, "t_points": 40,
-               "lmax": 12, "boxes": 64, "gaussians": 16, "seed": SEED,
-               "near_field_tiles": list(op.tiles)}, clocks, 3 * 40 + 9,
-              {"accuracy": {"vs": "single-box FP64 operator of the same kernel (no coda)",
-                            "max_rel": err,
-                            "energy_rel": abs(E - Ed) / abs(Ed)}})
+               "lmax": 12, "boxes": 64, "gaussians": 16, "seed": SEED, "precision": prec,
+               "near_field_tiles": list(op.tiles)}, clocks, 3 * 40 + 9, extra)
     elif wl == "bubbles_inject_301":
         rng = np.random.default_rng(SEED)
         bub, gcube = _molecule_bubbles(dage, rng)
@@ -739,7 +763,8 @@ def run_workload(args, world, rank, local):
             rhos.append(rho)
             outs.append(torch.empty_like(rho))
         quad = dage.GaussQuad(20, 20, 0.0, TLIN, TLOG)
-        bt = dage.GBFMMBatch(grids, lmax=lmax, quad=quad)
+        prec = "fp64" if args.precision == "fp64" else "fp16x3"
+        bt = dage.GBFMMBatch(grids, lmax=lmax, quad=quad, precision=prec)
         if energies is not None:
             bt.set_energies(energies)
         Ebox = {}
@@ -751,26 +776,55 @@ def run_workload(args, world, rank, local):
         # per-density check of a few densities against the single-density operator
         chk = []
         for i in range(3):
-            op = (dage.GBFMMHelmholtz3D(grids[i], energies[i], lmax=lmax, quad=quad)
-                  if energies is not None else dage.GBFMMCoulomb3D(grids[i], lmax=lmax, quad=quad))
+            op = (dage.GBFMMHelmholtz3D(grids[i], energies[i], lmax=lmax, quad=quad, precision=prec)
+                  if energies is not None else
+                  dage.GBFMMCoulomb3D(grids[i], lmax=lmax, quad=quad, precision=prec))
             V1 = torch.empty_like(rhos[i])
             op.apply(rhos[i], out=V1)
             chk.append(float((outs[i] - V1).abs().max() / V1.abs().max()))
+            del op
         pts = float(sum(int(gr.shape[0]) ** 3 for gr in grids))
-        metric = ("GBFMM batch Mpts/s, 256 densities 61^3..181^3, FP64, lmax 12"
+        metric = ("GBFMM batch Mpts/s, 256 densities 61^3..181^3, %s, lmax 12"
                   if wl == "gbfmm_batch_256" else
-                  "Helmholtz GBFMM batch Mpts/s, 64 orbitals 301^3, FP64, lmax 10")
+                  "Helmholtz GBFMM batch Mpts/s, 64 orbitals 301^3, %s, lmax 10") % (
+                      "FP64" if prec == "fp64" else "fp16x3 near field")
         extra = {"per_density_check": {"vs": "single-density operator", "max_rel": max(chk)},
-                 "batch": {"densities": nd, "plans": nplans, "near_chunks": nchunks,
-                           "tiles": list(tiles), "graph_nodes": nodes},
-                 "mixed_precision": "not available for the GBFMM paths (FP64 only)"}
+                 "batch": {"densities": nd, "plans": nplans,
+                           "near_chunks" if prec == "fp64" else "near_sets": nchunks,
+                           "tiles": list(tiles), "graph_nodes": nodes}}
+        if prec != "fp64":
+            # the FP64 batch on the same densities: per-instance errors of the
+            # split precision and the FP64 time
+            E16 = Ebox["e"]
+            del bt
+            torch.cuda.empty_cache()
+            b64 = dage.GBFMMBatch(grids, lmax=lmax, quad=quad)
+            if energies is not None:
+                b64.set_energies(energies)
+            outs64 = [torch.empty_like(r) for r in rhos]
+            E64box = {}
+            ms64 = _timed(lambda: E64box.update(e=b64.apply(rhos, outs64, energy=True)), 1, 1, sync)
+            E64 = E64box["e"]
+            vmax, vrms, erel = [], [], []
+            for i in range(nd):
+                d = (outs[i] - outs64[i]).abs()
+                s64 = outs64[i].abs().max()
+                vmax.append(float(d.max() / s64))
+                vrms.append(float(d.pow(2).mean().sqrt() / s64))
+                erel.append(abs(E16[i] - E64[i]) / abs(E64[i]))
+            extra["mixed_vs_fp64"] = {
+                "per_instance_max_rel": {"max": max(vmax), "median": float(np.median(vmax))},
+                "per_instance_rms_rel": {"max": max(vrms), "median": float(np.median(vrms))},
+                "per_instance_energy_rel": {"max": max(erel), "median": float(np.median(erel))},
+                "fp64_ms_per_step": ms64, "speedup_vs_fp64": ms64 / ms}
+            del b64, outs64
         if inject_ms is not None:
             extra["bubbles_inject"] = {"ms": inject_ms, "atoms": 20, "lmax": 2,
                                        "points": 301 ** 3,
                                        "Mpts_per_s": 301 ** 3 / inject_ms / 1e3}
-        _line(args, world, metric, pts / ms / 1e3, "Mpts/s", ms, "f64",
+        _line(args, world, metric, pts / ms / 1e3, "Mpts/s", ms, "f64" if prec == "fp64" else "f16",
               {"workload": wl, "densities": nd, "step_bohr": step, "t_points": 40,
-               "lmax": lmax, "boxes": 64, "seed": SEED,
+               "lmax": lmax, "boxes": 64, "seed": SEED, "precision": prec,
                "sizes": sorted(set(int(6 * x + 1) for x in cells))}, clocks, nodes, extra)
 
 

@@ -124,6 +124,9 @@ struct GInst {
   int fine_off, m2m_base;
   const double *Wm2m;
   const int *m2m_disp;
+  // Helmholtz instances: dense N x N translation matrix per displacement
+  // (column k = input lm), Wm2m_h + m2m_disp[g - m2m_base] * N * N
+  const double *Wm2m_h;
 };
 
 constexpr int kEnergyBlocks = 256;
@@ -603,6 +606,20 @@ __device__ __forceinline__ size_t wpos(int i, int j, int N) {
 __global__ void m2m_kernel(const GInst *__restrict__ insts, int N, int poff, int coff) {
   const GInst &I = insts[blockIdx.y];
   const int p = blockIdx.x;
+  if (I.kappa > 0.0) {
+    // Helmholtz: the dense translation of the regular basis i_l Y_lm
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      double acc = 0.0;
+      for (int c = 0; c < 8; ++c) {
+        const int gc = coff + 8 * p + c;
+        const double *qc = I.q + (size_t)gc * N;
+        const double *W = I.Wm2m_h + (size_t)I.m2m_disp[gc - I.m2m_base] * N * N;
+        for (int j = 0; j < N; ++j) acc += W[(size_t)j * N + i] * qc[j];
+      }
+      I.q[(size_t)(poff + p) * N + i] = acc;
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     double acc = 0.0;
     for (int c = 0; c < 8; ++c) {
@@ -625,6 +642,22 @@ __global__ void l2l_kernel(const GInst *__restrict__ insts, int N, int poff, int
   const GInst &I = insts[blockIdx.y];
   const int c = blockIdx.x, gc = coff + c;
   const double *Lp = I.L + (size_t)(poff + c / 8) * N;
+  if (I.kappa > 0.0) {
+    // Helmholtz: the local expansion multiplies (2l+1) i_l Y_lm and the
+    // moments i_l Y_lm, so with q(parent) = W q(child) the child's expansion
+    // is L(child)_i = sum_j W_ji (2 l_j + 1) L(parent)_j / (2 l_i + 1)
+    const double *W = I.Wm2m_h + (size_t)I.m2m_disp[gc - I.m2m_base] * N * N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      double t = 0.0;
+      for (int j = 0; j < N; ++j) {
+        const int lj = (int)sqrtf((float)j + 0.5f);
+        t += W[(size_t)i * N + j] * (2 * lj + 1) * Lp[j];
+      }
+      const int li = (int)sqrtf((float)i + 0.5f);
+      I.L[(size_t)gc * N + i] += t / (2 * li + 1);
+    }
+    return;
+  }
   const double *W = I.Wm2m + (size_t)I.m2m_disp[gc - I.m2m_base] * ((size_t)N * (N + 1) / 2);
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     double t = Lp[i];
@@ -1046,6 +1079,8 @@ struct dage_gbfmm {
   int nbtot = 0, fine_off = 0, nm2m = 0;
   std::vector<double> centers;
   DevBuf d_Wm2m, d_m2m_disp;
+  std::vector<double> m2m_dvec;  // child - parent of each distinct M2M displacement
+  DevBuf d_Wm2m_h;               // Helmholtz M2M matrices for the current kappa
   int wstride = 0, nslab = 16, ndisp = 0;
   DevBuf d_U, d_W, d_desc[3];
   size_t U_per_box = 0, W_per_box = 0;
@@ -1125,6 +1160,69 @@ void coaxial_ml(const std::vector<double> &k, int L, std::vector<double> &out) {
                          A(n, m);
     for (int l = m; l <= L; ++l)
       c(l, m + 1, m + 1) = (-B(l, -m - 1) * c(l - 1, m, m) - B(l + 1, m) * c(l + 1, m, m)) /
+                           B(m + 1, -m - 1);
+  }
+  out.resize((size_t)(L + 1) * (L + 1) * (L + 1));
+  for (int l = 0; l <= L; ++l)
+    for (int n = 0; n <= L; ++n)
+      for (int m = 0; m <= L; ++m) out[((size_t)l * (L + 1) + n) * (L + 1) + m] = c(l, n, m);
+}
+
+// i_0..i_L(x), modified spherical Bessel functions of the first kind, by
+// their all-positive series x^l sum_k (x^2/2)^k / (k! (2l+1)(2l+3)..(2l+2k+1))
+// in long double.
+void bessel_i_host(double x, int L, std::vector<double> &out) {
+  typedef long double ext;
+  out.assign(L + 1, 0.0);
+  const ext X = x, h = X * X / 2;
+  ext lead = 1;  // x^l / (2l+1)!!
+  for (int l = 0; l <= L; ++l) {
+    if (l > 0) lead *= X / (2 * l + 1);
+    ext term = lead, sum = lead;
+    for (int k = 1; k < 1000 && term > sum * 1e-22L; ++k) {
+      term *= h / (k * (ext)(2 * l + 2 * k + 1));
+      sum += term;
+    }
+    out[l] = (double)sum;
+  }
+}
+
+// Coaxial multipole-to-multipole coefficients C(l, n, m), l, n, m <= L, from
+// i_0..i_{L+1}(kappa d): the recurrence of src/bubbles/
+// helmholtz_multipole_tools.F90:513-588 (get_all_aligned_translation_
+// coefficients; a/b coefficients :591-607, zero for n < 0).
+void coaxial_mm(const std::vector<double> &ib, int L, std::vector<double> &out) {
+  const int D = L + 3;  // indices -1 .. L+1
+  std::vector<double> C((size_t)D * D * D, 0.0);
+  auto c = [&](int l, int n, int m) -> double & {
+    return C[((size_t)(l + 1) * D + (n + 1)) * D + (m + 1)];
+  };
+  auto A = [](int n, int m) {
+    if (n < 0) return 0.0;
+    const int am = std::abs(m);
+    return std::sqrt((double)((n + 1 + am) * (n + 1 - am)) / ((2 * n + 1) * (2 * n + 3)));
+  };
+  auto B = [](int n, int m) {
+    if (n < 0 || std::abs(m) > n) return 0.0;
+    const double b = std::sqrt((double)((n - m - 1) * (n - m)) / ((2 * n - 1) * (2 * n + 1)));
+    return m < 0 ? -b : b;
+  };
+  for (int n = 0; n <= L + 1; ++n) {
+    c(n, 0, 0) = ((n & 1) ? -1.0 : 1.0) * std::sqrt(2.0 * n + 1) * ib[n];
+    c(0, n, 0) = ((n & 1) ? -1.0 : 1.0) * c(n, 0, 0);
+  }
+  for (int n = 1; n <= L; ++n) {
+    c(1, n, 0) = (A(n, 0) * c(0, n + 1, 0) + A(n - 1, 0) * c(0, n - 1, 0)) / A(0, 0);
+    c(n, 1, 0) = (((1 + n) & 1) ? -1.0 : 1.0) * c(1, n, 0);
+  }
+  for (int m = 0; m <= L; ++m) {
+    for (int n = m; n <= L; ++n)
+      for (int l = m; l <= L; ++l)
+        c(l, n + 1, m) = (A(l, m) * c(l + 1, n, m) + A(l - 1, m) * c(l - 1, n, m) -
+                          A(n - 1, m) * c(l, n - 1, m)) /
+                         A(n, m);
+    for (int l = m; l <= L; ++l)
+      c(l, m + 1, m + 1) = (B(l, -m - 1) * c(l - 1, m, m) + B(l + 1, m) * c(l + 1, m, m)) /
                            B(m + 1, -m - 1);
   }
   out.resize((size_t)(L + 1) * (L + 1) * (L + 1));
@@ -1253,6 +1351,40 @@ int build_m2l_into(const dage_gbfmm *g, double kappa, DevBuf &T) {
 }
 
 int build_m2l(dage_gbfmm *g) { return build_m2l_into(g, g->kappa, g->d_Tm2l); }
+
+// Helmholtz M2M matrices of the plan's child-to-parent displacements for
+// kappa: the HelmholtzMultipoleTranslator (helmholtz_multipole_tools.F90:
+// 172-278 with :338-378: rotation to the axis parent - child, coaxial
+// translation by i_l(kappa d), rotation back), assembled like the M2L
+// converter (the same scalings and real-basis coaxial action), into W.
+int build_helm_m2m_into(const dage_gbfmm *g, double kappa, DevBuf &W) {
+  if (g->nm2m == 0 || kappa <= 0.0) return 0;
+  cudaStream_t s = g->stream;
+  const int lmax = g->lmax;
+  const int rblk = (lmax + 1) * (2 * lmax + 1) * (2 * lmax + 3) / 3;
+  const size_t cblk = (size_t)(lmax + 1) * (lmax + 1) * (lmax + 1);
+  std::vector<double> R((size_t)g->nm2m * rblk), C(g->nm2m * cblk), r, c, ib;
+  for (int d = 0; d < g->nm2m; ++d) {
+    const double *dv = &g->m2m_dvec[3 * d];  // child - parent
+    const double dir[3] = {-dv[0], -dv[1], -dv[2]};
+    rotation_blocks(dir, lmax, r);
+    std::copy(r.begin(), r.begin() + rblk, R.begin() + (size_t)d * rblk);
+    bessel_i_host(kappa * std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]), lmax + 1, ib);
+    coaxial_mm(ib, lmax, c);
+    std::copy(c.begin(), c.end(), C.begin() + (size_t)d * cblk);
+  }
+  DevBuf dR, dC;
+  DAGE_TRY(W.alloc(sizeof(double) * (size_t)g->nm2m * g->N * g->N));
+  DAGE_TRY(dR.alloc(sizeof(double) * R.size()));
+  DAGE_TRY(dC.alloc(sizeof(double) * C.size()));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(dR.ptr, R.data(), sizeof(double) * R.size(), cudaMemcpyHostToDevice, s));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(dC.ptr, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, s));
+  helm_m2l_matrices_kernel<<<g->nm2m, 256, 0, s>>>(dR.as<double>(), rblk, dC.as<double>(), lmax,
+                                                    W.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
 
 // Near-field weights w_p = 2/sqrt(pi) tw_p, times e^(2E/(4 t_p^2)) for the
 // Helmholtz kernel when E < -0.005 (src/gbfmm/gbfmm_helmholtz3d.F90:478-516).
@@ -1488,6 +1620,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
         m2m_disp.push_back(ti);
       }
     g->nm2m = (int)tindex.size();
+    g->m2m_dvec = tdisp;
     if (g->nm2m > 0) {
       const int M = g->N * (g->N + 1) / 2;
       TransTables t;
@@ -1616,6 +1749,7 @@ GInst plan_inst(const dage_gbfmm *g, const double *rho, double *V, double *q, do
   I.m2m_base = g->level > g->lev0 ? g->lev_off[g->lev0 + 1] : 0;
   I.Wm2m = g->d_Wm2m.as<double>();
   I.m2m_disp = g->d_m2m_disp.as<int>();
+  I.Wm2m_h = g->d_Wm2m_h.as<double>();
   return I;
 }
 
@@ -2004,6 +2138,7 @@ void gbfmm_destroy_impl(dage_gbfmm *g) {
   near_f16_set_destroy(g->near16set);
   near_f16_plan_destroy(g->near16);
   g->d_wn.release();
+  g->d_Wm2m_h.release();
   for (int d = 0; d < 3; ++d) {
     for (auto &b : g->Tnear[d]) b.release();
     for (auto &b : g->band_near[d]) b.release();
@@ -2069,6 +2204,7 @@ struct dage_gbfmm_batch {
     NearF16Set *set = nullptr;
   };
   std::vector<MSet> msets;
+  DevBuf ws16[3];  // the sets' shared workspace: split input, U, W
   int mt[3] = {0, 0, 0}, nt[3] = {0, 0, 0}, maxown = 0;
   int tile_n[3] = {64, 64, 64};
   bool tuned = false;
@@ -2087,6 +2223,7 @@ struct dage_gbfmm_batch {
     int plan = 0;
     double energy = 0.0;
     DevBuf T, w;  // M2L matrices of the plan's displacements; near-field weights
+    DevBuf Wh;    // Helmholtz M2M matrices (maxlevel >= 3)
   };
   std::vector<Kern> kerns;
   std::vector<int> kern_of;  // per density, -1: Coulomb
@@ -2120,9 +2257,10 @@ void batch_destroy_impl(dage_gbfmm_batch *b) {
   for (auto &k : b->kerns) {
     k.T.release();
     k.w.release();
+    k.Wh.release();
   }
   for (DevBuf *d : {&b->q, &b->L, &b->partial, &b->epart, &b->energy, &b->inst, &b->U, &b->W,
-                    &b->stage_rho, &b->stage_V})
+                    &b->ws16[0], &b->ws16[1], &b->ws16[2], &b->stage_rho, &b->stage_V})
     d->release();
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -2197,10 +2335,24 @@ int batch_create_impl(dage_gbfmm_batch *b, int n, const dage_grid1d *grids, int 
       }
       if (!cur.dens.empty()) b->msets.push_back(cur);
     }
+    // one workspace for all sets (they run one after another on the stream)
+    size_t wsb[3] = {0, 0, 0};
+    for (auto &m : b->msets) {
+      const dage_gbfmm *g = b->plans[m.plan];
+      size_t sb[3];
+      near_f16_set_sizes(g->near16, near_boxes(g), (int)m.dens.size(), sb);
+      for (int k = 0; k < 3; ++k) wsb[k] = std::max(wsb[k], sb[k]);
+    }
+    void *ws[3];
+    for (int k = 0; k < 3; ++k) {
+      DAGE_TRY(b->ws16[k].alloc(wsb[k]));
+      DAGE_CUDA_TRY(cudaMemsetAsync(b->ws16[k].ptr, 0, wsb[k], b->stream));
+      ws[k] = b->ws16[k].ptr;
+    }
     for (auto &m : b->msets) {
       const dage_gbfmm *g = b->plans[m.plan];
       DAGE_TRY(near_f16_set_create(&m.set, g->near16, near_boxes(g), (int)m.dens.size(),
-                                   g->tile_n[0], b->stream));
+                                   g->tile_n[0], b->stream, ws));
     }
     for (int d = 0; d < 3; ++d) b->tile_n[d] = b->plans[0]->tile_n[d];
     b->tuned = true;
@@ -2255,6 +2407,7 @@ int batch_tables(dage_gbfmm_batch *b, const double *const *rho, double *const *V
       const auto &k = b->kerns[b->kern_of[i]];
       ins[i].kappa = std::sqrt(-2.0 * k.energy);
       ins[i].Tm2l = k.T.as<double>();
+      ins[i].Wm2m_h = k.Wh.as<double>();
     }
   }
   DAGE_CUDA_TRY(cudaMemcpyAsync(b->inst.ptr, ins.data(), sizeof(GInst) * b->n,
@@ -2385,14 +2538,12 @@ int dage_gbfmm_set_energy(dage_gbfmm *g, double energy) {
   clear_error();
   if (!g) return fail(DAGE_E_INVALID, "null handle");
   if (!(energy <= 0.0)) return fail(DAGE_E_INVALID, "energy must be <= 0 (got %g)", energy);
-  if (energy < 0.0 && (g->level > 2 || g->lev0 < 2))
-    return fail(DAGE_E_UNSUPPORTED,
-                "the Helmholtz GBFMM runs with maxlevel 2, not adaptive (no Helmholtz M2M/L2L)");
   DAGE_CUDA_TRY(cudaSetDevice(g->device));
   g->energy = energy;
   g->kappa = energy < 0.0 ? std::sqrt(-2.0 * energy) : 0.0;
   set_weights(g);
   if (g->near16) DAGE_TRY(upload_near_w(g));
+  DAGE_TRY(build_helm_m2m_into(g, g->kappa, g->d_Wm2m_h));
   return build_m2l(g);
 }
 
@@ -2632,16 +2783,14 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
 int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies) {
   clear_error();
   if (!b || !energies) return fail(DAGE_E_INVALID, "null argument");
-  for (int i = 0; i < b->n; ++i) {
+  for (int i = 0; i < b->n; ++i)
     if (!(energies[i] <= 0.0)) return fail(DAGE_E_INVALID, "energy %d must be <= 0", i);
-    if (energies[i] < 0.0 && b->plans[0]->level > 2)
-      return fail(DAGE_E_UNSUPPORTED, "the Helmholtz GBFMM runs with maxlevel 2 (no Helmholtz M2M/L2L)");
-  }
   DAGE_CUDA_TRY(cudaSetDevice(b->device));
   DAGE_CUDA_TRY(cudaStreamSynchronize(b->stream));
   for (auto &k : b->kerns) {
     k.T.release();
     k.w.release();
+    k.Wh.release();
   }
   b->kerns.clear();
   for (int i = 0; i < b->n; ++i) {
@@ -2657,6 +2806,7 @@ int dage_gbfmm_batch_set_energies(dage_gbfmm_batch *b, const double *energies) {
     k.energy = energies[i];
     const dage_gbfmm *g = b->plans[k.plan];
     DAGE_TRY(build_m2l_into(g, std::sqrt(-2.0 * k.energy), k.T));
+    DAGE_TRY(build_helm_m2m_into(g, std::sqrt(-2.0 * k.energy), k.Wh));
     std::vector<double> w;
     weights_for(g, k.energy, w);
     DAGE_TRY(k.w.alloc(sizeof(double) * w.size()));

@@ -55,7 +55,7 @@ namespace {
 constexpr int BKN = 64;            // K extent of one shared-memory stage (128-byte rows)
 constexpr int kNThreads = 576;     // 18 warps
 constexpr int kNEpiThreads = 512;  // warps 2-17
-constexpr int kNMaxGroup = 8;      // t-points summed per pass of the last stage
+constexpr int kNMaxGroup = 4;      // t-points summed per pass of the last stage (W slots)
 constexpr int kRowsA = 32, kRowsB = 4;  // tile rows: 32 along a x 4 along b
 static_assert(kRowsA * kRowsB == BM, "tile rows");
 
@@ -630,7 +630,8 @@ struct NearF16Set {
   int zpad = 0, xpad = 0;
   long long xsl = 0, ysl = 0;   // x slices of U, y slices of W per slot
   long long xs_rows = 0;        // rows (y, z) of one density's split input
-  DevBuf X, U, W;               // two FP16 planes each
+  DevBuf X, U, W;               // two FP16 planes each (when the set owns them)
+  __half *xp = nullptr, *up = nullptr, *wp = nullptr;  // the planes in use
   DevBuf jobs[3], tiles[3];
   int ntiles[3] = {0, 0, 0};
   std::vector<int4> htiles[3];
@@ -744,16 +745,22 @@ SetDims set_dims(const NearF16Plan *pl, const std::vector<NearBox> &boxes, int n
 
 }  // namespace
 
-size_t near_f16_set_bytes(const NearF16Plan *pl, const std::vector<NearBox> &boxes, int n) {
+void near_f16_set_sizes(const NearF16Plan *pl, const std::vector<NearBox> &boxes, int n,
+                        size_t bytes[3]) {
   const SetDims d = set_dims(pl, boxes, n);
-  const size_t x = (size_t)n * d.xs_rows * d.ld[0];
-  const size_t u = (size_t)d.xsl * d.zpad * d.ld[1];
-  const size_t w = (size_t)d.G * d.ysl * d.xpad * d.ld[2];
-  return sizeof(__half) * 2 * (x + u + w);
+  bytes[0] = sizeof(__half) * 2 * ((size_t)n * d.xs_rows * d.ld[0]);
+  bytes[1] = sizeof(__half) * 2 * ((size_t)d.xsl * d.zpad * d.ld[1]);
+  bytes[2] = sizeof(__half) * 2 * ((size_t)d.G * d.ysl * d.xpad * d.ld[2]);
+}
+
+size_t near_f16_set_bytes(const NearF16Plan *pl, const std::vector<NearBox> &boxes, int n) {
+  size_t b[3];
+  near_f16_set_sizes(pl, boxes, n, b);
+  return b[0] + b[1] + b[2];
 }
 
 int near_f16_set_create(NearF16Set **out, const NearF16Plan *pl, const std::vector<NearBox> &boxes,
-                        int n, int tile_n, cudaStream_t s0) {
+                        int n, int tile_n, cudaStream_t s0, void *const ws[3]) {
   if (tile_n != 64 && tile_n != 128) return fail(DAGE_E_INVALID, "near-field tile width %d", tile_n);
   auto *st = new NearF16Set();
   *out = st;
@@ -777,13 +784,24 @@ int near_f16_set_create(NearF16Set **out, const NearF16Plan *pl, const std::vect
   const size_t xe = (size_t)n * d.xs_rows * d.ld[0];
   const size_t ue = (size_t)d.xsl * d.zpad * d.ld[1];
   const size_t we = (size_t)d.G * d.ysl * d.xpad * d.ld[2];
-  DAGE_TRY(st->X.alloc(sizeof(__half) * 2 * xe));
-  DAGE_TRY(st->U.alloc(sizeof(__half) * 2 * ue));
-  DAGE_TRY(st->W.alloc(sizeof(__half) * 2 * we));
-  // the rows and columns the stages never write are the zero padding the
-  // next stage reads
-  DAGE_CUDA_TRY(cudaMemsetAsync(st->U.ptr, 0, st->U.bytes, s0));
-  DAGE_CUDA_TRY(cudaMemsetAsync(st->W.ptr, 0, st->W.bytes, s0));
+  if (ws) {  // shared workspace (sets that run one after another)
+    st->xp = static_cast<__half *>(ws[0]);
+    st->up = static_cast<__half *>(ws[1]);
+    st->wp = static_cast<__half *>(ws[2]);
+  } else {
+    DAGE_TRY(st->X.alloc(sizeof(__half) * 2 * xe));
+    DAGE_TRY(st->U.alloc(sizeof(__half) * 2 * ue));
+    DAGE_TRY(st->W.alloc(sizeof(__half) * 2 * we));
+    // Elements the stages never write (tile edges, padding) are read only
+    // against zero matrix columns or into rows that are not stored: they
+    // must be finite, so the buffers start as zeros (every later write is
+    // a finite FP16 value).
+    DAGE_CUDA_TRY(cudaMemsetAsync(st->U.ptr, 0, st->U.bytes, s0));
+    DAGE_CUDA_TRY(cudaMemsetAsync(st->W.ptr, 0, st->W.bytes, s0));
+    st->xp = st->X.as<__half>();
+    st->up = st->U.as<__half>();
+    st->wp = st->W.as<__half>();
+  }
   DAGE_TRY(st->maxbits.alloc(sizeof(unsigned) * n));
   DAGE_TRY(st->gin.alloc(sizeof(float) * n));
   DAGE_TRY(st->g01.alloc(sizeof(float) * 2 * g.P * n));
@@ -793,7 +811,7 @@ int near_f16_set_create(NearF16Set **out, const NearF16Plan *pl, const std::vect
   DAGE_TRY(st->err.alloc(sizeof(int)));
   DAGE_CUDA_TRY(cudaMemsetAsync(st->err.ptr, 0, sizeof(int), s0));
   // A maps: x stage over the densities stacked along z; U; W with its slots
-  __half *x0 = st->X.as<__half>(), *u0 = st->U.as<__half>(), *w0 = st->W.as<__half>();
+  __half *x0 = st->xp, *u0 = st->up, *w0 = st->wp;
   for (int part = 0; part < 2; ++part) {
     DAGE_TRY(make_map_3d(&st->mapA[0][part], x0 + part * xe, g.npts[0], g.npts[1],
                          (long long)n * g.npts[2], d.ld[0], g.npts[1]));
@@ -940,7 +958,7 @@ int near_f16_set_run(NearF16Set *st, cudaStream_t s) {
   const int sx = (int)std::min<long long>((per + 255) / 256, sm_count() * 8LL);
   near_split_input_kernel<<<dim3(sx, n), 256, 0, s>>>(
       st->rhoptr.as<const double *>(), g.npts[0], st->xs_rows, st->ld[0], st->gin.as<float>(),
-      st->X.as<__half>(), st->X.as<__half>() + xe);
+      st->xp, st->xp + xe);
   DAGE_CUDA_TRY(cudaGetLastError());
 
   const long long ue = st->xsl * st->zpad * st->ld[1];
@@ -967,8 +985,8 @@ int near_f16_set_run(NearF16Set *st, cudaStream_t s) {
       a.ntiles = st->ntiles[0];
       a.p = p;
       a.gscale = st->g01.as<float>();
-      a.out0 = st->U.as<__half>();
-      a.out1 = st->U.as<__half>() + ue;
+      a.out0 = st->up;
+      a.out1 = st->up + ue;
       a.oslice0 = 0;
       a.opad = st->zpad;
       a.ldn = st->ld[1];
@@ -981,8 +999,8 @@ int near_f16_set_run(NearF16Set *st, cudaStream_t s) {
       a.ntiles = st->ntiles[1];
       a.p = p;
       a.gscale = st->g01.as<float>() + P;
-      a.out0 = st->W.as<__half>();
-      a.out1 = st->W.as<__half>() + we;
+      a.out0 = st->wp;
+      a.out1 = st->wp + we;
       a.oslice0 = (long long)slot * st->ysl;
       a.opad = st->xpad;
       a.ldn = st->ld[2];

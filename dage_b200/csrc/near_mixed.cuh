@@ -39,10 +39,15 @@ struct NearF16Set;   // intermediates, tensor maps and job tables of n densities
 int near_f16_plan_create(NearF16Plan **out, const NearGeom &geom, cudaStream_t s);
 void near_f16_plan_destroy(NearF16Plan *p);
 
-// n densities of one plan; tile width 64 or 128 output columns.
+// n densities of one plan; tile width 64 or 128 output columns.  ws: null
+// (the set allocates its intermediates) or three zero-initialised device
+// buffers of at least near_f16_set_sizes bytes (split input, U, W) that
+// sets running one after another on one stream may share.
 int near_f16_set_create(NearF16Set **out, const NearF16Plan *plan, const std::vector<NearBox> &boxes,
-                        int n, int tile_n, cudaStream_t s);
+                        int n, int tile_n, cudaStream_t s, void *const ws[3] = nullptr);
 void near_f16_set_destroy(NearF16Set *s);
+void near_f16_set_sizes(const NearF16Plan *plan, const std::vector<NearBox> &boxes, int n,
+                        size_t bytes[3]);
 size_t near_f16_set_bytes(const NearF16Plan *plan, const std::vector<NearBox> &boxes, int n);
 
 // Binds device cubes and per-density t-point weights (device arrays of P

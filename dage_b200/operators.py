@@ -344,7 +344,7 @@ class GBFMMCoulomb3D:
     reference's GaussQuad(25, 25).  ``adaptive_mode``: the reference's
     adaptive mode (gbfmm_coulomb3d.F90:374-384, 1386-1433): multipoles up to
     level 1, and neighbours of a box's parent that hold none of the box's
-    nearest neighbours interact as whole parent-level boxes (Coulomb only).
+    nearest neighbours interact as whole parent-level boxes.
     ``precision``: "fp64" (the drop-in) or "fp16x3" (the near field on the
     tensor cores in the split precision; multipoles, M2L and L2P stay FP64)."""
 
@@ -445,8 +445,10 @@ class GBFMMHelmholtz3D(GBFMMCoulomb3D):
     operator with the kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)."""
 
     def __init__(self, grid: Grid3D, energy: float, lmax: int = 12, maxlevel: int = 2,
-                 quad: GaussQuad | None = None, precision: str = "fp64"):
-        super().__init__(grid, lmax=lmax, maxlevel=maxlevel, quad=quad, precision=precision)
+                 quad: GaussQuad | None = None, precision: str = "fp64",
+                 adaptive_mode: bool = False):
+        super().__init__(grid, lmax=lmax, maxlevel=maxlevel, quad=quad, precision=precision,
+                         adaptive_mode=adaptive_mode)
         self.set_energy(energy)
 
     def set_energy(self, energy: float) -> None:

@@ -156,11 +156,17 @@ typedef struct dage_gbfmm dage_gbfmm;
  * the GPU.  maxlevel 2..5 (the reference default is 2: 4x4x4 boxes, whose
  * local far field needs no M2M/L2L; deeper levels run the upward M2M pass,
  * M2L at every level and the downward L2L pass of gbfmm_coulomb3d.F90:
- * 650-905, 1502-1621); lmax <= 15; precision must be DAGE_FP64.  Boxes take
+ * 650-905, 1502-1621); lmax <= 15.  precision: DAGE_FP64 (the drop-in) or
+ * DAGE_MIXED_FP16X3: the near field on the tensor cores in the FP16 split
+ * precision of the cube operator (one grouped tcgen05 launch over all boxes
+ * per contraction stage and t-point), the far field in FP64.  Boxes take
  * ncell/2^maxlevel cells per axis; when that does not divide, the first
  * ncell mod 2^maxlevel boxes along the axis take one cell more, and a box
  * of a coarser level is the union of its children.  The Helmholtz kernel
- * (dage_gbfmm_set_energy with E < 0) runs with maxlevel 2 only.
+ * (dage_gbfmm_set_energy with E < 0) runs at every maxlevel and in the
+ * adaptive mode: M2M by the reference's Helmholtz multipole translator
+ * (gbfmm_helmholtz3d.F90:598-601, 1223-1278), L2L by the transposed relation
+ * that M2M implies (the reference has no Helmholtz L2L).
  * Replaces GBFMMCoulomb3D_init + init_nearfield + init_interaction_matrices
  * and gbfmmcoulomb3d_init_cuda (src/gbfmm/gbfmm_coulomb3d.F90:331-508,
  * 1313-1438; src/gbfmm/gbfmm_coulomb3d.cu:583-600). */
@@ -174,7 +180,7 @@ int dage_gbfmm_create(const dage_grid1d grid[3], int maxlevel, int lmax, const d
  * translated up to level 1; a box of level l >= 2 takes M2L from the children
  * of its parent's neighbours that contain one of its nearest neighbours
  * (minus those neighbours) and, as whole boxes of level l - 1, from its
- * parent's other neighbours.  Coulomb kernel only. */
+ * parent's other neighbours.  Coulomb and Helmholtz kernels. */
 int dage_gbfmm_create_adaptive(const dage_grid1d grid[3], int maxlevel, int lmax,
                                const dage_quad *quad, int precision, dage_gbfmm **g);
 
@@ -228,7 +234,8 @@ int dage_gbfmm_destroy(dage_gbfmm *g);
  * (moments, M2L, near field per t-point and contraction stage, L2P, energy)
  * is one launch over all densities.  The near field's intermediates are
  * processed in chunks of densities that fit near_budget_bytes (0 = 8 GiB).
- * grids holds 3 axes per density; maxlevel must be 2. */
+ * grids holds 3 axes per density.  precision: DAGE_FP64 or DAGE_MIXED_FP16X3
+ * (near field on the tensor cores; the chunks then share one workspace). */
 typedef struct dage_gbfmm_batch dage_gbfmm_batch;
 typedef struct dage_bubbles dage_bubbles;
 int dage_gbfmm_batch_create(int n, const dage_grid1d *grids, int maxlevel, int lmax,

@@ -147,6 +147,11 @@ int orc_helm_m2l_lsq(int lmax, int lin, double kappa, const double *M, const dou
                      const double *dst, double *L);
 int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double *src,
                  const double *dst, double *L);
+void orc_aligned_mm(const double *bessel, int lmax, int lin, double *out);
+int orc_helm_m2m(int lmax, int lin, double kappa, const double *M, const double *src,
+                 const double *dst, double *out);
+int orc_helm_matrix(int kind, int lmax, int lin, double kappa, const double *src,
+                    const double *dst, double *out);
 int orc_helm_box_multipoles(int lmax, double kappa, int nx, const double *px, const double *wx,
                             int ny, const double *py, const double *wy, int nz, const double *pz,
                             const double *wz, const double *rho, const double *center, double *q);

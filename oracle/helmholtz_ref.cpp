@@ -344,6 +344,56 @@ void orc_aligned_ml(const double *bessel, int lmax, int lin, double *out) {
       }
 }
 
+// helmholtz_multipole_tools.F90:513-588 get_all_aligned_translation_
+// coefficients (coaxial multipole-to-multipole translation along +z,
+// conventional normalisation), bessel values i_0 .. i_{lin+1}(kappa d); the
+// layout of orc_aligned_ml.
+void orc_aligned_mm(const double *bessel, int lmax, int lin, double *out) {
+  const int E = lin + 1;
+  const int D = E + 2;
+  std::vector<double> C((size_t)D * D * D, 0.0);
+  auto c = [&](int l, int n, int m) -> double & {
+    return C[((size_t)(l + 1) * D + (n + 1)) * D + (m + 1)];
+  };
+  auto A = [](int n, int m) {
+    if (n < 0) return 0.0;
+    const int am = std::abs(m);
+    return std::sqrt((double)((n + 1 + am) * (n + 1 - am)) / ((2 * n + 1) * (2 * n + 3)));
+  };
+  auto B = [](int n, int m) {
+    if (n < 0) return 0.0;
+    double b = std::sqrt((double)((n - m - 1) * (n - m)) / ((2 * n - 1) * (2 * n + 1)));
+    if (std::abs(m) > n) return 0.0;
+    if (m < 0) b = -b;
+    return b;
+  };
+  // (:534-537) seeds (n, 0, 0) and (0, n, 0) for n = 0 .. lin + 1
+  for (int n = 0; n <= lin + 1; ++n) {
+    c(n, 0, 0) = ((n & 1) ? -1.0 : 1.0) * std::sqrt(2.0 * n + 1) * bessel[n];
+    c(0, n, 0) = ((n & 1) ? -1.0 : 1.0) * c(n, 0, 0);
+  }
+  for (int n = 1; n <= lin; ++n) {  // (:543-551)
+    c(1, n, 0) = (A(n, 0) * c(0, n + 1, 0) + A(n - 1, 0) * c(0, n - 1, 0)) / A(0, 0);
+    c(n, 1, 0) = (((1 + n) & 1) ? -1.0 : 1.0) * c(1, n, 0);
+  }
+  for (int m = 0; m <= lin; ++m) {  // (:563-585)
+    for (int n = m; n <= lin; ++n)
+      for (int l = m; l <= lin; ++l)
+        c(l, n + 1, m) = (A(l, m) * c(l + 1, n, m) + A(l - 1, m) * c(l - 1, n, m) -
+                          A(n - 1, m) * c(l, n - 1, m)) /
+                         A(n, m);
+    for (int l = m; l <= lin; ++l)
+      c(l, m + 1, m + 1) = (B(l, -m - 1) * c(l - 1, m, m) + B(l + 1, m) * c(l + 1, m, m)) /
+                           B(m + 1, -m - 1);
+  }
+  for (int l = 0; l <= lmax; ++l)
+    for (int n = 0; n <= lin; ++n)
+      for (int m = 0; m <= lmax; ++m) {
+        const bool in = l <= lin + 1 && m <= lin + 1;
+        out[((size_t)l * (lin + 1) + n) * (lmax + 1) + m] = in ? c(l, n, m) : 0.0;
+      }
+}
+
 // Rotation of real spherical-harmonic expansions (Racah or orthonormal: the
 // same per-l matrices) to the frame whose z axis is dhat: R_l[m' + l][m + l]
 // with f'_(l m') = sum_m R_l[m'][m] f_(l m).  Built from its defining
@@ -427,8 +477,10 @@ void orc_ref_real_rotation(double alpha, double beta, double gamma, int lmax, in
 // the axis destination - source, coaxial translation (real basis:
 // C(l, n, |m|) acting on (n, m) for both signs of m, :280-331 with
 // :760-800), rotation back, orthonormal -> Racah scaling.
+// kind 0: the multipole-to-local converter (k_l, orc_aligned_ml); kind 1:
+// the multipole translator (i_l, orc_aligned_mm, :338-378).
 static int helm_m2l_impl(int lmax, int lin, double kappa, const double *M, const double *src,
-                         const double *dst, double *L, bool lsq) {
+                         const double *dst, double *L, bool lsq, int kind = 0) {
   const double pi = 3.14159265358979323846;
   const double d[3] = {dst[0] - src[0], dst[1] - src[1], dst[2] - src[2]};
   const double dist = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -461,9 +513,14 @@ static int helm_m2l_impl(int lmax, int lin, double kappa, const double *M, const
   }
   // coaxial translation (:245-246)
   std::vector<double> bess(lin + 2);
-  orc_bessel_k(kappa * dist, lin + 1, bess.data());
   std::vector<double> C((size_t)(lmax + 1) * (lin + 1) * (lmax + 1));
-  orc_aligned_ml(bess.data(), lmax, lin, C.data());
+  if (kind == 0) {
+    orc_bessel_k(kappa * dist, lin + 1, bess.data());
+    orc_aligned_ml(bess.data(), lmax, lin, C.data());
+  } else {
+    orc_bessel_i(kappa * dist, lin + 1, bess.data());
+    orc_aligned_mm(bess.data(), lmax, lin, C.data());
+  }
   std::vector<double> b(Nout, 0.0), c(Nout, 0.0);
   for (int l = 0; l <= lmax; ++l)
     for (int m = -l; m <= l; ++m) {
@@ -504,6 +561,31 @@ int orc_helm_m2l(int lmax, int lin, double kappa, const double *M, const double 
 int orc_helm_m2l_lsq(int lmax, int lin, double kappa, const double *M, const double *src,
                      const double *dst, double *L) {
   return helm_m2l_impl(lmax, lin, kappa, M, src, dst, L, true);
+}
+
+// helmholtz_multipole_tools.F90:172-278 translate_real with the
+// HelmholtzMultipoleTranslator (:338-378): multipoles M about src moved to
+// dst (GBFMMHelmholtz3D_translate_multipoles, gbfmm_helmholtz3d.F90:1223-1278).
+int orc_helm_m2m(int lmax, int lin, double kappa, const double *M, const double *src,
+                 const double *dst, double *out) {
+  return helm_m2l_impl(lmax, lin, kappa, M, src, dst, out, false, 1);
+}
+
+// The whole (lmax+1)^2 x (lin+1)^2 matrix of the converter (kind 0) or the
+// translator (kind 1) for src -> dst, column k = the image of unit input k;
+// out[k * Nout + i].
+int orc_helm_matrix(int kind, int lmax, int lin, double kappa, const double *src,
+                    const double *dst, double *out) {
+  const int Nin = (lin + 1) * (lin + 1), Nout = (lmax + 1) * (lmax + 1);
+  std::vector<double> e(Nin, 0.0);
+  for (int k = 0; k < Nin; ++k) {
+    e[k] = 1.0;
+    const int rc = helm_m2l_impl(lmax, lin, kappa, e.data(), src, dst, out + (size_t)k * Nout,
+                                 false, kind);
+    e[k] = 0.0;
+    if (rc) return rc;
+  }
+  return 0;
 }
 
 // gbfmm_helmholtz3d.F90:1491-1577: q_lm(box) = sum rho w i_l(kappa r) Y_lm(rhat)

@@ -29,9 +29,11 @@ _F = ctypes.c_double
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with ``make -C oracle``; returns the library path."""
-    if force or not (os.path.exists(_LIB_PATH) and os.path.exists(_LIB_1ULP_PATH)):
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile the oracle with ``make -C oracle`` (make rebuilds what is out
+    of date); returns the library path."""
+    if force:
+        subprocess.run(["make", "-s", "-C", _HERE, "clean"], check=True)
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
 
@@ -50,6 +52,9 @@ def lib(libm_1ulp: bool = False):
             "orc_rotation": (None, [_D, _I, _D]),
             "orc_helm_m2l": (_I, [_I, _I, _F, _D, _D, _D, _D]),
             "orc_helm_m2l_lsq": (_I, [_I, _I, _F, _D, _D, _D, _D]),
+            "orc_helm_m2m": (_I, [_I, _I, _F, _D, _D, _D, _D]),
+            "orc_helm_matrix": (_I, [_I, _I, _I, _F, _D, _D, _D]),
+            "orc_aligned_mm": (None, [_D, _I, _I, _D]),
             "orc_ref_real_rotation": (None, [_F, _F, _F, _I, _I, _D]),
             "orc_helm_box_multipoles": (_I, [_I, _F, _I, _D, _D, _I, _D, _D, _I, _D, _D, _D, _D,
                                              _D]),
@@ -590,6 +595,92 @@ def helm_m2l(lmax, kappa, M, src, dst, lin=None, least_squares=False):
     return L
 
 
+def helm_m2m(lmax, kappa, M, src, dst):
+    """Helmholtz multipoles M about src moved to dst (the reference's
+    HelmholtzMultipoleTranslator, helmholtz_multipole_tools.F90:172-278 and
+    :338-378, first-kind Bessel functions and the coaxial recurrence
+    :513-588; rotations by the reference's recursions, repaired)."""
+    out = np.zeros((lmax + 1) ** 2)
+    rc = lib().orc_helm_m2m(lmax, lmax, float(kappa), _p(_f64(M)), _p(_f64(src)), _p(_f64(dst)),
+                            _p(out))
+    if rc:
+        raise ValueError("zero translation distance")
+    return out
+
+
+_HELM_MATS = {}
+
+
+def helm_matrix(kind, lmax, kappa, src, dst):
+    """Matrix (N x N, column k = image of unit input k) of the converter
+    (kind "m2l") or the translator (kind "m2m") from src to dst; cached per
+    displacement."""
+    d = np.asarray(dst, dtype=np.float64) - np.asarray(src, dtype=np.float64)
+    key = (kind, lmax, float(kappa), tuple(np.round(d, 12)))
+    T = _HELM_MATS.get(key)
+    if T is None:
+        N = (lmax + 1) ** 2
+        out = np.zeros(N * N)
+        rc = lib().orc_helm_matrix(0 if kind == "m2l" else 1, lmax, lmax, float(kappa),
+                                   _p(np.zeros(3)), _p(_f64(d)), _p(out))
+        if rc:
+            raise ValueError("zero translation distance")
+        T = out.reshape(N, N).T.copy()  # T[i, k]
+        _HELM_MATS[key] = T
+    return T
+
+
+def helm_l2l(lmax, kappa, Lp, parent, child):
+    """Local expansion of the child box from its parent's.  The reference has
+    no Helmholtz L2L (its level loop, gbfmm_helmholtz3d.F90:789-937, adds
+    every level's local expansions into the finest level's box slots about
+    the wrong centres); this is the translation the moments' M2M implies:
+    with q(parent) = W q(child) for the regular basis i_l Y_lm and the L2P
+    factor (2l+1) of local expansions (:1019-1105), L(child)_i =
+    sum_j W_ji (2 l_j + 1) L(parent)_j / (2 l_i + 1)."""
+    W = helm_matrix("m2m", lmax, kappa, child, parent)
+    ls = np.repeat(np.arange(lmax + 1), 2 * np.arange(lmax + 1) + 1)
+    c = 2.0 * ls + 1.0
+    return (W.T @ (c * Lp)) / c
+
+
+def _far_field_levels_helm(plan, q_fine, lmax, kappa, adaptive=False):
+    """Multi-level Helmholtz far field: the levels of _far_field_levels with
+    the reference's Helmholtz M2M (translate_multipoles, gbfmm_helmholtz3d.F90:
+    598-601, 1223-1278), the Helmholtz converter at every level (and, in the
+    adaptive mode, from whole parent-level boxes, :811-937) and helm_l2l."""
+    N = (lmax + 1) ** 2
+    top = plan.level
+    q = {top: q_fine}
+    for lev in range(top - 1, 0 if adaptive else 1, -1):
+        nb = 8 ** lev
+        ql = np.zeros((N, nb))
+        for p in range(1, nb + 1):
+            cp = plan.center_at(p, lev)
+            for c in range((p - 1) * 8 + 1, p * 8 + 1):
+                ql[:, p - 1] += helm_matrix("m2m", lmax, kappa, plan.center_at(c, lev + 1), cp) @ \
+                    q[lev + 1][:, c - 1]
+        q[lev] = ql
+    Lprev = None
+    for lev in range(2, top + 1):
+        nb = 8 ** lev
+        Ll = np.zeros((N, nb))
+        for i in range(1, nb + 1):
+            ci = plan.center_at(i, lev)
+            if Lprev is not None:
+                par = (i - 1) // 8 + 1
+                Ll[:, i - 1] += helm_l2l(lmax, kappa, Lprev[:, par - 1], plan.center_at(par, lev - 1), ci)
+            if adaptive:
+                partial, whole = local_farfield_adaptive(i, lev)
+                srcs = [(j, lev) for j in partial] + [(j, lev - 1) for j in whole]
+            else:
+                srcs = [(j, lev) for j in local_farfield(i, lev)]
+            for j, lj in srcs:
+                Ll[:, i - 1] += helm_matrix("m2l", lmax, kappa, plan.center_at(j, lj), ci) @ q[lj][:, j - 1]
+        Lprev = Ll
+    return Lprev
+
+
 def ref_real_rotation(alpha, beta, gamma, lmax, repaired=True):
     """The reference's real spherical-harmonic rotation coefficients
     (get_real_spherical_harmonic_rotation_coefficients,
@@ -788,7 +879,8 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
     GBFMMHelmholtz3D kernel e^(-kappa r)/r, kappa = sqrt(-2 energy)
     (gbfmm_helmholtz3d.F90:478-1105): Helmholtz near-field weights, Bessel
     multipoles, the Helmholtz multipole-to-local converter and L2P.
-    adaptive: the reference's adaptive mode (Coulomb only, _far_field_levels).
+    adaptive: the reference's adaptive mode (_far_field_levels, and
+    _far_field_levels_helm for the Helmholtz kernel).
     blas: each box's near-field contraction as DGEMMs (transform_cube_blas,
     the same sums in BLAS order; for grids of 181^3 and more)."""
     plan = GBFMMPlan(grid, maxlevel)
@@ -805,9 +897,8 @@ def gbfmm_apply(grid: Grid3D, rho, lmax=12, maxlevel=2, quad=(25, 25, 0.0, 2.0, 
         q[:, b - 1] = (helm_box_multipoles(lmax, kappa, *args) if helm
                        else box_multipoles(lmax, *args))
     if maxlevel > 2 or adaptive:
-        if helm:
-            raise ValueError("multi-level GBFMM is restated for the Coulomb kernel only")
-        L = _far_field_levels(plan, q, lmax, adaptive)
+        L = (_far_field_levels_helm(plan, q, lmax, kappa, adaptive) if helm
+             else _far_field_levels(plan, q, lmax, adaptive))
     else:
         L = np.zeros((N, plan.nbox))
         for i in range(1, plan.nbox + 1):

@@ -126,3 +126,34 @@ def test_helmholtz_l2p_plane_wave_identity(dage, oracle, lmax, energy):
     tail = ((2 * lt + 1) * oracle.bessel_i(kappa * rmax, lmax + 29)[lmax + 1:]).sum()
     err = np.abs(V - Vx).max()
     assert err <= 2 * tail + 1e-13 * np.abs(Vx).max(), (err, tail)
+
+
+# maxlevel 3 (8^3 boxes of 2 cells): the Helmholtz M2M of the reference's
+# translator, M2L at levels 2 and 3 (adaptive: level-1 moments and whole
+# parent-level sources) and the L2L the M2M implies; against the oracle's
+# restatement (rotations by the reference's recursion, the product's by least
+# squares)
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_helmholtz_multilevel_matches_oracle(dage, oracle, adaptive):
+    g, go, rho = _setup(dage, oracle, 16)
+    quad, lmax, energy = (6, 6, 0.0, 2.0, 1e3), 6, -0.5
+    op = dage.GBFMMHelmholtz3D(g, energy, lmax=lmax, maxlevel=3, quad=dage.GaussQuad(*quad),
+                               adaptive_mode=adaptive)
+    V, E = op.apply(rho, energy=True)
+    Lg = op.local_expansions()
+    Vo, _, Lo, Vn = oracle.gbfmm_apply(go, rho, lmax=lmax, maxlevel=3, quad=quad, energy=energy,
+                                       adaptive=adaptive, return_parts=True)
+    Vn1 = oracle.gbfmm_near_field(go, rho, 3, quad, libm_1ulp=True, energy=energy)
+    scale = np.abs(Vo).max()
+    spread = np.abs(Vn1 - Vn).max() / scale
+    err = np.abs(V - Vo).max() / scale
+    print(f"adaptive={adaptive}: L {np.abs(Lg - Lo).max() / np.abs(Lo).max():.2e}, "
+          f"V {err:.2e} (spread {spread:.2e})")
+    assert np.abs(Lg - Lo).max() <= 1e-11 * np.abs(Lo).max()
+    assert err <= max(1e-10, 10 * spread), (err, spread)
+    Eo = oracle.integrate_cube(go, rho * Vo)
+    assert abs(E - Eo) <= 1e-11 * abs(Eo), (E, Eo)
+    # and the far-field truncation against the direct Helmholtz operator
+    direct = dage.Helmholtz3D(dage.Coulomb3D(g, quad=dage.GaussQuad(*quad)), energy)
+    Vd, _ = direct.apply(rho, energy=True, coda=False)
+    assert np.abs(V - Vd).max() <= 1e-4 * np.abs(Vd).max()

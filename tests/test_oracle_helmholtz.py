@@ -125,3 +125,43 @@ def test_repaired_rotation_matches_least_squares(oracle, lmax):
         b = oracle.helm_m2l(lmax, 1.1, M, src, src + d, least_squares=True)
         worst = max(worst, np.abs(a - b).max() / np.abs(b).max())
     assert worst < 1e-13, worst
+
+
+def test_helmholtz_m2m_matches_direct_moments(oracle):
+    """The restated HelmholtzMultipoleTranslator moves point-charge moments
+    from a child centre to a parent centre as a direct evaluation about the
+    parent does (up to the lmax truncation)."""
+    lmax, kappa = 8, 0.7
+    rng = np.random.default_rng(0)
+    pts, qs = rng.uniform(-0.5, 0.5, (20, 3)), rng.uniform(-1, 1, 20)
+    cc, cp = np.array([0.3, -0.2, 0.4]), np.zeros(3)
+
+    def moments(center):
+        out = np.zeros((lmax + 1) ** 2)
+        for p, q in zip(pts, qs):
+            out += oracle.helm_box_multipoles(lmax, kappa, [p[0] + cc[0]], [q], [p[1] + cc[1]],
+                                              [1.0], [p[2] + cc[2]], [1.0], np.ones((1, 1, 1)),
+                                              center)
+        return out
+
+    qc, qp = moments(cc), moments(cp)
+    qt = oracle.helm_m2m(lmax, kappa, qc, cc, cp)
+    assert np.abs(qt - qp).max() <= 1e-10 * np.abs(qp).max()
+    W = oracle.helm_matrix("m2m", lmax, kappa, cc, cp)
+    assert np.abs(W @ qc - qt).max() <= 1e-14 * np.abs(qt).max()
+
+
+def test_helmholtz_l2l_preserves_potential(oracle):
+    """helm_l2l re-expands a local expansion about a child centre: its L2P at
+    points of the child box equals the parent expansion's."""
+    lmax, kappa = 8, 0.7
+    rng = np.random.default_rng(1)
+    cp, cc = np.zeros(3), np.array([0.3, -0.2, 0.4])
+    Lp = rng.normal(size=(lmax + 1) ** 2) * np.repeat(0.3 ** np.arange(lmax + 1),
+                                                       2 * np.arange(lmax + 1) + 1)
+    Lc = oracle.helm_l2l(lmax, kappa, Lp, cp, cc)
+    xs, ys, zs = (c + np.linspace(-0.2, 0.2, 3) for c in cc)
+    V1, V2 = np.zeros((3, 3, 3), order="F"), np.zeros((3, 3, 3), order="F")
+    oracle.helm_l2p(lmax, kappa, Lp, cp, xs, ys, zs, V1)
+    oracle.helm_l2p(lmax, kappa, Lc, cc, xs, ys, zs, V2)
+    assert np.abs(V1 - V2).max() <= 1e-12 * np.abs(V1).max()
