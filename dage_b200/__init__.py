@@ -20,7 +20,8 @@ from .operators import (  # noqa: F401
     dot,
     integrate,
     multiply,
+    set_tune_cache,
 )
 
 __all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GBFMMHelmholtz3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
-           "DageError", "apply_batched", "dot", "integrate", "load", "multiply"]
+           "DageError", "apply_batched", "dot", "integrate", "load", "multiply", "set_tune_cache"]

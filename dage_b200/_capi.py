@@ -67,6 +67,7 @@ SIGNATURES = {
     "dage_op3d_set_timing": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dage_op3d_get_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), _D]),
     "dage_op3d_destroy": (ctypes.c_int, [_VP]),
+    "dage_op3d_tiles": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "dage_gbfmm_create": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(DageQuad), ctypes.c_int,
                                          ctypes.POINTER(_VP)]),
@@ -117,6 +118,7 @@ SIGNATURES = {
     "dage_last_error": (ctypes.c_char_p, []),
     "dage_abi_version": (ctypes.c_int, []),
     "dage_set_wait_limit": (ctypes.c_int, [ctypes.c_longlong]),
+    "dage_set_tune_cache": (ctypes.c_int, [ctypes.c_char_p]),
 }
 
 _lib = None

@@ -34,6 +34,7 @@
 
 #include "fp64_stage.cuh"
 #include "near_mixed.cuh"
+#include "tune.h"
 #include "op3d.cuh"
 
 struct dage_gbfmm;
@@ -1956,20 +1957,21 @@ int autotune_tiles(const StageDesc *const d_desc[3], int njobs, const int mt[3],
   return rc;
 }
 
-// The plan's own tiles, cached per (points per axis, t-points, boxes) for
-// the process; tuned on scratch input and output cubes.
-std::mutex g_tune_mutex;
-std::map<std::array<int, 5>, std::array<int, 3>> g_tune_cache;
+// Key of a plan in the tune cache: device, points per axis, t-points, boxes.
+std::string plan_key(const dage_gbfmm *g, const char *what) {
+  return tune_device_key() + "/" + what + "/" + std::to_string(g->npts[0]) + "x" +
+         std::to_string(g->npts[1]) + "x" + std::to_string(g->npts[2]) + ",P" +
+         std::to_string(g->P) + ",boxes" + std::to_string(g->nbox);
+}
 
+// The plan's own tiles, from the tune cache or tuned on scratch input and
+// output cubes.
 int gbfmm_autotune(dage_gbfmm *g) {
-  const std::array<int, 5> key = {g->npts[0], g->npts[1], g->npts[2], g->P, g->nbox};
-  {
-    std::lock_guard<std::mutex> lock(g_tune_mutex);
-    auto it = g_tune_cache.find(key);
-    if (it != g_tune_cache.end()) {
-      for (int d = 0; d < 3; ++d) g->tile_n[d] = it->second[d];
-      return 0;
-    }
+  const std::string key = plan_key(g, "gbfmm_near_fp64");
+  std::vector<int> v;
+  if (tune_lookup(key, v) && v.size() == 3) {
+    for (int d = 0; d < 3; ++d) g->tile_n[d] = v[d];
+    return 0;
   }
   cudaStream_t s = g->stream;
   const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
@@ -1991,8 +1993,7 @@ int gbfmm_autotune(dage_gbfmm *g) {
   rho.release();
   V.release();
   if (rc) return rc;
-  std::lock_guard<std::mutex> lock(g_tune_mutex);
-  g_tune_cache[key] = {g->tile_n[0], g->tile_n[1], g->tile_n[2]};
+  tune_store(key, {g->tile_n[0], g->tile_n[1], g->tile_n[2]});
   return 0;
 }
 
@@ -2038,24 +2039,19 @@ int upload_near_w(dage_gbfmm *g) {
 }
 
 // Tile width of the fp16x3 near field (64 or 128 output columns), chosen by
-// timing one near-field pass of each on scratch cubes; cached per (points
-// per axis, t-points, boxes) for the process.
-std::map<std::array<int, 5>, int> g_tune16_cache;
-
+// timing one near-field pass of each on scratch cubes; kept in the tune
+// cache per (device, points per axis, t-points, boxes).
 int near16_tune(dage_gbfmm *g, int *tile) {
   // DAGE_NEAR16_TILE=64|128 fixes the width (tests of both code paths)
   if (const char *e = std::getenv("DAGE_NEAR16_TILE")) {
     *tile = std::atoi(e) == 128 ? 128 : 64;
     return 0;
   }
-  const std::array<int, 5> key = {g->npts[0], g->npts[1], g->npts[2], g->P, g->nbox};
-  {
-    std::lock_guard<std::mutex> lock(g_tune_mutex);
-    auto it = g_tune16_cache.find(key);
-    if (it != g_tune16_cache.end()) {
-      *tile = it->second;
-      return 0;
-    }
+  const std::string key = plan_key(g, "gbfmm_near_fp16x3");
+  std::vector<int> v;
+  if (tune_lookup(key, v) && v.size() == 1) {
+    *tile = v[0];
+    return 0;
   }
   cudaStream_t s = g->stream;
   const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
@@ -2096,8 +2092,7 @@ int near16_tune(dage_gbfmm *g, int *tile) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  std::lock_guard<std::mutex> lock(g_tune_mutex);
-  g_tune16_cache[key] = *tile;
+  tune_store(key, {*tile});
   return 0;
 }
 
@@ -2732,10 +2727,25 @@ int dage_gbfmm_batch_apply(dage_gbfmm_batch *b, const double *const *rho, double
   if (!use_graph || key != b->graph_key || !b->exec) {
     DAGE_TRY(batch_tables(b, dr.data(), dv.data()));
     if (!b->tuned) {
-      const auto &c = b->chunks[0];
-      const StageDesc *dd[3] = {c.desc[0].as<StageDesc>(), c.desc[1].as<StageDesc>(),
-                                c.desc[2].as<StageDesc>()};
-      DAGE_TRY(autotune_tiles(dd, c.njobs, b->mt, b->nt, s, b->tile_n));
+      // keyed on the batch: device, t-points, the densities' points per axis
+      std::map<std::string, int> sizes;  // grid -> densities on it
+      for (int i = 0; i < b->n; ++i) {
+        const dage_gbfmm *g = b->plans[b->plan_of[i]];
+        ++sizes[std::to_string(g->npts[0]) + "x" + std::to_string(g->npts[1]) + "x" +
+                std::to_string(g->npts[2])];
+      }
+      std::string key = tune_device_key() + "/gbfmm_batch_fp64/P" + std::to_string(b->P);
+      for (const auto &kv : sizes) key += "," + kv.first + "*" + std::to_string(kv.second);
+      std::vector<int> v;
+      if (tune_lookup(key, v) && v.size() == 3) {
+        for (int d = 0; d < 3; ++d) b->tile_n[d] = v[d];
+      } else {
+        const auto &c = b->chunks[0];
+        const StageDesc *dd[3] = {c.desc[0].as<StageDesc>(), c.desc[1].as<StageDesc>(),
+                                  c.desc[2].as<StageDesc>()};
+        DAGE_TRY(autotune_tiles(dd, c.njobs, b->mt, b->nt, s, b->tile_n));
+        tune_store(key, {b->tile_n[0], b->tile_n[1], b->tile_n[2]});
+      }
       b->tuned = true;
     }
     if (use_graph) {

@@ -21,6 +21,7 @@
 #include "expo.cuh"
 #include "fp64_stage.cuh"
 #include "op3d.cuh"
+#include "tune.h"
 
 namespace dage {
 
@@ -459,8 +460,9 @@ int launch_fp64_stages(const StageDesc *d_descs, int ndesc, int mtiles, int ncol
 
 int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,
                       long long ldt, double *out, double alpha, bool accumulate,
-                      cudaStream_t s, const int2 *krange) {
-  return launch_fp64_stage(cube_stage(X, ldx, M, N, K, T, ldt, out, krange), alpha, accumulate, s);
+                      cudaStream_t s, const int2 *krange, int tn) {
+  return launch_fp64_stage(cube_stage(X, ldx, M, N, K, T, ldt, out, krange), alpha, accumulate, s,
+                           tn);
 }
 
 int launch_band(const double *T, int K, int N, int P, int2 *range, cudaStream_t s) {
@@ -585,6 +587,8 @@ static int upload_weights(dage_op3d *op) {
   return 0;
 }
 
+static int tune_fp64(dage_op3d *op);
+
 static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
                        const dage_quad *quad, int precision, dage_op3d *op) {
   if (!grid_in || !grid_out || !quad) return fail(DAGE_E_INVALID, "null argument");
@@ -625,6 +629,7 @@ static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[
   if (precision != DAGE_FP64) DAGE_TRY(mixed_setup(op));
   DAGE_TRY(upload_weights(op));
   DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
+  if (precision == DAGE_FP64) DAGE_TRY(tune_fp64(op));
   return 0;
 }
 
@@ -650,6 +655,70 @@ static void destroy_impl(dage_op3d *op) {
   delete op;
 }
 
+// Autotuner of the FP64 path: the tile width (32, 64 or 128 output columns)
+// of each stage, timed on the operator's own matrices at three t-points
+// (first, middle, last: the widest and narrowest bands) over scratch cubes;
+// keyed on (device, input and output points per axis, t-points) in the tune
+// cache.  Small cubes fill the GPU only with narrow tiles (121^3: 115 row
+// tiles of 128 for 148 SMs).
+static int tune_fp64(dage_op3d *op) {
+  std::string key = tune_device_key() + "/op3d_fp64/";
+  for (int d = 0; d < 3; ++d) key += std::to_string(op->nin[d]) + "x" + std::to_string(op->nout[d]) + ",";
+  key += "P" + std::to_string(op->P);
+  std::vector<int> v;
+  if (tune_lookup(key, v) && v.size() == 3) {
+    for (int d = 0; d < 3; ++d) op->tile_n[d] = v[d];
+    return 0;
+  }
+  cudaStream_t s = op->stream;
+  const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
+  const int nox = op->nout[0], noy = op->nout[1], noz = op->nout[2];
+  DevBuf X, U, W, V;
+  DAGE_TRY(X.alloc(sizeof(double) * (size_t)nix * niy * niz));
+  DAGE_TRY(U.alloc(sizeof(double) * (size_t)niy * niz * nox));
+  DAGE_TRY(W.alloc(sizeof(double) * (size_t)niz * nox * noy));
+  DAGE_TRY(V.alloc(sizeof(double) * (size_t)nox * noy * noz));
+  DAGE_CUDA_TRY(cudaMemsetAsync(X.ptr, 0, X.bytes, s));
+  DAGE_CUDA_TRY(cudaMemsetAsync(U.ptr, 0, U.bytes, s));
+  DAGE_CUDA_TRY(cudaMemsetAsync(W.ptr, 0, W.bytes, s));
+  cudaEvent_t e0, e1;
+  DAGE_CUDA_TRY(cudaEventCreate(&e0));
+  DAGE_CUDA_TRY(cudaEventCreate(&e1));
+  const size_t sT[3] = {(size_t)nox * nix, (size_t)noy * niy, (size_t)noz * niz};
+  const double *in[3] = {X.as<double>(), U.as<double>(), W.as<double>()};
+  double *outp[3] = {U.as<double>(), W.as<double>(), V.as<double>()};
+  const int M[3] = {niy * niz, niz * nox, nox * noy}, N[3] = {nox, noy, noz}, K[3] = {nix, niy, niz};
+  const int ps[3] = {0, op->P / 2, op->P - 1};
+  int rc = 0;
+  for (int d = 0; d < 3 && !rc; ++d) {
+    float best = 1e30f;
+    for (int tn : {32, 64, 128}) {
+      auto run = [&](int p) {
+        const int2 *band = op->band[op->Towner[d]].as<int2>() + (size_t)p * ceil_div(N[d], BN);
+        return launch_stage_fp64(in[d], K[d], M[d], N[d], K[d], op->T(d) + sT[d] * p, K[d], outp[d],
+                                 1.0, false, s, band, tn);
+      };
+      rc = run(ps[0]);  // warm-up
+      if (!rc) rc = cudaEventRecord(e0, s) == cudaSuccess ? 0 : fail(DAGE_E_CUDA, "event");
+      for (int i = 0; i < 3 && !rc; ++i) rc = run(ps[i]);
+      if (rc) break;
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        op->tile_n[d] = tn;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  tune_store(key, {op->tile_n[0], op->tile_n[1], op->tile_n[2]});
+  return 0;
+}
+
 static int apply_fp64(dage_op3d *op, const double *rho, double *V, bool accumulate) {
   cudaStream_t s = op->stream;
   const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
@@ -664,15 +733,15 @@ static int apply_fp64(dage_op3d *op, const double *rho, double *V, bool accumula
   for (int p = 0; p < op->P; ++p) {
     int t = op->tmark_begin(0);
     DAGE_TRY(launch_stage_fp64(rho, nix, niy * niz, nox, nix, op->T(0) + sx * p, nix, U, 1.0,
-                               false, s, band(0, p)));
+                               false, s, band(0, p), op->tile_n[0]));
     op->tmark_end(t);
     t = op->tmark_begin(0);
     DAGE_TRY(launch_stage_fp64(U, niy, niz * nox, noy, niy, op->T(1) + sy * p, niy, W, 1.0,
-                               false, s, band(1, p)));
+                               false, s, band(1, p), op->tile_n[1]));
     op->tmark_end(t);
     t = op->tmark_begin(0);
     DAGE_TRY(launch_stage_fp64(W, niz, nox * noy, noz, niz, op->T(2) + sz * p, niz, V,
-                               op->w[p], accumulate || p > 0, s, band(2, p)));
+                               op->w[p], accumulate || p > 0, s, band(2, p), op->tile_n[2]));
     op->tmark_end(t);
   }
   return 0;
@@ -725,6 +794,12 @@ int dage_op3d_create(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3]
     return rc;
   }
   *out = op;
+  return 0;
+}
+
+int dage_op3d_tiles(const dage_op3d *op, int tile_n[3]) {
+  if (!op || !tile_n) return fail(DAGE_E_INVALID, "null argument");
+  for (int d = 0; d < 3; ++d) tile_n[d] = op->precision == DAGE_FP64 ? op->tile_n[d] : 128;
   return 0;
 }
 

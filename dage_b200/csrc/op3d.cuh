@@ -36,6 +36,10 @@ struct dage_op3d {
   dage::DevBuf tmp1, tmp2;   // intermediates of the FP64 path
   dage::DevBuf partials;     // energy reduction partial sums
 
+  // FP64 path: contraction tile width (32, 64 or 128 output columns) of each
+  // stage, from the autotuner (tune.h)
+  int tile_n[3] = {128, 128, 128};
+
   // mixed-precision state (op3d_mixed.cu)
   void *mixed = nullptr;
 
@@ -63,7 +67,7 @@ namespace dage {
 // krange (optional): per 128-column tile of out, the K band [first, last].
 int launch_stage_fp64(const double *X, long long ldx, int M, int N, int K, const double *T,
                       long long ldt, double *out, double alpha, bool accumulate,
-                      cudaStream_t s, const int2 *krange = nullptr);
+                      cudaStream_t s, const int2 *krange = nullptr, int tn = 128);
 
 // K band of every (t-point, 128-row tile) of an axis matrix T[p][n][K]: the
 // first and last K index holding an entry above 2^-64 of its row's scale.

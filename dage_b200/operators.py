@@ -319,6 +319,12 @@ class Helmholtz3D:
         return V, (bubbles.helmholtz_potential(self.energy) if bubbles is not None else None)
 
 
+def set_tune_cache(path: str | None) -> None:
+    """Autotuner cache file: tile-width choices are read from it and appended
+    to it, keyed on the problem and the device (None: this process only)."""
+    check(load().dage_set_tune_cache(path.encode() if path else None))
+
+
 def integrate(grid: Grid3D, f1, f2=None) -> float:
     """Cube part of Function3D_integrate / Function3D_dot_product: the
     LIP-weighted integral of f1 (times f2 when given)."""
@@ -375,6 +381,14 @@ class GBFMMCoulomb3D:
         """Near-field stage tile widths chosen by the autotuner (x, y, z)."""
         t = (ctypes.c_int * 3)()
         check(load().dage_gbfmm_tiles(self._h, t))
+        return tuple(t)
+
+    @property
+    def tiles(self):
+        """Contraction tile widths of the three stages (FP64: the autotuner's
+        choice, keyed on points per axis and t-points)."""
+        t = (ctypes.c_int * 3)()
+        check(load().dage_op3d_tiles(self._h, t))
         return tuple(t)
 
     def __del__(self):

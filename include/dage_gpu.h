@@ -141,6 +141,10 @@ int dage_op3d_last_time_ms(const dage_op3d *op, float *ms);
 int dage_op3d_set_timing(dage_op3d *op, int enable);
 int dage_op3d_get_timing(const dage_op3d *op, int kind, long long *launches, double *ms);
 
+/* Tile widths (32, 64 or 128 output columns) the autotuner chose for the three
+ * FP64 contraction stages (the split-precision stages use 128).  No reference
+ * counterpart: the reference's stages are cuBLAS DGEMMs. */
+int dage_op3d_tiles(const dage_op3d *op, int tile_n[3]);
 int dage_op3d_destroy(dage_op3d *op);
 
 /* ---------------------------------------------------------------------------
@@ -377,6 +381,15 @@ int dage_op3d_apply_fp64_noalloc(int nix, int niy, int niz, int nox, int noy, in
  * Library
  * ------------------------------------------------------------------------ */
 const char *dage_last_error(void);
+/* Autotuner cache file (no reference counterpart: the reference has no
+ * autotuner).  Launch choices the library times (tile widths of the FP64
+ * contraction stages and of the GBFMM near field) are keyed on the problem
+ * (points per axis, t-points, boxes or batch) and the device, kept for the
+ * process and, with a path, read from and appended to this text file so that
+ * later processes skip the timing.  NULL or "" keeps choices in the process
+ * only.  The DAGE_TUNE_CACHE environment variable sets the path when this is
+ * never called. */
+int dage_set_tune_cache(const char *path);
 int dage_abi_version(void);
 /* Device-side timeout (in device clock cycles) for bounded waits. */
 int dage_set_wait_limit(long long cycles);
