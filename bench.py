@@ -813,10 +813,18 @@ def run_workload(args, world, rank, local):
                 vmax.append(float(d.max() / s64))
                 vrms.append(float(d.pow(2).mean().sqrt() / s64))
                 erel.append(abs(E16[i] - E64[i]) / abs(E64[i]))
+            w = int(np.argmax(erel))
+            # cancellation of the worst instance: |int rho V| / int |rho V|
+            absE = dage.integrate(grids[w], rhos[w].abs(), outs64[w].abs())
             extra["mixed_vs_fp64"] = {
                 "per_instance_max_rel": {"max": max(vmax), "median": float(np.median(vmax))},
                 "per_instance_rms_rel": {"max": max(vrms), "median": float(np.median(vrms))},
                 "per_instance_energy_rel": {"max": max(erel), "median": float(np.median(erel))},
+                "instances_over_bars": {"potential_1e-6": int(sum(v > 1e-6 for v in vmax)),
+                                        "energy_1e-7": int(sum(e > 1e-7 for e in erel))},
+                "worst_energy_instance": {"index": w, "points_per_axis": int(grids[w].shape[0]),
+                                          "energy_rel": erel[w],
+                                          "abs_energy_over_int_abs_rho_V": abs(E64[w]) / absE},
                 "fp64_ms_per_step": ms64, "speedup_vs_fp64": ms64 / ms}
             del b64, outs64
         if inject_ms is not None:

@@ -15,6 +15,8 @@
 // the same arithmetic as the reference's per-slice DGEMMs
 // (src/bubbles/function3d.F90:4296-4332), reordered for coalescing.
 #include <cmath>
+#include <cstdio>
+#include <string>
 #include <mutex>
 #include <cstring>
 
@@ -548,7 +550,118 @@ int build_axis_matrix(const Axis &ai, const double *out_points, int n_out, const
   return 0;
 }
 
-static int build_matrices(dage_op3d *op) {
+// ---------------------------------------------------------------------------
+// On-disk operator cache (dage_op3d_create_cached).  A file holds the key
+// and the FP64 matrices, in the stream-access layout of the reference's
+// store_Grid1Ds / resume_Grid1Ds (src/bubbles/grid.F90:2024-2068): per grid
+// ncell, nlip, cell_scales, grid_type (int32 / float64), here preceded by a
+// magic and version and followed by qmin (the reference resumes grids at
+// qmin = 0; the operator's matrices depend on it), for the 3 input and the 3
+// output axes; then the quadrature (nlin, nlog, tstart, tlin, tlog), P, and
+// per axis its owner index and, for owner axes, the P x n_out x n_in matrix.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr char kCacheMagic[8] = {'D', 'A', 'G', 'E', 'O', 'P', '3', 'D'};
+constexpr int kCacheVersion = 1;
+
+void put_axis(std::string &b, const Axis &a) {
+  auto put = [&](const void *p, size_t n) { b.append(static_cast<const char *>(p), n); };
+  const int32_t nc = a.ncell, nl = a.nlip, gt = a.grid_type;
+  put(&nc, 4);
+  put(&nl, 4);
+  put(a.h.data(), sizeof(double) * a.h.size());
+  put(&gt, 4);
+  put(&a.qmin, 8);
+}
+
+// the key bytes: magic, version, the six axes and the quadrature
+std::string cache_key(const dage_op3d *op) {
+  std::string b(kCacheMagic, 8);
+  const int32_t v = kCacheVersion, three = 3;
+  b.append(reinterpret_cast<const char *>(&v), 4);
+  for (const Axis *ax : {op->in, op->out}) {
+    b.append(reinterpret_cast<const char *>(&three), 4);
+    for (int d = 0; d < 3; ++d) put_axis(b, ax[d]);
+  }
+  const int32_t q[2] = {op->quad.nlin, op->quad.nlog};
+  const double t[3] = {op->quad.tstart, op->quad.tlin, op->quad.tlog};
+  b.append(reinterpret_cast<const char *>(q), 8);
+  b.append(reinterpret_cast<const char *>(t), 24);
+  return b;
+}
+
+std::string cache_file(const std::string &dir, const std::string &key) {
+  uint64_t h = 1469598103934665603ull;  // FNV-1a 64
+  for (unsigned char c : key) h = (h ^ c) * 1099511628211ull;
+  char name[40];
+  std::snprintf(name, sizeof(name), "/op3d_%016llx.bin", (unsigned long long)h);
+  return dir + name;
+}
+}  // namespace
+
+// Reads the matrices of op from a cache file whose key matches; returns 1 if
+// they were loaded, 0 if there is no matching file.
+static int cache_load(dage_op3d *op, const std::string &path) {
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) return 0;
+  const std::string key = cache_key(op);
+  std::string got(key.size(), '\0');
+  bool ok = std::fread(&got[0], 1, key.size(), f) == key.size() && got == key;
+  int32_t P = 0, owner[3] = {0, 1, 2};
+  ok = ok && std::fread(&P, 4, 1, f) == 1 && P == op->P;
+  std::vector<double> host;
+  for (int d = 0; d < 3 && ok; ++d) {
+    ok = std::fread(&owner[d], 4, 1, f) == 1 && owner[d] == op->Towner[d];
+    if (!ok || owner[d] != d) continue;
+    const size_t nT = (size_t)op->P * op->nout[d] * op->nin[d];
+    host.resize(nT);
+    ok = std::fread(host.data(), sizeof(double), nT, f) == nT;
+    if (ok) {
+      if (op->Tbuf[d].alloc(sizeof(double) * nT) ||
+          cudaMemcpy(op->Tbuf[d].ptr, host.data(), sizeof(double) * nT, cudaMemcpyHostToDevice) !=
+              cudaSuccess) {
+        std::fclose(f);
+        return fail(DAGE_E_CUDA, "cache upload failed");
+      }
+    }
+  }
+  std::fclose(f);
+  return ok ? 1 : 0;
+}
+
+static int cache_store(const dage_op3d *op, const std::string &path) {
+  const std::string tmp = path + ".tmp";
+  FILE *f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return fail(DAGE_E_INVALID, "cannot write operator cache %s", tmp.c_str());
+  const std::string key = cache_key(op);
+  bool ok = std::fwrite(key.data(), 1, key.size(), f) == key.size();
+  const int32_t P = op->P;
+  ok = ok && std::fwrite(&P, 4, 1, f) == 1;
+  std::vector<double> host;
+  for (int d = 0; d < 3 && ok; ++d) {
+    const int32_t owner = op->Towner[d];
+    ok = std::fwrite(&owner, 4, 1, f) == 1;
+    if (!ok || owner != d) continue;
+    const size_t nT = (size_t)op->P * op->nout[d] * op->nin[d];
+    host.resize(nT);
+    if (cudaMemcpy(host.data(), op->Tbuf[d].ptr, sizeof(double) * nT, cudaMemcpyDeviceToHost) !=
+        cudaSuccess) {
+      std::fclose(f);
+      return fail(DAGE_E_CUDA, "cache download failed");
+    }
+    ok = std::fwrite(host.data(), sizeof(double), nT, f) == nT;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) {
+    std::remove(tmp.c_str());
+    return fail(DAGE_E_INVALID, "cannot write operator cache %s", path.c_str());
+  }
+  return 0;
+}
+
+// Matrices from the cache directory when a file with this operator's key is
+// there (cache_dir non-null), else built on the GPU (and stored there).
+static int build_matrices(dage_op3d *op, const char *cache_dir = nullptr) {
   cudaStream_t s = op->stream;
   DevBuf d_tp;
   DAGE_TRY(build_quadrature(op->quad, op->tp, op->tw, d_tp, s));
@@ -564,18 +677,35 @@ static int build_matrices(dage_op3d *op) {
         op->Towner[d] = op->Towner[e];
         break;
       }
+  }
+  std::string path;
+  int loaded = 0;
+  if (cache_dir) {
+    DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+    path = cache_file(cache_dir, cache_key(op));
+    loaded = cache_load(op, path);
+    if (loaded < 0 || loaded > 1) return loaded;  // an error code
+  }
+  op->from_cache = loaded == 1;
+  for (int d = 0; d < 3; ++d) {
     if (op->Towner[d] != d) continue;
     const Axis &ai = op->in[d];
     const Axis &ao = op->out[d];
     const size_t nT = (size_t)op->P * ao.n() * ai.n();
-    DAGE_TRY(op->Tbuf[d].alloc(sizeof(double) * nT));
-    DAGE_TRY(build_axis_matrix(ai, ao.points.data(), ao.n(), d_tp.as<double>(), op->P,
-                               op->Tbuf[d].as<double>(), s));
+    if (!loaded) {
+      DAGE_TRY(op->Tbuf[d].alloc(sizeof(double) * nT));
+      DAGE_TRY(build_axis_matrix(ai, ao.points.data(), ao.n(), d_tp.as<double>(), op->P,
+                                 op->Tbuf[d].as<double>(), s));
+    }
     DAGE_TRY(op->band[d].alloc(sizeof(int2) * (size_t)op->P * ceil_div(ao.n(), BN)));
     DAGE_TRY(launch_band(op->Tbuf[d].as<double>(), ai.n(), ao.n(), op->P,
                          op->band[d].as<int2>(), s));
   }
   d_tp.release();
+  if (cache_dir && !loaded) {
+    DAGE_CUDA_TRY(cudaStreamSynchronize(s));
+    DAGE_TRY(cache_store(op, path));
+  }
   return 0;
 }
 
@@ -590,7 +720,8 @@ static int upload_weights(dage_op3d *op) {
 static int tune_fp64(dage_op3d *op);
 
 static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
-                       const dage_quad *quad, int precision, dage_op3d *op) {
+                       const dage_quad *quad, int precision, dage_op3d *op,
+                       const char *cache_dir = nullptr) {
   if (!grid_in || !grid_out || !quad) return fail(DAGE_E_INVALID, "null argument");
   if (quad->nlin < 0 || quad->nlog < 0 || quad->nlin + quad->nlog < 1 ||
       quad->nlin > 256 || quad->nlog > 256)
@@ -618,7 +749,7 @@ static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[
   op->stream = op->own_stream;
   DAGE_CUDA_TRY(cudaEventCreate(&op->ev0));
   DAGE_CUDA_TRY(cudaEventCreate(&op->ev1));
-  DAGE_TRY(build_matrices(op));
+  DAGE_TRY(build_matrices(op, cache_dir));
   for (int d = 0; d < 3; ++d) {
     DAGE_TRY(op->wts[d].alloc(sizeof(double) * op->nout[d]));
     DAGE_CUDA_TRY(cudaMemcpyAsync(op->wts[d].ptr, op->out[d].weights.data(),
@@ -793,6 +924,23 @@ int dage_op3d_create(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3]
     destroy_impl(op);
     return rc;
   }
+  *out = op;
+  return 0;
+}
+
+int dage_op3d_create_cached(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
+                            const dage_quad *quad, int precision, const char *cache_dir,
+                            int *from_cache, dage_op3d **out) {
+  clear_error();
+  if (!out || !cache_dir || !*cache_dir) return fail(DAGE_E_INVALID, "null argument");
+  *out = nullptr;
+  dage_op3d *op = new dage_op3d();
+  int rc = create_impl(grid_in, grid_out, quad, precision, op, cache_dir);
+  if (rc) {
+    destroy_impl(op);
+    return rc;
+  }
+  if (from_cache) *from_cache = op->from_cache ? 1 : 0;
   *out = op;
   return 0;
 }

@@ -39,6 +39,7 @@ struct dage_op3d {
   // FP64 path: contraction tile width (32, 64 or 128 output columns) of each
   // stage, from the autotuner (tune.h)
   int tile_n[3] = {128, 128, 128};
+  bool from_cache = false;  // matrices read from an operator cache file
 
   // mixed-precision state (op3d_mixed.cu)
   void *mixed = nullptr;

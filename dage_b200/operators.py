@@ -136,7 +136,11 @@ class Operator3D:
     (+ coda rho).  ``Coulomb3D`` and ``Helmholtz3D`` are its two kernels."""
 
     def __init__(self, gridin: Grid3D, gridout: Grid3D | None = None,
-                 quad: GaussQuad | None = None, precision: str = "fp64"):
+                 quad: GaussQuad | None = None, precision: str = "fp64",
+                 cache_dir: str | None = None):
+        """``cache_dir``: on-disk cache of the operator matrices keyed by the
+        grids and the quadrature (read when present, written otherwise;
+        ``from_cache`` tells which)."""
         lib = load()
         self.gridin = gridin
         self.gridout = gridout if gridout is not None else gridin
@@ -146,8 +150,17 @@ class Operator3D:
             raise ValueError(f"precision must be one of {list(PRECISIONS)}")
         self._keep = (self.gridin.c(), self.gridout.c(), self.quad.c())
         h = ctypes.c_void_p()
-        check(lib.dage_op3d_create(self._keep[0], self._keep[1], ctypes.byref(self._keep[2]),
-                                   PRECISIONS[precision], ctypes.byref(h)))
+        self.from_cache = False
+        if cache_dir:
+            fc = ctypes.c_int(0)
+            check(lib.dage_op3d_create_cached(self._keep[0], self._keep[1],
+                                              ctypes.byref(self._keep[2]), PRECISIONS[precision],
+                                              cache_dir.encode(), ctypes.byref(fc),
+                                              ctypes.byref(h)))
+            self.from_cache = bool(fc.value)
+        else:
+            check(lib.dage_op3d_create(self._keep[0], self._keep[1], ctypes.byref(self._keep[2]),
+                                       PRECISIONS[precision], ctypes.byref(h)))
         self._h = h
 
     def __del__(self):
@@ -158,6 +171,14 @@ class Operator3D:
             except Exception:
                 pass
             self._h = None
+
+    @property
+    def tiles(self):
+        """Contraction tile widths of the three stages (FP64: the autotuner's
+        choice, keyed on points per axis and t-points)."""
+        t = (ctypes.c_int * 3)()
+        check(load().dage_op3d_tiles(self._h, t))
+        return tuple(t)
 
     # -- quadrature -------------------------------------------------------
     def quadrature(self):
@@ -381,14 +402,6 @@ class GBFMMCoulomb3D:
         """Near-field stage tile widths chosen by the autotuner (x, y, z)."""
         t = (ctypes.c_int * 3)()
         check(load().dage_gbfmm_tiles(self._h, t))
-        return tuple(t)
-
-    @property
-    def tiles(self):
-        """Contraction tile widths of the three stages (FP64: the autotuner's
-        choice, keyed on points per axis and t-points)."""
-        t = (ctypes.c_int * 3)()
-        check(load().dage_op3d_tiles(self._h, t))
         return tuple(t)
 
     def __del__(self):

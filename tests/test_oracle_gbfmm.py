@@ -205,3 +205,21 @@ def test_adaptive_gbfmm_matches_direct_operator(oracle):
     Va = oracle.gbfmm_apply(g, rho, lmax=8, maxlevel=3, quad=quad, adaptive=True)
     Vd = oracle.coulomb_apply(g, rho, quad=quad, coda=False)
     assert np.abs(Va - Vd).max() / np.abs(Vd).max() < 5e-3
+
+
+def test_iterator_test_multipoles_of_s_plus_p_gaussian(oracle):
+    """tests/iterator_test.F90:41-107: the spherical multipoles (lmax 15) of
+    rho = pi^(-3/2) e^(-r^2) (1 + x + y + z) are q_00 = 1, q_1m = 0.5 and zero
+    above (1e-8, the reference's tolerance).  The reference sums Cartesian
+    moments with the monomial coefficients of the solid harmonics
+    (HarmonicIter); here the same integrals come from the oracle's Racah
+    solid harmonics (the ones the box moments use) evaluated at a 12-point
+    Gauss-Hermite product rule, exact for the degree-16 integrands."""
+    lmax = 15
+    x, w = np.polynomial.hermite.hermgauss(12)
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    poly = np.asfortranarray(np.pi ** -1.5 * (1.0 + X + Y + Z))
+    q = oracle.box_multipoles(lmax, x, w, x, w, x, w, poly, np.zeros(3))
+    assert abs(q[0] - 1.0) <= 1e-12
+    assert np.abs(q[1:4] - 0.5).max() <= 1e-12
+    assert np.abs(q[4:]).max() <= 1e-8, np.abs(q[4:]).max()

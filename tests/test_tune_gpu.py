@@ -56,3 +56,29 @@ def test_tuned_tiles_give_the_same_potential(dage, oracle):
     V, E = op.apply(rho, energy=True)
     Vo = oracle.coulomb_apply(go, rho, quad=(20, 20, 0.0, 2.0, 1e3))
     assert np.abs(V - Vo).max() <= 1e-10 * np.abs(Vo).max()
+
+
+def test_operator_cache_on_disk(dage, oracle, tmp_path):
+    """dage_op3d_create_cached writes the matrices on the first create and
+    reads them on the next (same grids and quadrature: identical potential,
+    bit for bit); another quadrature is another key."""
+    g = dage.Grid3D.cube(-3.0, 5, 0.2)
+    go = oracle.Grid3D.cube(-3.0, 5, 0.2)
+    rho = oracle.gauss_cube(go, [1.0, -0.5], [1.2, 2.5], [[0.1, 0.2, -0.3], [-0.4, 0.0, 0.5]])
+    q = dage.GaussQuad(8, 8)
+    d = str(tmp_path)
+    a = dage.Coulomb3D(g, quad=q, cache_dir=d)
+    assert not a.from_cache
+    files = os.listdir(d)
+    assert len(files) == 1 and files[0].startswith("op3d_") and files[0].endswith(".bin")
+    b = dage.Coulomb3D(g, quad=q, cache_dir=d)
+    assert b.from_cache
+    Va, Ea = a.apply(rho, energy=True)
+    Vb, Eb = b.apply(rho, energy=True)
+    assert np.array_equal(Va, Vb) and Ea == Eb
+    for k in range(3):  # the stored matrices are the built ones
+        assert np.array_equal(a.matrix(k), b.matrix(k))
+    c = dage.Coulomb3D(g, quad=dage.GaussQuad(6, 6), cache_dir=d)
+    assert not c.from_cache and len(os.listdir(d)) == 2
+    m = dage.Coulomb3D(g, quad=q, cache_dir=d, precision="fp16x3")  # mixed ops read it too
+    assert m.from_cache
