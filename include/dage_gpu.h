@@ -141,6 +141,19 @@ int dage_op3d_last_time_ms(const dage_op3d *op, float *ms);
 int dage_op3d_set_timing(dage_op3d *op, int enable);
 int dage_op3d_get_timing(const dage_op3d *op, int kind, long long *launches, double *ms);
 
+/* As dage_op3d_create, with an on-disk cache of the operator matrices keyed by
+ * (input grids, output grids, quadrature): when cache_dir holds a file with
+ * this key (op3d_<hash>.bin), the FP64 matrices are read from it instead of
+ * being built on the GPU; otherwise they are built and the file is written.
+ * *from_cache (may be NULL) tells which happened.  The file layout follows
+ * the reference's stream dump of grids (store_Grid1Ds / resume_Grid1Ds,
+ * src/bubbles/grid.F90:2024-2068) for its key.  The GPU build takes ~5-60 ms
+ * for the largest operators, so the cache serves callers that reuse
+ * operators across processes rather than speed. */
+int dage_op3d_create_cached(const dage_grid1d grid_in[3], const dage_grid1d grid_out[3],
+                            const dage_quad *quad, int precision, const char *cache_dir,
+                            int *from_cache, dage_op3d **op);
+
 /* Tile widths (32, 64 or 128 output columns) the autotuner chose for the three
  * FP64 contraction stages (the split-precision stages use 128).  No reference
  * counterpart: the reference's stages are cuBLAS DGEMMs. */

@@ -129,12 +129,6 @@ def test_multilevel_matches_oracle(dage, oracle, ncell, lmax):
     assert abs(E - Eo) <= 1e-11 * abs(Eo)
 
 
-def test_multilevel_helmholtz_is_refused(dage):
-    g = dage.Grid3D.cube(-9.6, 16, 0.2)
-    with pytest.raises(Exception, match="maxlevel 2"):
-        dage.GBFMMHelmholtz3D(g, -0.5, lmax=4, maxlevel=3, quad=dage.GaussQuad(4, 4))
-
-
 @pytest.mark.parametrize("ncell,lmax,maxlevel", [(16, 8, 2), (16, 8, 3), (18, 6, 3)])
 def test_adaptive_matches_oracle(dage, oracle, ncell, lmax, maxlevel):
     """The adaptive mode (multipoles up to level 1, whole parent-level boxes
@@ -160,9 +154,3 @@ def test_adaptive_matches_oracle(dage, oracle, ncell, lmax, maxlevel):
     Eo = oracle.integrate_cube(go, rho * Vo)
     assert abs(E - Eo) <= 1e-11 * abs(Eo)
 
-
-def test_adaptive_helmholtz_is_refused(dage):
-    g = dage.Grid3D.cube(-9.6, 16, 0.2)
-    op = dage.GBFMMCoulomb3D(g, lmax=4, maxlevel=2, quad=dage.GaussQuad(4, 4), adaptive_mode=True)
-    with pytest.raises(dage.DageError, match="not adaptive"):
-        dage._capi.check(dage.load().dage_gbfmm_set_energy(op._h, -0.5))
