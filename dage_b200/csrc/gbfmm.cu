@@ -130,7 +130,7 @@ struct GInst {
   const double *Wm2m_h;
 };
 
-constexpr int kEnergyBlocks = 256;
+constexpr int kEnergyBlocks = 148 * 6;  // partial sums per density (6 blocks per SM)
 
 // ---------------------------------------------------------------------------
 // Modified spherical Bessel functions of the first kind, as the ratios
@@ -811,14 +811,26 @@ __global__ void __launch_bounds__(kL2pHelmThreads)
 __global__ void energy_kernel(const GInst *__restrict__ insts) {
   __shared__ double sh[32];
   const GInst &I = insts[blockIdx.y];
-  const long long n = (long long)I.Nx * I.Ny * I.Nz;
+  // one warp per x row (y, z): its weight wy wz once, lanes over x
+  const int lane = threadIdx.x & 31;
+  const long long rows = (long long)I.Ny * I.Nz;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   double acc = 0.0;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(e % I.Nx);
-    const long long r = e / I.Nx;
-    const int y = (int)(r % I.Ny), z = (int)(r / I.Ny);
-    acc += I.rho[e] * I.V[e] * (I.wx[x] * I.wy[y] * I.wz[z]);
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += nwarps) {
+    const size_t base = (size_t)r * I.Nx;
+    double srow = 0.0;
+    // four independent elements per lane per pass (loads in flight together)
+    for (int x0 = lane; x0 < I.Nx; x0 += 128) {
+      double p[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int x = x0 + 32 * u;
+        p[u] = x < I.Nx ? I.rho[base + x] * I.V[base + x] * I.wx[x] : 0.0;
+      }
+      srow += (p[0] + p[1]) + (p[2] + p[3]);
+    }
+    acc += srow * (I.wy[r % I.Ny] * I.wz[r / I.Ny]);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);

@@ -539,16 +539,18 @@ __global__ void near_split_input_kernel(const double *const *rho, int Nx, long l
   const int i = blockIdx.y;
   const double *x = rho[i];
   const double g = (double)gin[i];
-  const long long n = rows * ld;
-  const size_t base = (size_t)i * n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long r = e / ld;
-    const int k = (int)(e % ld);
-    __half p[2];
-    split_f16_f64(k < Nx ? x[r * Nx + k] * g : 0.0, p);
-    o0[base + e] = p[0];
-    o1[base + e] = p[1];
+  const size_t base = (size_t)i * rows * ld;
+  // one warp per row, lanes over x (no per-element index division)
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += nwarps) {
+    for (int k = lane; k < ld; k += 32) {
+      __half p[2];
+      split_f16_f64(k < Nx ? x[r * Nx + k] * g : 0.0, p);
+      o0[base + r * ld + k] = p[0];
+      o1[base + r * ld + k] = p[1];
+    }
   }
 }
 

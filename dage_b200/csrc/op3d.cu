@@ -349,29 +349,35 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 }
 
 __global__ void __launch_bounds__(kRedThreads)
-    finalize_kernel(const double *__restrict__ f1, double *f2, const double *__restrict__ rho,
+    finalize_kernel(const double *__restrict__ f1, double *__restrict__ f2,
+                    const double *__restrict__ rho,
                     double coda, const double *__restrict__ wx, const double *__restrict__ wy,
                     const double *__restrict__ wz, int nx, int ny, int nz, double *partials,
                     int want_integral) {
   __shared__ double sh[32];
-  const long long n = (long long)nx * ny * nz;
+  // one warp per x row (y, z): the row's weight wy wz once, lanes over x
+  // (coalesced, no per-element index division)
+  const int lane = threadIdx.x & 31;
+  const long long rows = (long long)ny * nz;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   double s = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    double v2 = 1.0;
-    if (f2) {
-      v2 = f2[i];
-      if (rho) {
-        v2 = v2 + coda * rho[i];
-        f2[i] = v2;
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += nwarps) {
+    const size_t base = (size_t)r * nx;
+    double srow = 0.0;
+    for (int x = lane; x < nx; x += 32) {
+      const size_t i = base + x;
+      double v2 = 1.0;
+      if (f2) {
+        v2 = f2[i];
+        if (rho) {
+          v2 = v2 + coda * rho[i];
+          f2[i] = v2;
+        }
       }
+      if (want_integral) srow += f1[i] * v2 * wx[x];
     }
-    if (want_integral) {
-      const int x = (int)(i % nx);
-      const long long r = i / nx;
-      const int y = (int)(r % ny), z = (int)(r / ny);
-      s += f1[i] * v2 * (wx[x] * wy[y] * wz[z]);
-    }
+    if (want_integral) s += srow * (wy[r % ny] * wz[r / ny]);
   }
   if (!want_integral) return;
   s = block_sum(s, sh);

@@ -689,15 +689,17 @@ __global__ void split_input_f16_kernel(const double *__restrict__ rho, int K, lo
                                        long long ld, const float *__restrict__ gin, __half *o0,
                                        __half *o1) {
   const double g = (double)*gin;
-  const long long n = rows * ld;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long r = e / ld;
-    const int k = (int)(e % ld);
-    __half p[2];
-    split_f16_f64(k < K ? rho[r * K + k] * g : 0.0, p);
-    o0[e] = p[0];
-    o1[e] = p[1];
+  // one warp per row, lanes over k (no per-element index division)
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += nwarps) {
+    for (int k = lane; k < ld; k += 32) {
+      __half p[2];
+      split_f16_f64(k < K ? rho[r * K + k] * g : 0.0, p);
+      o0[r * ld + k] = p[0];
+      o1[r * ld + k] = p[1];
+    }
   }
 }
 

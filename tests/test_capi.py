@@ -59,3 +59,15 @@ def test_fortran_interface_block_binds_every_entry_point():
     bound = set(re.findall(r'bind\(C, name="(dage_[a-z0-9_]+)"\)', block))
     assert bound == declared_functions(), (sorted(declared_functions() - bound),
                                            sorted(bound - declared_functions()))
+
+
+def test_tune_cache_path_host_only(dage_host, tmp_path):
+    """dage_set_tune_cache is host logic: it creates the cache file, loads
+    what is in it and refuses a path it cannot write (no GPU call)."""
+    lib = dage_host.load()
+    path = tmp_path / "tune.txt"
+    path.write_text("dev/op3d_fp64/5x5,5x5,5x5,P2 32 64 128\n")
+    assert lib.dage_set_tune_cache(str(path).encode()) == 0
+    assert lib.dage_set_tune_cache(str(tmp_path).encode()) == -1  # a directory
+    assert b"tune cache" in lib.dage_last_error()
+    assert lib.dage_set_tune_cache(None) == 0
