@@ -17,6 +17,8 @@ from .operators import (  # noqa: F401
     Helmholtz3D,
     Operator3D,
     apply_batched,
+    cart2sph_table,
+    cube_contaminants,
     dot,
     integrate,
     multiply,
@@ -24,4 +26,4 @@ from .operators import (  # noqa: F401
 )
 
 __all__ = ["Bubbles", "Coulomb3D", "GBFMMBatch", "GBFMMCoulomb3D", "GBFMMHelmholtz3D", "GaussQuad", "Grid1D", "Grid3D", "Helmholtz3D", "Operator3D",
-           "DageError", "apply_batched", "dot", "integrate", "load", "multiply", "set_tune_cache"]
+           "DageError", "apply_batched", "cart2sph_table", "cube_contaminants", "dot", "integrate", "load", "multiply", "set_tune_cache"]

@@ -13,6 +13,8 @@ DAGE_NO_CODA = 4
 DAGE_ACCUMULATE = 8
 DAGE_NO_GRAPH = 16
 DAGE_PRODUCT_COMPLETE = 32
+DAGE_TAYLOR_EXACT = 64
+DAGE_TAYLOR_IGNORE_BUBBLES = 128
 
 DAGE_FP64 = 0
 DAGE_MIXED_BF16X3 = 1
@@ -115,6 +117,18 @@ SIGNATURES = {
     "dage_function3d_multiply": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, _VP, _VP,
                                                 _VP, _VP, ctypes.c_uint]),
     "dage_bubbles_destroy": (ctypes.c_int, [_VP]),
+    "dage_bubbles_contaminants": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
+    "dage_cube_contaminants": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, ctypes.c_int, _D,
+                                              ctypes.c_int, ctypes.c_uint, _D]),
+    "dage_bubbles_make_taylor": (ctypes.c_int, [_VP, _D, _D, ctypes.c_int, ctypes.c_uint,
+                                                ctypes.POINTER(_VP)]),
+    "dage_bubbles_taylor": (ctypes.c_int, [_VP, ctypes.POINTER(DageGrid1D), _VP, ctypes.c_int,
+                                           ctypes.c_uint, ctypes.POINTER(_VP)]),
+    "dage_bubbles_multiply_taylor": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_uint,
+                                                    ctypes.POINTER(_VP)]),
+    "dage_cart2sph_table": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                           _D, ctypes.POINTER(ctypes.c_int)]),
     "dage_integrate": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), _VP, _VP, ctypes.c_uint, _D]),
     "dage_op3d_apply_fp64_noalloc": (ctypes.c_int, [ctypes.c_int] * 7 + [_VP, _VP, _VP, _D, _VP,
                                                                        _VP, _VP]),

@@ -21,59 +21,12 @@
 #include <cmath>
 #include <vector>
 
-#include "common.cuh"
-#include "grid_host.h"
-
-struct dage_bubbles;
+#include "bubbles.cuh"
 
 namespace dage {
 namespace {
 
 constexpr int kMaxAtomsSmem = 256;
-
-// Racah-normalised real spherical harmonics of a unit vector: the regular
-// solid-harmonic recursion with r^2 = 1, visiting each (l, m) once.
-template <class F>
-__host__ __device__ __forceinline__ void unit_harmonics(int lmax, double x, double y, double z, F &&f) {
-  f(0, 1.0);
-  if (lmax == 0) return;
-  {
-    double p2 = 1.0, p1 = z;
-    f(2, z);
-    for (int l = 2; l <= lmax; ++l) {
-      double cur = (2.0 * l - 1.0) * (z * p1) - sqrt((double)((l - 1) * (l - 1))) * p2;
-      cur = cur * (1.0 / sqrt((double)(l * l)));
-      f(l * (l + 1), cur);
-      p2 = p1;
-      p1 = cur;
-    }
-  }
-  double top = x, bot = y;
-  for (int mm = 1; mm <= lmax; ++mm) {
-    if (mm >= 2) {
-      const double c = sqrt(1.0 - 0.5 / mm);
-      const double nb = c * (top * y + bot * x);
-      const double nt = c * (top * x - bot * y);
-      top = nt;
-      bot = nb;
-    }
-    f(mm * (mm + 1) + mm, top);
-    f(mm * (mm + 1) - mm, bot);
-#pragma unroll 1
-    for (int sg = 0; sg < 2; ++sg) {
-      const int m = sg ? -mm : mm;
-      double p2 = 0.0, p1 = sg ? bot : top;
-      for (int l = mm + 1; l <= lmax; ++l) {
-        double cur = (2.0 * l - 1.0) * (p1 * z);
-        if (l - mm > 1) cur = cur - sqrt((l + m - 1.0) * (l - m - 1.0)) * p2;
-        cur = (1.0 / sqrt(1.0 * (l - m) * (l + m))) * cur;
-        f(l * (l + 1) + m, cur);
-        p2 = p1;
-        p1 = cur;
-      }
-    }
-  }
-}
 
 // The same recursion for a compile-time lmax, fully unrolled, so that every
 // callback sees a constant lm.
@@ -181,10 +134,6 @@ struct BrickGrid {
   }
 };
 
-struct AtomTab {
-  double cx, cy, cz, rmax;
-  int cell0, ncell;
-};
 
 // LS >= 0: lmax <= LS and 7-point cells (harmonics unrolled, 16-byte
 // coefficient loads); LS = -1: any lmax and cell size.
@@ -269,23 +218,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Radial cell of distance d (1-based, Grid1D_get_icell), 0 when d is outside.
-__device__ __forceinline__ int radial_cell(const double *cd, int ncell, double d) {
-  if (cd[ncell - 1] <= d) return ncell;
-  int icell = ncell / 2, maxi = ncell - 1, mini = 1;
-  for (int it = 0; it < 64; ++it) {
-    if (d >= cd[icell]) {
-      if (d < cd[icell + 1]) return icell + 1;
-      mini = icell + 2;
-    } else {
-      if (d >= cd[icell - 1]) return icell;
-      maxi = icell - 1;
-    }
-    icell = (mini + maxi) / 2;
-  }
-  return 0;
-}
-
 // The cube part of a function product in one pass (Function3D_multiply,
 // function3d.F90:1097-1409; the reference GPU path injects each bubble set
 // in its own launches per atom, multiplies the cubes, then de-injects,
@@ -359,10 +291,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-struct ProdTerm {
-  int a, b, lm, pad;
-  double c;
-};
 
 // Radial product of two bubble sets on the same atoms and radial points
 // (Bubble_product_kernel, bubbles_multiplier.cu:65-106): one thread per
@@ -399,19 +327,6 @@ __global__ void bubbles_product_kernel(const double *__restrict__ f1, int N1,
 
 using namespace dage;
 
-struct dage_bubbles {
-  int device = 0, natom = 0, lmax = 0, k = 0, nlip = 7, N = 1;
-  double first = -3.0;
-  DevBuf atoms, celld, hcell, coef, xs, ys, zs;
-  int gshape[3] = {0, 0, 0};
-  // the radial values as given (without r^k), the radial points, per-atom
-  // point counts and offsets; host copies of the centres and radial grids
-  DevBuf fraw, rpts, np, foff;
-  std::vector<double> centers;
-  std::vector<dage_grid1d> radial;
-  std::vector<std::vector<double>> scales;
-  size_t nvals = 0;
-};
 
 namespace dage {
 namespace {
@@ -494,7 +409,7 @@ int dage_bubbles_create(int natom, const double *centers, const dage_grid1d *rad
     if (ax.points.front() != 0.0) return cleanup(fail(DAGE_E_INVALID, "radial grids start at r = 0"));
   }
   // upload, then LIP values -> monomial coefficients on the GPU
-  DevBuf d_rf, d_np, d_foff, d_cell0, d_lipc;
+  TmpBuf d_rf, d_np, d_foff, d_cell0, d_lipc;
   if ((rc = b->atoms.alloc(sizeof(AtomTab) * natom)) || (rc = b->celld.alloc(sizeof(double) * celld.size())) ||
       (rc = b->hcell.alloc(sizeof(double) * hcell.size())) ||
       (rc = b->coef.alloc(sizeof(double) * 8 * (size_t)cell0[natom] * b->N)) ||
@@ -743,6 +658,8 @@ void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w) {
   }
 }
 
+}  // namespace
+
 // Expansion of products of real harmonics, Y_a Y_b = sum C_ab^LM Y_LM
 // (the table of YProduct_init, harmonic.F90:884-951), for a <= b < (lmax+1)^2
 // and L <= result_lmax.  Each coefficient is the projection
@@ -806,7 +723,6 @@ bool same_layout(const dage_bubbles *x, const dage_bubbles *y) {
   return true;
 }
 
-}  // namespace
 }  // namespace dage
 
 extern "C" {
@@ -826,7 +742,7 @@ int dage_bubbles_inject(dage_bubbles *b, const dage_grid1d grid[3], int lmin, do
                              cudaMemcpyHostToDevice));
   }
   const size_t n = (size_t)ax[0].n() * ax[1].n() * ax[2].n();
-  DevBuf staging;
+  TmpBuf staging;
   double *d_cube = cube;
   if (!(flags & DAGE_DEVICE_PTRS)) {
     DAGE_TRY(staging.alloc(sizeof(double) * n));
@@ -867,14 +783,14 @@ int bubbles_radial_potential(const dage_bubbles *in, bool helm, double kappa, da
       outi[(size_t)i * n + j] = anti(i, L.first + j + 1) - anti(i, L.first);
       ini[(size_t)i * n + j] = anti(i, L.last) - anti(i, L.first + j);
     }
-  DevBuf d_out, d_in, d_V;
+  TmpBuf d_out, d_in, d_V;
   DAGE_TRY(d_out.alloc(sizeof(double) * outi.size()));
   DAGE_TRY(d_in.alloc(sizeof(double) * ini.size()));
   DAGE_TRY(d_V.alloc(sizeof(double) * in->nvals));
   DAGE_CUDA_TRY(cudaMemcpy(d_out.ptr, outi.data(), sizeof(double) * outi.size(), cudaMemcpyHostToDevice));
   DAGE_CUDA_TRY(cudaMemcpy(d_in.ptr, ini.data(), sizeof(double) * ini.size(), cudaMemcpyHostToDevice));
   const int total = (int)(in->nvals / in->N);
-  DevBuf d_I, d_K;
+  TmpBuf d_I, d_K;
   if (helm) {
     DAGE_TRY(d_I.alloc(sizeof(double) * (size_t)(in->lmax + 1) * total));
     DAGE_TRY(d_K.alloc(sizeof(double) * (size_t)(in->lmax + 1) * total));
@@ -940,7 +856,7 @@ int dage_bubbles_multiply(const dage_bubbles *x, const dage_bubbles *y, unsigned
     poff[a + 1] = poff[a] + np[a];
   }
   const size_t nout = (size_t)Nr * poff[x->natom];
-  DevBuf d_terms, d_np, d_poff, d_out;
+  TmpBuf d_terms, d_np, d_poff, d_out;
   DAGE_TRY(d_terms.alloc(sizeof(ProdTerm) * std::max<size_t>(terms.size(), 1)));
   DAGE_TRY(d_np.alloc(sizeof(int) * np.size()));
   DAGE_TRY(d_poff.alloc(sizeof(int) * poff.size()));
@@ -995,7 +911,7 @@ int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, con
   Axis ax[3];
   for (int d = 0; d < 3; ++d) DAGE_TRY(make_axis(grid[d], ax[d]));
   const size_t n = (size_t)ax[0].n() * ax[1].n() * ax[2].n();
-  DevBuf pts[3], s1, s2, so;
+  TmpBuf pts[3], s1, s2, so;
   for (int d = 0; d < 3; ++d) {
     DAGE_TRY(pts[d].alloc(sizeof(double) * ax[d].n()));
     DAGE_CUDA_TRY(cudaMemcpy(pts[d].ptr, ax[d].points.data(), sizeof(double) * ax[d].n(),

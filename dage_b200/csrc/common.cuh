@@ -51,4 +51,13 @@ struct DevBuf {
   }
 };
 
+// A DevBuf released when it leaves scope: the temporaries of setup and
+// host-pointer calls.  Not copyable, so no second owner can free it.
+struct TmpBuf : DevBuf {
+  TmpBuf() = default;
+  TmpBuf(const TmpBuf &) = delete;
+  TmpBuf &operator=(const TmpBuf &) = delete;
+  ~TmpBuf() { release(); }
+};
+
 }  // namespace dage

@@ -1325,7 +1325,7 @@ int build_m2l_into(const dage_gbfmm *g, double kappa, DevBuf &T) {
       coaxial_ml(k, lmax, c);
       std::copy(c.begin(), c.end(), C.begin() + (size_t)d * cblk);
     }
-    DevBuf dR, dC;
+    TmpBuf dR, dC;
     DAGE_TRY(dR.alloc(sizeof(double) * R.size()));
     DAGE_TRY(dC.alloc(sizeof(double) * C.size()));
     DAGE_CUDA_TRY(cudaMemcpyAsync(dR.ptr, R.data(), sizeof(double) * R.size(), cudaMemcpyHostToDevice, s));
@@ -1338,7 +1338,7 @@ int build_m2l_into(const dage_gbfmm *g, double kappa, DevBuf &T) {
   }
   M2LTables t;
   m2l_tables(lmax, t);
-  DevBuf dd, c1, c2, l1, l2, pr, pc;
+  TmpBuf dd, c1, c2, l1, l2, pr, pc;
   const size_t M = t.c1.size();
   DAGE_TRY(dd.alloc(sizeof(double) * g->disp.size()));
   DAGE_TRY(c1.alloc(sizeof(double) * M));
@@ -1386,7 +1386,7 @@ int build_helm_m2m_into(const dage_gbfmm *g, double kappa, DevBuf &W) {
     coaxial_mm(ib, lmax, c);
     std::copy(c.begin(), c.end(), C.begin() + (size_t)d * cblk);
   }
-  DevBuf dR, dC;
+  TmpBuf dR, dC;
   DAGE_TRY(W.alloc(sizeof(double) * (size_t)g->nm2m * g->N * g->N));
   DAGE_TRY(dR.alloc(sizeof(double) * R.size()));
   DAGE_TRY(dC.alloc(sizeof(double) * C.size()));
@@ -1638,7 +1638,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
       const int M = g->N * (g->N + 1) / 2;
       TransTables t;
       translation_tables(lmax, t);
-      DevBuf dd, c1, c2, l1, l2;
+      TmpBuf dd, c1, c2, l1, l2;
       DAGE_TRY(dd.alloc(sizeof(double) * tdisp.size()));
       DAGE_TRY(c1.alloc(sizeof(double) * M));
       DAGE_TRY(c2.alloc(sizeof(double) * M));
@@ -1678,7 +1678,7 @@ int gbfmm_create_impl(dage_gbfmm *g, const dage_grid1d grid[3], int maxlevel, in
   DAGE_TRY(g->d_partial.alloc(sizeof(double) * (size_t)g->nbox * g->nslab * g->N));
 
   // --- near-field sub-operator matrices per axis position --------------------
-  DevBuf d_tp;
+  TmpBuf d_tp;
   DAGE_TRY(build_quadrature(g->quad, g->tp, g->tw, d_tp, s));
   set_weights(g);
   for (int d = 0; d < 3; ++d) {
@@ -1987,7 +1987,7 @@ int gbfmm_autotune(dage_gbfmm *g) {
   }
   cudaStream_t s = g->stream;
   const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
-  DevBuf rho, V;
+  TmpBuf rho, V;
   DAGE_TRY(rho.alloc(sizeof(double) * n));
   DAGE_TRY(V.alloc(sizeof(double) * n));
   DAGE_CUDA_TRY(cudaMemsetAsync(rho.ptr, 0, sizeof(double) * n, s));
@@ -2067,7 +2067,7 @@ int near16_tune(dage_gbfmm *g, int *tile) {
   }
   cudaStream_t s = g->stream;
   const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
-  DevBuf rho, V;
+  TmpBuf rho, V;
   DAGE_TRY(rho.alloc(sizeof(double) * n));
   DAGE_TRY(V.alloc(sizeof(double) * n));
   DAGE_CUDA_TRY(cudaMemsetAsync(rho.ptr, 0, sizeof(double) * n, s));
@@ -2647,7 +2647,7 @@ int dage_gbfmm_evaluate_le(dage_gbfmm *g, const double *local_expansions, double
   DAGE_CUDA_TRY(cudaSetDevice(g->device));
   cudaStream_t s = g->stream;
   const size_t n = (size_t)g->npts[0] * g->npts[1] * g->npts[2];
-  DevBuf dL;
+  TmpBuf dL;
   DAGE_TRY(dL.alloc(sizeof(double) * g->nbox * g->N));
   DAGE_CUDA_TRY(cudaMemcpyAsync(dL.ptr, local_expansions, sizeof(double) * g->nbox * g->N,
                                 cudaMemcpyHostToDevice, s));

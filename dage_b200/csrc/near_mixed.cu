@@ -676,7 +676,7 @@ int near_f16_plan_create(NearF16Plan **out, const NearGeom &geom, cudaStream_t s
     DAGE_TRY(pl->psc[d].alloc(sizeof(double) * P));
     // per-position tables on the device
     std::vector<long long> tab;  // T pointers, then own, nq, brow, koff as int
-    DevBuf dT, dI, stats;
+    TmpBuf dT, dI, stats;
     DAGE_TRY(dT.alloc(sizeof(double *) * npos));
     DAGE_TRY(dI.alloc(sizeof(int) * 4 * npos));
     DAGE_TRY(stats.alloc(sizeof(double) * 2 * npos * P));

@@ -505,7 +505,7 @@ int launch_finalize(const double *f1, double *f2_or_V, const double *rho_for_cod
 int build_quadrature(const dage_quad &q, std::vector<double> &tp, std::vector<double> &tw,
                      DevBuf &d_tp, cudaStream_t s) {
   const int P = q.nlin + q.nlog;
-  DevBuf d_tw;
+  TmpBuf d_tw;
   DAGE_TRY(d_tp.alloc(sizeof(double) * P));
   DAGE_TRY(d_tw.alloc(sizeof(double) * P));
   quad_kernel<<<2, 128, 0, s>>>(q.nlin, q.nlog, q.tstart, q.tlin, q.tlog, d_tp.as<double>(),
@@ -525,7 +525,7 @@ int build_axis_matrix(const Axis &ai, const double *out_points, int n_out, const
   DAGE_TRY(make_lip_basis(ai.nlip, ai.grid_type, L));
   const size_t nT = (size_t)P * n_out * ai.n();
   DAGE_CUDA_TRY(cudaMemsetAsync(d_T, 0, sizeof(double) * nT, s));
-  DevBuf d_celld, d_h, d_x, d_c;
+  TmpBuf d_celld, d_h, d_x, d_c;
   DAGE_TRY(d_celld.alloc(sizeof(double) * ai.ncell));
   DAGE_TRY(d_h.alloc(sizeof(double) * ai.ncell));
   DAGE_TRY(d_x.alloc(sizeof(double) * n_out));
@@ -669,7 +669,7 @@ static int cache_store(const dage_op3d *op, const std::string &path) {
 // there (cache_dir non-null), else built on the GPU (and stored there).
 static int build_matrices(dage_op3d *op, const char *cache_dir = nullptr) {
   cudaStream_t s = op->stream;
-  DevBuf d_tp;
+  TmpBuf d_tp;
   DAGE_TRY(build_quadrature(op->quad, op->tp, op->tw, d_tp, s));
   const double two_over_sqrtpi = 2.0 / std::sqrt(std::acos(-1.0));
   op->w.resize(op->P);
@@ -810,7 +810,7 @@ static int tune_fp64(dage_op3d *op) {
   cudaStream_t s = op->stream;
   const int nix = op->nin[0], niy = op->nin[1], niz = op->nin[2];
   const int nox = op->nout[0], noy = op->nout[1], noz = op->nout[2];
-  DevBuf X, U, W, V;
+  TmpBuf X, U, W, V;
   DAGE_TRY(X.alloc(sizeof(double) * (size_t)nix * niy * niz));
   DAGE_TRY(U.alloc(sizeof(double) * (size_t)niy * niz * nox));
   DAGE_TRY(W.alloc(sizeof(double) * (size_t)niz * nox * noy));
@@ -1132,7 +1132,7 @@ int dage_integrate(const dage_grid1d grid[3], const double *f1, const double *f2
   for (int d = 0; d < 3; ++d) DAGE_TRY(make_axis(grid[d], ax[d]));
   const size_t n = (size_t)ax[0].n() * ax[1].n() * ax[2].n();
   const bool dev = (flags & DAGE_DEVICE_PTRS) != 0;
-  DevBuf w[3], b1, b2, part;
+  TmpBuf w[3], b1, b2, part;
   for (int d = 0; d < 3; ++d) {
     DAGE_TRY(w[d].alloc(sizeof(double) * ax[d].n()));
     DAGE_CUDA_TRY(cudaMemcpy(w[d].ptr, ax[d].weights.data(), sizeof(double) * ax[d].n(),

@@ -659,6 +659,79 @@ class Bubbles:
 
     __mul__ = multiply
 
+    def contaminants(self, tmax: int = 2) -> np.ndarray:
+        """Bubble contaminants (Bubbles_get_contaminants, bubbles.F90:2844-2910):
+        (natom, ncart) array whose row B holds the partial derivatives
+        d^kappa, |kappa| <= tmax (CartIter order), of the other atoms'
+        bubbles at atom B, computed on the GPU."""
+        nc = (tmax + 1) * (tmax + 2) * (tmax + 3) // 6
+        out = np.zeros((self.natom, nc))
+        check(load().dage_bubbles_contaminants(self._h, int(tmax),
+                                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def make_taylor(self, bubble_contaminants=None, cube_contaminants=None, tmax: int = 2,
+                    exact: bool = False) -> "Bubbles":
+        """Taylor-series bubbles from contaminants (Bubbles_make_taylor,
+        bubbles.F90:1435-1530); lmax = max(self.lmax, tmax).  ``exact`` uses
+        the true Taylor series instead of the reference's |kappa|! and dvpos
+        conventions."""
+        nc = (tmax + 1) * (tmax + 2) * (tmax + 3) // 6
+        dp = ctypes.POINTER(ctypes.c_double)
+
+        def arr(a):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(self.natom, nc))
+            return a, a.ctypes.data_as(dp)
+        cb, pb = arr(bubble_contaminants)
+        cc, pc = arr(cube_contaminants)
+        h = ctypes.c_void_p()
+        check(load().dage_bubbles_make_taylor(self._h, pb, pc, int(tmax),
+                                              _capi.DAGE_TAYLOR_EXACT if exact else 0,
+                                              ctypes.byref(h)))
+        res = Bubbles._wrap(h, self)
+        res.lmax = max(self.lmax, tmax)
+        return res
+
+    def taylor_series(self, grid: Grid3D | None = None, cube=None, tmax: int = 2,
+                      ignore_bubbles: bool = False, exact: bool = False) -> "Bubbles":
+        """Taylor-series contaminant bubbles of the function cube + self
+        (Function3D_get_taylor_series_bubbles, function3d.F90:1332-1405): the
+        contaminants of the other atoms' bubbles and of the cube (when given,
+        host array or CUDA tensor) at every atom, turned into bubbles, all on
+        the GPU."""
+        flags = (_capi.DAGE_TAYLOR_EXACT if exact else 0) | \
+            (_capi.DAGE_TAYLOR_IGNORE_BUBBLES if ignore_bubbles else 0)
+        p, g = None, None
+        if cube is not None:
+            if grid is None:
+                raise ValueError("a cube needs its grid")
+            p, dev = _ptr(cube, int(np.prod(grid.shape)))
+            g = grid.c()
+            if dev:
+                flags |= _capi.DAGE_DEVICE_PTRS
+        h = ctypes.c_void_p()
+        check(load().dage_bubbles_taylor(self._h, g, p, int(tmax), flags, ctypes.byref(h)))
+        res = Bubbles._wrap(h, self)
+        res.lmax = max(self.lmax, tmax)
+        return res
+
+    def multiply_taylor(self, other: "Bubbles", taylor_self: "Bubbles", taylor_other: "Bubbles",
+                        complete: bool = False) -> "Bubbles":
+        """Radial product with Taylor series (option (1) of
+        BubblesMultiplier_multiply, bubbles.F90:3567-3640):
+        (self + taylor_self)(other + taylor_other) - taylor_self taylor_other,
+        each Taylor set cut at its bubbles' lmax; lmax and k add."""
+        h = ctypes.c_void_p()
+        check(load().dage_bubbles_multiply_taylor(self._h, other._h, taylor_self._h,
+                                                  taylor_other._h,
+                                                  _capi.DAGE_PRODUCT_COMPLETE if complete else 0,
+                                                  ctypes.byref(h)))
+        res = Bubbles._wrap(h, self)
+        res.lmax = self.lmax + other.lmax
+        return res
+
     def inject(self, grid: Grid3D, cube=None, lmin: int = 0, factor: float = 1.0):
         """cube += factor * bubbles at the grid points; returns the cube."""
         n = int(np.prod(grid.shape))
@@ -669,6 +742,36 @@ class Bubbles:
         check(load().dage_bubbles_inject(self._h, g, lmin, float(factor), p,
                                          _capi.DAGE_DEVICE_PTRS if dev else 0))
         return cube
+
+
+def cube_contaminants(grid: Grid3D, cube, centers, tmax: int = 2) -> np.ndarray:
+    """Cube contaminants (Function3D_get_cube_contaminants,
+    function3d.F90:1570-1624): (natom, ncart) partial derivatives of the
+    cube's LIP interpolant at the centres, 0 outside the grid; the cube is a
+    host array or a CUDA tensor."""
+    c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+    nc = (tmax + 1) * (tmax + 2) * (tmax + 3) // 6
+    out = np.zeros((len(c), nc))
+    p, dev = _ptr(cube, int(np.prod(grid.shape)))
+    dp = ctypes.POINTER(ctypes.c_double)
+    check(load().dage_cube_contaminants(grid.c(), p, len(c), c.ctypes.data_as(dp), int(tmax),
+                                        _capi.DAGE_DEVICE_PTRS if dev else 0,
+                                        out.ctypes.data_as(dp)))
+    return out
+
+
+def cart2sph_table(tmax: int, exact: bool = False):
+    """The monomial -> harmonic table of the Taylor bubbles (host only):
+    list of (CartIter position, lm, coefficient)."""
+    lib = load()
+    flags = _capi.DAGE_TAYLOR_EXACT if exact else 0
+    n = ctypes.c_int()
+    check(lib.dage_cart2sph_table(int(tmax), flags, 0, None, None, None, ctypes.byref(n)))
+    ki = (ctypes.c_int * n.value)()
+    lm = (ctypes.c_int * n.value)()
+    c = (ctypes.c_double * n.value)()
+    check(lib.dage_cart2sph_table(int(tmax), flags, n.value, ki, lm, c, ctypes.byref(n)))
+    return [(ki[i], lm[i], c[i]) for i in range(n.value)]
 
 
 def multiply(grid: Grid3D, cube1, cube2, bubbles1: Bubbles | None = None,

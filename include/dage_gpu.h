@@ -43,6 +43,9 @@ extern "C" {
 #define DAGE_ACCUMULATE 8u    /* V += result instead of V = result */
 #define DAGE_NO_GRAPH 16u     /* batch apply: launch the pipeline directly, no CUDA graph */
 #define DAGE_PRODUCT_COMPLETE 32u /* bubble product: also the terms the reference table omits */
+#define DAGE_TAYLOR_EXACT 64u     /* Taylor bubbles: the true series (1/kappa!, exact harmonic
+                                     expansion) instead of the reference's */
+#define DAGE_TAYLOR_IGNORE_BUBBLES 128u /* Taylor bubbles: leave out the other atoms' bubbles */
 
 /* operator precisions */
 #define DAGE_FP64 0            /* FP64 everywhere: the drop-in */
@@ -355,6 +358,78 @@ int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, con
                              double *out, unsigned flags);
 
 int dage_bubbles_destroy(dage_bubbles *b);
+
+/* ---------------------------------------------------------------------------
+ * Taylor-series contaminant bubbles
+ * ------------------------------------------------------------------------ */
+
+/* Contaminants are the partial derivatives d^kappa = d^(a+b+c)/dx^a dy^b dz^c,
+ * |kappa| = a+b+c <= tmax (0 <= tmax <= 3), of the smooth part of a function
+ * at each atom centre, stored contams[atom * ncart + i] with
+ * ncart = (tmax+1)(tmax+2)(tmax+3)/6 and i the position of kappa in the
+ * reference's CartIter order (last index fastest: 000, 001, 002, 010, ...;
+ * src/bubbles/cartiter.F90:169-223).  Host arrays. */
+
+/* Bubble contaminants: at each atom B, the derivatives of the sum of the
+ * OTHER atoms' bubbles, sum_{A != B} [r^k f_A,lm](r_A) Y_lm (Bubbles_get_contaminants,
+ * src/bubbles/bubbles.F90:2844-2910).  Derivatives are exact (Taylor-
+ * polynomial arithmetic on the GPU) on the LIP interpolant of each radial
+ * function; an atom beyond another's radial grid contributes 0.  Atoms may
+ * not share a centre. */
+int dage_bubbles_contaminants(const dage_bubbles *b, int tmax, double *contams);
+
+/* Cube contaminants: the derivatives of the cube's 3-D LIP interpolant at
+ * natom centres (Function3D_get_cube_contaminants,
+ * src/bubbles/function3d.F90:1570-1624); 0 for a centre outside the grid.
+ * DAGE_DEVICE_PTRS: `cube` is a device pointer (centres and contams stay on
+ * the host). */
+int dage_cube_contaminants(const dage_grid1d grid[3], const double *cube, int natom,
+                           const double *centers, int tmax, unsigned flags, double *contams);
+
+/* Taylor bubbles from contaminants (Bubbles_make_taylor,
+ * src/bubbles/bubbles.F90:1435-1530): a new set on b's atoms and radial grids
+ * with lmax = max(lmax_b, tmax) and k = k_b whose radial functions are
+ *   f_lm(r) = sum_kappa (Cb + Cc)_kappa r^(|kappa|-k) w(r) / |kappa|! S_lm(kappa)
+ * with w(r) = erfc(r - 2/r) / 2 (1 at r = 0) and x^kappa = r^|kappa| sum S_lm Y_lm
+ * (Cart2SphIter, src/bubbles/harmonic.F90:1096-1265, looked up through the
+ * reference's dvpos, which for |kappa| = 3 takes the expansion of the
+ * preceding monomial).  Either contaminant array may be NULL (zero).
+ * DAGE_TAYLOR_EXACT: 1/kappa! and the exact expansion, i.e. the true
+ * truncated Taylor series of the contaminated function times w. */
+int dage_bubbles_make_taylor(const dage_bubbles *b, const double *bubble_contams,
+                             const double *cube_contams, int tmax, unsigned flags,
+                             dage_bubbles **out);
+
+/* Contaminants and Taylor bubbles in one call, with the contaminants kept on
+ * the GPU (Function3D_get_taylor_series_bubbles,
+ * src/bubbles/function3d.F90:1332-1405; the reference's default order is 2).
+ * cube (with its grid) may be NULL: no cube contaminants (ignore_cube).
+ * Flags: DAGE_DEVICE_PTRS (cube on the device), DAGE_TAYLOR_IGNORE_BUBBLES,
+ * DAGE_TAYLOR_EXACT.  The reference's non_overlapping switch selects between
+ * two identical damping functions and has no counterpart. */
+int dage_bubbles_taylor(const dage_bubbles *b, const dage_grid1d grid[3], const double *cube,
+                        int tmax, unsigned flags, dage_bubbles **out);
+
+/* Bubble product with Taylor series (option (1) of BubblesMultiplier_multiply,
+ * src/bubbles/bubbles.F90:3567-3640; BubblesMultiplier::multiplyBubble,
+ * src/bubbles/bubbles_multiplier.cu:240-292):
+ *   (b1 + t1)(b2 + t2) - t1 t2 = b1 b2 + b1 t2 + t1 b2
+ * on the radial points, each Taylor set cut at its bubble set's lmax; the
+ * result has lmax = lmax1 + lmax2 (<= 12) and k = k1 + k2.  All four sets
+ * share atoms and radial grids, and t_i has b_i's k.  Its result is the
+ * `br` of dage_function3d_multiply for a product of cuspy functions.
+ * DAGE_PRODUCT_COMPLETE as in dage_bubbles_multiply. */
+int dage_bubbles_multiply_taylor(const dage_bubbles *b1, const dage_bubbles *b2,
+                                 const dage_bubbles *t1, const dage_bubbles *t2, unsigned flags,
+                                 dage_bubbles **out);
+
+/* The monomial -> harmonic table make_taylor uses (host only, no GPU call):
+ * entry e says that multi-index kappa_index[e] (CartIter position) adds
+ * c[e] * Y_lm[e].  Sets *n; fills the arrays when cap >= *n.
+ * DAGE_TAYLOR_EXACT as above. */
+int dage_cart2sph_table(int tmax, unsigned flags, int cap, int *kappa_index, int *lm, double *c,
+                        int *n);
+
 
 /* ---------------------------------------------------------------------------
  * Integration (Function3D_integrate / Function3D_dot_product cube part)

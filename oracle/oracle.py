@@ -1180,3 +1180,256 @@ def bubbles_helmholtz_potential(ncell, cell_scales, lmax, f, kappa, k=0, nlip=7)
             t2[0] = 3 * t2[1] - 3 * t2[2] + t2[3] if l == 0 else 0.0
             V[lm] = 8 * kappa * (K[l] * outwards(t1) + I[l] * inwards(t2))
     return V
+
+
+# ---------------------------------------------------------------------------
+# Taylor-series contaminant bubbles
+# ---------------------------------------------------------------------------
+def cart_iter(tmax):
+    """CartIter(3, tmax) (cartiter.F90:169-223): the multi-indices with
+    |kappa| <= tmax, the last index running fastest."""
+    return [(a, b, c) for a in range(tmax + 1) for b in range(tmax + 1 - a)
+            for c in range(tmax + 1 - a - b)]
+
+
+def dvpos_shell(dv):
+    """Position (1-based) of dv in its shell (harmonic.F90:1378-1385)."""
+    k = sum(dv)
+    return (dv[0] * (3 + 2 * k - dv[0]) + 2) // 2 + dv[1]
+
+
+def dvpos(dv):
+    """The reference's position of dv in the shell-grouped series
+    (harmonic.F90:1369-1376): dvpos_shell + |dv|^2, which is the true offset
+    |dv|(|dv|+1)(|dv|+2)/6 for |dv| <= 2 only."""
+    return dvpos_shell(dv) + sum(dv) ** 2
+
+
+def grid1d_icell(celld, qmin, qmax, x):
+    """Grid1D_get_icell (grid.F90:1212-1245): 1-based cell of x, 0 outside."""
+    ncell = len(celld)
+    if x > qmax or x < qmin:
+        return 0
+    if celld[ncell - 1] <= x:
+        return ncell
+    icell, maxi, mini = ncell // 2, ncell - 1, 1
+    while True:
+        if x >= celld[icell]:
+            if x < celld[icell + 1]:
+                return icell + 1
+            mini = icell + 2
+            icell = (mini + maxi) // 2
+        else:
+            if x >= celld[icell - 1]:
+                return icell
+            maxi = icell - 1
+            icell = (mini + maxi) // 2
+
+
+def lip_interp_derivatives(g: Grid1D, vals, x, order):
+    """Interpolator1D_eval (evaluators.F90:766-830): d^j/dx^j, j <= order, of
+    the LIP interpolant of the point values ``vals`` (shape (..., g.n)) at
+    x; zeros outside the grid."""
+    vals = np.asarray(vals, dtype=np.float64)
+    out = np.zeros(vals.shape[:-1] + (order + 1,))
+    ic = grid1d_icell(g.celld, g.points[0], g.points[-1], x)
+    if ic == 0:
+        return out
+    c, first, _ = lip_coeffs(g.nlip, g.grid_type)
+    h = g.cell_scales[ic - 1]
+    crd = (x - g.celld[ic - 1]) / h + first
+    s = (ic - 1) * (g.nlip - 1)
+    block = vals[..., s:s + g.nlip]
+    for j in range(order + 1):
+        pv = np.array([np.polyval(np.polyder(c[i], j) if j else c[i], crd) for i in range(g.nlip)])
+        out[..., j] = (block @ pv) * h ** (-j)
+    return out
+
+
+def _sympy_xyzr():
+    import sympy as sp
+    return sp, sp.symbols("x y z r", real=True)
+
+
+def ybundle_polys(lmax):
+    """YBundle_init (harmonic.F90:612-660): the Racah-normalised real
+    harmonics as polynomials in x/r, y/r, z/r (the recursion's r2 monomial is
+    1), exact sympy expressions in x, y, z, r; index lm = l(l+1)+m."""
+    sp, (x, y, z, r) = _sympy_xyzr()
+    X, Y, Z = x / r, y / r, z / r
+    N = (lmax + 1) ** 2
+    P = [None] * N
+    P[0] = sp.Integer(1)
+    if lmax > 0:
+        P[1], P[2], P[3] = Y, Z, X
+    for l in range(2, lmax + 1):
+        f1 = sp.sqrt(1 - sp.Rational(1, 2 * l))
+        P[l * (l + 1) - l] = f1 * (P[(l - 1) * l + (l - 1)] * Y + P[(l - 1) * l - (l - 1)] * X)
+        for m in range(-(l - 1), l):
+            e = (2 * l - 1) * P[(l - 1) * l + m] * Z
+            if l - abs(m) > 1:
+                e = e - sp.sqrt((l + m - 1) * (l - m - 1)) * P[(l - 2) * (l - 1) + m]
+            P[l * (l + 1) + m] = e / sp.sqrt((l - m) * (l + m))
+        P[l * (l + 1) + l] = f1 * (P[(l - 1) * l + (l - 1)] * X - P[(l - 1) * l - (l - 1)] * Y)
+    return [sp.expand(p) for p in P]
+
+
+_EVAL_COEFFS = {}
+
+
+def y_eval_coeffs(lmax, dv):
+    """Y_eval_coeffs (harmonic.F90:806-860): for every lm, the polynomials
+    P_i(x, y, z, r), i <= |dv|, with d^dv [Y_lm f(r)] = sum_i P_i f^(i)(r);
+    returned as numpy callables of (x, y, z, r).  Differentiating in x_m a
+    term P f^(i) gives (dP/dx_m + dP/dr x_m/r) f^(i) + P x_m/r f^(i+1)."""
+    key = (lmax, tuple(dv))
+    if key in _EVAL_COEFFS:
+        return _EVAL_COEFFS[key]
+    sp, (x, y, z, r) = _sympy_xyzr()
+    xs = (x, y, z)
+    out = []
+    for Y in ybundle_polys(lmax):
+        prev = [Y]
+        for m in range(3):
+            for _ in range(dv[m]):
+                new = [sp.Integer(0)] * (len(prev) + 1)
+                for i, p in enumerate(prev):
+                    new[i] += sp.diff(p, xs[m]) + sp.diff(p, r) * xs[m] / r
+                    new[i + 1] += p * xs[m] / r
+                prev = new
+        out.append([sp.lambdify((x, y, z, r), p, "numpy") for p in prev])
+    _EVAL_COEFFS[key] = out
+    return out
+
+
+def bubble_contaminants(centers, grids, lmax, f, k, tmax):
+    """Bubbles_get_contaminants (bubbles.F90:2844-2910) with the radial
+    derivatives of Bubbles_get_radial_derivatives (bubbles.F90:2272-2300,
+    k >= 0: derivatives of the LIP interpolant of r^k f): contams[B, i] =
+    sum_{A != B} sum_lm d^kappa_i [(r^k f_A,lm)(r_A) Y_lm](R_B)."""
+    centers = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
+    nat = len(centers)
+    kap = cart_iter(tmax)
+    out = np.zeros((nat, len(kap)))
+    polys = [y_eval_coeffs(lmax, dv) for dv in kap]
+    for A in range(nat):
+        g = grids[A]
+        rk = np.asarray(f[A], dtype=np.float64) * g.points ** k
+        for B in range(nat):
+            if A == B:
+                continue
+            v = centers[B] - centers[A]
+            d = float(np.sqrt(v @ v))
+            rfs = lip_interp_derivatives(g, rk, d, tmax)  # (N, tmax+1)
+            for i, dv in enumerate(kap):
+                s = 0.0
+                for lm, P in enumerate(polys[i]):
+                    s += sum(float(Pi(v[0], v[1], v[2], d)) * rfs[lm, j] for j, Pi in enumerate(P))
+                out[B, i] += s
+    return out
+
+
+def cube_contaminants(grid: Grid3D, cube, centers, tmax):
+    """Function3D_get_cube_contaminants (function3d.F90:1570-1624) through
+    the Interpolator (evaluators.F90:853-1000): partial derivatives of the
+    cube's LIP interpolant at the centres (x's LIP basis for every axis),
+    0 for a centre outside the grid."""
+    centers = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
+    kap = cart_iter(tmax)
+    out = np.zeros((len(centers), len(kap)))
+    nlip = grid.axes[0].nlip
+    c, first, _ = lip_coeffs(nlip, grid.axes[0].grid_type)
+    for B, R in enumerate(centers):
+        P, s = [], []
+        for d, g in enumerate(grid.axes):
+            ic = grid1d_icell(g.celld, g.points[0], g.points[-1], R[d])
+            if ic == 0:
+                break
+            h = g.cell_scales[ic - 1]
+            crd = (R[d] - g.celld[ic - 1]) / h + first
+            P.append([np.array([np.polyval(np.polyder(c[i], j) if j else c[i], crd)
+                                for i in range(nlip)]) * h ** (-j) for j in range(tmax + 1)])
+            s.append((ic - 1) * (nlip - 1))
+        if len(P) < 3:
+            continue
+        blk = np.asarray(cube)[s[0]:s[0] + nlip, s[1]:s[1] + nlip, s[2]:s[2] + nlip]
+        for i, (a, b, cc) in enumerate(kap):
+            out[B, i] = np.einsum("ijk,i,j,k->", blk, P[0][a], P[1][b], P[2][cc])
+    return out
+
+
+def cart_to_sph(lmax):
+    """Cart2SphIter_init (harmonic.F90:1096-1165): the (lmax+1)^2 x ncart
+    matrix whose column for a monomial x^kappa (columns grouped by shell,
+    dvpos_shell order within a shell) holds its expansion
+    x^kappa = r^|kappa| sum_lm S_lm Y_lm, from the inverse of each shell's
+    matrix of the monomial coefficients of r^(k-l) S_lm."""
+    sp, (x, y, z, r) = _sympy_xyzr()
+    Y = ybundle_polys(lmax)
+    ncart = (lmax + 1) * (lmax + 2) * (lmax + 3) // 6
+    out = np.zeros(((lmax + 1) ** 2, ncart))
+    for k in range(lmax + 1):
+        mono = [(a, b, k - a - b) for a in range(k + 1) for b in range(k + 1 - a)]
+        sph = [(l, m) for l in range(k % 2, k + 1, 2) for m in range(-l, l + 1)]
+        M = np.zeros((len(mono), len(sph)))
+        for s, (l, m) in enumerate(sph):
+            # r^k Y_lm: the reference's poly%extend(k)
+            e = sp.expand(sp.expand(Y[l * (l + 1) + m] * r ** k).subs(r, sp.sqrt(x * x + y * y + z * z)))
+            poly = sp.Poly(e, x, y, z)
+            for row, (a, b, c) in enumerate(mono):
+                M[row, s] = float(poly.coeff_monomial(x ** a * y ** b * z ** c))
+        inv = np.linalg.inv(M)
+        base = k * (k + 1) * (k + 2) // 6
+        for s, (l, m) in enumerate(sph):
+            out[l * (l + 1) + m, base:base + len(mono)] = inv[s]
+    out[np.abs(out) <= 1e-16] = 0.0
+    return out
+
+
+def make_taylor(grids, lmax, k, bubble_contams, cube_contams, tmax, exact=False):
+    """Bubbles_make_taylor (bubbles.F90:1435-1530) with the damping w
+    (bubbles.F90:1532-1558) and Bubbles_rpow (bubbles.F90:3363-3378): per
+    atom, ((max(lmax, tmax)+1)^2, npoints) radial values (without r^k).
+    ``exact``: 1/kappa! and the shell-grouped column instead of 1/|kappa|!
+    and dvpos."""
+    import math
+    lnew = max(lmax, tmax)
+    C = cart_to_sph(max(lnew, 3))
+    out = []
+    for A, g in enumerate(grids):
+        rr = g.points
+        w = np.array([0.5 * math.erfc(v - 2.0 / v) if v > np.finfo(float).eps else 1.0 for v in rr])
+        f = np.zeros(((lnew + 1) ** 2, g.n))
+        for kappa in cart_iter(tmax):
+            K = sum(kappa)
+            n = K - k
+            if n >= 0:
+                rp = rr ** n
+            else:
+                rp = np.concatenate([[0.0], rr[1:] ** n])
+            if exact:
+                fac = 1.0 / (math.factorial(kappa[0]) * math.factorial(kappa[1]) * math.factorial(kappa[2]))
+                col = K * (K + 1) * (K + 2) // 6 + dvpos_shell(kappa) - 1
+            else:
+                fac = 1.0 / math.factorial(K)
+                col = dvpos(kappa) - 1
+            i = cart_iter(tmax).index(kappa)
+            cval = (bubble_contams[A][i] if bubble_contams is not None else 0.0) + \
+                (cube_contams[A][i] if cube_contams is not None else 0.0)
+            val = cval * (rp * w * fac)
+            for lm in np.nonzero(C[:, col])[0]:
+                if lm < f.shape[0]:
+                    f[lm] += C[lm, col] * val
+        out.append(f)
+    return out
+
+
+def bubbles_multiply_taylor(f1, lmax1, t1, f2, lmax2, t2):
+    """Option (1) of BubblesMultiplier_multiply (bubbles.F90:3567-3640;
+    BubblesMultiplier::multiplyBubble, bubbles_multiplier.cu:240-292) for one
+    atom: (b1 + t1)(b2 + t2) - t1 t2 with each Taylor set cut at its bubbles'
+    lmax (Bubble::add, bubbles_cuda.cu:2629-2680)."""
+    N1, N2 = (lmax1 + 1) ** 2, (lmax2 + 1) ** 2
+    f1, f2 = np.asarray(f1, dtype=np.float64), np.asarray(f2, dtype=np.float64)
+    u1, u2 = np.asarray(t1, dtype=np.float64)[:N1], np.asarray(t2, dtype=np.float64)[:N2]
+    return bubbles_multiply(f1 + u1, lmax1, f2 + u2, lmax2) - bubbles_multiply(u1, lmax1, u2, lmax2)
