@@ -108,6 +108,7 @@ SIGNATURES = {
                                            ctypes.c_double, _VP, ctypes.c_uint]),
     "dage_bubbles_coulomb_potential": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "dage_bubbles_get_f": (ctypes.c_int, [_VP, _D]),
+    "dage_bubbles_integrate": (ctypes.c_int, [_VP, _D]),
     "dage_bubbles_helmholtz_potential": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.POINTER(_VP)]),
     "dage_bubbles_multiply": (ctypes.c_int, [_VP, _VP, ctypes.c_uint, ctypes.POINTER(_VP)]),
     "dage_product_table": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int,

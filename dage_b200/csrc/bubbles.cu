@@ -322,6 +322,40 @@ __global__ void bubbles_product_kernel(const double *__restrict__ f1, int N1,
   }
 }
 
+// Integral of a bubble set over all space (Bubbles_integrate_pick /
+// Bubbles_integrate_all, bubbles.F90:3146-3240): only the s functions
+// survive, 4 pi sum_A int r^(2+k) f_A,00(r) dr with the radial grids' LIP
+// weights.  One block: each atom's points are summed by the block in a
+// fixed order, the atoms one after the other.
+__global__ void bubbles_integrate_kernel(const double *__restrict__ f,
+                                         const double *__restrict__ rpts,
+                                         const double *__restrict__ w, const int *__restrict__ np,
+                                         const int *__restrict__ foff, int natom, int k,
+                                         double *out) {
+  __shared__ double red[256];
+  double total = 0.0;
+  int p0 = 0;
+  for (int a = 0; a < natom; ++a) {
+    double s = 0.0;
+    for (int j = threadIdx.x; j < np[a]; j += blockDim.x) {
+      const double r = rpts[p0 + j];
+      double rp = 1.0;
+      for (int e = 0; e < 2 + k; ++e) rp *= r;
+      s += w[p0 + j] * (f[foff[a] + j] * rp);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+      if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) total += 4.0 * M_PI * red[0];
+    __syncthreads();
+    p0 += np[a];
+  }
+  if (threadIdx.x == 0) *out = total;
+}
+
 }  // namespace
 }  // namespace dage
 
@@ -952,6 +986,37 @@ int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, con
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
   DAGE_CUDA_TRY(cudaDeviceSynchronize());
+  return 0;
+}
+
+int dage_bubbles_integrate(const dage_bubbles *b, double *out) {
+  clear_error();
+  if (!b || !out) return fail(DAGE_E_INVALID, "null argument");
+  DAGE_CUDA_TRY(cudaSetDevice(b->device));
+  // LIP integration weights of every atom's radial points, in the layout of
+  // the radial points (atoms one after the other)
+  std::vector<double> w;
+  std::vector<int> np(b->natom), foff(b->natom);
+  for (int a = 0; a < b->natom; ++a) {
+    Axis ax;
+    DAGE_TRY(make_axis(b->radial[a], ax));
+    np[a] = ax.n();
+    foff[a] = (int)((size_t)b->N * w.size());
+    w.insert(w.end(), ax.weights.begin(), ax.weights.end());
+  }
+  TmpBuf d_w, d_i, d_out;
+  DAGE_TRY(d_w.alloc(sizeof(double) * w.size()));
+  DAGE_TRY(d_i.alloc(sizeof(int) * 2 * b->natom));
+  DAGE_TRY(d_out.alloc(sizeof(double)));
+  DAGE_CUDA_TRY(cudaMemcpy(d_w.ptr, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+  DAGE_CUDA_TRY(cudaMemcpy(d_i.ptr, np.data(), sizeof(int) * b->natom, cudaMemcpyHostToDevice));
+  DAGE_CUDA_TRY(cudaMemcpy(d_i.as<int>() + b->natom, foff.data(), sizeof(int) * b->natom,
+                           cudaMemcpyHostToDevice));
+  bubbles_integrate_kernel<<<1, 256>>>(b->fraw.as<double>(), b->rpts.as<double>(), d_w.as<double>(),
+                                       d_i.as<int>(), d_i.as<int>() + b->natom, b->natom, b->k,
+                                       d_out.as<double>());
+  DAGE_CUDA_TRY(cudaGetLastError());
+  DAGE_CUDA_TRY(cudaMemcpy(out, d_out.ptr, sizeof(double), cudaMemcpyDeviceToHost));
   return 0;
 }
 

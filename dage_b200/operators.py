@@ -632,6 +632,13 @@ class Bubbles:
         check(load().dage_bubbles_helmholtz_potential(self._h, float(energy), ctypes.byref(h)))
         return Bubbles._wrap(h, self)
 
+    def integrate(self) -> float:
+        """Integral of the bubbles over all space (Bubbles_integrate_all,
+        bubbles.F90:3146-3240): 4 pi sum_A int r^(2+k) f_A,00 dr, on the GPU."""
+        out = ctypes.c_double()
+        check(load().dage_bubbles_integrate(self._h, ctypes.byref(out)))
+        return out.value
+
     def radial_values(self):
         """Per atom, the ((lmax+1)^2, npoints) radial values (as given)."""
         sizes = [int(gr.ncell * (gr.nlip - 1) + 1) for gr in self._grids]

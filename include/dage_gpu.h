@@ -324,6 +324,12 @@ int dage_bubbles_coulomb_potential(const dage_bubbles *in, dage_bubbles **out);
  * k_0 = pi/2 e^-x/x (helmholtz3d.F90:851-1060), computed on the GPU. */
 int dage_bubbles_helmholtz_potential(const dage_bubbles *in, double energy, dage_bubbles **out);
 
+/* Integral of a bubble set over all space (Bubbles_integrate_all,
+ * src/bubbles/bubbles.F90:3146-3240): 4 pi sum_atoms int r^(2+k) f_00(r) dr
+ * with the radial grids' LIP weights, on the GPU.  With dage_integrate of
+ * the cube this is Function3D_integrate (function3d.F90:1793-1840). */
+int dage_bubbles_integrate(const dage_bubbles *b, double *out);
+
 /* Copies the radial values of a bubble set (as given at creation: per atom,
  * (lmax+1)^2 functions of the atom's radial points) to host memory. */
 int dage_bubbles_get_f(const dage_bubbles *b, double *f);

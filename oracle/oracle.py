@@ -1433,3 +1433,10 @@ def bubbles_multiply_taylor(f1, lmax1, t1, f2, lmax2, t2):
     f1, f2 = np.asarray(f1, dtype=np.float64), np.asarray(f2, dtype=np.float64)
     u1, u2 = np.asarray(t1, dtype=np.float64)[:N1], np.asarray(t2, dtype=np.float64)[:N2]
     return bubbles_multiply(f1 + u1, lmax1, f2 + u2, lmax2) - bubbles_multiply(u1, lmax1, u2, lmax2)
+
+
+def bubbles_integrate(grids, f, k=0):
+    """Bubbles_integrate_all (bubbles.F90:3146-3240): 4 pi sum_A
+    int r^(2+k) f_A,00(r) dr with each radial grid's LIP weights."""
+    return float(sum(4.0 * np.pi * np.sum(g.weights() * (np.asarray(fa)[0] * g.points ** (2 + k)))
+                     for g, fa in zip(grids, f)))
