@@ -526,6 +526,8 @@ def run_gpu(args, world, rank, local):
             "gpu_launches": int(launches), "accuracy": accuracy, "energy": energy,
             "alternatives": alternative,
             "operator_build_ms": build_ms,
+            "schedule": ({"ring_stages": op.schedule[0], "tpoint_group": op.schedule[1]}
+                         if op.schedule else {"tiles": list(op.tiles)}),
         }
         print(json.dumps(line), flush=True)
 

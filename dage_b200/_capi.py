@@ -70,6 +70,8 @@ SIGNATURES = {
     "dage_op3d_get_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), _D]),
     "dage_op3d_destroy": (ctypes.c_int, [_VP]),
     "dage_op3d_tiles": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
+    "dage_op3d_mixed_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_int)]),
     "dage_op3d_create_cached": (ctypes.c_int, [ctypes.POINTER(DageGrid1D), ctypes.POINTER(DageGrid1D),
                                                ctypes.POINTER(DageQuad), ctypes.c_int, ctypes.c_char_p,
                                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_VP)]),

@@ -767,6 +767,7 @@ static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[
   DAGE_TRY(upload_weights(op));
   DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
   if (precision == DAGE_FP64) DAGE_TRY(tune_fp64(op));
+  else DAGE_TRY(mixed_tune(op));
   return 0;
 }
 
@@ -955,6 +956,12 @@ int dage_op3d_tiles(const dage_op3d *op, int tile_n[3]) {
   if (!op || !tile_n) return fail(DAGE_E_INVALID, "null argument");
   for (int d = 0; d < 3; ++d) tile_n[d] = op->precision == DAGE_FP64 ? op->tile_n[d] : 128;
   return 0;
+}
+
+int dage_op3d_mixed_schedule(const dage_op3d *op, int *ring_stages, int *tpoint_group) {
+  clear_error();
+  if (!op || !ring_stages || !tpoint_group) return fail(DAGE_E_INVALID, "null argument");
+  return mixed_schedule(op, ring_stages, tpoint_group);
 }
 
 int dage_op3d_destroy(dage_op3d *op) {

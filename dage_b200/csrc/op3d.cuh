@@ -101,6 +101,8 @@ int bubbles_inject_launch(const dage_bubbles *b, const double *xs, int nx, const
 int mixed_setup(dage_op3d *op);
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s);
 int mixed_set_weights(dage_op3d *op);
+int mixed_tune(dage_op3d *op);
+int mixed_schedule(const dage_op3d *op, int *ring_stages, int *group);
 void mixed_destroy(dage_op3d *op);
 
 }  // namespace dage

@@ -68,10 +68,12 @@
 
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "op3d.cuh"
 #include "tc_common.cuh"
+#include "tune.h"
 
 namespace dage {
 
@@ -845,7 +847,9 @@ int make_map(CUtensorMap *m, const void *base, long long inner, long long rows, 
 struct MixedState {
   bool f16 = false; // FP16 parts (fp16x3) instead of BF16
   int nparts = 2;   // BF16 parts per operand
-  int G = 1;        // t-points per pass of the last stage (slots of X[2])
+  int G = 1;        // t-points per pass of the last stage (used slots of X[2])
+  int Gmax = 1;     // allocated slots of X[2]
+  int ns = 6;       // TMA/MMA ring stages of the stage kernel (autotuned)
   DevBuf wdev;      // w_p as FP32 on the device
   long long ld[3];  // padded K extent of each stage's input rows
   long long rows[3];
@@ -949,7 +953,7 @@ int run_stages(dage_op3d *op, MixedState &st, const double *d_rho, double *d_V, 
   };
   // last-stage input: slot p % G of X[2], parts stored [part][slot][rows][ld]
   auto slot_plane = [&](int part, int slot) {
-    return plane(st.X[2], part, pe[2] * st.G) + (size_t)slot * pe[2];
+    return plane(st.X[2], part, pe[2] * st.Gmax) + (size_t)slot * pe[2];
   };
   int p0 = 0;  // first t-point of the open group
   for (int p = 0; p < op->P; ++p) {
@@ -1011,10 +1015,11 @@ int mixed_setup(dage_op3d *op) {
   st->rows[0] = (long long)niy * niz;
   st->rows[1] = (long long)niz * nox;
   st->rows[2] = (long long)nox * noy;
-  st->G = std::min(op->P, kMaxGroup);
+  st->G = st->Gmax = std::min(op->P, kMaxGroup);
+  st->ns = st->nparts == 3 ? 4 : 6;
   for (int s = 0; s < 3; ++s) {
     st->ld[s] = round_up(ni[s], 8);
-    const int slots = s == 2 ? st->G : 1;
+    const int slots = s == 2 ? st->Gmax : 1;
     const long long pe = st->rows[s] * st->ld[s] * slots;
     DAGE_TRY(st->X[s].alloc(sizeof(__nv_bfloat16) * pe * st->nparts));
     DAGE_CUDA_TRY(cudaMemsetAsync(st->X[s].ptr, 0, st->X[s].bytes, op->stream));
@@ -1081,9 +1086,15 @@ int mixed_set_weights(dage_op3d *op) {
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
   auto *st = static_cast<MixedState *>(op->mixed);
   if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
-  const int rc = st->f16 ? run_stages<2, 6, true>(op, *st, d_rho, d_V, s)
-                 : st->nparts == 2 ? run_stages<2, 6, false>(op, *st, d_rho, d_V, s)
-                                   : run_stages<3, 4, false>(op, *st, d_rho, d_V, s);
+  int rc;
+  if (st->f16)
+    rc = st->ns == 4 ? run_stages<2, 4, true>(op, *st, d_rho, d_V, s)
+                     : run_stages<2, 6, true>(op, *st, d_rho, d_V, s);
+  else if (st->nparts == 2)
+    rc = st->ns == 4 ? run_stages<2, 4, false>(op, *st, d_rho, d_V, s)
+                     : run_stages<2, 6, false>(op, *st, d_rho, d_V, s);
+  else
+    rc = run_stages<3, 4, false>(op, *st, d_rho, d_V, s);
   if (rc) return rc;
   int herr = 0;
   DAGE_CUDA_TRY(cudaMemcpyAsync(&herr, st->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1092,6 +1103,77 @@ int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s)
     cudaMemsetAsync(st->err.ptr, 0, sizeof(int), s);
     return fail(DAGE_E_TIMEOUT, "tensor-core stage kernel timed out waiting on an mbarrier");
   }
+  return 0;
+}
+
+namespace {
+__global__ void fill_kernel(double *x, size_t n, double v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+}  // namespace
+
+// Autotuner of the tensor-core path: ring depth of the stage kernel (4 or 6
+// TMA/MMA stages; bf16x6's three-part stages fit 4 only) and the t-points
+// summed per pass of the last stage (4 or 8), each candidate timed over
+// one apply of a scratch cube after one untimed apply; keyed on (device,
+// precision, points per axis, t-points) in the tune cache.
+int mixed_tune(dage_op3d *op) {
+  auto *st = static_cast<MixedState *>(op->mixed);
+  if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
+  std::string key = tune_device_key() + "/op3d_mixed" + std::to_string(op->precision) + "/";
+  for (int d = 0; d < 3; ++d) key += std::to_string(op->nin[d]) + "x" + std::to_string(op->nout[d]) + ",";
+  key += "P" + std::to_string(op->P);
+  std::vector<int> v;
+  if (tune_lookup(key, v) && v.size() == 2 && (v[0] == 4 || v[0] == 6) && v[1] >= 1 &&
+      v[1] <= st->Gmax && (st->nparts == 2 || v[0] == 4)) {
+    st->ns = v[0];
+    st->G = v[1];
+    return 0;
+  }
+  const size_t nin = (size_t)op->nin[0] * op->nin[1] * op->nin[2];
+  const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
+  TmpBuf rho, V;
+  DAGE_TRY(rho.alloc(sizeof(double) * nin));
+  DAGE_TRY(V.alloc(sizeof(double) * nout));
+  cudaStream_t s = op->stream;
+  fill_kernel<<<(int)std::min<size_t>((nin + 255) / 256, (size_t)sm_count() * 16), 256, 0, s>>>(
+      rho.as<double>(), nin, 1.0);
+  DAGE_CUDA_TRY(cudaGetLastError());
+  std::vector<int> nss = st->nparts == 2 ? std::vector<int>{6, 4} : std::vector<int>{4};
+  std::vector<int> gs = {st->Gmax};
+  if (st->Gmax > 4) gs.push_back(4);
+  int best_ns = st->ns, best_g = st->G;
+  float best = 0.0f;
+  for (int ns : nss)
+    for (int g : gs) {
+      st->ns = ns;
+      st->G = g;
+      DAGE_TRY(mixed_apply(op, rho.as<double>(), V.as<double>(), s));
+      DAGE_CUDA_TRY(cudaEventRecord(op->ev0, s));
+      DAGE_TRY(mixed_apply(op, rho.as<double>(), V.as<double>(), s));
+      DAGE_CUDA_TRY(cudaEventRecord(op->ev1, s));
+      DAGE_CUDA_TRY(cudaEventSynchronize(op->ev1));
+      float ms = 0.0f;
+      DAGE_CUDA_TRY(cudaEventElapsedTime(&ms, op->ev0, op->ev1));
+      if (best == 0.0f || ms < best) {
+        best = ms;
+        best_ns = ns;
+        best_g = g;
+      }
+    }
+  st->ns = best_ns;
+  st->G = best_g;
+  tune_store(key, {best_ns, best_g});
+  return 0;
+}
+
+int mixed_schedule(const dage_op3d *op, int *ring_stages, int *group) {
+  const auto *st = static_cast<const MixedState *>(op->mixed);
+  if (!st) return fail(DAGE_E_INVALID, "not a split-precision operator");
+  *ring_stages = st->ns;
+  *group = st->G;
   return 0;
 }
 

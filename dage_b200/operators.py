@@ -180,6 +180,17 @@ class Operator3D:
         check(load().dage_op3d_tiles(self._h, t))
         return tuple(t)
 
+    @property
+    def schedule(self):
+        """Split-precision operators: (ring stages, t-points per last-stage
+        pass) of the tensor-core stages as the autotuner chose them; None in
+        FP64."""
+        if self.precision == _capi.DAGE_FP64:
+            return None
+        ns, g = ctypes.c_int(), ctypes.c_int()
+        check(load().dage_op3d_mixed_schedule(self._h, ctypes.byref(ns), ctypes.byref(g)))
+        return ns.value, g.value
+
     # -- quadrature -------------------------------------------------------
     def quadrature(self):
         P = self.quad.npoints

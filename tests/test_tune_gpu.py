@@ -1,7 +1,8 @@
 """GPU tests of the autotuner and its cache: the FP64 cube operator's stage
-tile widths are timed once and stored under a key of the device, the points
-per axis and the quadrature count; a cache file is appended to, read back by
-a new process, and an entry in it decides the tiles without timing."""
+tile widths and the split-precision operator's tensor-core schedule are
+timed once and stored under a key of the device, the points per axis and the
+quadrature count; a cache file is appended to, read back by a new process,
+and an entry in it decides the choice without timing."""
 import os
 import subprocess
 import sys
@@ -82,3 +83,51 @@ def test_operator_cache_on_disk(dage, oracle, tmp_path):
     assert not c.from_cache and len(os.listdir(d)) == 2
     m = dage.Coulomb3D(g, quad=q, cache_dir=d, precision="fp16x3")  # mixed ops read it too
     assert m.from_cache
+
+
+MIXED_CHILD = r"""
+import sys
+import numpy as np
+sys.path.insert(0, {root!r})
+import dage_b200 as dage
+from oracle import oracle as O
+dage.set_tune_cache({path!r})
+g = dage.Grid3D.cube(-6.0, 10, 0.2)
+go = O.Grid3D.cube(-6.0, 10, 0.2)
+rho = O.gauss_cube(go, [1.0, 0.6], [1.5, 3.0], [[0.3, -0.2, 0.1], [-0.9, 0.8, 0.4]])
+op = dage.Coulomb3D(g, quad=dage.GaussQuad(10, 10), precision="fp16x3")
+V, E = op.apply(rho, energy=True)
+np.save({out!r}, np.concatenate([V.reshape(-1, order="F"), [E]]))
+print("SCHEDULE", *op.schedule)
+"""
+
+
+def _mixed_child(path, out):
+    r = subprocess.run([sys.executable, "-c", MIXED_CHILD.format(root=ROOT, path=path, out=out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = [l for l in r.stdout.splitlines() if l.startswith("SCHEDULE")][0]
+    return tuple(int(x) for x in line.split()[1:]), np.load(out)
+
+
+def test_mixed_schedule_tuned_and_forced(dage, oracle, tmp_path):
+    """The tensor-core schedule (ring stages, t-points per last-stage pass)
+    is timed once and cached; an edited entry forces another schedule in a
+    new process, and every schedule gives the same potential to the
+    split-precision bars (the ring depth changes no arithmetic, the group
+    only the order of the last stage's FP32 sums)."""
+    path = str(tmp_path / "tune.txt")
+    sched, ref = _mixed_child(path, str(tmp_path / "a.npy"))
+    assert sched[0] in (4, 6) and sched[1] in (4, 8)
+    key = [l for l in open(path).read().splitlines() if "/op3d_mixed3/61x61,61x61,61x61,P20" in l]
+    assert key
+    for forced in ((4, 4), (6, 8), (4, 8)):
+        with open(path, "a") as f:
+            f.write(key[-1].split()[0] + " %d %d\n" % forced)
+        got, res = _mixed_child(path, str(tmp_path / "b.npy"))
+        assert got == forced
+        V, Vr = res[:-1], ref[:-1]
+        assert np.abs(V - Vr).max() <= 2e-7 * np.abs(Vr).max()
+        assert abs(res[-1] - ref[-1]) <= 5e-8 * abs(ref[-1])
+        if forced[1] == sched[1]:
+            assert np.array_equal(res, ref)  # same group: identical sums
