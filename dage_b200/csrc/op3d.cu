@@ -786,6 +786,17 @@ static void destroy_impl(dage_op3d *op) {
   op->tmp1.release();
   op->tmp2.release();
   op->partials.release();
+  if (op->pipe_in) cudaStreamSynchronize(op->pipe_in);
+  if (op->pipe_out) cudaStreamSynchronize(op->pipe_out);
+  for (int k = 0; k < 2; ++k) {
+    op->pipe_rho[k].release();
+    op->pipe_V[k].release();
+    for (cudaEvent_t e : {op->pipe_h2d[k], op->pipe_comp[k], op->pipe_d2h[k]})
+      if (e) cudaEventDestroy(e);
+  }
+  op->pipe_res.release();
+  if (op->pipe_in) cudaStreamDestroy(op->pipe_in);
+  if (op->pipe_out) cudaStreamDestroy(op->pipe_out);
   for (cudaEvent_t e : op->tev) cudaEventDestroy(e);
   if (op->ev0) cudaEventDestroy(op->ev0);
   if (op->ev1) cudaEventDestroy(op->ev1);
@@ -1080,6 +1091,87 @@ int op3d_enqueue(dage_op3d *op, const double *rho, double *V, unsigned flags, do
   return 0;
 }
 
+// Host-pointer apply through the pipeline: the copy-in of this item (into
+// staging slot k) waits only for the compute that last read slot k, the
+// compute for its copy-in and for the copy-out that last read slot k, the
+// copy-out for the compute -- so item i's copies overlap items i-1's and
+// i+1's compute.  With pinned host memory the copies are asynchronous.
+int op3d_enqueue_piped(dage_op3d *op, const double *rho, double *V, unsigned flags,
+                       double *energy) {
+  if (!op || !rho || !V) return fail(DAGE_E_INVALID, "null argument");
+  if ((flags & DAGE_ENERGY) && !energy) return fail(DAGE_E_INVALID, "energy pointer is null");
+  const bool acc = (flags & DAGE_ACCUMULATE) != 0;
+  if (acc && op->precision != DAGE_FP64)
+    return fail(DAGE_E_UNSUPPORTED, "DAGE_ACCUMULATE with a mixed operator");
+  DAGE_CUDA_TRY(cudaSetDevice(op->device));
+  if (!op->pipe_in) {
+    DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_in, cudaStreamNonBlocking));
+    DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_out, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k)
+      for (cudaEvent_t *e : {&op->pipe_h2d[k], &op->pipe_comp[k], &op->pipe_d2h[k]})
+        DAGE_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    DAGE_TRY(op->pipe_res.alloc(sizeof(double) * 2));
+  }
+  const size_t nin = (size_t)op->nin[0] * op->nin[1] * op->nin[2];
+  const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
+  const int k = op->pipe_next++ & 1;
+  DAGE_TRY(op->pipe_rho[k].alloc(sizeof(double) * nin));
+  DAGE_TRY(op->pipe_V[k].alloc(sizeof(double) * nout));
+  double *d_rho = op->pipe_rho[k].as<double>(), *d_V = op->pipe_V[k].as<double>();
+  cudaStream_t s = op->stream;
+  if (!op->pipe_open) {
+    DAGE_CUDA_TRY(cudaEventRecord(op->ev0, op->pipe_in));
+    op->pipe_open = true;
+  }
+  // copy in
+  DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_in, op->pipe_comp[k], 0));
+  if (acc) DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_in, op->pipe_d2h[k], 0));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(d_rho, rho, sizeof(double) * nin, cudaMemcpyHostToDevice,
+                                op->pipe_in));
+  if (acc)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(d_V, V, sizeof(double) * nout, cudaMemcpyHostToDevice,
+                                  op->pipe_in));
+  DAGE_CUDA_TRY(cudaEventRecord(op->pipe_h2d[k], op->pipe_in));
+  // compute
+  DAGE_CUDA_TRY(cudaStreamWaitEvent(s, op->pipe_h2d[k], 0));
+  DAGE_CUDA_TRY(cudaStreamWaitEvent(s, op->pipe_d2h[k], 0));
+  if (op->precision == DAGE_FP64)
+    DAGE_TRY(apply_fp64(op, d_rho, d_V, acc));
+  else
+    DAGE_TRY(mixed_enqueue(op, d_rho, d_V, s));
+  const bool coda = op->same_grid && op->coda != 0.0 && !(flags & DAGE_NO_CODA);
+  double *d_res = (flags & DAGE_ENERGY) ? op->pipe_res.as<double>() + k : nullptr;
+  const int tf = op->tmark_begin(2);
+  DAGE_TRY(launch_finalize(d_rho, d_V, coda ? d_rho : nullptr, op->coda, op->wts[0].as<double>(),
+                           op->wts[1].as<double>(), op->wts[2].as<double>(), op->nout[0],
+                           op->nout[1], op->nout[2], op->partials.as<double>(),
+                           finalize_partials_count(), d_res, s));
+  op->tmark_end(tf);
+  DAGE_CUDA_TRY(cudaEventRecord(op->pipe_comp[k], s));
+  // copy out
+  DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_out, op->pipe_comp[k], 0));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * nout, cudaMemcpyDeviceToHost,
+                                op->pipe_out));
+  if (d_res)
+    DAGE_CUDA_TRY(cudaMemcpyAsync(energy, d_res, sizeof(double), cudaMemcpyDeviceToHost,
+                                  op->pipe_out));
+  DAGE_CUDA_TRY(cudaEventRecord(op->pipe_d2h[k], op->pipe_out));
+  DAGE_CUDA_TRY(cudaEventRecord(op->ev1, op->pipe_out));
+  return 0;
+}
+
+int op3d_pipe_finish(dage_op3d *op) {
+  DAGE_CUDA_TRY(cudaSetDevice(op->device));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(op->pipe_out));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
+  DAGE_CUDA_TRY(cudaStreamSynchronize(op->pipe_in));
+  op->pipe_open = false;
+  DAGE_CUDA_TRY(cudaEventElapsedTime(&op->last_ms, op->ev0, op->ev1));
+  DAGE_TRY(op->tcollect());
+  if (op->precision != DAGE_FP64) DAGE_TRY(mixed_check(op, op->stream));
+  return 0;
+}
+
 int op3d_finish(dage_op3d *op) {
   DAGE_CUDA_TRY(cudaSetDevice(op->device));
   DAGE_CUDA_TRY(cudaStreamSynchronize(op->stream));
@@ -1102,15 +1194,22 @@ int dage_op3d_apply_batched(int n, dage_op3d *const *ops, const double *const *r
   if (n < 0 || (n > 0 && (!ops || !rho || !V))) return fail(DAGE_E_INVALID, "null argument");
   if ((flags & DAGE_ENERGY) && n > 0 && !energies)
     return fail(DAGE_E_INVALID, "energies pointer is null");
-  for (int i = 0; i < n; ++i)
-    DAGE_TRY(op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr));
-  // one wait per distinct operator, after everything is queued
+  // host pointers go through each operator's copy/compute pipeline
+  const bool piped = !(flags & DAGE_DEVICE_PTRS);
+  int rc = 0;
+  for (int i = 0; i < n && !rc; ++i)
+    rc = piped ? op3d_enqueue_piped(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr)
+               : op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr);
+  // one wait per distinct operator, after everything is queued (also after
+  // a failed enqueue: nothing queued is left running)
   for (int i = 0; i < n; ++i) {
     bool seen = false;
     for (int j = 0; j < i && !seen; ++j) seen = ops[j] == ops[i];
-    if (!seen) DAGE_TRY(op3d_finish(ops[i]));
+    if (seen || !ops[i]) continue;
+    const int r = piped ? (ops[i]->pipe_open ? op3d_pipe_finish(ops[i]) : 0) : op3d_finish(ops[i]);
+    if (!rc) rc = r;
   }
-  return 0;
+  return rc;
 }
 
 int dage_op3d_set_timing(dage_op3d *op, int enable) {

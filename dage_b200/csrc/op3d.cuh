@@ -55,6 +55,16 @@ struct dage_op3d {
   void tmark_end(int slot);
   int tcollect();                        // after stream sync
 
+  // pipelined host-pointer applies (dage_op3d_apply_batched): two staging
+  // slots, copy-in and copy-out streams beside the compute stream, per-slot
+  // events ordering copy-in -> compute -> copy-out and the slots' reuse
+  dage::DevBuf pipe_rho[2], pipe_V[2], pipe_res;
+  cudaStream_t pipe_in = nullptr, pipe_out = nullptr;
+  cudaEvent_t pipe_h2d[2] = {nullptr, nullptr}, pipe_comp[2] = {nullptr, nullptr},
+              pipe_d2h[2] = {nullptr, nullptr};
+  int pipe_next = 0;
+  bool pipe_open = false;  // items queued since the last pipeline wait
+
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -100,6 +110,10 @@ int bubbles_inject_launch(const dage_bubbles *b, const double *xs, int nx, const
 // mixed-precision path (op3d_mixed.cu)
 int mixed_setup(dage_op3d *op);
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s);
+// the same in two halves: the launches, then (after any further work on s)
+// the wait and the check of the kernels' timeout flag
+int mixed_enqueue(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s);
+int mixed_check(dage_op3d *op, cudaStream_t s);
 int mixed_set_weights(dage_op3d *op);
 int mixed_tune(dage_op3d *op);
 int mixed_schedule(const dage_op3d *op, int *ring_stages, int *group);

@@ -1084,6 +1084,11 @@ int mixed_set_weights(dage_op3d *op) {
 }
 
 int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
+  DAGE_TRY(mixed_enqueue(op, d_rho, d_V, s));
+  return mixed_check(op, s);
+}
+
+int mixed_enqueue(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s) {
   auto *st = static_cast<MixedState *>(op->mixed);
   if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
   int rc;
@@ -1095,7 +1100,12 @@ int mixed_apply(dage_op3d *op, const double *d_rho, double *d_V, cudaStream_t s)
                      : run_stages<2, 6, false>(op, *st, d_rho, d_V, s);
   else
     rc = run_stages<3, 4, false>(op, *st, d_rho, d_V, s);
-  if (rc) return rc;
+  return rc;
+}
+
+int mixed_check(dage_op3d *op, cudaStream_t s) {
+  auto *st = static_cast<MixedState *>(op->mixed);
+  if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
   int herr = 0;
   DAGE_CUDA_TRY(cudaMemcpyAsync(&herr, st->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
   DAGE_CUDA_TRY(cudaStreamSynchronize(s));

@@ -103,10 +103,15 @@ int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
 
 /* n applies queued back to back (each as dage_op3d_apply with the same
  * flags) on their operators' streams, with one wait per distinct operator at
- * the end: applies on distinct operators overlap.  energies[i] receives apply
- * i's energy with DAGE_ENERGY.  An operator's last_time_ms covers its last
- * apply of the batch.  Replaces the per-orbital loop of operate calls with
- * Operator3D_transform_cuda_cube (src/bubbles/function3d.F90:4354-4480). */
+ * the end: applies on distinct operators overlap.  With host pointers each
+ * operator pipelines its applies through two device staging slots and
+ * copy-in/copy-out streams, so one density's copies overlap the neighbouring
+ * densities' compute (asynchronously when the host arrays are pinned).
+ * energies[i] receives apply i's energy with DAGE_ENERGY.  An operator's
+ * last_time_ms covers its last apply of the batch (host pointers: the whole
+ * pipeline, first copy-in to last copy-out).  Replaces the per-orbital loop
+ * of operate calls with Operator3D_transform_cuda_cube
+ * (src/bubbles/function3d.F90:4354-4480). */
 int dage_op3d_apply_batched(int n, dage_op3d *const *ops, const double *const *rho,
                             double *const *V, unsigned flags, double *energies);
 

@@ -238,6 +238,36 @@ def test_invalid_arguments_raise(dage):
         op.apply(np.zeros((3, 3, 3), order="F"))
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp16x3"])
+def test_pipelined_host_batch_matches_single_applies(dage, oracle, prec):
+    """Host cubes through the batched call's copy/compute pipeline: seven
+    densities on one operator (both staging slots reused three times), from
+    pinned and from pageable memory, equal to one apply each, bit for bit."""
+    import torch
+
+    g = dage.Grid3D.cube(-3.6, 6, 0.2)
+    go = oracle.Grid3D.cube(-3.6, 6, 0.2)
+    op = dage.Coulomb3D(g, quad=dage.GaussQuad(8, 8), precision=prec)
+    rng = np.random.default_rng(5)
+    rhos = [oracle.gauss_cube(go, rng.uniform(0.5, 2, 2), rng.uniform(0.5, 4, 2),
+                              rng.uniform(-1, 1, (2, 3))) for _ in range(7)]
+    want = [op.apply(r, energy=True) for r in rhos]
+    n = go.shape[0]
+
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        t.copy_(torch.from_numpy(a.reshape(-1, order="F").copy()))
+        return t.numpy().reshape(n, n, n).T
+
+    for host in ("pinned", "pageable"):
+        ins = [pinned(r) if host == "pinned" else r for r in rhos]
+        outs = [pinned(np.zeros(go.shape, order="F")) if host == "pinned"
+                else np.zeros(go.shape, order="F") for _ in rhos]
+        E = dage.apply_batched([op] * 7, ins, outs, energy=True)
+        for (Vw, Ew), V, e in zip(want, outs, E):
+            assert np.array_equal(np.asarray(V), Vw) and e == Ew, host
+
+
 def test_apply_batched_matches_single_applies(dage, oracle):
     """Several densities through two operators (FP64 and split precision) in
     one batched call, device and host cubes, equal to one apply each."""
