@@ -1091,18 +1091,16 @@ int op3d_enqueue(dage_op3d *op, const double *rho, double *V, unsigned flags, do
   return 0;
 }
 
-// Host-pointer apply through the pipeline: the copy-in of this item (into
-// staging slot k) waits only for the compute that last read slot k, the
+// Host-pointer applies through a pipeline: two device staging slots per
+// operator and copy-in / copy-out streams beside the compute stream.  The
+// copy-in into slot k waits for the compute that last read slot k, the
 // compute for its copy-in and for the copy-out that last read slot k, the
-// copy-out for the compute -- so item i's copies overlap items i-1's and
-// i+1's compute.  With pinned host memory the copies are asynchronous.
-int op3d_enqueue_piped(dage_op3d *op, const double *rho, double *V, unsigned flags,
-                       double *energy) {
-  if (!op || !rho || !V) return fail(DAGE_E_INVALID, "null argument");
-  if ((flags & DAGE_ENERGY) && !energy) return fail(DAGE_E_INVALID, "energy pointer is null");
-  const bool acc = (flags & DAGE_ACCUMULATE) != 0;
-  if (acc && op->precision != DAGE_FP64)
-    return fail(DAGE_E_UNSUPPORTED, "DAGE_ACCUMULATE with a mixed operator");
+// copy-out for the compute.  An apply queues ~20 launches per t-point, more
+// than the launch queue holds, so the host blocks while queueing a compute;
+// each copy-in is therefore issued two applies ahead, right after the
+// compute that frees its slot, and runs during the next compute.  With
+// pinned host memory the copies are asynchronous.
+int pipe_open(dage_op3d *op) {
   DAGE_CUDA_TRY(cudaSetDevice(op->device));
   if (!op->pipe_in) {
     DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_in, cudaStreamNonBlocking));
@@ -1114,25 +1112,34 @@ int op3d_enqueue_piped(dage_op3d *op, const double *rho, double *V, unsigned fla
   }
   const size_t nin = (size_t)op->nin[0] * op->nin[1] * op->nin[2];
   const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
-  const int k = op->pipe_next++ & 1;
-  DAGE_TRY(op->pipe_rho[k].alloc(sizeof(double) * nin));
-  DAGE_TRY(op->pipe_V[k].alloc(sizeof(double) * nout));
-  double *d_rho = op->pipe_rho[k].as<double>(), *d_V = op->pipe_V[k].as<double>();
-  cudaStream_t s = op->stream;
-  if (!op->pipe_open) {
-    DAGE_CUDA_TRY(cudaEventRecord(op->ev0, op->pipe_in));
-    op->pipe_open = true;
+  for (int k = 0; k < 2; ++k) {
+    DAGE_TRY(op->pipe_rho[k].alloc(sizeof(double) * nin));
+    DAGE_TRY(op->pipe_V[k].alloc(sizeof(double) * nout));
   }
-  // copy in
+  DAGE_CUDA_TRY(cudaEventRecord(op->ev0, op->pipe_in));
+  op->pipe_open = true;
+  return 0;
+}
+
+int pipe_copy_in(dage_op3d *op, int k, const double *rho, const double *V, bool acc) {
+  const size_t nin = (size_t)op->nin[0] * op->nin[1] * op->nin[2];
+  const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
   DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_in, op->pipe_comp[k], 0));
   if (acc) DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_in, op->pipe_d2h[k], 0));
-  DAGE_CUDA_TRY(cudaMemcpyAsync(d_rho, rho, sizeof(double) * nin, cudaMemcpyHostToDevice,
-                                op->pipe_in));
+  DAGE_CUDA_TRY(cudaMemcpyAsync(op->pipe_rho[k].ptr, rho, sizeof(double) * nin,
+                                cudaMemcpyHostToDevice, op->pipe_in));
   if (acc)
-    DAGE_CUDA_TRY(cudaMemcpyAsync(d_V, V, sizeof(double) * nout, cudaMemcpyHostToDevice,
-                                  op->pipe_in));
+    DAGE_CUDA_TRY(cudaMemcpyAsync(op->pipe_V[k].ptr, V, sizeof(double) * nout,
+                                  cudaMemcpyHostToDevice, op->pipe_in));
   DAGE_CUDA_TRY(cudaEventRecord(op->pipe_h2d[k], op->pipe_in));
-  // compute
+  return 0;
+}
+
+int pipe_compute_out(dage_op3d *op, int k, double *V, unsigned flags, double *energy) {
+  const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
+  const bool acc = (flags & DAGE_ACCUMULATE) != 0;
+  double *d_rho = op->pipe_rho[k].as<double>(), *d_V = op->pipe_V[k].as<double>();
+  cudaStream_t s = op->stream;
   DAGE_CUDA_TRY(cudaStreamWaitEvent(s, op->pipe_h2d[k], 0));
   DAGE_CUDA_TRY(cudaStreamWaitEvent(s, op->pipe_d2h[k], 0));
   if (op->precision == DAGE_FP64)
@@ -1148,7 +1155,6 @@ int op3d_enqueue_piped(dage_op3d *op, const double *rho, double *V, unsigned fla
                            finalize_partials_count(), d_res, s));
   op->tmark_end(tf);
   DAGE_CUDA_TRY(cudaEventRecord(op->pipe_comp[k], s));
-  // copy out
   DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_out, op->pipe_comp[k], 0));
   DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * nout, cudaMemcpyDeviceToHost,
                                 op->pipe_out));
@@ -1157,6 +1163,37 @@ int op3d_enqueue_piped(dage_op3d *op, const double *rho, double *V, unsigned fla
                                   op->pipe_out));
   DAGE_CUDA_TRY(cudaEventRecord(op->pipe_d2h[k], op->pipe_out));
   DAGE_CUDA_TRY(cudaEventRecord(op->ev1, op->pipe_out));
+  return 0;
+}
+
+// The batch's host-pointer applies: per operator its applies in order,
+// slot = position % 2; first copy-ins of every operator, then per apply
+// its compute and copy-out followed by the copy-in two places later.
+int pipe_batch(int n, dage_op3d *const *ops, const double *const *rho, double *const *V,
+               unsigned flags, double *energies) {
+  const bool acc = (flags & DAGE_ACCUMULATE) != 0;
+  std::vector<int> pos(n), later(n, -1);  // position in its operator's list; item 2 later
+  std::vector<std::pair<dage_op3d *, std::vector<int>>> lists;
+  for (int i = 0; i < n; ++i) {
+    if (!ops[i] || !rho[i] || !V[i]) return fail(DAGE_E_INVALID, "null argument");
+    if (acc && ops[i]->precision != DAGE_FP64)
+      return fail(DAGE_E_UNSUPPORTED, "DAGE_ACCUMULATE with a mixed operator");
+    size_t l = 0;
+    while (l < lists.size() && lists[l].first != ops[i]) ++l;
+    if (l == lists.size()) lists.push_back({ops[i], {}});
+    std::vector<int> &v = lists[l].second;
+    pos[i] = (int)v.size();
+    if (v.size() >= 2) later[v[v.size() - 2]] = i;
+    v.push_back(i);
+  }
+  for (auto &l : lists) DAGE_TRY(pipe_open(l.first));
+  for (int i = 0; i < n; ++i)
+    if (pos[i] < 2) DAGE_TRY(pipe_copy_in(ops[i], pos[i] & 1, rho[i], V[i], acc));
+  for (int i = 0; i < n; ++i) {
+    DAGE_TRY(pipe_compute_out(ops[i], pos[i] & 1, V[i], flags, energies ? energies + i : nullptr));
+    const int j = later[i];
+    if (j >= 0) DAGE_TRY(pipe_copy_in(ops[j], pos[j] & 1, rho[j], V[j], acc));
+  }
   return 0;
 }
 
@@ -1197,9 +1234,11 @@ int dage_op3d_apply_batched(int n, dage_op3d *const *ops, const double *const *r
   // host pointers go through each operator's copy/compute pipeline
   const bool piped = !(flags & DAGE_DEVICE_PTRS);
   int rc = 0;
-  for (int i = 0; i < n && !rc; ++i)
-    rc = piped ? op3d_enqueue_piped(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr)
-               : op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr);
+  if (piped)
+    rc = pipe_batch(n, ops, rho, V, flags, energies);
+  else
+    for (int i = 0; i < n && !rc; ++i)
+      rc = op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr);
   // one wait per distinct operator, after everything is queued (also after
   // a failed enqueue: nothing queued is left running)
   for (int i = 0; i < n; ++i) {

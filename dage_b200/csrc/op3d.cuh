@@ -62,8 +62,7 @@ struct dage_op3d {
   cudaStream_t pipe_in = nullptr, pipe_out = nullptr;
   cudaEvent_t pipe_h2d[2] = {nullptr, nullptr}, pipe_comp[2] = {nullptr, nullptr},
               pipe_d2h[2] = {nullptr, nullptr};
-  int pipe_next = 0;
-  bool pipe_open = false;  // items queued since the last pipeline wait
+  bool pipe_open = false;  // applies queued since the last pipeline wait
 
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
