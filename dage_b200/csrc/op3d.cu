@@ -751,7 +751,11 @@ static int create_impl(const dage_grid1d grid_in[3], const dage_grid1d grid_out[
   }
   op->same_grid = same_axis(op->in[0], op->out[0]) && same_axis(op->in[1], op->out[1]) &&
                   same_axis(op->in[2], op->out[2]);
+  // the compute stream and the host-pointer pipeline's copy-in and copy-out
+  // streams
   DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->own_stream, cudaStreamNonBlocking));
+  DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_in, cudaStreamNonBlocking));
+  DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_out, cudaStreamNonBlocking));
   op->stream = op->own_stream;
   DAGE_CUDA_TRY(cudaEventCreate(&op->ev0));
   DAGE_CUDA_TRY(cudaEventCreate(&op->ev1));
@@ -794,7 +798,6 @@ static void destroy_impl(dage_op3d *op) {
     for (cudaEvent_t e : {op->pipe_h2d[k], op->pipe_comp[k], op->pipe_d2h[k]})
       if (e) cudaEventDestroy(e);
   }
-  op->pipe_res.release();
   if (op->pipe_in) cudaStreamDestroy(op->pipe_in);
   if (op->pipe_out) cudaStreamDestroy(op->pipe_out);
   for (cudaEvent_t e : op->tev) cudaEventDestroy(e);
@@ -1095,20 +1098,16 @@ int op3d_enqueue(dage_op3d *op, const double *rho, double *V, unsigned flags, do
 // operator and copy-in / copy-out streams beside the compute stream.  The
 // copy-in into slot k waits for the compute that last read slot k, the
 // compute for its copy-in and for the copy-out that last read slot k, the
-// copy-out for the compute.  An apply queues ~20 launches per t-point, more
-// than the launch queue holds, so the host blocks while queueing a compute;
-// each copy-in is therefore issued two applies ahead, right after the
-// compute that frees its slot, and runs during the next compute.  With
-// pinned host memory the copies are asynchronous.
+// copy-out for the compute.  Each copy-in is issued two applies ahead, right
+// after the compute that frees its slot, so it is queued before the next
+// compute and runs beside it.  With pinned host memory the copies are
+// asynchronous (a pageable array makes the host wait for its copy).
 int pipe_open(dage_op3d *op) {
   DAGE_CUDA_TRY(cudaSetDevice(op->device));
-  if (!op->pipe_in) {
-    DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_in, cudaStreamNonBlocking));
-    DAGE_CUDA_TRY(cudaStreamCreateWithFlags(&op->pipe_out, cudaStreamNonBlocking));
+  if (!op->pipe_h2d[0]) {
     for (int k = 0; k < 2; ++k)
       for (cudaEvent_t *e : {&op->pipe_h2d[k], &op->pipe_comp[k], &op->pipe_d2h[k]})
         DAGE_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    DAGE_TRY(op->pipe_res.alloc(sizeof(double) * 2));
   }
   const size_t nin = (size_t)op->nin[0] * op->nin[1] * op->nin[2];
   const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
@@ -1135,7 +1134,8 @@ int pipe_copy_in(dage_op3d *op, int k, const double *rho, const double *V, bool 
   return 0;
 }
 
-int pipe_compute_out(dage_op3d *op, int k, double *V, unsigned flags, double *energy) {
+// d_energy: device pointer (or null) for the apply's energy
+int pipe_compute_out(dage_op3d *op, int k, double *V, unsigned flags, double *d_energy) {
   const size_t nout = (size_t)op->nout[0] * op->nout[1] * op->nout[2];
   const bool acc = (flags & DAGE_ACCUMULATE) != 0;
   double *d_rho = op->pipe_rho[k].as<double>(), *d_V = op->pipe_V[k].as<double>();
@@ -1147,20 +1147,16 @@ int pipe_compute_out(dage_op3d *op, int k, double *V, unsigned flags, double *en
   else
     DAGE_TRY(mixed_enqueue(op, d_rho, d_V, s));
   const bool coda = op->same_grid && op->coda != 0.0 && !(flags & DAGE_NO_CODA);
-  double *d_res = (flags & DAGE_ENERGY) ? op->pipe_res.as<double>() + k : nullptr;
   const int tf = op->tmark_begin(2);
   DAGE_TRY(launch_finalize(d_rho, d_V, coda ? d_rho : nullptr, op->coda, op->wts[0].as<double>(),
                            op->wts[1].as<double>(), op->wts[2].as<double>(), op->nout[0],
                            op->nout[1], op->nout[2], op->partials.as<double>(),
-                           finalize_partials_count(), d_res, s));
+                           finalize_partials_count(), d_energy, s));
   op->tmark_end(tf);
   DAGE_CUDA_TRY(cudaEventRecord(op->pipe_comp[k], s));
   DAGE_CUDA_TRY(cudaStreamWaitEvent(op->pipe_out, op->pipe_comp[k], 0));
   DAGE_CUDA_TRY(cudaMemcpyAsync(V, d_V, sizeof(double) * nout, cudaMemcpyDeviceToHost,
                                 op->pipe_out));
-  if (d_res)
-    DAGE_CUDA_TRY(cudaMemcpyAsync(energy, d_res, sizeof(double), cudaMemcpyDeviceToHost,
-                                  op->pipe_out));
   DAGE_CUDA_TRY(cudaEventRecord(op->pipe_d2h[k], op->pipe_out));
   DAGE_CUDA_TRY(cudaEventRecord(op->ev1, op->pipe_out));
   return 0;
@@ -1168,9 +1164,12 @@ int pipe_compute_out(dage_op3d *op, int k, double *V, unsigned flags, double *en
 
 // The batch's host-pointer applies: per operator its applies in order,
 // slot = position % 2; first copy-ins of every operator, then per apply
-// its compute and copy-out followed by the copy-in two places later.
-int pipe_batch(int n, dage_op3d *const *ops, const double *const *rho, double *const *V,
-               unsigned flags, double *energies) {
+// its compute and copy-out followed by the copy-in two places later; then
+// one wait per operator.  The energies stay on the device until the end: a
+// copy into pageable host memory would block the host behind the copy-out
+// queued before it.
+int pipe_batch_enqueue(int n, dage_op3d *const *ops, const double *const *rho, double *const *V,
+                       unsigned flags, double *d_energies) {
   const bool acc = (flags & DAGE_ACCUMULATE) != 0;
   std::vector<int> pos(n), later(n, -1);  // position in its operator's list; item 2 later
   std::vector<std::pair<dage_op3d *, std::vector<int>>> lists;
@@ -1190,11 +1189,33 @@ int pipe_batch(int n, dage_op3d *const *ops, const double *const *rho, double *c
   for (int i = 0; i < n; ++i)
     if (pos[i] < 2) DAGE_TRY(pipe_copy_in(ops[i], pos[i] & 1, rho[i], V[i], acc));
   for (int i = 0; i < n; ++i) {
-    DAGE_TRY(pipe_compute_out(ops[i], pos[i] & 1, V[i], flags, energies ? energies + i : nullptr));
+    DAGE_TRY(pipe_compute_out(ops[i], pos[i] & 1, V[i], flags,
+                              d_energies ? d_energies + i : nullptr));
     const int j = later[i];
     if (j >= 0) DAGE_TRY(pipe_copy_in(ops[j], pos[j] & 1, rho[j], V[j], acc));
   }
   return 0;
+}
+
+int op3d_pipe_finish(dage_op3d *op);
+
+int pipe_batch(int n, dage_op3d *const *ops, const double *const *rho, double *const *V,
+               unsigned flags, double *energies) {
+  TmpBuf d_e;
+  if ((flags & DAGE_ENERGY) && n > 0) DAGE_TRY(d_e.alloc(sizeof(double) * n));
+  int rc = pipe_batch_enqueue(n, ops, rho, V, flags, d_e.as<double>());
+  // one wait per distinct operator (also after a failed enqueue: nothing
+  // queued is left running)
+  for (int i = 0; i < n; ++i) {
+    bool seen = false;
+    for (int j = 0; j < i && !seen; ++j) seen = ops[j] == ops[i];
+    if (seen || !ops[i] || !ops[i]->pipe_open) continue;
+    const int r = op3d_pipe_finish(ops[i]);
+    if (!rc) rc = r;
+  }
+  if (!rc && d_e.ptr)
+    DAGE_CUDA_TRY(cudaMemcpy(energies, d_e.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  return rc;
 }
 
 int op3d_pipe_finish(dage_op3d *op) {
@@ -1232,20 +1253,17 @@ int dage_op3d_apply_batched(int n, dage_op3d *const *ops, const double *const *r
   if ((flags & DAGE_ENERGY) && n > 0 && !energies)
     return fail(DAGE_E_INVALID, "energies pointer is null");
   // host pointers go through each operator's copy/compute pipeline
-  const bool piped = !(flags & DAGE_DEVICE_PTRS);
+  if (!(flags & DAGE_DEVICE_PTRS)) return pipe_batch(n, ops, rho, V, flags, energies);
   int rc = 0;
-  if (piped)
-    rc = pipe_batch(n, ops, rho, V, flags, energies);
-  else
-    for (int i = 0; i < n && !rc; ++i)
-      rc = op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr);
+  for (int i = 0; i < n && !rc; ++i)
+    rc = op3d_enqueue(ops[i], rho[i], V[i], flags, energies ? energies + i : nullptr);
   // one wait per distinct operator, after everything is queued (also after
   // a failed enqueue: nothing queued is left running)
   for (int i = 0; i < n; ++i) {
     bool seen = false;
     for (int j = 0; j < i && !seen; ++j) seen = ops[j] == ops[i];
     if (seen || !ops[i]) continue;
-    const int r = piped ? (ops[i]->pipe_open ? op3d_pipe_finish(ops[i]) : 0) : op3d_finish(ops[i]);
+    const int r = op3d_finish(ops[i]);
     if (!rc) rc = r;
   }
   return rc;

@@ -58,7 +58,7 @@ struct dage_op3d {
   // pipelined host-pointer applies (dage_op3d_apply_batched): two staging
   // slots, copy-in and copy-out streams beside the compute stream, per-slot
   // events ordering copy-in -> compute -> copy-out and the slots' reuse
-  dage::DevBuf pipe_rho[2], pipe_V[2], pipe_res;
+  dage::DevBuf pipe_rho[2], pipe_V[2];
   cudaStream_t pipe_in = nullptr, pipe_out = nullptr;
   cudaEvent_t pipe_h2d[2] = {nullptr, nullptr}, pipe_comp[2] = {nullptr, nullptr},
               pipe_d2h[2] = {nullptr, nullptr};
