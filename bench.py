@@ -292,7 +292,7 @@ def run_e2e(op, rho, n, npts, world, args):
     rho_h.copy_(rho.cpu())
     fview = lambda t: t.numpy().reshape(n, n, n).T  # Fortran-ordered (x, y, z) view
     rho_np, V_np, V2_np = fview(rho_h), fview(V_h), fview(V2_h)
-    e2e_steps = max(2, min(args.steps, 8))
+    e2e_steps = max(2, min(2 * args.steps, 16))
     # sequential: one dage_op3d_apply per step
     op.apply(rho_np, out=V_np, energy=True)
     barrier(world)
