@@ -48,12 +48,12 @@ def test_bubble_contaminants_match_oracle(dage, oracle, lmax, k, tmax, natom, rm
         assert np.all(got[3] == 0.0)
 
 
-@pytest.mark.parametrize("tmax", [0, 2, 3])
-def test_cube_contaminants_match_oracle(dage, oracle, tmax):
+@pytest.mark.parametrize("tmax,gtype", [(0, 1), (2, 1), (3, 1), (2, 2)])  # 2: Gauss-Lobatto cells
+def test_cube_contaminants_match_oracle(dage, oracle, tmax, gtype):
     import torch
 
-    g = dage.Grid3D.cube(-3.0, 6, 0.2)
-    go = oracle.Grid3D.cube(-3.0, 6, 0.2)
+    g = dage.Grid3D.cube(-3.0, 6, 0.2, grid_type=gtype)
+    go = oracle.Grid3D.cube(-3.0, 6, 0.2, grid_type=gtype)
     cube = np.asfortranarray(np.random.default_rng(tmax).standard_normal(go.shape))
     # inside, on a cell boundary, on the last point, outside
     cen = np.array([[0.13, -0.41, 0.57], [0.6, 1.8, -0.6], [4.2, 4.2, 4.2], [5.0, 0.0, 0.0]])
