@@ -748,12 +748,34 @@ def run_workload(args, world, rank, local):
 
         ms_unfused = _timed(unfused, max(1, args.steps // 2), 1, sync)
         err = float((t1 - out).abs().max() / out.abs().max())
+        # the cusp form of the same product (Function3D_multiply_bubbles with
+        # Taylor series, order 2): contaminants of both factors (other atoms'
+        # bubbles and the cube), Taylor bubbles, their product, then the cube
+        # product with those result bubbles
+        def taylor_setup():
+            ta = b1.taylor_series(gcube, c1, 2)
+            tb = b2.taylor_series(gcube, c2, 2)
+            return b1.multiply_taylor(b2, ta, tb)
+
+        brt = taylor_setup()
+        sync()
+        reps = max(1, args.steps // 2)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            brt = taylor_setup()
+        sync()
+        setup_ms = (time.perf_counter() - t0) * 1e3 / reps
+        ms_cusp = _timed(lambda: dage.multiply(gcube, c1, c2, b1, b2, brt, out=t2),
+                         max(1, args.steps // 2), 1, sync)
         _line(args, world, "Function3D product Mpts/s @301^3 (20 atoms, bubbles lmax 2 x 2 -> 4)",
               n / ms / 1e3, "Mpts/s", ms, "f64",
               {"workload": wl, "points_per_axis": 301, "step_bohr": 0.1, "atoms": 20,
                "lmax": [2, 2, 4], "radial_points": 199, "seed": SEED}, clocks, 1,
               {"hbm_GBps": 24.0 * n / ms / 1e6,
-               "separate_passes": {"ms": ms_unfused, "launches": 4, "max_rel_diff": err}})
+               "separate_passes": {"ms": ms_unfused, "launches": 4, "max_rel_diff": err},
+               "taylor_cusp": {"setup_ms": setup_ms, "product_ms": ms_cusp, "taylor_order": 2,
+                               "setup": "contaminants (bubbles + cube) and Taylor bubbles of "
+                                        "both factors, option-(1) bubble product; host calls"}})
     elif wl in ("gbfmm_batch_256", "helmholtz_step_301"):
         rng = np.random.default_rng(SEED)
         if wl == "gbfmm_batch_256":
