@@ -183,3 +183,38 @@ def test_taylor_refusals(dage, oracle):
     t = b.taylor_series(tmax=2)
     with pytest.raises(dage.DageError):
         b.multiply_taylor(other, t, t)
+
+
+def test_single_atom_and_high_lmax(dage, oracle):
+    """One atom has no other atoms to contaminate it (zero contaminants, and
+    the Taylor bubbles of the bubbles alone vanish); lmax 6 bubbles with
+    tmax 3 exercise the harmonic recursion on jets up to l = 6."""
+    centers, g, h, f = _set(oracle, 2, 81, natom=1)
+    b = _gpu(dage, centers, h, f, 2)
+    assert np.all(b.contaminants(3) == 0.0)
+    t = b.taylor_series(tmax=2)
+    assert all(np.all(v == 0.0) for v in t.radial_values())
+    centers, g, h, f = _set(oracle, 6, 82, natom=3)
+    b = _gpu(dage, centers, h, f, 6)
+    got = b.contaminants(3)
+    ref = oracle.bubble_contaminants(centers, [g] * 3, 6, f, 0, 3)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_multiply_taylor_complete_table(dage, oracle):
+    """DAGE_PRODUCT_COMPLETE in the Taylor product: the plain complete product
+    plus the complete products with the Taylor sets (bilinearity)."""
+    centers, g, h, f1 = _set(oracle, 2, 91, 3)
+    _, _, _, f2 = _set(oracle, 1, 92, 3)
+    b1, b2 = _gpu(dage, centers, h, f1, 2), _gpu(dage, centers, h, f2, 1)
+    t1, t2 = b1.taylor_series(tmax=2), b2.taylor_series(tmax=2)
+    p = b1.multiply_taylor(b2, t1, t2, complete=True).radial_values()
+    q = b1.multiply(b2, complete=True).radial_values()
+    tv1, tv2 = t1.radial_values(), t2.radial_values()
+    c1 = dage.Bubbles(centers, [dage.Grid1D(0.0, 33, 7, 1, h)] * 3, [v[:9] for v in tv1], 2)
+    c2 = dage.Bubbles(centers, [dage.Grid1D(0.0, 33, 7, 1, h)] * 3, [v[:4] for v in tv2], 1)
+    r1 = b1.multiply(c2, complete=True).radial_values()
+    r2 = c1.multiply(b2, complete=True).radial_values()
+    for a in range(3):
+        ref = q[a] + r1[a] + r2[a]
+        assert np.abs(p[a] - ref).max() <= 1e-13 * np.abs(ref).max()
