@@ -28,29 +28,44 @@ namespace {
 
 constexpr int kMaxAtomsSmem = 256;
 
+// Two points' values side by side: the harmonics recursion below runs on
+// both at once, each lane of the pair with exactly the single-point
+// arithmetic.
+struct Pair {
+  double a, b;
+  __device__ Pair() {}
+  __device__ Pair(double v) : a(v), b(v) {}
+  __device__ Pair(double x, double y) : a(x), b(y) {}
+};
+__device__ __forceinline__ Pair operator*(Pair x, Pair y) { return Pair(x.a * y.a, x.b * y.b); }
+__device__ __forceinline__ Pair operator*(double s, Pair x) { return Pair(s * x.a, s * x.b); }
+__device__ __forceinline__ Pair operator*(Pair x, double s) { return Pair(x.a * s, x.b * s); }
+__device__ __forceinline__ Pair operator+(Pair x, Pair y) { return Pair(x.a + y.a, x.b + y.b); }
+__device__ __forceinline__ Pair operator-(Pair x, Pair y) { return Pair(x.a - y.a, x.b - y.b); }
+
 // The same recursion for a compile-time lmax, fully unrolled, so that every
-// callback sees a constant lm.
-template <int LS, class F>
-__device__ __forceinline__ void unit_harmonics_fixed(double x, double y, double z, F &&f) {
-  f(0, 1.0);
+// callback sees a constant lm; T = double (one point) or Pair (two).
+template <int LS, class T, class F>
+__device__ __forceinline__ void unit_harmonics_fixed(T x, T y, T z, F &&f) {
+  f(0, T(1.0));
   if constexpr (LS > 0) {
-    double p2 = 1.0, p1 = z;
+    T p2 = T(1.0), p1 = z;
     f(2, z);
 #pragma unroll
     for (int l = 2; l <= LS; ++l) {
-      double cur = (2.0 * l - 1.0) * (z * p1) - sqrt((double)((l - 1) * (l - 1))) * p2;
+      T cur = (2.0 * l - 1.0) * (z * p1) - sqrt((double)((l - 1) * (l - 1))) * p2;
       cur = cur * (1.0 / sqrt((double)(l * l)));
       f(l * (l + 1), cur);
       p2 = p1;
       p1 = cur;
     }
-    double top = x, bot = y;
+    T top = x, bot = y;
 #pragma unroll
     for (int mm = 1; mm <= LS; ++mm) {
       if (mm >= 2) {
         const double c = sqrt(1.0 - 0.5 / mm);
-        const double nb = c * (top * y + bot * x);
-        const double nt = c * (top * x - bot * y);
+        const T nb = c * (top * y + bot * x);
+        const T nt = c * (top * x - bot * y);
         top = nt;
         bot = nb;
       }
@@ -59,10 +74,10 @@ __device__ __forceinline__ void unit_harmonics_fixed(double x, double y, double 
 #pragma unroll
       for (int sg = 0; sg < 2; ++sg) {
         const int m = sg ? -mm : mm;
-        double q2 = 0.0, q1 = sg ? bot : top;
+        T q2 = T(0.0), q1 = sg ? bot : top;
 #pragma unroll
         for (int l = mm + 1; l <= LS; ++l) {
-          double cur = (2.0 * l - 1.0) * (q1 * z);
+          T cur = (2.0 * l - 1.0) * (q1 * z);
           if (l - mm > 1) cur = cur - sqrt((l + m - 1.0) * (l - m - 1.0)) * q2;
           cur = (1.0 / sqrt(1.0 * (l - m) * (l + m))) * cur;
           f(l * (l + 1) + m, cur);
@@ -86,6 +101,24 @@ __device__ __forceinline__ double horner7(const double *c, double t) {
   v = v * t + e.x;
   v = v * t + e.y;
   return v * t + g.x;
+}
+
+// The same polynomial at two cell coordinates, its coefficients read once.
+__device__ __forceinline__ Pair horner7_pair(const double *c, double t0, double t1) {
+  const double2 *q = reinterpret_cast<const double2 *>(c);
+  const double2 a = __ldg(q), b = __ldg(q + 1), e = __ldg(q + 2), g = __ldg(q + 3);
+  double v = a.x, w = a.x;
+  v = v * t0 + a.y;
+  w = w * t1 + a.y;
+  v = v * t0 + b.x;
+  w = w * t1 + b.x;
+  v = v * t0 + b.y;
+  w = w * t1 + b.y;
+  v = v * t0 + e.x;
+  w = w * t1 + e.x;
+  v = v * t0 + e.y;
+  w = w * t1 + e.y;
+  return Pair(v * t0 + g.x, w * t1 + g.x);
 }
 
 // LIP values of one cell -> monomial coefficients in the cell coordinate
@@ -131,6 +164,24 @@ struct BrickGrid {
     iy = by * 8 + ((threadIdx.x >> 3) & 7);
     iz = bz * 4 + (threadIdx.x >> 6);
     return ix < nx && iy < ny && iz < nz;
+  }
+};
+
+// 8 x 8 x 8 bricks for two points per thread: thread t holds (x, y) =
+// (t % 8, (t / 8) % 8) and z = t / 64 and t / 64 + 4 of the brick.
+struct BrickGrid2 {
+  int nx, ny, nz, nbx, nby;
+  long long count;
+  __device__ BrickGrid2(int nx_, int ny_, int nz_)
+      : nx(nx_), ny(ny_), nz(nz_), nbx((nx_ + 7) / 8), nby((ny_ + 7) / 8),
+        count((long long)((nx_ + 7) / 8) * ((ny_ + 7) / 8) * ((nz_ + 7) / 8)) {}
+  __device__ void point(long long bk, int &ix, int &iy, int &iz) const {
+    const int bx = (int)(bk % nbx);
+    const long long r = bk / nbx;
+    const int by = (int)(r % nby), bz = (int)(r / nby);
+    ix = bx * 8 + (threadIdx.x & 7);
+    iy = by * 8 + ((threadIdx.x >> 3) & 7);
+    iz = bz * 8 + (threadIdx.x >> 6);
   }
 };
 
@@ -218,6 +269,89 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// inject_kernel with two points per thread (z and z + 4 of an 8 x 8 x 8
+// brick), each radial polynomial's coefficients read once for both points
+// when they share the atom's radial cell; each point keeps the
+// single-point kernel's arithmetic.  7-point cells, lmax <= LS.
+template <int LS>
+__global__ void __launch_bounds__(256)
+    inject_pair_kernel(const AtomTab *__restrict__ atoms, int natom,
+                       const double *__restrict__ celld, const double *__restrict__ hcell,
+                       const double *__restrict__ coef, int N, int lmin, double first,
+                       const double *__restrict__ xs, int nx, const double *__restrict__ ys,
+                       int ny, const double *__restrict__ zs, int nz, double factor,
+                       double *cube) {
+  __shared__ AtomTab sa[kMaxAtomsSmem];
+  for (int a = threadIdx.x; a < natom && a < kMaxAtomsSmem; a += blockDim.x) sa[a] = atoms[a];
+  __syncthreads();
+  const int lm0 = lmin * lmin;
+  const BrickGrid2 B(nx, ny, nz);
+  for (long long bk = blockIdx.x; bk < B.count; bk += gridDim.x) {
+    int ix, iy, iz0;
+    B.point(bk, ix, iy, iz0);
+    const int iz1 = iz0 + 4;
+    if (ix >= nx || iy >= ny || iz0 >= nz) continue;
+    const bool has1 = iz1 < nz;
+    const double px = xs[ix], py = ys[iy], pz0 = zs[iz0], pz1 = has1 ? zs[iz1] : pz0;
+    Pair acc(0.0);
+    for (int a = 0; a < natom; ++a) {
+      const AtomTab A = a < kMaxAtomsSmem ? sa[a] : atoms[a];
+      const double dx = px - A.cx, dy = py - A.cy, dz0 = pz0 - A.cz, dz1 = pz1 - A.cz;
+      const double d0 = sqrt(dx * dx + dy * dy + dz0 * dz0);
+      const double d1 = sqrt(dx * dx + dy * dy + dz1 * dz1);
+      const bool in0 = d0 <= A.rmax, in1 = has1 && d1 <= A.rmax;
+      if (!in0 && !in1) continue;
+      const double *cd = celld + A.cell0;
+      const int ic0 = in0 ? radial_cell(cd, A.ncell, d0) : 0;
+      const int ic1 = in1 ? radial_cell(cd, A.ncell, d1) : 0;
+      if (!ic0 && !ic1) continue;
+      const double t0 = ic0 ? (d0 - cd[ic0 - 1]) / hcell[A.cell0 + ic0 - 1] + first : 0.0;
+      const double t1 = ic1 ? (d1 - cd[ic1 - 1]) / hcell[A.cell0 + ic1 - 1] + first : 0.0;
+      const bool ctr0 = !(d0 > 0.0), ctr1 = !(d1 > 0.0);
+      double ux0 = 0.0, uy0 = 0.0, uz0 = 0.0, ux1 = 0.0, uy1 = 0.0, uz1 = 0.0;
+      if (!ctr0) {
+        const double inv = 1.0 / d0;
+        ux0 = dx * inv;
+        uy0 = dy * inv;
+        uz0 = dz0 * inv;
+      }
+      if (!ctr1) {
+        const double inv = 1.0 / d1;
+        ux1 = dx * inv;
+        uy1 = dy * inv;
+        uz1 = dz1 * inv;
+      }
+      if (ic0 == ic1) {
+        const double *cf = coef + ((size_t)(A.cell0 + ic0 - 1) * N) * 8;
+        unit_harmonics_fixed<LS>(Pair(ux0, ux1), Pair(uy0, uy1), Pair(uz0, uz1),
+                                 [&](int lm, Pair Y) {
+          if (lm < lm0 || lm >= N) return;
+          const Pair h = horner7_pair(cf + (size_t)lm * 8, t0, t1);
+          if (!(ctr0 && lm > 0)) acc.a += h.a * Y.a;
+          if (!(ctr1 && lm > 0)) acc.b += h.b * Y.b;
+        });
+      } else {
+        auto one = [&](int ic, double t, double ux, double uy, double uz, bool ctr, double &w) {
+          const double *cf = coef + ((size_t)(A.cell0 + ic - 1) * N) * 8;
+          unit_harmonics_fixed<LS>(ux, uy, uz, [&](int lm, double Y) {
+            if (lm < lm0 || lm >= N) return;
+            if (ctr && lm > 0) return;
+            w += horner7(cf + (size_t)lm * 8, t) * Y;
+          });
+        };
+        if (ic0) one(ic0, t0, ux0, uy0, uz0, ctr0, acc.a);
+        if (ic1) one(ic1, t1, ux1, uy1, uz1, ctr1, acc.b);
+      }
+    }
+    const long long i0 = ix + (long long)nx * (iy + (long long)ny * iz0);
+    cube[i0] += factor * acc.a;
+    if (has1) {
+      const long long i1 = ix + (long long)nx * (iy + (long long)ny * iz1);
+      cube[i1] += factor * acc.b;
+    }
+  }
+}
+
 // The cube part of a function product in one pass (Function3D_multiply,
 // function3d.F90:1097-1409; the reference GPU path injects each bubble set
 // in its own launches per atom, multiplies the cubes, then de-injects,
@@ -288,6 +422,111 @@ __global__ void __launch_bounds__(256)
       }
     }
     out[i] = (c1[i] + v1) * (c2[i] + v2) - vr;
+  }
+}
+
+
+// function_product_kernel with two points per thread, z and z + 4 of an
+// 8 x 8 x 8 brick.  The kernel is bound by the L1 traffic of the radial
+// coefficients (4 16-byte loads per polynomial, 43 polynomials per atom at
+// lmax 2 x 2 -> 4); when an atom puts both points in the same radial cell
+// -- nearly always, the points are 0.4 bohr apart -- each polynomial's
+// coefficients are read once for both.  Every point keeps the single-point
+// kernel's arithmetic and summation order.  7-point cells, lmax <= LS.
+template <int LS>
+__global__ void __launch_bounds__(256)
+    function_product_pair_kernel(const AtomTab *__restrict__ atoms, int natom,
+                                 const double *__restrict__ celld,
+                                 const double *__restrict__ hcell,
+                                 const double *__restrict__ coef1, int N1,
+                                 const double *__restrict__ coef2, int N2,
+                                 const double *__restrict__ coefr, int Nr, double first,
+                                 const double *__restrict__ xs, int nx,
+                                 const double *__restrict__ ys, int ny,
+                                 const double *__restrict__ zs, int nz, const double *c1,
+                                 const double *c2, double *out) {
+  __shared__ AtomTab sa[kMaxAtomsSmem];
+  for (int a = threadIdx.x; a < natom && a < kMaxAtomsSmem; a += blockDim.x) sa[a] = atoms[a];
+  __syncthreads();
+  const BrickGrid2 B(nx, ny, nz);
+  for (long long bk = blockIdx.x; bk < B.count; bk += gridDim.x) {
+    int ix, iy, iz0;
+    B.point(bk, ix, iy, iz0);
+    const int iz1 = iz0 + 4;
+    if (ix >= nx || iy >= ny || iz0 >= nz) continue;
+    const bool has1 = iz1 < nz;
+    const double px = xs[ix], py = ys[iy], pz0 = zs[iz0], pz1 = has1 ? zs[iz1] : pz0;
+    Pair v1(0.0), v2(0.0), vr(0.0);
+    for (int a = 0; a < natom; ++a) {
+      const AtomTab A = a < kMaxAtomsSmem ? sa[a] : atoms[a];
+      const double dx = px - A.cx, dy = py - A.cy, dz0 = pz0 - A.cz, dz1 = pz1 - A.cz;
+      const double d0 = sqrt(dx * dx + dy * dy + dz0 * dz0);
+      const double d1 = sqrt(dx * dx + dy * dy + dz1 * dz1);
+      const bool in0 = d0 <= A.rmax, in1 = has1 && d1 <= A.rmax;
+      if (!in0 && !in1) continue;
+      const double *cd = celld + A.cell0;
+      const int ic0 = in0 ? radial_cell(cd, A.ncell, d0) : 0;
+      const int ic1 = in1 ? radial_cell(cd, A.ncell, d1) : 0;
+      if (!ic0 && !ic1) continue;
+      const double t0 = ic0 ? (d0 - cd[ic0 - 1]) / hcell[A.cell0 + ic0 - 1] + first : 0.0;
+      const double t1 = ic1 ? (d1 - cd[ic1 - 1]) / hcell[A.cell0 + ic1 - 1] + first : 0.0;
+      const bool ctr0 = !(d0 > 0.0), ctr1 = !(d1 > 0.0);
+      double ux0 = 0.0, uy0 = 0.0, uz0 = 0.0, ux1 = 0.0, uy1 = 0.0, uz1 = 0.0;
+      if (!ctr0) {
+        const double inv = 1.0 / d0;
+        ux0 = dx * inv;
+        uy0 = dy * inv;
+        uz0 = dz0 * inv;
+      }
+      if (!ctr1) {
+        const double inv = 1.0 / d1;
+        ux1 = dx * inv;
+        uy1 = dy * inv;
+        uz1 = dz1 * inv;
+      }
+      if (ic0 == ic1) {
+        const size_t cell = (size_t)(A.cell0 + ic0 - 1);
+        unit_harmonics_fixed<LS>(Pair(ux0, ux1), Pair(uy0, uy1), Pair(uz0, uz1),
+                                 [&](int lm, Pair Y) {
+          const bool use0 = !(ctr0 && lm > 0), use1 = !(ctr1 && lm > 0);
+          if (lm < N1) {
+            const Pair h = horner7_pair(coef1 + (cell * N1 + lm) * 8, t0, t1);
+            if (use0) v1.a += h.a * Y.a;
+            if (use1) v1.b += h.b * Y.b;
+          }
+          if (lm < N2) {
+            const Pair h = horner7_pair(coef2 + (cell * N2 + lm) * 8, t0, t1);
+            if (use0) v2.a += h.a * Y.a;
+            if (use1) v2.b += h.b * Y.b;
+          }
+          if (lm < Nr) {
+            const Pair h = horner7_pair(coefr + (cell * Nr + lm) * 8, t0, t1);
+            if (use0) vr.a += h.a * Y.a;
+            if (use1) vr.b += h.b * Y.b;
+          }
+        });
+      } else {
+        // the points in different cells (or one of them outside): each alone
+        auto one = [&](int ic, double t, double ux, double uy, double uz, bool ctr, double &w1,
+                       double &w2, double &wr) {
+          const size_t cell = (size_t)(A.cell0 + ic - 1);
+          unit_harmonics_fixed<LS>(ux, uy, uz, [&](int lm, double Y) {
+            if (ctr && lm > 0) return;
+            if (lm < N1) w1 += horner7(coef1 + (cell * N1 + lm) * 8, t) * Y;
+            if (lm < N2) w2 += horner7(coef2 + (cell * N2 + lm) * 8, t) * Y;
+            if (lm < Nr) wr += horner7(coefr + (cell * Nr + lm) * 8, t) * Y;
+          });
+        };
+        if (ic0) one(ic0, t0, ux0, uy0, uz0, ctr0, v1.a, v2.a, vr.a);
+        if (ic1) one(ic1, t1, ux1, uy1, uz1, ctr1, v1.b, v2.b, vr.b);
+      }
+    }
+    const long long i0 = ix + (long long)nx * (iy + (long long)ny * iz0);
+    out[i0] = (c1[i0] + v1.a) * (c2[i0] + v2.a) - vr.a;
+    if (has1) {
+      const long long i1 = ix + (long long)nx * (iy + (long long)ny * iz1);
+      out[i1] = (c1[i1] + v1.b) * (c2[i1] + v2.b) - vr.b;
+    }
   }
 }
 
@@ -372,10 +611,17 @@ void inject_dispatch(const dage_bubbles *b, int blocks, cudaStream_t s, int lmin
                                   b->hcell.as<double>(), b->coef.as<double>(), b->N, b->lmax, lmin,
                                   b->nlip, b->first, xs, nx, ys, ny, zs, nz, factor, d_cube);
   };
+  const size_t bricks = (size_t)((nx + 7) / 8) * ((ny + 7) / 8) * ((nz + 7) / 8);
+  const int blocks2 = (int)std::min<size_t>(bricks, (size_t)sm_count() * 16);
+  auto go2 = [&](auto kernel) {
+    kernel<<<blocks2, 256, 0, s>>>(b->atoms.as<AtomTab>(), b->natom, b->celld.as<double>(),
+                                   b->hcell.as<double>(), b->coef.as<double>(), b->N, lmin, b->first,
+                                   xs, nx, ys, ny, zs, nz, factor, d_cube);
+  };
   if (b->nlip != 7 || b->lmax > 6) go(inject_kernel<-1>);
-  else if (b->lmax <= 2) go(inject_kernel<2>);
-  else if (b->lmax <= 4) go(inject_kernel<4>);
-  else go(inject_kernel<6>);
+  else if (b->lmax <= 2) go2(inject_pair_kernel<2>);
+  else if (b->lmax <= 4) go2(inject_pair_kernel<4>);
+  else go2(inject_pair_kernel<6>);
 }
 }  // namespace
 }  // namespace dage
@@ -978,10 +1224,20 @@ int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, con
         ref ? ref->first : 0.0, pts[0].as<double>(), ax[0].n(), pts[1].as<double>(), ax[1].n(),
         pts[2].as<double>(), ax[2].n(), d1, d2, dout);
   };
+  auto go2 = [&](auto kernel) {
+    const size_t bricks = (size_t)((ax[0].n() + 7) / 8) * ((ax[1].n() + 7) / 8) * ((ax[2].n() + 7) / 8);
+    const int blocks2 = (int)std::min<size_t>(bricks, (size_t)sm_count() * 16);
+    kernel<<<blocks2, 256>>>(
+        ref ? ref->atoms.as<AtomTab>() : nullptr, ref ? ref->natom : 0,
+        ref ? ref->celld.as<double>() : nullptr, ref ? ref->hcell.as<double>() : nullptr,
+        coef(b1), rows(b1), coef(b2), rows(b2), coef(br), rows(br), ref ? ref->first : 0.0,
+        pts[0].as<double>(), ax[0].n(), pts[1].as<double>(), ax[1].n(), pts[2].as<double>(),
+        ax[2].n(), d1, d2, dout);
+  };
   if (nlip != 7 || lmax > 6) go(function_product_kernel<-1>);
-  else if (lmax <= 2) go(function_product_kernel<2>);
-  else if (lmax <= 4) go(function_product_kernel<4>);
-  else go(function_product_kernel<6>);
+  else if (lmax <= 2) go2(function_product_pair_kernel<2>);
+  else if (lmax <= 4) go2(function_product_pair_kernel<4>);
+  else go2(function_product_pair_kernel<6>);
   DAGE_CUDA_TRY(cudaGetLastError());
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
