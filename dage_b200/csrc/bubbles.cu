@@ -431,9 +431,12 @@ __global__ void __launch_bounds__(256)
 // coefficients (4 16-byte loads per polynomial, 43 polynomials per atom at
 // lmax 2 x 2 -> 4); when an atom puts both points in the same radial cell
 // -- nearly always, the points are 0.4 bohr apart -- each polynomial's
-// coefficients are read once for both.  Every point keeps the single-point
-// kernel's arithmetic and summation order.  7-point cells, lmax <= LS.
-template <int LS>
+// coefficients are read once for both.  The two factors' sets (lmax <= LSB)
+// and the result set (lmax <= LSR) run in two harmonics passes, so that few
+// sums are live at once; the recursion visits the harmonics below any l in
+// the same order whatever its top l, so every point keeps the single-point
+// kernel's arithmetic and summation order.  7-point cells.
+template <int LSB, int LSR>
 __global__ void __launch_bounds__(256)
     function_product_pair_kernel(const AtomTab *__restrict__ atoms, int natom,
                                  const double *__restrict__ celld,
@@ -486,8 +489,8 @@ __global__ void __launch_bounds__(256)
       }
       if (ic0 == ic1) {
         const size_t cell = (size_t)(A.cell0 + ic0 - 1);
-        unit_harmonics_fixed<LS>(Pair(ux0, ux1), Pair(uy0, uy1), Pair(uz0, uz1),
-                                 [&](int lm, Pair Y) {
+        const Pair X(ux0, ux1), Yv(uy0, uy1), Z(uz0, uz1);
+        unit_harmonics_fixed<LSB>(X, Yv, Z, [&](int lm, Pair Y) {
           const bool use0 = !(ctr0 && lm > 0), use1 = !(ctr1 && lm > 0);
           if (lm < N1) {
             const Pair h = horner7_pair(coef1 + (cell * N1 + lm) * 8, t0, t1);
@@ -499,21 +502,25 @@ __global__ void __launch_bounds__(256)
             if (use0) v2.a += h.a * Y.a;
             if (use1) v2.b += h.b * Y.b;
           }
-          if (lm < Nr) {
-            const Pair h = horner7_pair(coefr + (cell * Nr + lm) * 8, t0, t1);
-            if (use0) vr.a += h.a * Y.a;
-            if (use1) vr.b += h.b * Y.b;
-          }
+        });
+        unit_harmonics_fixed<LSR>(X, Yv, Z, [&](int lm, Pair Y) {
+          if (lm >= Nr) return;
+          const Pair h = horner7_pair(coefr + (cell * Nr + lm) * 8, t0, t1);
+          if (!(ctr0 && lm > 0)) vr.a += h.a * Y.a;
+          if (!(ctr1 && lm > 0)) vr.b += h.b * Y.b;
         });
       } else {
         // the points in different cells (or one of them outside): each alone
         auto one = [&](int ic, double t, double ux, double uy, double uz, bool ctr, double &w1,
                        double &w2, double &wr) {
           const size_t cell = (size_t)(A.cell0 + ic - 1);
-          unit_harmonics_fixed<LS>(ux, uy, uz, [&](int lm, double Y) {
+          unit_harmonics_fixed<LSB>(ux, uy, uz, [&](int lm, double Y) {
             if (ctr && lm > 0) return;
             if (lm < N1) w1 += horner7(coef1 + (cell * N1 + lm) * 8, t) * Y;
             if (lm < N2) w2 += horner7(coef2 + (cell * N2 + lm) * 8, t) * Y;
+          });
+          unit_harmonics_fixed<LSR>(ux, uy, uz, [&](int lm, double Y) {
+            if (ctr && lm > 0) return;
             if (lm < Nr) wr += horner7(coefr + (cell * Nr + lm) * 8, t) * Y;
           });
         };
@@ -1234,10 +1241,20 @@ int dage_function3d_multiply(const dage_grid1d grid[3], const double *cube1, con
         pts[0].as<double>(), ax[0].n(), pts[1].as<double>(), ax[1].n(), pts[2].as<double>(),
         ax[2].n(), d1, d2, dout);
   };
+  // harmonics passes: the factors' sets up to lb, the result set up to lr
+  int lb = 0, lr = 0;
+  for (const dage_bubbles *x : {b1, b2})
+    if (x) lb = std::max(lb, x->lmax);
+  if (br) lr = br->lmax;
+  auto up = [](int l) { return l <= 2 ? 2 : l <= 4 ? 4 : 6; };
+  const int kb = up(lb), kr = std::max(up(lr), kb);
   if (nlip != 7 || lmax > 6) go(function_product_kernel<-1>);
-  else if (lmax <= 2) go2(function_product_pair_kernel<2>);
-  else if (lmax <= 4) go2(function_product_pair_kernel<4>);
-  else go2(function_product_pair_kernel<6>);
+  else if (kb == 2 && kr == 2) go2(function_product_pair_kernel<2, 2>);
+  else if (kb == 2 && kr == 4) go2(function_product_pair_kernel<2, 4>);
+  else if (kb == 2) go2(function_product_pair_kernel<2, 6>);
+  else if (kb == 4 && kr == 4) go2(function_product_pair_kernel<4, 4>);
+  else if (kb == 4) go2(function_product_pair_kernel<4, 6>);
+  else go2(function_product_pair_kernel<6, 6>);
   DAGE_CUDA_TRY(cudaGetLastError());
   if (!(flags & DAGE_DEVICE_PTRS))
     DAGE_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
