@@ -1125,10 +1125,13 @@ __global__ void fill_kernel(double *x, size_t n, double v) {
 }  // namespace
 
 // Autotuner of the tensor-core path: ring depth of the stage kernel (4 or 6
-// TMA/MMA stages; bf16x6's three-part stages fit 4 only) and the t-points
-// summed per pass of the last stage (4 or 8), each candidate timed over
-// one apply of a scratch cube after one untimed apply; keyed on (device,
-// precision, points per axis, t-points) in the tune cache.
+// TMA/MMA stages; bf16x6's three-part stages fit 4 only), each candidate
+// timed over one apply of a scratch cube after one untimed apply; keyed on
+// (device, precision, points per axis, t-points) in the tune cache.  The
+// ring depth changes no arithmetic.  The t-points summed per pass of the
+// last stage stay at min(P, 8) unless a cache entry names another group:
+// the group sets the order of the last stage's FP32 sums, and a choice by
+// timing could differ from process to process.
 int mixed_tune(dage_op3d *op) {
   auto *st = static_cast<MixedState *>(op->mixed);
   if (!st) return fail(DAGE_E_INVALID, "mixed state missing");
@@ -1152,8 +1155,7 @@ int mixed_tune(dage_op3d *op) {
       rho.as<double>(), nin, 1.0);
   DAGE_CUDA_TRY(cudaGetLastError());
   std::vector<int> nss = st->nparts == 2 ? std::vector<int>{6, 4} : std::vector<int>{4};
-  std::vector<int> gs = {st->Gmax};
-  if (st->Gmax > 4) gs.push_back(4);
+  const std::vector<int> gs = {st->Gmax};
   int best_ns = st->ns, best_g = st->G;
   float best = 0.0f;
   for (int ns : nss)

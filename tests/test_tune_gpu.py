@@ -112,13 +112,14 @@ def _mixed_child(path, out):
 
 def test_mixed_schedule_tuned_and_forced(dage, oracle, tmp_path):
     """The tensor-core schedule (ring stages, t-points per last-stage pass)
-    is timed once and cached; an edited entry forces another schedule in a
-    new process, and every schedule gives the same potential to the
-    split-precision bars (the ring depth changes no arithmetic, the group
-    only the order of the last stage's FP32 sums)."""
+    is timed once and cached (the ring depth; the group stays at min(P, 8)
+    so that results do not depend on a timing); an edited entry forces
+    another schedule in a new process, and every schedule gives the same
+    potential to the split-precision bars (the ring depth changes no
+    arithmetic, the group only the order of the last stage's FP32 sums)."""
     path = str(tmp_path / "tune.txt")
     sched, ref = _mixed_child(path, str(tmp_path / "a.npy"))
-    assert sched[0] in (4, 6) and sched[1] in (4, 8)
+    assert sched[0] in (4, 6) and sched[1] == 8
     key = [l for l in open(path).read().splitlines() if "/op3d_mixed3/61x61,61x61,61x61,P20" in l]
     assert key
     for forced in ((4, 4), (6, 8), (4, 8)):
