@@ -166,10 +166,10 @@ int dage_op3d_create_cached(const dage_grid1d grid_in[3], const dage_grid1d grid
  * FP64 contraction stages (the split-precision stages use 128).  No reference
  * counterpart: the reference's stages are cuBLAS DGEMMs. */
 int dage_op3d_tiles(const dage_op3d *op, int tile_n[3]);
-/* The schedule the autotuner chose for a split-precision operator's
- * tensor-core stages: TMA/MMA ring stages (4 or 6) and t-points summed per
- * pass of the last stage (<= 8).  DAGE_E_INVALID for an FP64 operator.  No
- * reference counterpart. */
+/* The schedule of a split-precision operator's tensor-core stages: the
+ * TMA/MMA ring stages the autotuner chose (4 or 6) and the t-points summed
+ * per pass of the last stage (min(P, 8) unless a tune-cache entry sets it).
+ * DAGE_E_INVALID for an FP64 operator.  No reference counterpart. */
 int dage_op3d_mixed_schedule(const dage_op3d *op, int *ring_stages, int *tpoint_group);
 int dage_op3d_destroy(dage_op3d *op);
 
