@@ -106,7 +106,9 @@ int dage_op3d_apply(dage_op3d *op, const double *rho, double *V, unsigned flags,
  * the end: applies on distinct operators overlap.  With host pointers each
  * operator pipelines its applies through two device staging slots and
  * copy-in/copy-out streams, so one density's copies overlap the neighbouring
- * densities' compute (asynchronously when the host arrays are pinned).
+ * densities' compute (asynchronously when the host arrays are pinned); the
+ * slots are two input and two output cubes of device memory per operator,
+ * allocated on its first host-pointer batch and held until it is destroyed.
  * energies[i] receives apply i's energy with DAGE_ENERGY.  An operator's
  * last_time_ms covers its last apply of the batch (host pointers: the whole
  * pipeline, first copy-in to last copy-out).  Replaces the per-orbital loop
